@@ -1,0 +1,710 @@
+// Host side of the engine: context construction (shell pairs, primitive-pair
+// tables, Schwarz bounds, class lists), the stored and direct builds, and the
+// C ABI declared in include/hfgpu.h.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/hfgpu.h"
+#include "eri_dispatch.cuh"
+
+namespace hfg {
+
+static thread_local std::string g_last_error;
+
+static hfg_status fail(hfg_status st, const std::string &msg) {
+  g_last_error = msg;
+  return st;
+}
+
+#define HFG_CUDA(call)                                                                        \
+  do {                                                                                        \
+    cudaError_t err__ = (call);                                                               \
+    if (err__ != cudaSuccess)                                                                 \
+      return fail(err__ == cudaErrorMemoryAllocation ? HFG_OOM_BUDGET : HFG_DEVICE_ERROR,      \
+                  std::string(#call) + ": " + cudaGetErrorString(err__));                     \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Boys table F_m(T_i), T_i = i * kBoysStep, m = 0 .. kBoysOrders-1, from the
+// convergent series F_m(T) = e^-T sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1))
+// evaluated in extended precision (all terms positive, no cancellation).
+// ---------------------------------------------------------------------------
+static const std::vector<double> &boys_table_host() {
+  static std::vector<double> tab;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    tab.resize((size_t)kBoysGrid * kBoysOrders);
+    for (int i = 0; i < kBoysGrid; ++i) {
+      const long double T = (long double)i * (long double)kBoysStep;
+      for (int m = 0; m < kBoysOrders; ++m) {
+        long double term = 1.0L / (2 * m + 1), sum = 0;
+        for (int k = 0; k < 2000; ++k) {
+          sum += term;
+          term *= 2.0L * T / (2 * m + 2 * k + 3);
+          if (term < sum * 1e-21L) break;
+        }
+        tab[(size_t)i * kBoysOrders + m] = (double)(expl(-T) * sum);
+      }
+    }
+  });
+  return tab;
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct HostShell {
+  double c[3];
+  int L, nprim, prim_off, ao;
+};
+
+struct PairClassList {
+  std::vector<int> pairs;  // pair indices sorted by Q descending
+  int *d_pairs = nullptr;
+};
+
+struct QuartetClass {
+  int cls;       // index into kClasses
+  int bra_pc, ket_pc;
+  std::vector<int> ket_count;
+  std::vector<Task> tasks;
+  int *d_ket_count = nullptr;
+  Task *d_tasks = nullptr;
+  int64_t shell_quartets = 0, function_quartets = 0, prim_quartets = 0;
+  double flops = 0;
+};
+
+template <class T>
+static hfg_status upload(T **dst, const std::vector<T> &src) {
+  *dst = nullptr;
+  if (src.empty()) return HFG_OK;
+  HFG_CUDA(cudaMalloc((void **)dst, src.size() * sizeof(T)));
+  HFG_CUDA(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return HFG_OK;
+}
+
+}  // namespace hfg
+
+using namespace hfg;
+
+struct hfg_ctx {
+  hfg_opts opts{};
+  int device = 0;
+  int nbf = 0;
+  std::vector<HostShell> shells;
+  int npairs = 0;
+  std::vector<int> pair_sa, pair_sb, pair_cls;
+  std::vector<double> pair_Q;
+  PairClassList pclass[kNumPairClasses];
+  std::vector<QuartetClass> qclasses;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int num_sms = 148;
+  // device tables
+  PrimPair *d_prim = nullptr;
+  int *d_pair_prim_off = nullptr, *d_pair_nprim = nullptr, *d_pair_sa = nullptr, *d_pair_sb = nullptr;
+  int *d_pair_ao_a = nullptr, *d_pair_ao_b = nullptr;
+  double *d_pair_AB = nullptr, *d_pair_Q = nullptr, *d_boys = nullptr;
+  float *d_pair_Dmax = nullptr;
+  // work buffers
+  double *d_J = nullptr, *d_Ka = nullptr, *d_Kb = nullptr, *d_P = nullptr, *d_Pb = nullptr, *d_Pt = nullptr;
+  double *d_G = nullptr, *d_Gb = nullptr, *d_block = nullptr;
+  hfg_stats stats{};
+  EngineView view() const {
+    EngineView v{};
+    v.prim = d_prim;
+    v.pair_prim_off = d_pair_prim_off;
+    v.pair_nprim = d_pair_nprim;
+    v.pair_sa = d_pair_sa;
+    v.pair_sb = d_pair_sb;
+    v.pair_ao_a = d_pair_ao_a;
+    v.pair_ao_b = d_pair_ao_b;
+    v.pair_AB = d_pair_AB;
+    v.pair_Q = d_pair_Q;
+    v.pair_Dmax = d_pair_Dmax;
+    v.boys_table = d_boys;
+    v.nbf = nbf;
+    v.reference_convention = opts.eri_convention == HFG_ERI_REFERENCE;
+    return v;
+  }
+  ~hfg_ctx() {
+    cudaSetDevice(device);
+    for (auto &q : qclasses) {
+      cudaFree(q.d_ket_count);
+      cudaFree(q.d_tasks);
+    }
+    for (auto &p : pclass) cudaFree(p.d_pairs);
+    void *bufs[] = {d_prim, d_pair_prim_off, d_pair_nprim, d_pair_sa, d_pair_sb, d_pair_ao_a, d_pair_ao_b,
+                    d_pair_AB, d_pair_Q, d_boys, d_pair_Dmax, d_J, d_Ka, d_Kb, d_P, d_Pb, d_Pt, d_G, d_Gb, d_block};
+    for (void *b : bufs) cudaFree(b);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace hfg {
+
+static int pair_class_index(int la, int lb) {
+  for (int i = 0; i < kNumPairClasses; ++i)
+    if (kPairClasses[i][0] == la && kPairClasses[i][1] == lb) return i;
+  return -1;
+}
+
+static int class_index(int la, int lb, int lc, int ld) {
+  for (int i = 0; i < kNumClasses; ++i)
+    if (kClasses[i].la == la && kClasses[i].lb == lb && kClasses[i].lc == lc && kClasses[i].ld == ld) return i;
+  return -1;
+}
+
+static double prim_flops(int cls, bool reference) {
+  for (const auto &f : kEriClassFlops)
+    if (f.la == kClasses[cls].la && f.lb == kClasses[cls].lb && f.lc == kClasses[cls].lc &&
+        f.ld == kClasses[cls].ld)
+      return reference ? f.prim_reference : f.prim_exact;
+  return 0;
+}
+static double hrr_flops(int cls) {
+  for (const auto &f : kEriClassFlops)
+    if (f.la == kClasses[cls].la && f.lb == kClasses[cls].lb && f.lc == kClasses[cls].lc &&
+        f.ld == kClasses[cls].ld)
+      return f.hrr;
+  return 0;
+}
+// Boys (7-term Horner, exp, downward recursion) + prefactor/geometry per
+// primitive quartet, counted as 2 flops per FMA, exp as 1
+static double boys_geom_flops(int ltot) { return 14 + 3 * ltot + 40; }
+
+static inline int ncart_h(int L) { return (L + 1) * (L + 2) / 2; }
+
+// number of 8-fold unique function quartets in a pair's function block
+static inline int64_t pair_functions(const hfg_ctx *c, int p) {
+  const int na = ncart_h(c->shells[c->pair_sa[p]].L), nb = ncart_h(c->shells[c->pair_sb[p]].L);
+  return c->pair_sa[p] == c->pair_sb[p] ? (int64_t)na * (na + 1) / 2 : (int64_t)na * nb;
+}
+
+// Build per-class quartet task lists with Schwarz screening at `threshold`.
+static void build_quartet_classes(hfg_ctx *c, double threshold) {
+  c->qclasses.clear();
+  for (int ci = 0; ci < kNumClasses; ++ci) {
+    const ClassEntry &ce = kClasses[ci];
+    QuartetClass q;
+    q.cls = ci;
+    q.bra_pc = pair_class_index(ce.la, ce.lb);
+    q.ket_pc = pair_class_index(ce.lc, ce.ld);
+    const auto &bras = c->pclass[q.bra_pc].pairs;
+    const auto &kets = c->pclass[q.ket_pc].pairs;
+    if (bras.empty() || kets.empty()) continue;
+    const bool same = q.bra_pc == q.ket_pc;
+    // prefix sums over the ket list for quartet accounting
+    std::vector<int64_t> kfun(kets.size() + 1, 0), kprim(kets.size() + 1, 0);
+    std::vector<double> kq(kets.size());
+    for (size_t k = 0; k < kets.size(); ++k) {
+      kfun[k + 1] = kfun[k] + pair_functions(c, kets[k]);
+      const HostShell &sa = c->shells[c->pair_sa[kets[k]]], &sb = c->shells[c->pair_sb[kets[k]]];
+      kprim[k + 1] = kprim[k] + (int64_t)sa.nprim * sb.nprim;
+      kq[k] = c->pair_Q[kets[k]];
+    }
+    q.ket_count.resize(bras.size());
+    const double pf = prim_flops(ci, c->opts.eri_convention == HFG_ERI_REFERENCE);
+    const double hf = hrr_flops(ci);
+    const int ltot = ce.la + ce.lb + ce.lc + ce.ld;
+    for (size_t b = 0; b < bras.size(); ++b) {
+      const double qb = c->pair_Q[bras[b]];
+      // kets sorted by Q descending: count those with qb * qk >= threshold
+      int64_t lo = 0, hi = (int64_t)kets.size();
+      if (qb <= 0) hi = 0;
+      else {
+        const double need = threshold / qb;
+        while (lo < hi) {
+          const int64_t mid = (lo + hi) / 2;
+          if (kq[mid] >= need) lo = mid + 1;
+          else hi = mid;
+        }
+        hi = lo;
+      }
+      int64_t cnt = hi;
+      if (same) cnt = std::min<int64_t>(cnt, (int64_t)b + 1);
+      q.ket_count[b] = (int)cnt;
+      for (int64_t s = 0; s < cnt; s += 32) q.tasks.push_back(Task{(int)b, (int)s});
+      q.shell_quartets += cnt;
+      const int64_t bf = pair_functions(c, bras[b]);
+      const HostShell &sa = c->shells[c->pair_sa[bras[b]]], &sb = c->shells[c->pair_sb[bras[b]]];
+      const int64_t bprim = (int64_t)sa.nprim * sb.nprim;
+      if (same && cnt == (int64_t)b + 1) {
+        // diagonal quartet (bra == ket) counts its unique half
+        q.function_quartets += bf * kfun[cnt - 1] + bf * (bf + 1) / 2;
+      } else {
+        q.function_quartets += bf * kfun[cnt];
+      }
+      q.prim_quartets += bprim * kprim[cnt];
+    }
+    q.flops = (double)q.prim_quartets * (pf + boys_geom_flops(ltot)) + (double)q.shell_quartets * hf;
+    if (!q.tasks.empty()) c->qclasses.push_back(std::move(q));
+  }
+  // largest classes first
+  std::sort(c->qclasses.begin(), c->qclasses.end(),
+            [](const QuartetClass &a, const QuartetClass &b) { return a.flops > b.flops; });
+}
+
+static hfg_status upload_classes(hfg_ctx *c) {
+  for (auto &q : c->qclasses) {
+    hfg_status st = upload(&q.d_ket_count, q.ket_count);
+    if (st != HFG_OK) return st;
+    st = upload(&q.d_tasks, q.tasks);
+    if (st != HFG_OK) return st;
+  }
+  return HFG_OK;
+}
+
+static int grid_for(const hfg_ctx *c, int ntasks) {
+  const int blocks = (ntasks + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  return std::max(1, std::min(blocks, c->num_sms * 16));
+}
+
+static ClassLaunch base_launch(const hfg_ctx *c, const QuartetClass &q) {
+  ClassLaunch cl{};
+  cl.bra_list = c->pclass[q.bra_pc].d_pairs;
+  cl.ket_list = c->pclass[q.ket_pc].d_pairs;
+  cl.ket_count = q.d_ket_count;
+  cl.tasks = q.d_tasks;
+  cl.ntasks = (int)q.tasks.size();
+  cl.same_class = q.bra_pc == q.ket_pc;
+  return cl;
+}
+
+__global__ void finalize_rhf(const double *J, const double *K, double *G, int n) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n * n; x += gridDim.x * blockDim.x) {
+    const int i = x / n, j = x - i * n;
+    const double jv = J[i * n + j] + J[j * n + i];
+    const double kv = K[i * n + j] + K[j * n + i];
+    G[x] = jv - 0.5 * kv;
+  }
+}
+
+__global__ void finalize_uhf(const double *J, const double *Ka, const double *Kb, double *Ga, double *Gb, int n) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n * n; x += gridDim.x * blockDim.x) {
+    const int i = x / n, j = x - i * n;
+    const double jv = J[i * n + j] + J[j * n + i];
+    Ga[x] = jv - (Ka[i * n + j] + Ka[j * n + i]);
+    Gb[x] = jv - (Kb[i * n + j] + Kb[j * n + i]);
+  }
+}
+
+__global__ void add_densities(const double *a, const double *b, double *t, int nn) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < nn; x += gridDim.x * blockDim.x) t[x] = a[x] + b[x];
+}
+
+static hfg_status ensure(double **p, size_t count) {
+  if (*p) return HFG_OK;
+  HFG_CUDA(cudaMalloc((void **)p, count * sizeof(double)));
+  return HFG_OK;
+}
+
+// Direct J/K build: all classes on `s`, then G.
+static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const double *dPb, double *dGa, double *dGb,
+                               cudaStream_t s) {
+  const size_t nn = (size_t)c->nbf * c->nbf;
+  hfg_status st;
+  if ((st = ensure(&c->d_J, nn)) != HFG_OK || (st = ensure(&c->d_Ka, nn)) != HFG_OK) return st;
+  if (uhf && ((st = ensure(&c->d_Kb, nn)) != HFG_OK || (st = ensure(&c->d_Pt, nn)) != HFG_OK)) return st;
+  HFG_CUDA(cudaMemsetAsync(c->d_J, 0, nn * sizeof(double), s));
+  HFG_CUDA(cudaMemsetAsync(c->d_Ka, 0, nn * sizeof(double), s));
+  int launches = 2;
+  if (uhf) {
+    HFG_CUDA(cudaMemsetAsync(c->d_Kb, 0, nn * sizeof(double), s));
+    add_densities<<<256, 256, 0, s>>>(dPa, dPb, c->d_Pt, (int)nn);
+    launches += 2;
+  }
+  HFG_CUDA(cudaEventRecord(c->ev0, s));
+  const EngineView v = c->view();
+  const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
+  c->stats = hfg_stats{};
+  for (const auto &q : c->qclasses) {
+    ClassLaunch cl = base_launch(c, q);
+    cl.Da = dPa;
+    cl.Db = dPb;
+    cl.Dt = uhf ? c->d_Pt : dPa;
+    cl.J = c->d_J;
+    cl.Ka = c->d_Ka;
+    cl.Kb = c->d_Kb;
+    kClasses[q.cls].launch(v, cl, uhf ? kJkUhf : kJkRhf, ref, grid_for(c, cl.ntasks), s);
+    ++launches;
+    c->stats.shell_quartets += q.shell_quartets;
+    c->stats.function_quartets += q.function_quartets;
+    c->stats.primitive_quartets += q.prim_quartets;
+    c->stats.flops += q.flops;
+  }
+  HFG_CUDA(cudaGetLastError());
+  HFG_CUDA(cudaEventRecord(c->ev1, s));
+  const int n = c->nbf;
+  const int fg = std::max(1, std::min(1024, (int)((nn + 255) / 256)));
+  if (uhf) finalize_uhf<<<fg, 256, 0, s>>>(c->d_J, c->d_Ka, c->d_Kb, dGa, dGb, n);
+  else finalize_rhf<<<fg, 256, 0, s>>>(c->d_J, c->d_Ka, dGa, n);
+  ++launches;
+  HFG_CUDA(cudaGetLastError());
+  c->stats.kernel_launches = launches;
+  c->stats.shell_pairs = c->npairs;
+  return HFG_OK;
+}
+
+static hfg_status finish_timing(hfg_ctx *c) {
+  HFG_CUDA(cudaEventSynchronize(c->ev1));
+  float ms = 0;
+  HFG_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->stats.last_build_ms = ms;
+  return HFG_OK;
+}
+
+static hfg_status stored_build(hfg_ctx *c, double *d_out, int64_t count, cudaStream_t s) {
+  HFG_CUDA(cudaMemsetAsync(d_out, 0, (size_t)count * sizeof(double), s));
+  HFG_CUDA(cudaEventRecord(c->ev0, s));
+  const EngineView v = c->view();
+  const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
+  c->stats = hfg_stats{};
+  int launches = 1;
+  for (const auto &q : c->qclasses) {
+    ClassLaunch cl = base_launch(c, q);
+    cl.packed = d_out;
+    kClasses[q.cls].launch(v, cl, kStorePacked, ref, grid_for(c, cl.ntasks), s);
+    ++launches;
+    c->stats.shell_quartets += q.shell_quartets;
+    c->stats.function_quartets += q.function_quartets;
+    c->stats.primitive_quartets += q.prim_quartets;
+    c->stats.flops += q.flops;
+  }
+  HFG_CUDA(cudaGetLastError());
+  HFG_CUDA(cudaEventRecord(c->ev1, s));
+  c->stats.kernel_launches = launches;
+  c->stats.shell_pairs = c->npairs;
+  return HFG_OK;
+}
+
+}  // namespace hfg
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+void hfg_default_opts(hfg_opts *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->schwarz_threshold = 1e-12;
+  o->mixed_cutoff = 0.0;
+  o->eri_convention = HFG_ERI_REFERENCE;
+  o->device = 0;
+  o->density_screening = 0;
+}
+
+const char *hfg_last_error(void) { return hfg::g_last_error.c_str(); }
+
+int32_t hfg_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+int64_t hfg_packed_size(int32_t n) {
+  if (n <= 0) return 0;
+  auto tri = [](int64_t a, int64_t b) { return a < b ? b * (b + 1) / 2 + a : a * (a + 1) / 2 + b; };
+  return tri(tri(n - 1, n - 1), tri(n - 1, n - 1)) + 1;
+}
+
+int32_t hfg_ctx_nbf(const hfg_ctx *c) { return c ? c->nbf : 0; }
+
+hfg_status hfg_ctx_create(const hfg_shells *sh, const hfg_opts *opts, hfg_ctx **out) {
+  using namespace hfg;
+  if (!out) return fail(HFG_INVALID_ARG, "out is null");
+  *out = nullptr;
+  if (!sh || sh->nshells <= 0 || !sh->center || !sh->L || !sh->nprim || !sh->prim_offset || !sh->ao_offset ||
+      !sh->exponent || !sh->coefficient || sh->nbf <= 0)
+    return fail(HFG_INVALID_ARG, "incomplete hfg_shells");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(HFG_NO_DEVICE, "no CUDA device");
+  auto ctx = std::make_unique<hfg_ctx>();
+  if (opts) ctx->opts = *opts;
+  else hfg_default_opts(&ctx->opts);
+  if (ctx->opts.device < 0 || ctx->opts.device >= ndev) return fail(HFG_INVALID_ARG, "device out of range");
+  if (!(ctx->opts.schwarz_threshold >= 0)) return fail(HFG_INVALID_ARG, "negative screening threshold");
+  ctx->device = ctx->opts.device;
+  HFG_CUDA(cudaSetDevice(ctx->device));
+  HFG_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  ctx->nbf = sh->nbf;
+  const int ns = sh->nshells;
+  ctx->shells.resize(ns);
+  int64_t funcs = 0;
+  for (int s = 0; s < ns; ++s) {
+    HostShell &h = ctx->shells[s];
+    for (int d = 0; d < 3; ++d) h.c[d] = sh->center[3 * s + d];
+    h.L = sh->L[s];
+    h.nprim = sh->nprim[s];
+    h.prim_off = sh->prim_offset[s];
+    h.ao = sh->ao_offset[s];
+    if (h.L < 0 || h.L > kMaxL) return fail(HFG_UNSUPPORTED_L, "shell angular momentum above d");
+    if (h.nprim <= 0 || h.prim_off < 0) return fail(HFG_INVALID_ARG, "shell without primitives");
+    if (h.ao < 0 || h.ao + ncart_h(h.L) > sh->nbf) return fail(HFG_INVALID_ARG, "AO offset outside nbf");
+    funcs += ncart_h(h.L);
+  }
+  if (funcs != sh->nbf) return fail(HFG_INVALID_ARG, "shell functions do not sum to nbf");
+
+  // ---- shell pairs and primitive pairs (pair index a*(a+1)/2 + b, a >= b)
+  const int np = ns * (ns + 1) / 2;
+  ctx->npairs = np;
+  std::vector<PrimPair> prim;
+  std::vector<int> poff(np), pn(np), psa(np), psb(np), paoa(np), paob(np);
+  std::vector<double> pab(3 * (size_t)np);
+  ctx->pair_sa.resize(np);
+  ctx->pair_sb.resize(np);
+  ctx->pair_cls.resize(np);
+  const double sqrt2pi54 = std::sqrt(2.0) * std::pow(M_PI, 1.25);
+  for (int a = 0; a < ns; ++a)
+    for (int b = 0; b <= a; ++b) {
+      const int p = a * (a + 1) / 2 + b;
+      int f = a, g = b;
+      if (ctx->shells[b].L > ctx->shells[a].L) std::swap(f, g);  // first = higher L, else higher index
+      const HostShell &A = ctx->shells[f], &B = ctx->shells[g];
+      psa[p] = f;
+      psb[p] = g;
+      ctx->pair_sa[p] = f;
+      ctx->pair_sb[p] = g;
+      paoa[p] = A.ao;
+      paob[p] = B.ao;
+      ctx->pair_cls[p] = pair_class_index(A.L, B.L);
+      double AB[3], ab2 = 0;
+      for (int d = 0; d < 3; ++d) {
+        AB[d] = A.c[d] - B.c[d];
+        pab[3 * (size_t)p + d] = AB[d];
+        ab2 += AB[d] * AB[d];
+      }
+      poff[p] = (int)prim.size();
+      for (int i = 0; i < A.nprim; ++i)
+        for (int j = 0; j < B.nprim; ++j) {
+          const double al = sh->exponent[A.prim_off + i], be = sh->exponent[B.prim_off + j];
+          // L-dependent part of GaussianOrbital::getNormalizationFactor
+          // (GaussianOrbital.cpp:25-30): (2a/pi)^(3/4) (4a)^(L/2)
+          const double na = std::pow(2 * al / M_PI, 0.75) * std::pow(4 * al, A.L / 2.0);
+          const double nb = std::pow(2 * be / M_PI, 0.75) * std::pow(4 * be, B.L / 2.0);
+          const double ca = sh->coefficient[A.prim_off + i] * na, cb = sh->coefficient[B.prim_off + j] * nb;
+          PrimPair pp;
+          pp.zeta = al + be;
+          pp.inv_zeta = 1.0 / pp.zeta;
+          const double P[3] = {(al * A.c[0] + be * B.c[0]) * pp.inv_zeta, (al * A.c[1] + be * B.c[1]) * pp.inv_zeta,
+                               (al * A.c[2] + be * B.c[2]) * pp.inv_zeta};
+          pp.Px = P[0];
+          pp.Py = P[1];
+          pp.Pz = P[2];
+          pp.PAx = P[0] - A.c[0];
+          pp.PAy = P[1] - A.c[1];
+          pp.PAz = P[2] - A.c[2];
+          pp.bABx = be * AB[0];
+          pp.bABy = be * AB[1];
+          pp.bABz = be * AB[2];
+          pp.K = ca * cb * std::exp(-al * be * pp.inv_zeta * ab2) * sqrt2pi54 * pp.inv_zeta;
+          prim.push_back(pp);
+        }
+      pn[p] = (int)prim.size() - poff[p];
+    }
+  hfg_status st;
+  if ((st = upload(&ctx->d_prim, prim)) != HFG_OK || (st = upload(&ctx->d_pair_prim_off, poff)) != HFG_OK ||
+      (st = upload(&ctx->d_pair_nprim, pn)) != HFG_OK || (st = upload(&ctx->d_pair_sa, psa)) != HFG_OK ||
+      (st = upload(&ctx->d_pair_sb, psb)) != HFG_OK || (st = upload(&ctx->d_pair_ao_a, paoa)) != HFG_OK ||
+      (st = upload(&ctx->d_pair_ao_b, paob)) != HFG_OK || (st = upload(&ctx->d_pair_AB, pab)) != HFG_OK ||
+      (st = upload(&ctx->d_boys, boys_table_host())) != HFG_OK)
+    return st;
+  HFG_CUDA(cudaMalloc((void **)&ctx->d_pair_Q, (size_t)np * sizeof(double)));
+  HFG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  HFG_CUDA(cudaEventCreate(&ctx->ev0));
+  HFG_CUDA(cudaEventCreate(&ctx->ev1));
+
+  // ---- Schwarz bounds per pair class
+  std::vector<std::vector<int>> by_class(kNumPairClasses);
+  for (int p = 0; p < np; ++p) by_class[ctx->pair_cls[p]].push_back(p);
+  const EngineView v0 = ctx->view();
+  std::vector<int *> tmp_lists;
+  for (int pc = 0; pc < kNumPairClasses; ++pc) {
+    if (by_class[pc].empty()) continue;
+    int *d_list = nullptr;
+    if ((st = upload(&d_list, by_class[pc])) != HFG_OK) return st;
+    tmp_lists.push_back(d_list);
+    launch_schwarz(kPairClasses[pc][0], kPairClasses[pc][1], v0, d_list, (int)by_class[pc].size(), ctx->d_pair_Q,
+                   ctx->stream);
+  }
+  HFG_CUDA(cudaGetLastError());
+  HFG_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int *l : tmp_lists) cudaFree(l);
+  ctx->pair_Q.resize(np);
+  HFG_CUDA(cudaMemcpy(ctx->pair_Q.data(), ctx->d_pair_Q, (size_t)np * sizeof(double), cudaMemcpyDeviceToHost));
+
+  // ---- class lists sorted by Q descending (ties by pair index)
+  for (int pc = 0; pc < kNumPairClasses; ++pc) {
+    auto &lst = ctx->pclass[pc].pairs;
+    lst = by_class[pc];
+    std::stable_sort(lst.begin(), lst.end(), [&](int x, int y) { return ctx->pair_Q[x] > ctx->pair_Q[y]; });
+    if ((st = upload(&ctx->pclass[pc].d_pairs, lst)) != HFG_OK) return st;
+  }
+  build_quartet_classes(ctx.get(), ctx->opts.schwarz_threshold);
+  if ((st = upload_classes(ctx.get())) != HFG_OK) return st;
+  *out = ctx.release();
+  return HFG_OK;
+}
+
+void hfg_ctx_destroy(hfg_ctx *c) { delete c; }
+
+hfg_status hfg_eri_packed_device(hfg_ctx *c, double *dev_out, int64_t count, void *stream) {
+  if (!c || !dev_out) return fail(HFG_INVALID_ARG, "null argument");
+  if (count != hfg_packed_size(c->nbf)) return fail(HFG_INVALID_ARG, "count != hfg_packed_size(nbf)");
+  HFG_CUDA(cudaSetDevice(c->device));
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  hfg_status st = stored_build(c, dev_out, count, s);
+  if (st != HFG_OK) return st;
+  return finish_timing(c);
+}
+
+hfg_status hfg_eri_packed(hfg_ctx *c, double *host_out, int64_t count) {
+  if (!c || !host_out) return fail(HFG_INVALID_ARG, "null argument");
+  if (count != hfg_packed_size(c->nbf)) return fail(HFG_INVALID_ARG, "count != hfg_packed_size(nbf)");
+  HFG_CUDA(cudaSetDevice(c->device));
+  double *d = nullptr;
+  HFG_CUDA(cudaMalloc((void **)&d, (size_t)count * sizeof(double)));
+  hfg_status st = stored_build(c, d, count, c->stream);
+  if (st == HFG_OK) st = finish_timing(c);
+  if (st == HFG_OK) {
+    cudaError_t e = cudaMemcpyAsync(host_out, d, (size_t)count * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) st = fail(HFG_DEVICE_ERROR, cudaGetErrorString(e));
+  }
+  cudaFree(d);
+  return st;
+}
+
+hfg_status hfg_fock_rhf_device(hfg_ctx *c, const double *dP, double *dG, void *stream) {
+  if (!c || !dP || !dG) return fail(HFG_INVALID_ARG, "null argument");
+  HFG_CUDA(cudaSetDevice(c->device));
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  hfg_status st = direct_build(c, false, dP, nullptr, dG, nullptr, s);
+  if (st != HFG_OK) return st;
+  return finish_timing(c);
+}
+
+hfg_status hfg_fock_uhf_device(hfg_ctx *c, const double *dPa, const double *dPb, double *dGa, double *dGb,
+                               void *stream) {
+  if (!c || !dPa || !dPb || !dGa || !dGb) return fail(HFG_INVALID_ARG, "null argument");
+  HFG_CUDA(cudaSetDevice(c->device));
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  hfg_status st = direct_build(c, true, dPa, dPb, dGa, dGb, s);
+  if (st != HFG_OK) return st;
+  return finish_timing(c);
+}
+
+hfg_status hfg_fock_rhf(hfg_ctx *c, const double *P, double *G) {
+  if (!c || !P || !G) return fail(HFG_INVALID_ARG, "null argument");
+  HFG_CUDA(cudaSetDevice(c->device));
+  const size_t nn = (size_t)c->nbf * c->nbf;
+  hfg_status st;
+  if ((st = ensure(&c->d_P, nn)) != HFG_OK || (st = ensure(&c->d_G, nn)) != HFG_OK) return st;
+  HFG_CUDA(cudaMemcpyAsync(c->d_P, P, nn * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if ((st = direct_build(c, false, c->d_P, nullptr, c->d_G, nullptr, c->stream)) != HFG_OK) return st;
+  HFG_CUDA(cudaMemcpyAsync(G, c->d_G, nn * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  HFG_CUDA(cudaStreamSynchronize(c->stream));
+  return finish_timing(c);
+}
+
+hfg_status hfg_fock_uhf(hfg_ctx *c, const double *Pa, const double *Pb, double *Ga, double *Gb) {
+  if (!c || !Pa || !Pb || !Ga || !Gb) return fail(HFG_INVALID_ARG, "null argument");
+  HFG_CUDA(cudaSetDevice(c->device));
+  const size_t nn = (size_t)c->nbf * c->nbf;
+  hfg_status st;
+  if ((st = ensure(&c->d_P, nn)) != HFG_OK || (st = ensure(&c->d_Pb, nn)) != HFG_OK ||
+      (st = ensure(&c->d_G, nn)) != HFG_OK || (st = ensure(&c->d_Gb, nn)) != HFG_OK)
+    return st;
+  HFG_CUDA(cudaMemcpyAsync(c->d_P, Pa, nn * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  HFG_CUDA(cudaMemcpyAsync(c->d_Pb, Pb, nn * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if ((st = direct_build(c, true, c->d_P, c->d_Pb, c->d_G, c->d_Gb, c->stream)) != HFG_OK) return st;
+  HFG_CUDA(cudaMemcpyAsync(Ga, c->d_G, nn * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  HFG_CUDA(cudaMemcpyAsync(Gb, c->d_Gb, nn * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  HFG_CUDA(cudaStreamSynchronize(c->stream));
+  return finish_timing(c);
+}
+
+hfg_status hfg_schwarz(hfg_ctx *c, double *host_out, int64_t count) {
+  if (!c || !host_out) return fail(HFG_INVALID_ARG, "null argument");
+  if (count != c->npairs) return fail(HFG_INVALID_ARG, "count != nshells*(nshells+1)/2");
+  std::memcpy(host_out, c->pair_Q.data(), (size_t)count * sizeof(double));
+  return HFG_OK;
+}
+
+hfg_status hfg_eri_quartet(hfg_ctx *c, int32_t i, int32_t j, int32_t k, int32_t l, double *out) {
+  using namespace hfg;
+  if (!c || !out) return fail(HFG_INVALID_ARG, "null argument");
+  const int n = c->nbf;
+  if (i < 0 || j < 0 || k < 0 || l < 0 || i >= n || j >= n || k >= n || l >= n)
+    return fail(HFG_INVALID_ARG, "function index out of range");
+  HFG_CUDA(cudaSetDevice(c->device));
+  auto shell_of = [&](int ao) {
+    for (size_t s = 0; s < c->shells.size(); ++s)
+      if (ao >= c->shells[s].ao && ao < c->shells[s].ao + ncart_h(c->shells[s].L)) return (int)s;
+    return -1;
+  };
+  auto pair_of = [](int a, int b) { return a >= b ? a * (a + 1) / 2 + b : b * (b + 1) / 2 + a; };
+  int sI = shell_of(i), sJ = shell_of(j), sK = shell_of(k), sL = shell_of(l);
+  int p1 = pair_of(sI, sJ), p2 = pair_of(sK, sL);
+  int bra = p1, ket = p2;
+  const int c1 = c->pair_cls[p1], c2 = c->pair_cls[p2];
+  // bra class must not precede the ket class in pair-class order
+  if (c1 < c2 || (c1 == c2 && c->pair_Q[p1] < c->pair_Q[p2])) std::swap(bra, ket);
+  const int cb = c->pair_cls[bra], ck = c->pair_cls[ket];
+  const int cls = class_index(kPairClasses[cb][0], kPairClasses[cb][1], kPairClasses[ck][0], kPairClasses[ck][1]);
+  if (cls < 0) return fail(HFG_INVALID_ARG, "no class for quartet");
+  // one-task launch over two one-element lists
+  std::vector<int> bl{bra}, kl{ket}, kc{1};
+  std::vector<Task> tk{Task{0, 0}};
+  int *d_bl = nullptr, *d_kl = nullptr, *d_kc = nullptr;
+  Task *d_tk = nullptr;
+  hfg_status st;
+  if ((st = upload(&d_bl, bl)) != HFG_OK || (st = upload(&d_kl, kl)) != HFG_OK || (st = upload(&d_kc, kc)) != HFG_OK ||
+      (st = upload(&d_tk, tk)) != HFG_OK || (st = ensure(&c->d_block, 1296)) != HFG_OK) {
+    cudaFree(d_bl); cudaFree(d_kl); cudaFree(d_kc); cudaFree(d_tk);
+    return st;
+  }
+  ClassLaunch cl{};
+  cl.bra_list = d_bl;
+  cl.ket_list = d_kl;
+  cl.ket_count = d_kc;
+  cl.tasks = d_tk;
+  cl.ntasks = 1;
+  cl.packed = c->d_block;
+  kClasses[cls].launch(c->view(), cl, kBlock, c->opts.eri_convention == HFG_ERI_REFERENCE, 1, c->stream);
+  double blk[1296];
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(blk, c->d_block, sizeof blk, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  cudaFree(d_bl); cudaFree(d_kl); cudaFree(d_kc); cudaFree(d_tk);
+  if (e != cudaSuccess) return fail(HFG_DEVICE_ERROR, cudaGetErrorString(e));
+  // locate (i j | k l) in the (first second | first second) block
+  const int fa = c->pair_sa[bra], fb = c->pair_sb[bra], fc = c->pair_sa[ket], fd = c->pair_sb[ket];
+  const int NB = ncart_h(c->shells[fb].L), NC = ncart_h(c->shells[fc].L), ND = ncart_h(c->shells[fd].L);
+  int x[4] = {i, j, k, l};
+  // orient the requested indices to the block's shells
+  if (bra != p1) { std::swap(x[0], x[2]); std::swap(x[1], x[3]); }
+  if (shell_of(x[0]) != fa) std::swap(x[0], x[1]);
+  if (shell_of(x[2]) != fc) std::swap(x[2], x[3]);
+  const int a = x[0] - c->shells[fa].ao, b = x[1] - c->shells[fb].ao, cc = x[2] - c->shells[fc].ao,
+            d = x[3] - c->shells[fd].ao;
+  *out = blk[((a * NB + b) * NC + cc) * ND + d];
+  return HFG_OK;
+}
+
+hfg_status hfg_ctx_stats(const hfg_ctx *c, hfg_stats *out) {
+  if (!c || !out) return hfg::fail(HFG_INVALID_ARG, "null argument");
+  *out = c->stats;
+  return HFG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,301 @@
+// Shell-quartet class kernels: one thread per contracted shell quartet, one
+// warp per (bra pair, 32 consecutive ket pairs).  The bra pair is shared by
+// the warp (its primitive pairs are broadcast loads), the ket pairs come from
+// the Schwarz-sorted ket list of the class.  The Boys table slice the class
+// needs is staged into shared memory once per block.
+#pragma once
+
+#include "eri_gen.cuh"
+#include "hfg_internal.cuh"
+
+namespace hfg {
+
+// full unrolling for blocks whose values fit in registers, rolled loops above
+template <int N>
+constexpr int kUnrollBlock = N <= 81 ? 64 : 1;
+
+__device__ __forceinline__ double inv_factorial(int k) {
+  // 1/k! for k = 0..6
+  const double t[7] = {1.0, 1.0, 0.5, 1.0 / 6.0, 1.0 / 24.0, 1.0 / 120.0, 1.0 / 720.0};
+  return t[k];
+}
+
+template <int LTOT>
+__device__ __forceinline__ void stage_boys(double *tab, const double *__restrict__ g) {
+  for (int x = threadIdx.x; x < kBoysGrid * kBoysTaylor; x += blockDim.x) {
+    const int i = x / kBoysTaylor, k = x - i * kBoysTaylor;
+    tab[x] = g[i * kBoysOrders + LTOT + k] * inv_factorial(k);
+  }
+  __syncthreads();
+}
+
+// Contracted (ab|cd) block of one shell quartet, bra pair `bp`, ket pair
+// `kp`, components in canonical order, normalisation applied.  `npk` = 0
+// yields an all-zero block (inactive lanes).
+template <int LA, int LB, int LC, int LD, bool REF>
+__device__ __forceinline__ void quartet_block(const EngineView &v, const double *tab, int bp, int kp, int npk,
+                                              double *out) {
+  constexpr int LTOT = LA + LB + LC + LD;
+  constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+  using Cls = EriClass<LA, LB, LC, LD, REF>;
+  double acc[Cls::kAcc];
+#pragma unroll
+  for (int x = 0; x < Cls::kAcc; ++x) acc[x] = 0.0;
+
+  const int offb = v.pair_prim_off[bp], npb = v.pair_nprim[bp];
+  const int offk = v.pair_prim_off[kp];
+  for (int ib = 0; ib < npb; ++ib) {
+    const PrimPair pb = v.prim[offb + ib];
+    for (int ik = 0; ik < npk; ++ik) {
+      const PrimPair pk = v.prim[offk + ik];
+      const double inv_zpe = 1.0 / (pb.zeta + pk.zeta);
+      const double rho = pb.zeta * pk.zeta * inv_zpe;
+      const double PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;
+      const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+      double F[LTOT + 1];
+      boys_eval<LTOT, double>(F, T, pb.K * pk.K * sqrt(inv_zpe), tab);
+      const double roz = rho * pb.inv_zeta;
+      const double ie = pk.inv_zeta;
+      Cls::template prim<double>(acc, F, pb.PAx, pb.PAy, pb.PAz, -roz * PQx, -roz * PQy, -roz * PQz,
+                                 0.5 * pb.inv_zeta, roz, -(pb.bABx + pk.bABx) * ie, -(pb.bABy + pk.bABy) * ie,
+                                 -(pb.bABz + pk.bABz) * ie, pb.zeta * ie, 0.5 * ie);
+    }
+  }
+  Cls::template hrr<double>(out, acc, v.pair_AB[3 * bp], v.pair_AB[3 * bp + 1], v.pair_AB[3 * bp + 2],
+                            v.pair_AB[3 * kp], v.pair_AB[3 * kp + 1], v.pair_AB[3 * kp + 2]);
+  constexpr int U = kUnrollBlock<NA * NB * NC * ND>;
+#pragma unroll U
+  for (int a = 0; a < NA; ++a)
+#pragma unroll U
+    for (int b = 0; b < NB; ++b)
+#pragma unroll U
+      for (int c = 0; c < NC; ++c)
+#pragma unroll U
+        for (int d = 0; d < ND; ++d)
+          out[((a * NB + b) * NC + c) * ND + d] *= comp_norm<LA>(a) * comp_norm<LB>(b) * comp_norm<LC>(c) *
+                                                   comp_norm<LD>(d);
+}
+
+// The reference evaluates each function quartet of a (dd|dd) shell quartet
+// with the bra/ket orientation its SwapOrbitals picks from function IDs
+// (IntegralsRepository.cpp:344-370); under the reference's electron-transfer
+// row range the orientation changes the value.  This reproduces the choice
+// per element: AO index == function ID.
+template <int LA, int LB, int LC, int LD, bool REF>
+__device__ __forceinline__ void quartet_values(const EngineView &v, const double *tab, int bp, int kp, int npk,
+                                               double *out) {
+  constexpr bool kOrient = REF && LA == 2 && LB == 2 && LC == 2 && LD == 2;
+  if constexpr (!kOrient) {
+    quartet_block<LA, LB, LC, LD, REF>(v, tab, bp, kp, npk, out);
+  } else {
+    constexpr int N = 6;
+    const int sab = v.pair_sa[bp], skt = v.pair_sa[kp];
+    if (sab > skt || npk == 0) {
+      quartet_block<2, 2, 2, 2, true>(v, tab, bp, kp, npk, out);
+      return;
+    }
+    double sw[N * N * N * N];
+    quartet_block<2, 2, 2, 2, true>(v, tab, kp, bp, v.pair_nprim[bp], sw);
+    if (sab < skt) {
+      for (int a = 0; a < N; ++a)
+        for (int b = 0; b < N; ++b)
+          for (int c = 0; c < N; ++c)
+            for (int d = 0; d < N; ++d) out[((a * N + b) * N + c) * N + d] = sw[((c * N + d) * N + a) * N + b];
+      return;
+    }
+    // same first shell: per-element orientation
+    quartet_block<2, 2, 2, 2, true>(v, tab, bp, kp, npk, out);
+    const int aoa = v.pair_ao_a[bp], aob = v.pair_ao_b[bp], aoc = v.pair_ao_a[kp], aod = v.pair_ao_b[kp];
+    const bool bdiag = v.pair_sa[bp] == v.pair_sb[bp], kdiag = v.pair_sa[kp] == v.pair_sb[kp];
+    for (int a = 0; a < N; ++a)
+      for (int b = 0; b < N; ++b)
+        for (int c = 0; c < N; ++c)
+          for (int d = 0; d < N; ++d) {
+            const int I = aoa + a, J = aob + b, K = aoc + c, L = aod + d;
+            const int o1 = bdiag ? max(I, J) : I, o2 = bdiag ? min(I, J) : J;
+            const int o3 = kdiag ? max(K, L) : K, o4 = kdiag ? min(K, L) : L;
+            const bool bra_first = o1 > o3 || (o1 == o3 && o2 >= o4);
+            if (!bra_first) out[((a * N + b) * N + c) * N + d] = sw[((c * N + d) * N + a) * N + b];
+          }
+  }
+}
+
+template <int LA, int LB, int LC, int LD, int MODE, bool REF>
+__global__ void __launch_bounds__(kThreads) eri_class_kernel(const EngineView v, const ClassLaunch cl) {
+  constexpr int LTOT = LA + LB + LC + LD;
+  constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+  __shared__ double tab[kBoysGrid * kBoysTaylor];
+  stage_boys<LTOT>(tab, v.boys_table);
+
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int n = v.nbf;
+  for (int t = blockIdx.x * kWarpsPerBlock + warp; t < cl.ntasks; t += gridDim.x * kWarpsPerBlock) {
+    const Task task = cl.tasks[t];
+    const int bp = cl.bra_list[task.bra_pos];
+    const int kpos = task.ket_start + lane;
+    const bool active = kpos < cl.ket_count[task.bra_pos];
+    const int kp = active ? cl.ket_list[kpos] : bp;
+    const int npk = active ? v.pair_nprim[kp] : 0;
+
+    double out[NA * NB * NC * ND];
+    quartet_values<LA, LB, LC, LD, REF>(v, tab, bp, kp, npk, out);
+    // blocks above 81 integrals live in local memory anyway: keep their
+    // epilogue loops rolled (code size, compile time)
+    constexpr int U = kUnrollBlock<NA * NB * NC * ND>;
+
+    const int aoa = v.pair_ao_a[bp], aob = v.pair_ao_b[bp], aoc = v.pair_ao_a[kp], aod = v.pair_ao_b[kp];
+    const bool bdiag = v.pair_sa[bp] == v.pair_sb[bp], kdiag = v.pair_sa[kp] == v.pair_sb[kp];
+    const bool same = bp == kp;
+
+    if constexpr (MODE == kBlock) {
+      // raw block of the first quartet (single-integral queries)
+      if (t == 0 && lane == 0 && active)
+        for (int x = 0; x < NA * NB * NC * ND; ++x) cl.packed[x] = out[x];
+    } else if constexpr (MODE == kStorePacked) {
+      if (active) {
+#pragma unroll U
+        for (int a = 0; a < NA; ++a)
+#pragma unroll U
+          for (int b = 0; b < NB; ++b)
+#pragma unroll U
+            for (int c = 0; c < NC; ++c)
+#pragma unroll U
+              for (int d = 0; d < ND; ++d) {
+                const int I = aoa + a, J = aob + b, K = aoc + c, L = aod + d;
+                if (bdiag && I < J) continue;
+                if (kdiag && K < L) continue;
+                const long long ij = tri(I, J), kl = tri(K, L);
+                if (same && ij < kl) continue;
+                cl.packed[tri(ij, kl)] = out[((a * NB + b) * NC + c) * ND + d];
+              }
+      }
+    } else {
+      // degeneracy of the unique quartet among its 8 permutations
+      const double s = (bdiag ? 0.5 : 1.0) * (kdiag ? 0.5 : 1.0) * (same ? 0.5 : 1.0);
+      constexpr bool kUhf = MODE == kJkUhf;
+      const double *DJ = kUhf ? cl.Dt : cl.Da;
+      double jab[NA * NB], jcd[NC * ND];
+      double kac[NA * NC], kad[NA * ND], kbc[NB * NC], kbd[NB * ND];
+      double kac2[kUhf ? NA * NC : 1], kad2[kUhf ? NA * ND : 1], kbc2[kUhf ? NB * NC : 1], kbd2[kUhf ? NB * ND : 1];
+#pragma unroll U
+      for (int x = 0; x < NA * NB; ++x) jab[x] = 0.0;
+#pragma unroll U
+      for (int x = 0; x < NC * ND; ++x) jcd[x] = 0.0;
+#pragma unroll U
+      for (int x = 0; x < NA * NC; ++x) kac[x] = 0.0;
+#pragma unroll U
+      for (int x = 0; x < NA * ND; ++x) kad[x] = 0.0;
+#pragma unroll U
+      for (int x = 0; x < NB * NC; ++x) kbc[x] = 0.0;
+#pragma unroll U
+      for (int x = 0; x < NB * ND; ++x) kbd[x] = 0.0;
+      if constexpr (kUhf) {
+#pragma unroll U
+        for (int x = 0; x < NA * NC; ++x) kac2[x] = 0.0;
+#pragma unroll U
+        for (int x = 0; x < NA * ND; ++x) kad2[x] = 0.0;
+#pragma unroll U
+        for (int x = 0; x < NB * NC; ++x) kbc2[x] = 0.0;
+#pragma unroll U
+        for (int x = 0; x < NB * ND; ++x) kbd2[x] = 0.0;
+      }
+      if (active) {
+#pragma unroll U
+        for (int a = 0; a < NA; ++a)
+#pragma unroll U
+          for (int b = 0; b < NB; ++b)
+#pragma unroll U
+            for (int c = 0; c < NC; ++c)
+#pragma unroll U
+              for (int d = 0; d < ND; ++d) {
+                const int I = aoa + a, J = aob + b, K = aoc + c, L = aod + d;
+                const double val = s * out[((a * NB + b) * NC + c) * ND + d];
+                jab[a * NB + b] += 2.0 * val * __ldg(&DJ[K * n + L]);
+                jcd[c * ND + d] += 2.0 * val * __ldg(&DJ[I * n + J]);
+                kac[a * NC + c] += val * __ldg(&cl.Da[J * n + L]);
+                kad[a * ND + d] += val * __ldg(&cl.Da[J * n + K]);
+                kbc[b * NC + c] += val * __ldg(&cl.Da[I * n + L]);
+                kbd[b * ND + d] += val * __ldg(&cl.Da[I * n + K]);
+                if constexpr (kUhf) {
+                  kac2[a * NC + c] += val * __ldg(&cl.Db[J * n + L]);
+                  kad2[a * ND + d] += val * __ldg(&cl.Db[J * n + K]);
+                  kbc2[b * NC + c] += val * __ldg(&cl.Db[I * n + L]);
+                  kbd2[b * ND + d] += val * __ldg(&cl.Db[I * n + K]);
+                }
+              }
+#pragma unroll U
+        for (int c = 0; c < NC; ++c)
+#pragma unroll U
+          for (int d = 0; d < ND; ++d) atomicAdd(&cl.J[(aoc + c) * n + aod + d], jcd[c * ND + d]);
+#pragma unroll U
+        for (int a = 0; a < NA; ++a) {
+#pragma unroll U
+          for (int c = 0; c < NC; ++c) atomicAdd(&cl.Ka[(aoa + a) * n + aoc + c], kac[a * NC + c]);
+#pragma unroll U
+          for (int d = 0; d < ND; ++d) atomicAdd(&cl.Ka[(aoa + a) * n + aod + d], kad[a * ND + d]);
+        }
+#pragma unroll U
+        for (int b = 0; b < NB; ++b) {
+#pragma unroll U
+          for (int c = 0; c < NC; ++c) atomicAdd(&cl.Ka[(aob + b) * n + aoc + c], kbc[b * NC + c]);
+#pragma unroll U
+          for (int d = 0; d < ND; ++d) atomicAdd(&cl.Ka[(aob + b) * n + aod + d], kbd[b * ND + d]);
+        }
+        if constexpr (kUhf) {
+#pragma unroll U
+          for (int a = 0; a < NA; ++a) {
+#pragma unroll U
+            for (int c = 0; c < NC; ++c) atomicAdd(&cl.Kb[(aoa + a) * n + aoc + c], kac2[a * NC + c]);
+#pragma unroll U
+            for (int d = 0; d < ND; ++d) atomicAdd(&cl.Kb[(aoa + a) * n + aod + d], kad2[a * ND + d]);
+          }
+#pragma unroll U
+          for (int b = 0; b < NB; ++b) {
+#pragma unroll U
+            for (int c = 0; c < NC; ++c) atomicAdd(&cl.Kb[(aob + b) * n + aoc + c], kbc2[b * NC + c]);
+#pragma unroll U
+            for (int d = 0; d < ND; ++d) atomicAdd(&cl.Kb[(aob + b) * n + aod + d], kbd2[b * ND + d]);
+          }
+        }
+      }
+      // the warp shares the bra pair: reduce its J block across lanes first
+#pragma unroll U
+      for (int x = 0; x < NA * NB; ++x) {
+        double r = jab[x];
+#pragma unroll U
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+        jab[x] = r;
+      }
+      if (lane == 0) {
+#pragma unroll U
+        for (int a = 0; a < NA; ++a)
+#pragma unroll U
+          for (int b = 0; b < NB; ++b) atomicAdd(&cl.J[(aoa + a) * n + aob + b], jab[a * NB + b]);
+      }
+    }
+  }
+}
+
+// Schwarz bounds: thread per pair of the class, (ab|ab) with the exact
+// recursion, Q = sqrt(max_ij |(ij|ij)|).
+template <int LA, int LB>
+__global__ void __launch_bounds__(kThreads) schwarz_kernel(const EngineView v, const int *pairs, int npairs,
+                                                           double *Q) {
+  constexpr int NA = ncart(LA), NB = ncart(LB);
+  __shared__ double tab[kBoysGrid * kBoysTaylor];
+  stage_boys<2 * (LA + LB)>(tab, v.boys_table);
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < npairs; x += gridDim.x * blockDim.x) {
+    const int p = pairs[x];
+    double out[NA * NB * NA * NB];
+    quartet_block<LA, LB, LA, LB, false>(v, tab, p, p, v.pair_nprim[p], out);
+    double m = 0.0;
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int b = 0; b < NB; ++b) m = fmax(m, fabs(out[((a * NB + b) * NA + a) * NB + b]));
+    Q[p] = sqrt(m);
+  }
+}
+
+}  // namespace hfg

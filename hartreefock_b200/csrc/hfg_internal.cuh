@@ -1,0 +1,135 @@
+// Internal definitions shared by the class kernels and the host context.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hfg {
+
+constexpr int kMaxL = 2;                      // compiled shells: s, p, d
+constexpr int kMaxLtot = 4 * kMaxL;           // highest Boys order used
+constexpr int kBoysTaylor = 7;                // Taylor terms around a grid point
+constexpr double kBoysStep = 0.05;            // grid spacing in T
+constexpr double kBoysTmax = 36.0;            // above: asymptotic F_0 + upward recursion
+constexpr int kBoysGrid = 721;                // 36 / 0.05 + 1 grid points
+constexpr int kBoysOrders = kMaxLtot + kBoysTaylor;  // orders 0 .. 14 tabulated
+
+constexpr int kWarpsPerBlock = 4;
+constexpr int kThreads = 32 * kWarpsPerBlock;
+
+enum Mode { kStorePacked = 0, kJkRhf = 1, kJkUhf = 2, kSchwarz = 3, kBlock = 4 };
+
+// One primitive pair of a shell pair (first shell A with exponent a, second
+// B with exponent b): zeta = a+b, P = (aA+bB)/zeta, PA = P-A,
+// bAB = b(A-B) and K = N_a c_a N_b c_b exp(-ab/zeta |AB|^2) sqrt(2) pi^(5/4) / zeta,
+// so that the quartet prefactor 2 pi^(5/2) / (zeta eta sqrt(zeta+eta))
+// exp(...) of GaussianTwoElectrons.cpp:44-45 is K_ab K_cd / sqrt(zeta+eta).
+struct __align__(16) PrimPair {
+  double zeta, Px, Py, Pz, PAx, PAy, PAz, bABx, bABy, bABz, K, inv_zeta;
+};
+
+// Device view of one context's tables.
+struct EngineView {
+  const PrimPair *prim;       // all primitive pairs, pair-major
+  const int *pair_prim_off;   // per pair
+  const int *pair_nprim;
+  const int *pair_sa;         // first shell (higher L; higher index on ties)
+  const int *pair_sb;
+  const int *pair_ao_a;       // first AO of each shell of the pair
+  const int *pair_ao_b;
+  const double *pair_AB;      // [3*npairs] A - B
+  const double *pair_Q;       // Schwarz bound
+  const float *pair_Dmax;     // max |D| over the pair's AO block (density screening)
+  const double *boys_table;   // [kBoysGrid][kBoysOrders] F_m(T_i)
+  int nbf;
+  int reference_convention;   // 1: reproduce the reference's (dd|dd) ET rows
+};
+
+// One unit of work: a bra pair position in the class's bra list and the
+// first ket position of a 32-wide ket chunk.
+struct Task {
+  int bra_pos;
+  int ket_start;
+};
+
+struct ClassLaunch {
+  const int *bra_list;   // pair indices of the bra class, sorted by Q desc
+  const int *ket_list;   // pair indices of the ket class, sorted by Q desc
+  const int *ket_count;  // valid kets per bra position
+  const Task *tasks;
+  int ntasks;
+  int same_class;        // bra class == ket class
+  double threshold;
+  // outputs by mode
+  double *packed;        // kStorePacked
+  const double *Da, *Db; // kJk*: densities (Db for UHF)
+  const double *Dt;      // total density for J in UHF
+  double *J, *Ka, *Kb;   // accumulators (n x n)
+  double *Qout;          // kSchwarz: per pair
+  int *fp32_counter;     // unused in FP64 kernels
+};
+
+// component normalisation f(l,m,n) = 1/sqrt((2l-1)!!(2m-1)!!(2n-1)!!) in the
+// canonical component order; the L-dependent part of the primitive
+// normalisation sits in the contraction coefficients
+template <int L>
+__device__ __forceinline__ double comp_norm(int c);
+template <>
+__device__ __forceinline__ double comp_norm<0>(int) { return 1.0; }
+template <>
+__device__ __forceinline__ double comp_norm<1>(int) { return 1.0; }
+template <>
+__device__ __forceinline__ double comp_norm<2>(int c) {
+  // xx xy xz yy yz zz
+  return (c == 0 || c == 3 || c == 5) ? 0.57735026918962576451 : 1.0;
+}
+
+__host__ __device__ constexpr int ncart(int L) { return (L + 1) * (L + 2) / 2; }
+
+// Packed 8-fold index (IntegralsRepository.h:151-162)
+__device__ __forceinline__ long long tri(long long a, long long b) {
+  return a < b ? b * (b + 1) / 2 + a : a * (a + 1) / 2 + b;
+}
+
+// Boys function F_0..F_M at T.  Below kBoysTmax: 7-term Taylor expansion of
+// F_M about the nearest grid point, F_M(T) = sum_k F_{M+k}(T_i) (-dT)^k / k!,
+// from the shared-memory slice tab[i][k] = F_{M+k}(T_i)/k!, then the downward
+// recursion F_m = (2T F_{m+1} + e^-T) / (2m+1) (BoysFunctions.cpp:17-20).
+// Above: F_0 = sqrt(pi/T)/2 (erfc(sqrt T) < 3e-17 there) and the upward
+// recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T).  The scale folds the
+// quartet prefactor into every order.
+template <int M, class R>
+__device__ __forceinline__ void boys_eval(R *F, double T, double scale, const double *__restrict__ tab) {
+  if (T < kBoysTmax) {
+    const int i = __double2int_rn(T * (1.0 / kBoysStep));
+    const double dt = i * kBoysStep - T;  // -(T - T_i)
+    const double *t = tab + i * kBoysTaylor;
+    double f = t[6];
+#pragma unroll
+    for (int k = 5; k >= 0; --k) f = fma(f, dt, t[k]);
+    double fm[M + 1];
+    fm[M] = f;
+    if (M > 0) {
+      const double e = exp(-T);
+      const double t2 = 2.0 * T;
+#pragma unroll
+      for (int m = M - 1; m >= 0; --m) fm[m] = fma(t2, fm[m + 1], e) * (1.0 / (2 * m + 1));
+    }
+#pragma unroll
+    for (int m = 0; m <= M; ++m) F[m] = (R)(fm[m] * scale);
+  } else {
+    double f = 0.88622692545275801365 * rsqrt(T);  // sqrt(pi)/2 / sqrt(T)
+    F[0] = (R)(f * scale);
+    if (M > 0) {
+      const double e = exp(-T);
+      const double h = 0.5 / T;
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        f = ((2 * m + 1) * f - e) * h;
+        F[m + 1] = (R)(f * scale);
+      }
+    }
+  }
+}
+
+}  // namespace hfg

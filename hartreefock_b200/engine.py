@@ -1,0 +1,191 @@
+"""ctypes binding of the engine's C ABI (include/hfgpu.h).
+
+The library is built in-tree (hartreefock_b200/libhfgpu.so, see build.py).
+There is no CPU fallback: loading fails loudly when the library or a CUDA
+device is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .basis_io import ShellTable, shell_table
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libhfgpu.so")
+
+HFG_OK = 0
+STATUS = {0: "HFG_OK", 1: "HFG_INVALID_ARG", 2: "HFG_UNSUPPORTED_L", 3: "HFG_OOM_BUDGET", 4: "HFG_DEVICE_ERROR",
+          5: "HFG_TIMEOUT", 6: "HFG_CANCELLED", 7: "HFG_NO_DEVICE"}
+ERI_REFERENCE, ERI_EXACT = 0, 1
+
+# every symbol include/hfgpu.h declares
+EXPORTED = ["hfg_default_opts", "hfg_last_error", "hfg_device_count", "hfg_ctx_create", "hfg_ctx_destroy",
+            "hfg_ctx_nbf", "hfg_packed_size", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet",
+            "hfg_fock_rhf", "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz",
+            "hfg_ctx_stats"]
+
+
+class HfgError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class hfg_shells(ctypes.Structure):
+    _fields_ = [("nshells", ctypes.c_int32), ("center", ctypes.c_void_p), ("L", ctypes.c_void_p),
+                ("nprim", ctypes.c_void_p), ("prim_offset", ctypes.c_void_p), ("ao_offset", ctypes.c_void_p),
+                ("exponent", ctypes.c_void_p), ("coefficient", ctypes.c_void_p), ("nbf", ctypes.c_int32)]
+
+
+class hfg_opts(ctypes.Structure):
+    _fields_ = [("schwarz_threshold", ctypes.c_double), ("mixed_cutoff", ctypes.c_double),
+                ("eri_convention", ctypes.c_int32), ("device", ctypes.c_int32),
+                ("density_screening", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
+
+
+class hfg_stats(ctypes.Structure):
+    _fields_ = [("shell_pairs", ctypes.c_int64), ("shell_quartets", ctypes.c_int64),
+                ("function_quartets", ctypes.c_int64), ("primitive_quartets", ctypes.c_int64),
+                ("fp32_shell_quartets", ctypes.c_int64), ("flops", ctypes.c_double),
+                ("last_build_ms", ctypes.c_double), ("kernel_launches", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+_lib = None
+
+
+def library(path: str = LIB_PATH):
+    """Load libhfgpu.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m hartreefock_b200.build`")
+    L = ctypes.CDLL(path)
+    vp, i32, i64, dp = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p
+    L.hfg_default_opts.argtypes = [ctypes.POINTER(hfg_opts)]
+    L.hfg_default_opts.restype = None
+    L.hfg_last_error.restype = ctypes.c_char_p
+    L.hfg_device_count.restype = i32
+    L.hfg_ctx_create.argtypes = [ctypes.POINTER(hfg_shells), ctypes.POINTER(hfg_opts), ctypes.POINTER(vp)]
+    L.hfg_ctx_destroy.argtypes = [vp]
+    L.hfg_ctx_destroy.restype = None
+    L.hfg_ctx_nbf.argtypes = [vp]
+    L.hfg_ctx_nbf.restype = i32
+    L.hfg_packed_size.argtypes = [i32]
+    L.hfg_packed_size.restype = i64
+    L.hfg_eri_packed.argtypes = [vp, dp, i64]
+    L.hfg_eri_packed_device.argtypes = [vp, dp, i64, vp]
+    L.hfg_eri_quartet.argtypes = [vp, i32, i32, i32, i32, ctypes.POINTER(ctypes.c_double)]
+    L.hfg_fock_rhf.argtypes = [vp, dp, dp]
+    L.hfg_fock_uhf.argtypes = [vp, dp, dp, dp, dp]
+    L.hfg_fock_rhf_device.argtypes = [vp, dp, dp, vp]
+    L.hfg_fock_uhf_device.argtypes = [vp, dp, dp, dp, dp, vp]
+    L.hfg_schwarz.argtypes = [vp, dp, i64]
+    L.hfg_ctx_stats.argtypes = [vp, ctypes.POINTER(hfg_stats)]
+    for name in ("hfg_ctx_create", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet", "hfg_fock_rhf",
+                 "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz", "hfg_ctx_stats"):
+        getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _check(st):
+    if st != HFG_OK:
+        raise HfgError(st, library().hfg_last_error().decode())
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def default_opts() -> hfg_opts:
+    o = hfg_opts()
+    library().hfg_default_opts(ctypes.byref(o))
+    return o
+
+
+class Engine:
+    """One molecule's ERI / Fock-build context on one GPU."""
+
+    def __init__(self, Z, xyz, basis: str, schwarz_threshold: float = 1e-12, eri_convention: int = ERI_REFERENCE,
+                 device: int = 0, mixed_cutoff: float = 0.0, density_screening: bool = False):
+        self.table: ShellTable = shell_table(Z, xyz, basis)
+        self.Z, self.xyz, self.basis = list(Z), np.asarray(xyz, dtype=np.float64).reshape(-1, 3), basis
+        t = self.table
+        self._keep = [np.ascontiguousarray(x) for x in (t.center.ravel(), t.L, t.nprim, t.prim_offset, t.ao_offset,
+                                                         t.exponent, t.coefficient)]
+        sh = hfg_shells(len(t.L), *[_ptr(x) for x in self._keep], t.nbf)
+        o = default_opts()
+        o.schwarz_threshold = schwarz_threshold
+        o.eri_convention = eri_convention
+        o.device = device
+        o.mixed_cutoff = mixed_cutoff
+        o.density_screening = int(density_screening)
+        self.opts = o
+        h = ctypes.c_void_p()
+        _check(library().hfg_ctx_create(ctypes.byref(sh), ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self.nbf = t.nbf
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().hfg_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def packed_size(self) -> int:
+        return library().hfg_packed_size(self.nbf)
+
+    def eri_packed(self) -> np.ndarray:
+        out = np.empty(self.packed_size(), dtype=np.float64)
+        _check(library().hfg_eri_packed(self._h, _ptr(out), out.size))
+        return out
+
+    def eri_packed_device(self, out_ptr: int, count: int, stream: int = 0):
+        _check(library().hfg_eri_packed_device(self._h, ctypes.c_void_p(out_ptr), count, ctypes.c_void_p(stream)))
+
+    def eri(self, i, j, k, l) -> float:
+        v = ctypes.c_double()
+        _check(library().hfg_eri_quartet(self._h, i, j, k, l, ctypes.byref(v)))
+        return v.value
+
+    def fock_rhf(self, P: np.ndarray) -> np.ndarray:
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        G = np.empty_like(P)
+        _check(library().hfg_fock_rhf(self._h, _ptr(P), _ptr(G)))
+        return G
+
+    def fock_uhf(self, Pa: np.ndarray, Pb: np.ndarray):
+        Pa = np.ascontiguousarray(Pa, dtype=np.float64)
+        Pb = np.ascontiguousarray(Pb, dtype=np.float64)
+        Ga, Gb = np.empty_like(Pa), np.empty_like(Pb)
+        _check(library().hfg_fock_uhf(self._h, _ptr(Pa), _ptr(Pb), _ptr(Ga), _ptr(Gb)))
+        return Ga, Gb
+
+    def fock_rhf_device(self, P_ptr: int, G_ptr: int, stream: int = 0):
+        _check(library().hfg_fock_rhf_device(self._h, ctypes.c_void_p(P_ptr), ctypes.c_void_p(G_ptr),
+                                             ctypes.c_void_p(stream)))
+
+    def fock_uhf_device(self, Pa_ptr, Pb_ptr, Ga_ptr, Gb_ptr, stream: int = 0):
+        _check(library().hfg_fock_uhf_device(self._h, ctypes.c_void_p(Pa_ptr), ctypes.c_void_p(Pb_ptr),
+                                             ctypes.c_void_p(Ga_ptr), ctypes.c_void_p(Gb_ptr),
+                                             ctypes.c_void_p(stream)))
+
+    def schwarz(self) -> np.ndarray:
+        n = len(self.table.L)
+        out = np.empty(n * (n + 1) // 2)
+        _check(library().hfg_schwarz(self._h, _ptr(out), out.size))
+        return out
+
+    def stats(self) -> dict:
+        s = hfg_stats()
+        _check(library().hfg_ctx_stats(self._h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in hfg_stats._fields_ if k != "reserved"}

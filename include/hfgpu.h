@@ -1,0 +1,143 @@
+/* hfgpu -- B200 (sm_100a) two-electron-integral and Fock-build engine.
+ *
+ * C ABI: plain pointers and sizes, no CUDA or C++ types, never throws.
+ * Every entry point returns an hfg_status; hfg_last_error() gives text for
+ * the calling thread's most recent failure.  Host matrices are row-major
+ * nbf x nbf doubles in the reference's atomic-orbital order: atoms in
+ * molecule order -> shells in basis-file order -> Cartesian components in
+ * canonical order (xx, xy, xz, yy, yz, zz), the s part of an SP shell before
+ * its p part.
+ *
+ * The reference interface each call replaces is cited as
+ * file:line of aromanro/HartreeFock (HartreeFock/ directory).
+ *
+ * Threading: a context is used by one host thread at a time; distinct
+ * contexts are independent (each owns its own CUDA stream), matching the
+ * reference's one-algorithm-per-thread model (HartreeFockDoc.cpp:372-405).
+ */
+#ifndef HFGPU_H
+#define HFGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  HFG_OK = 0,
+  HFG_INVALID_ARG = 1,
+  HFG_UNSUPPORTED_L = 2, /* a shell above the compiled angular momentum (d) */
+  HFG_OOM_BUDGET = 3,    /* device allocation or memory budget exceeded */
+  HFG_DEVICE_ERROR = 4,  /* CUDA error; context must be destroyed */
+  HFG_TIMEOUT = 5,
+  HFG_CANCELLED = 6,
+  HFG_NO_DEVICE = 7      /* no CUDA device / kernels not loadable */
+} hfg_status;
+
+/* Which electron-transfer rows the (dd|dd) class computes.
+ * HFG_ERI_REFERENCE reproduces GaussianTwoElectrons::ElectronTransfer
+ * (GaussianTwoElectrons.cpp:162), whose ket column f starts at total L(f)-1;
+ * for (dd|dd) quartets with a two-centre bra the reference therefore omits
+ * the [d0|g0] terms.  HFG_ERI_EXACT evaluates the full recursion. */
+typedef enum { HFG_ERI_REFERENCE = 0, HFG_ERI_EXACT = 1 } hfg_eri_convention;
+
+/* Basis of one molecule, shell by shell (structure of arrays).  One entry per
+ * shell letter: an SP line of the basis file is two shells (L=0 and L=1)
+ * sharing exponents.  Replaces the walk over Molecule::atoms -> shells ->
+ * basisFunctions (IntegralsRepository.cpp:566-578, Molecule.cpp:41-72). */
+typedef struct {
+  int32_t nshells;
+  const double *center;      /* [3*nshells], bohr */
+  const int32_t *L;          /* [nshells], 0..2 */
+  const int32_t *nprim;      /* [nshells] */
+  const int32_t *prim_offset; /* [nshells] into exponent/coefficient */
+  const int32_t *ao_offset;  /* [nshells] first AO index of the shell */
+  const double *exponent;    /* [sum nprim] */
+  const double *coefficient; /* [sum nprim] contraction coefficients from the
+                                basis file; the per-component primitive
+                                normalisation of GaussianOrbital.cpp:25-30 is
+                                applied inside */
+  int32_t nbf;               /* number of Cartesian basis functions */
+} hfg_shells;
+
+typedef struct {
+  double schwarz_threshold; /* skip quartets with Q_ab*Q_cd below this (1e-12) */
+  double mixed_cutoff;      /* direct Fock: quartets whose density-weighted
+                               Schwarz bound is below this run in FP32 with
+                               FP64 accumulation; 0 = all FP64 (default 0) */
+  int32_t eri_convention;   /* hfg_eri_convention, default HFG_ERI_REFERENCE */
+  int32_t device;           /* CUDA ordinal, default 0 */
+  int32_t density_screening;/* 1: direct Fock skips quartets whose
+                               Q_ab*Q_cd*max|D| block bound < threshold */
+  int32_t reserved[5];
+} hfg_opts;
+
+typedef struct hfg_ctx hfg_ctx;
+
+typedef struct {
+  int64_t shell_pairs;         /* significant shell pairs */
+  int64_t shell_quartets;      /* quartets evaluated by the last build */
+  int64_t function_quartets;   /* 8-fold unique function quartets, same build */
+  int64_t primitive_quartets;  /* primitive quartets, same build */
+  int64_t fp32_shell_quartets; /* of which evaluated in FP32 (mixed mode) */
+  double flops;                /* algorithmic flops of the last build */
+  double last_build_ms;        /* device time of the last build (events) */
+  int32_t kernel_launches;     /* kernels launched by the last build */
+  int32_t reserved;
+} hfg_stats;
+
+void hfg_default_opts(hfg_opts *opts);
+const char *hfg_last_error(void);
+/* Number of CUDA devices visible (0 if none). */
+int32_t hfg_device_count(void);
+
+/* Builds the shell pairs, primitive-pair tables, Schwarz bounds and class
+ * lists on the device.  Replaces IntegralsRepository(Molecule*) / Reset
+ * (IntegralsRepository.h:49-51, IntegralsRepository.cpp:19-27). */
+hfg_status hfg_ctx_create(const hfg_shells *shells, const hfg_opts *opts, hfg_ctx **out);
+void hfg_ctx_destroy(hfg_ctx *ctx);
+int32_t hfg_ctx_nbf(const hfg_ctx *ctx);
+
+/* Number of doubles of the packed 8-fold table: GetElectronElectronIndex(n-1,
+ * n-1, n-1, n-1) + 1 (IntegralsRepository.h:151-162). */
+int64_t hfg_packed_size(int32_t nbf);
+
+/* Stored mode: the packed ERI table, index T(T(i,j),T(k,l)) with
+ * T(a,b) = max(max+1)/2 + min.  Replaces
+ * IntegralsRepository::CalculateElectronElectronIntegrals
+ * (IntegralsRepository.cpp:566-584); entries of screened-out quartets are 0.
+ * host_out holds `count` doubles (hfg_packed_size). */
+hfg_status hfg_eri_packed(hfg_ctx *ctx, double *host_out, int64_t count);
+/* Same, into device memory on `stream` (a cudaStream_t, 0 = context stream). */
+hfg_status hfg_eri_packed_device(hfg_ctx *ctx, double *dev_out, int64_t count, void *stream);
+
+/* One contracted integral (i j | k l).  Replaces
+ * IntegralsRepository::getElectronElectron(contracted x4)
+ * (IntegralsRepository.cpp:372-433). */
+hfg_status hfg_eri_quartet(hfg_ctx *ctx, int32_t i, int32_t j, int32_t k, int32_t l, double *out);
+
+/* Direct RHF two-electron matrix G = J[P] - K[P]/2 from the density P,
+ * G_ij = sum_kl P_kl[(ij|kl) - 1/2 (il|kj)], without storing integrals.
+ * Replaces the iter > 0 branch of RestrictedHartreeFock::InitFockMatrix
+ * (RestrictedHartreeFock.cpp:187-203); the caller forms F = h + G. */
+hfg_status hfg_fock_rhf(hfg_ctx *ctx, const double *P, double *G);
+/* Direct UHF: G+ = J[P+ + P-] - K[P+], G- = J[P+ + P-] - K[P-].  Replaces
+ * UnrestrictedHartreeFock::InitFockMatrices (UnrestrictedHartreeFock.cpp:223-240). */
+hfg_status hfg_fock_uhf(hfg_ctx *ctx, const double *Pa, const double *Pb, double *Ga, double *Gb);
+/* Device-pointer forms on `stream` (cudaStream_t or 0). */
+hfg_status hfg_fock_rhf_device(hfg_ctx *ctx, const double *dP, double *dG, void *stream);
+hfg_status hfg_fock_uhf_device(hfg_ctx *ctx, const double *dPa, const double *dPb, double *dGa, double *dGb,
+                               void *stream);
+
+/* Schwarz bounds sqrt(max (ij|ij)) per shell pair (a >= b), in pair order
+ * a*(a+1)/2 + b; `count` = nshells*(nshells+1)/2. */
+hfg_status hfg_schwarz(hfg_ctx *ctx, double *host_out, int64_t count);
+
+hfg_status hfg_ctx_stats(const hfg_ctx *ctx, hfg_stats *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,76 @@
+"""Regenerate the golden fixtures from the reference itself.
+
+Runs the reference's own IntegralsRepository / RestrictedHartreeFock /
+UnrestrictedHartreeFock, compiled headless by oracle/Makefile into
+oracle/_ref/ref_driver, on the fixture molecules and stores what it printed.
+Only needed when fixtures change; needs the reference tree (REF_DIR).
+
+    make -C oracle ref && python tests/golden/make_golden.py
+"""
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, ROOT)
+import oracle as O  # noqa: E402
+from hartreefock_b200 import molecules  # noqa: E402
+from hartreefock_b200.basis_io import basis_path  # noqa: E402
+
+REF_DIR = os.environ.get("REF_DIR", "/root/reference/HartreeFock")
+
+
+def fixtures():
+    h2o_Z, h2o_xyz = molecules.H2O_README
+    return {
+        # README.md water, STO-3G, initGuess 0, alpha 0.5
+        "h2o_sto3g": dict(Z=h2o_Z, xyz=h2o_xyz, basis="sto-3g", ref_basis="sto3g.txt", eri=True,
+                          scf=[("rhf", 0.5, 0.0), ("uhf", 0.5, 0.0)]),
+        # two oxygens: exercises every class up to (dd|dd), two-centre bras included
+        "o2_631gs": dict(Z=[8, 8], xyz=np.array([[0.0, 0.0, 0.0], [0.3, -0.2, 2.3]]), basis="6-31g*",
+                         ref_basis="6-31g_st_.1.nw", eri=True, scf=[]),
+        "h2o_631gs": dict(Z=h2o_Z, xyz=h2o_xyz, basis="6-31g*", ref_basis="6-31g_st_.1.nw", eri=True,
+                          scf=[("rhf", 0.75, 0.75)]),
+        "oh_631g": dict(Z=molecules.hydroxyl()[0], xyz=molecules.hydroxyl()[1], basis="6-31g", ref_basis="6-31g.1.nw",
+                        eri=True, scf=[("uhf", 0.75, 0.75)]),
+        "h2o2_631gs": dict(Z=molecules.water_cluster(2, seed=0)[0], xyz=molecules.water_cluster(2, seed=0)[1],
+                           basis="6-31g*", ref_basis="6-31g_st_.1.nw", eri=False, scf=[("rhf", 0.75, 0.75)]),
+        "h2o_631ppgss": dict(Z=h2o_Z, xyz=h2o_xyz, basis="6-31+g**", ref_basis="6-31+g_st__st_.1.nw", eri=True,
+                             scf=[]),
+    }
+
+
+def main():
+    for name, fx in fixtures().items():
+        out = {"Z": np.array(fx["Z"]), "xyz": np.asarray(fx["xyz"]), "basis": np.array(fx["basis"])}
+        mol = O.Molecule(fx["Z"], fx["xyz"], os.path.join(REF_DIR, fx["ref_basis"]))
+        # the bundled subset must expand to the same basis as the reference file
+        mol_b = O.Molecule(fx["Z"], fx["xyz"], basis_path(fx["basis"]))
+        assert mol_b.nbf == mol.nbf
+        with tempfile.TemporaryDirectory() as td:
+            if fx["eri"]:
+                r = O.run_reference(mol, "eri", os.path.join(td, "eri.bin"))
+                out["eri_packed"] = r["eri_packed"]
+                out["h"] = r["h"].reshape(mol.nbf, mol.nbf)
+                out["enuc"] = r["enuc"]
+            for kind, alpha, guess in fx["scf"]:
+                r = O.run_reference(mol, kind, os.path.join(td, kind + ".bin"), alpha=alpha, init_guess=guess)
+                out[f"{kind}_energy"] = r["energy"]
+                out[f"{kind}_alpha"] = np.array(alpha)
+                out[f"{kind}_initguess"] = np.array(guess)
+                if kind == "rhf":
+                    out["rhf_density"] = r["density"].reshape(mol.nbf, mol.nbf)
+                else:
+                    out["uhf_density_alpha"] = r["density_alpha"].reshape(mol.nbf, mol.nbf)
+                    out["uhf_density_beta"] = r["density_beta"].reshape(mol.nbf, mol.nbf)
+                out["h"] = r["h"].reshape(mol.nbf, mol.nbf)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+        print(name, mol.nbf, {k: (v.shape if hasattr(v, "shape") else v) for k, v in out.items()})
+
+
+if __name__ == "__main__":
+    main()
