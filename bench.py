@@ -1,0 +1,277 @@
+"""Benchmark: direct FP64 Fock build (ERI evaluation + J/K digestion) of a
+water cluster, (H2O)_16 / 6-31G* (304 Cartesian basis functions), seeded
+synthetic geometry.
+
+A step is one two-electron Fock build G[P] over every Schwarz-significant
+shell quartet (threshold 1e-12).  The metric is ERI quartets/s: 8-fold
+unique contracted function quartets evaluated per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank builds the same molecule's
+Fock matrix: the build is replicated, not sharded (scaling "weak"); the
+sharded multi-GPU build lives in hartreefock_b200.multi.
+`--impl reference` times the reference's own CPU ERI path (oracle/_ref,
+compiled headless from the reference sources) on a bounded sample of the
+same workload with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WATERS = 16
+BASIS = "6-31g*"
+SEED = 0
+THRESHOLD = 1e-12
+METRIC = "ERI quartets/s"
+
+
+def workload():
+    from hartreefock_b200 import molecules
+    Z, xyz = molecules.water_cluster(WATERS, seed=SEED)
+    return Z, xyz
+
+
+def synthetic_density(n, seed=1):
+    """A symmetric density of realistic magnitude: 2 C C^T of random
+    orthonormal occupied vectors."""
+    rng = np.random.default_rng(seed)
+    nocc = max(1, n // 4)
+    Q, _ = np.linalg.qr(rng.normal(size=(n, nocc)))
+    return 2.0 * Q @ Q.T
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) > 8:
+                for k, name in enumerate(names):
+                    if r[5 + k].lower() == "active":
+                        reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def cpu_baseline(sample_per_thread: int, threads: int):
+    """The reference's own CPU ERI path (IntegralsRepository::getElectronElectron
+    over the build's loop order) on a sample of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # test infrastructure: the reference built headless
+    from hartreefock_b200.basis_io import basis_path
+    Z, xyz = workload()
+    mol = O.Molecule(Z, xyz, basis_path(BASIS))
+    if not os.path.exists(O.DRIVER_PATH):
+        raise RuntimeError("oracle/_ref/ref_driver missing (build with make -C oracle ref)")
+    r = O.run_reference(mol, "bench", "/dev/null", extra=f"sample {sample_per_thread}\nthreads {threads}")
+    out = json.loads(r["stdout"].strip().splitlines()[-1])
+    return out
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    per_step = []
+    for _ in range(args.warmup):
+        cpu_baseline(2000, threads)
+    for _ in range(args.steps):
+        out = cpu_baseline(args.ref_sample, threads)
+        per_step.append(out["quartets"] / out["seconds"])
+    value = float(np.mean(per_step))
+    line = {
+        "metric": METRIC, "value": value, "unit": "quartets/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * args.ref_sample * threads / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"(H2O)_{WATERS} {BASIS} direct Fock build, seed {SEED}", "nbf": 19 * WATERS,
+                   "schwarz_threshold": THRESHOLD},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "quartets/s", "cores": threads, "kind": "reference",
+                         "sample": f"{args.ref_sample} function quartets per thread through "
+                                   "IntegralsRepository::getElectronElectron, one repository per thread"},
+        "e2e": {"value": value, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--ref-sample", type=int, default=30000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    from hartreefock_b200 import engine as E
+
+    Z, xyz = workload()
+    eng = E.Engine(Z, xyz, BASIS, schwarz_threshold=THRESHOLD, device=local)
+    n = eng.nbf
+    P_host = synthetic_density(n)
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    dP = torch.from_numpy(P_host).cuda()
+    dG = torch.empty_like(dP)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+
+    def step():
+        eng.fock_rhf_device(dP.data_ptr(), dG.data_ptr(), sptr)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    stats = eng.stats()
+
+    # ---- device-timed value: per-step events, L2 flushed between steps
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for a, b in evs:
+            flush.zero_()
+            a.record(stream)
+            step()
+            b.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    quartets = stats["function_quartets"] * world
+    value = quartets * args.steps / (total_ms / 1e3)
+
+    # ---- end to end through the public host-buffer entry point hfg_fock_rhf
+    # (H2D of P, build, D2H of G inside the call; the call is synchronous)
+    P_pin = torch.from_numpy(P_host).pin_memory().numpy()
+    G_pin = torch.empty(n, n, dtype=torch.float64).pin_memory().numpy()
+    eng.fock_rhf(P_pin, out=G_pin)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.fock_rhf(P_pin, out=G_pin)
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    assert np.allclose(G_pin, dG.cpu().numpy(), atol=1e-9)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = quartets * args.steps / (e2e_ms / 1e3)
+
+    # ---- roofline of the dominant class kernel (profiled pass, events per class)
+    eng.set_profiling(True)
+    step()
+    torch.cuda.synchronize()
+    prof = eng.class_profile()
+    eng.set_profiling(False)
+    top = max(prof, key=lambda c: c["ms"])
+    peak = E.measure_fp64_peak(local)
+    achieved = top["flops"] / (top["ms"] / 1e3) / 1e12
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "quartets/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"(H2O)_{WATERS} {BASIS} direct RHF Fock build, seed {SEED}", "nbf": n,
+                   "schwarz_threshold": THRESHOLD, "shell_quartets": stats["shell_quartets"],
+                   "function_quartets": stats["function_quartets"], "l2": "flushed (256 MB write) between steps",
+                   "parallelism": f"replicated x{world}"},
+        "e2e": {"value": e2e, "unit": "quartets/s", "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": n * n * 8},
+        "gpu_launches": stats["kernel_launches"] * args.steps,
+        "roofline": {"bound": "fp64", "kernel": f"eri_class_kernel<{top['la']},{top['lb']},{top['lc']},{top['ld']}> (J/K)",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "peak_source": "measured in-run: FP64 FMA microbenchmark (hfg_measure_fp64_peak)",
+                     "traffic": None},
+        "build_tflops": stats["flops"] / (total_ms / args.steps / 1e3) / 1e12,
+        "classes": [{"class": f"({c['la']}{c['lb']}|{c['lc']}{c['ld']})", "ms": round(c["ms"], 4),
+                     "tflops": round(c["flops"] / max(c["ms"], 1e-9) / 1e9, 3)} for c in prof],
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = 1
+        cb = cpu_baseline(args.ref_sample, threads)
+        line["cpu_baseline"] = {"value": cb["quartets"] / cb["seconds"], "unit": "quartets/s", "cores": threads,
+                                "kind": "reference",
+                                "sample": f"{cb['quartets']} function quartets of the same cluster through the "
+                                          "reference's IntegralsRepository::getElectronElectron, 1 thread"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -78,6 +78,8 @@ struct QuartetClass {
   Task *d_tasks = nullptr;
   int64_t shell_quartets = 0, function_quartets = 0, prim_quartets = 0;
   double flops = 0;
+  cudaEvent_t ev_a = nullptr, ev_b = nullptr;  // per-class timing (profiling on)
+  float last_ms = 0;
 };
 
 template <class T>
@@ -116,6 +118,7 @@ struct hfg_ctx {
   double *d_J = nullptr, *d_Ka = nullptr, *d_Kb = nullptr, *d_P = nullptr, *d_Pb = nullptr, *d_Pt = nullptr;
   double *d_G = nullptr, *d_Gb = nullptr, *d_block = nullptr;
   hfg_stats stats{};
+  bool profiling = false;
   EngineView view() const {
     EngineView v{};
     v.prim = d_prim;
@@ -138,6 +141,8 @@ struct hfg_ctx {
     for (auto &q : qclasses) {
       cudaFree(q.d_ket_count);
       cudaFree(q.d_tasks);
+      if (q.ev_a) cudaEventDestroy(q.ev_a);
+      if (q.ev_b) cudaEventDestroy(q.ev_b);
     }
     for (auto &p : pclass) cudaFree(p.d_pairs);
     void *bufs[] = {d_prim, d_pair_prim_off, d_pair_nprim, d_pair_sa, d_pair_sb, d_pair_ao_a, d_pair_ao_b,
@@ -326,8 +331,9 @@ static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const do
   const EngineView v = c->view();
   const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
   c->stats = hfg_stats{};
-  for (const auto &q : c->qclasses) {
+  for (auto &q : c->qclasses) {
     ClassLaunch cl = base_launch(c, q);
+    if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_a, s));
     cl.Da = dPa;
     cl.Db = dPb;
     cl.Dt = uhf ? c->d_Pt : dPa;
@@ -335,6 +341,7 @@ static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const do
     cl.Ka = c->d_Ka;
     cl.Kb = c->d_Kb;
     kClasses[q.cls].launch(v, cl, uhf ? kJkUhf : kJkRhf, ref, grid_for(c, cl.ntasks), s);
+    if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_b, s));
     ++launches;
     c->stats.shell_quartets += q.shell_quartets;
     c->stats.function_quartets += q.function_quartets;
@@ -359,6 +366,8 @@ static hfg_status finish_timing(hfg_ctx *c) {
   float ms = 0;
   HFG_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
   c->stats.last_build_ms = ms;
+  if (c->profiling)
+    for (auto &q : c->qclasses) HFG_CUDA(cudaEventElapsedTime(&q.last_ms, q.ev_a, q.ev_b));
   return HFG_OK;
 }
 
@@ -369,10 +378,12 @@ static hfg_status stored_build(hfg_ctx *c, double *d_out, int64_t count, cudaStr
   const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
   c->stats = hfg_stats{};
   int launches = 1;
-  for (const auto &q : c->qclasses) {
+  for (auto &q : c->qclasses) {
     ClassLaunch cl = base_launch(c, q);
     cl.packed = d_out;
+    if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_a, s));
     kClasses[q.cls].launch(v, cl, kStorePacked, ref, grid_for(c, cl.ntasks), s);
+    if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_b, s));
     ++launches;
     c->stats.shell_quartets += q.shell_quartets;
     c->stats.function_quartets += q.function_quartets;
@@ -698,6 +709,32 @@ hfg_status hfg_eri_quartet(hfg_ctx *c, int32_t i, int32_t j, int32_t k, int32_t 
   const int a = x[0] - c->shells[fa].ao, b = x[1] - c->shells[fb].ao, cc = x[2] - c->shells[fc].ao,
             d = x[3] - c->shells[fd].ao;
   *out = blk[((a * NB + b) * NC + cc) * ND + d];
+  return HFG_OK;
+}
+
+hfg_status hfg_set_profiling(hfg_ctx *c, int32_t on) {
+  if (!c) return hfg::fail(HFG_INVALID_ARG, "null context");
+  HFG_CUDA(cudaSetDevice(c->device));
+  for (auto &q : c->qclasses) {
+    if (!q.ev_a) HFG_CUDA(cudaEventCreate(&q.ev_a));
+    if (!q.ev_b) HFG_CUDA(cudaEventCreate(&q.ev_b));
+  }
+  c->profiling = on != 0;
+  return HFG_OK;
+}
+
+hfg_status hfg_class_profile(const hfg_ctx *c, hfg_class_time *out, int32_t cap, int32_t *count) {
+  using namespace hfg;
+  if (!c || !out || !count) return fail(HFG_INVALID_ARG, "null argument");
+  int n = 0;
+  for (const auto &q : c->qclasses) {
+    if (n >= cap) break;
+    const ClassEntry &e = kClasses[q.cls];
+    out[n] = hfg_class_time{e.la, e.lb, e.lc, e.ld, q.shell_quartets, q.function_quartets, q.prim_quartets,
+                            q.flops, (double)q.last_ms};
+    ++n;
+  }
+  *count = n;
   return HFG_OK;
 }
 

@@ -24,7 +24,7 @@ ERI_REFERENCE, ERI_EXACT = 0, 1
 EXPORTED = ["hfg_default_opts", "hfg_last_error", "hfg_device_count", "hfg_ctx_create", "hfg_ctx_destroy",
             "hfg_ctx_nbf", "hfg_packed_size", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet",
             "hfg_fock_rhf", "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz",
-            "hfg_ctx_stats"]
+            "hfg_ctx_stats", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak"]
 
 
 class HfgError(RuntimeError):
@@ -51,6 +51,12 @@ class hfg_stats(ctypes.Structure):
                 ("fp32_shell_quartets", ctypes.c_int64), ("flops", ctypes.c_double),
                 ("last_build_ms", ctypes.c_double), ("kernel_launches", ctypes.c_int32),
                 ("reserved", ctypes.c_int32)]
+
+
+class hfg_class_time(ctypes.Structure):
+    _fields_ = [("la", ctypes.c_int32), ("lb", ctypes.c_int32), ("lc", ctypes.c_int32), ("ld", ctypes.c_int32),
+                ("shell_quartets", ctypes.c_int64), ("function_quartets", ctypes.c_int64),
+                ("primitive_quartets", ctypes.c_int64), ("flops", ctypes.c_double), ("ms", ctypes.c_double)]
 
 
 _lib = None
@@ -85,7 +91,10 @@ def library(path: str = LIB_PATH):
     L.hfg_fock_uhf_device.argtypes = [vp, dp, dp, dp, dp, vp]
     L.hfg_schwarz.argtypes = [vp, dp, i64]
     L.hfg_ctx_stats.argtypes = [vp, ctypes.POINTER(hfg_stats)]
-    for name in ("hfg_ctx_create", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet", "hfg_fock_rhf",
+    L.hfg_set_profiling.argtypes = [vp, i32]
+    L.hfg_class_profile.argtypes = [vp, ctypes.POINTER(hfg_class_time), i32, ctypes.POINTER(i32)]
+    L.hfg_measure_fp64_peak.argtypes = [i32, ctypes.POINTER(ctypes.c_double)]
+    for name in ("hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak", "hfg_ctx_create", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet", "hfg_fock_rhf",
                  "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz", "hfg_ctx_stats"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
@@ -99,6 +108,12 @@ def _check(st):
 
 def _ptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def measure_fp64_peak(device: int = 0) -> float:
+    v = ctypes.c_double()
+    _check(library().hfg_measure_fp64_peak(device, ctypes.byref(v)))
+    return v.value
 
 
 def default_opts() -> hfg_opts:
@@ -157,9 +172,10 @@ class Engine:
         _check(library().hfg_eri_quartet(self._h, i, j, k, l, ctypes.byref(v)))
         return v.value
 
-    def fock_rhf(self, P: np.ndarray) -> np.ndarray:
+    def fock_rhf(self, P: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
         P = np.ascontiguousarray(P, dtype=np.float64)
-        G = np.empty_like(P)
+        G = np.empty_like(P) if out is None else out
+        assert G.flags.c_contiguous and G.dtype == np.float64 and G.shape == P.shape
         _check(library().hfg_fock_rhf(self._h, _ptr(P), _ptr(G)))
         return G
 
@@ -184,6 +200,15 @@ class Engine:
         out = np.empty(n * (n + 1) // 2)
         _check(library().hfg_schwarz(self._h, _ptr(out), out.size))
         return out
+
+    def set_profiling(self, on: bool = True):
+        _check(library().hfg_set_profiling(self._h, int(on)))
+
+    def class_profile(self) -> list:
+        arr = (hfg_class_time * 64)()
+        n = ctypes.c_int32()
+        _check(library().hfg_class_profile(self._h, arr, 64, ctypes.byref(n)))
+        return [{k: getattr(arr[i], k) for k, _ in hfg_class_time._fields_} for i in range(n.value)]
 
     def stats(self) -> dict:
         s = hfg_stats()

@@ -137,6 +137,26 @@ hfg_status hfg_schwarz(hfg_ctx *ctx, double *host_out, int64_t count);
 
 hfg_status hfg_ctx_stats(const hfg_ctx *ctx, hfg_stats *out);
 
+/* Per-class timing of the builds (no reference counterpart: instrumentation
+ * for the roofline accounting).  With profiling on, every class launch of a
+ * build is bracketed by CUDA events on the build's stream. */
+typedef struct {
+  int32_t la, lb, lc, ld;   /* class (La Lb | Lc Ld) */
+  int64_t shell_quartets;
+  int64_t function_quartets;
+  int64_t primitive_quartets;
+  double flops;             /* algorithmic flops of the class in one build */
+  double ms;                /* device time of the class kernel, last build */
+} hfg_class_time;
+hfg_status hfg_set_profiling(hfg_ctx *ctx, int32_t on);
+/* Writes up to `cap` entries (largest flops first); *count = entries written. */
+hfg_status hfg_class_profile(const hfg_ctx *ctx, hfg_class_time *out, int32_t cap, int32_t *count);
+
+/* Device peak of dependent-free FP64 FMA issue, measured by a short
+ * microbenchmark on `device` (TFLOP/s, 2 flops per FMA).  Instrumentation
+ * for the roofline denominator; no reference counterpart. */
+hfg_status hfg_measure_fp64_peak(int32_t device, double *tflops);
+
 #ifdef __cplusplus
 }
 #endif

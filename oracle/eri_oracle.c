@@ -280,7 +280,8 @@ double orc_eri(const orc_function *fn, const orc_primitive *pr, int i, int j, in
                                        &pr[o3->prim_offset + p3], &pr[o4->prim_offset + p4]};
           const orc_function *gf[4] = {o1, o2, o3, o4};
           int gid[4] = {o1->prim_offset + p1, o2->prim_offset + p2, o3->prim_offset + p3, o4->prim_offset + p4};
-          const double factor = g[0]->coef_norm * g[1]->coef_norm * g[2]->coef_norm * g[3]->coef_norm;
+          const double factor = g[0]->norm * g[1]->norm * g[2]->norm * g[3]->norm * g[0]->coef * g[1]->coef *
+                                g[2]->coef * g[3]->coef;
           /* getElectronElectronVerticalAndTransfer (IntegralsRepository.cpp:436-475) */
           int ord[4] = {0, 1, 2, 3}, tt;
           if (L1 == L2 && gid[ord[0]] < gid[ord[1]]) { tt = ord[0]; ord[0] = ord[1]; ord[1] = tt; }
@@ -513,7 +514,8 @@ static double nuclear_pair(const orc_function *o1, const orc_function *o2, const
           M[ci * size + m] = v;
         }
       }
-      const double f = g1->coef_norm * g2->coef_norm;
+      /* IntegralsRepository.cpp:273 */
+      const double f = g1->norm * g2->norm * g1->coef * g2->coef;
       for (int r = 0; r < rowsN; ++r) acc[r] += f * M[r * size];
     }
   free(M);
@@ -561,8 +563,9 @@ void orc_one_electron(int n, const orc_function *f, const orc_primitive *p, int 
           for (int d = 0; d < 3; ++d) d2 += (o1->center[d] - o2->center[d]) * (o1->center[d] - o2->center[d]);
           const double inv = 1. / (g1->alpha + g2->alpha);
           const double factor = exp(-g1->alpha * g2->alpha * inv * d2) * pow(M_PI * inv, 1.5);
-          const double cc = g1->coef_norm * g2->coef_norm;
-          s += cc * factor * sx[o1->l][o2->l] * sy[o1->m][o2->m] * sz[o1->n][o2->n];
+          /* IntegralsRepository.cpp:96-106, 182-192 */
+          const double cc = g1->norm * g2->norm * g1->coef * g2->coef;
+          s += cc * (factor * sx[o1->l][o2->l] * sy[o1->m][o2->m] * sz[o1->n][o2->n]);
           /* GaussianKinetic::getKinetic (GaussianKinetic.cpp:42-57) */
           t += cc * factor *
                (kinetic_1d(g1->alpha, g2->alpha, o1->l, o2->l, sx) * sy[o1->m][o2->m] * sz[o1->n][o2->n] +

@@ -30,11 +30,14 @@ typedef struct {
   int nprim;
 } orc_function;
 
-/* Primitive: exponent and coefficient * per-component normalisation
- * (GaussianOrbital.cpp:25-30, applied at basis load Basis.cpp:77-78). */
+/* Primitive: exponent, contraction coefficient and per-component
+ * normalisation (GaussianOrbital.cpp:25-30, set at basis load
+ * Basis.cpp:77-78), kept apart because the reference multiplies them in the
+ * order N1 N2 N3 N4 c1 c2 c3 c4 (IntegralsRepository.cpp:405-406). */
 typedef struct {
   double alpha;
-  double coef_norm;
+  double coef;
+  double norm;
 } orc_primitive;
 
 /* BoysFunction::operator() (BoysFunction.cpp:7-25) with

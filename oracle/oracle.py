@@ -124,7 +124,7 @@ class OrcFunction(ctypes.Structure):
 
 
 class OrcPrimitive(ctypes.Structure):
-    _fields_ = [("alpha", ctypes.c_double), ("coef_norm", ctypes.c_double)]
+    _fields_ = [("alpha", ctypes.c_double), ("coef", ctypes.c_double), ("norm", ctypes.c_double)]
 
 
 @dataclass
@@ -157,12 +157,12 @@ class Molecule:
                         f.prim_offset = len(prims)
                         f.nprim = len(sh.exponents)
                         for e, c in zip(sh.exponents, sh.coefs[li]):
-                            prims.append((e, c * primitive_norm(e, lmn)))
+                            prims.append((e, c, primitive_norm(e, lmn)))
                         funcs.append(f)
                 shell_id += 1
         self.nbf = len(funcs)
         self.functions = (OrcFunction * len(funcs))(*funcs)
-        self.primitives = (OrcPrimitive * len(prims))(*[OrcPrimitive(e, c) for e, c in prims])
+        self.primitives = (OrcPrimitive * len(prims))(*[OrcPrimitive(e, c, nf) for e, c, nf in prims])
         nel = int(sum(self.Z))
         if self.alpha_electrons == 0 and self.beta_electrons == 0:
             self.alpha_electrons = nel // 2
@@ -480,8 +480,9 @@ def run_reference(mol: Molecule, mode: str, out_path: str, alpha=0.75, init_gues
                   post_diis=500, extra: str = "", timeout=3600) -> dict:
     lines = [f"basis {mol.basis_path}"]
     for z, p in zip(mol.Z, mol.xyz):
-        lines.append(f"atom {z} {p[0]!r} {p[1]!r} {p[2]!r}")
-    lines += [f"alpha {alpha!r}", f"initguess {init_guess!r}", f"diis {int(use_diis)}", f"postdiis {post_diis}",
+        lines.append(f"atom {int(z)} {float(p[0]):.17g} {float(p[1]):.17g} {float(p[2]):.17g}")
+    lines += [f"alpha {float(alpha):.17g}", f"initguess {float(init_guess):.17g}", f"diis {int(use_diis)}",
+              f"postdiis {int(post_diis)}",
               f"mode {mode}", f"out {out_path}", extra]
     r = subprocess.run([DRIVER_PATH], input="\n".join(lines) + "\n", capture_output=True, text=True,
                        timeout=timeout)

@@ -181,8 +181,9 @@ int main() {
     // (IntegralsRepository.cpp:484-528) through the public contracted
     // accessor.  Each thread owns its own repository, as each GUI job thread
     // owns its own algorithm (HartreeFockDoc.cpp:372-405), and evaluates
-    // `sample` canonical function quartets starting at a thread-dependent row;
-    // maps are cleared per row as in the low-memory mode (.cpp:499-505).
+    // `sample` canonical function quartets starting at a thread-dependent row,
+    // keeping the primitive and contracted maps as the default
+    // useLotsOfMemory mode does (IntegralsRepository.h:184).
     const auto fns = Functions(molecule);
     const long n = static_cast<long>(fns.size());
     std::atomic<long> done{0};
@@ -205,7 +206,6 @@ int main() {
                                                 fns[static_cast<size_t>(k)], fns[static_cast<size_t>(l)]);
                 ++count;
               }
-            repo.ClearElectronElectronMaps();
           }
         }
         sink[static_cast<size_t>(t)] = acc;
