@@ -47,8 +47,8 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
     stamp = os.path.join(CSRC, "eri_gen.cuh")
     if _stale(stamp, [gen]):
         _run([sys.executable, gen, CSRC])
-    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
-        glob.glob(os.path.join(ROOT, "include", "*.h"))
+    kernel_headers = glob.glob(os.path.join(CSRC, "*.cuh"))
+    all_headers = kernel_headers + glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
     units = sorted(glob.glob(os.path.join(CSRC, "*.cu"))) + sorted(glob.glob(os.path.join(CSRC, "*.cpp")))
     jobs_list = []
     for src in units:
@@ -57,6 +57,8 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
             cmd = [NVCC] + CUFLAGS + ["-Xptxas", "-v", "-c", src, "-o", obj]
         else:
             cmd = ["g++"] + CXXFLAGS + ["-c", src, "-o", obj]
+        # the generated class kernels see only the kernel headers
+        headers = kernel_headers if os.path.basename(src).startswith("eri_") else all_headers
         jobs_list.append((src, obj, cmd, _stale(obj, [src] + headers)))
     logs = []
     todo = [j for j in jobs_list if j[3]]

@@ -44,10 +44,12 @@ __device__ __forceinline__ void quartet_block(const EngineView &v, const double 
 
   const int offb = v.pair_prim_off[bp], npb = v.pair_nprim[bp];
   const int offk = v.pair_prim_off[kp];
-  for (int ib = 0; ib < npb; ++ib) {
-    const PrimPair pb = v.prim[offb + ib];
-    for (int ik = 0; ik < npk; ++ik) {
-      const PrimPair pk = v.prim[offk + ik];
+  // ket primitive pairs differ across the warp's lanes: load each once; the
+  // bra primitive pairs are shared by the warp (broadcast loads)
+  for (int ik = 0; ik < npk; ++ik) {
+    const PrimPair pk = v.prim[offk + ik];
+    for (int ib = 0; ib < npb; ++ib) {
+      const PrimPair pb = v.prim[offb + ib];
       const double inv_zpe = 1.0 / (pb.zeta + pk.zeta);
       const double rho = pb.zeta * pk.zeta * inv_zpe;
       const double PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;
@@ -80,43 +82,48 @@ __device__ __forceinline__ void quartet_block(const EngineView &v, const double 
 // with the bra/ket orientation its SwapOrbitals picks from function IDs
 // (IntegralsRepository.cpp:344-370); under the reference's electron-transfer
 // row range the orientation changes the value.  This reproduces the choice
-// per element: AO index == function ID.
-template <int LA, int LB, int LC, int LD, bool REF>
-__device__ __forceinline__ void quartet_values(const EngineView &v, const double *tab, int bp, int kp, int npk,
-                                               double *out) {
-  constexpr bool kOrient = REF && LA == 2 && LB == 2 && LC == 2 && LD == 2;
-  if constexpr (!kOrient) {
-    quartet_block<LA, LB, LC, LD, REF>(v, tab, bp, kp, npk, out);
-  } else {
-    constexpr int N = 6;
-    const int sab = v.pair_sa[bp], skt = v.pair_sa[kp];
-    if (sab > skt || npk == 0) {
-      quartet_block<2, 2, 2, 2, true>(v, tab, bp, kp, npk, out);
-      return;
-    }
-    double sw[N * N * N * N];
-    quartet_block<2, 2, 2, 2, true>(v, tab, kp, bp, v.pair_nprim[bp], sw);
-    if (sab < skt) {
-      for (int a = 0; a < N; ++a)
-        for (int b = 0; b < N; ++b)
-          for (int c = 0; c < N; ++c)
-            for (int d = 0; d < N; ++d) out[((a * N + b) * N + c) * N + d] = sw[((c * N + d) * N + a) * N + b];
-      return;
-    }
-    // same first shell: per-element orientation
+// per element (AO index == function ID).  Kept out of line: it holds three
+// (dd|dd) blocks and is only reached by the rare two-d-shell quartets.
+static __device__ __noinline__ void dddd_reference_values(const EngineView &v, const double *tab, int bp, int kp, int npk,
+                                                   double *out) {
+  constexpr int N = 6;
+  const int sab = v.pair_sa[bp], skt = v.pair_sa[kp];
+  if (sab > skt || npk == 0) {
     quartet_block<2, 2, 2, 2, true>(v, tab, bp, kp, npk, out);
-    const int aoa = v.pair_ao_a[bp], aob = v.pair_ao_b[bp], aoc = v.pair_ao_a[kp], aod = v.pair_ao_b[kp];
-    const bool bdiag = v.pair_sa[bp] == v.pair_sb[bp], kdiag = v.pair_sa[kp] == v.pair_sb[kp];
+    return;
+  }
+  double sw[N * N * N * N];
+  quartet_block<2, 2, 2, 2, true>(v, tab, kp, bp, v.pair_nprim[bp], sw);
+  if (sab < skt) {
     for (int a = 0; a < N; ++a)
       for (int b = 0; b < N; ++b)
         for (int c = 0; c < N; ++c)
-          for (int d = 0; d < N; ++d) {
-            const int I = aoa + a, J = aob + b, K = aoc + c, L = aod + d;
-            const int o1 = bdiag ? max(I, J) : I, o2 = bdiag ? min(I, J) : J;
-            const int o3 = kdiag ? max(K, L) : K, o4 = kdiag ? min(K, L) : L;
-            const bool bra_first = o1 > o3 || (o1 == o3 && o2 >= o4);
-            if (!bra_first) out[((a * N + b) * N + c) * N + d] = sw[((c * N + d) * N + a) * N + b];
-          }
+          for (int d = 0; d < N; ++d) out[((a * N + b) * N + c) * N + d] = sw[((c * N + d) * N + a) * N + b];
+    return;
+  }
+  // same first shell: per-element orientation
+  quartet_block<2, 2, 2, 2, true>(v, tab, bp, kp, npk, out);
+  const int aoa = v.pair_ao_a[bp], aob = v.pair_ao_b[bp], aoc = v.pair_ao_a[kp], aod = v.pair_ao_b[kp];
+  const bool bdiag = v.pair_sa[bp] == v.pair_sb[bp], kdiag = v.pair_sa[kp] == v.pair_sb[kp];
+  for (int a = 0; a < N; ++a)
+    for (int b = 0; b < N; ++b)
+      for (int c = 0; c < N; ++c)
+        for (int d = 0; d < N; ++d) {
+          const int I = aoa + a, J = aob + b, K = aoc + c, L = aod + d;
+          const int o1 = bdiag ? max(I, J) : I, o2 = bdiag ? min(I, J) : J;
+          const int o3 = kdiag ? max(K, L) : K, o4 = kdiag ? min(K, L) : L;
+          const bool bra_first = o1 > o3 || (o1 == o3 && o2 >= o4);
+          if (!bra_first) out[((a * N + b) * N + c) * N + d] = sw[((c * N + d) * N + a) * N + b];
+        }
+}
+
+template <int LA, int LB, int LC, int LD, bool REF>
+__device__ __forceinline__ void quartet_values(const EngineView &v, const double *tab, int bp, int kp, int npk,
+                                               double *out) {
+  if constexpr (REF && LA == 2 && LB == 2 && LC == 2 && LD == 2) {
+    dddd_reference_values(v, tab, bp, kp, npk, out);
+  } else {
+    quartet_block<LA, LB, LC, LD, REF>(v, tab, bp, kp, npk, out);
   }
 }
 

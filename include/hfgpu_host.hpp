@@ -1,0 +1,259 @@
+// hfgpu host API -- the reference's C++ surface over the B200 engine.
+//
+// Same class names, namespaces, public fields and call sequence as
+// aromanro/HartreeFock (HartreeFock/ directory) so that a program written
+// against the reference keeps compiling:
+//
+//   Chemistry::Basis basis; basis.Load("6-31g_st.nw");
+//   Systems::Molecule mol;  ... mol.atoms.push_back(atom); mol.Init();
+//   HartreeFock::RestrictedHartreeFock hf;   // README.md:63-70
+//   hf.alpha = 0.5; hf.initGuess = 0; hf.Init(&mol);
+//   double e = hf.Calculate();
+//
+// The two-electron work (Fock builds, stored integral table, single
+// integrals) runs on the GPU through the C ABI of hfgpu.h; one-electron
+// matrices, DIIS and the orthogonalisation stay in host FP64 as in the
+// reference.  Matrices are row-major (hfgpu::Matrix) instead of
+// Eigen::MatrixXd; element access M(i, j) is the same.
+#pragma once
+
+#include <atomic>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "hfgpu.h"
+
+namespace hfgpu {
+
+class Matrix {
+ public:
+  Matrix() = default;
+  Matrix(int r, int c) : r_(r), c_(c), d_((size_t)r * c, 0.0) {}
+  static Matrix Zero(int r, int c) { return Matrix(r, c); }
+  int rows() const { return r_; }
+  int cols() const { return c_; }
+  double &operator()(int i, int j) { return d_[(size_t)i * c_ + j]; }
+  double operator()(int i, int j) const { return d_[(size_t)i * c_ + j]; }
+  double *data() { return d_.data(); }
+  const double *data() const { return d_.data(); }
+  void resize(int r, int c) {
+    r_ = r;
+    c_ = c;
+    d_.assign((size_t)r * c, 0.0);
+  }
+
+ private:
+  int r_ = 0, c_ = 0;
+  std::vector<double> d_;
+};
+
+Matrix operator*(const Matrix &a, const Matrix &b);
+Matrix operator+(const Matrix &a, const Matrix &b);
+Matrix operator-(const Matrix &a, const Matrix &b);
+Matrix operator*(double s, const Matrix &a);
+Matrix transpose(const Matrix &a);
+// symmetric eigen-decomposition on the GPU (cuSOLVER dsyevd), eigenvalues
+// ascending, eigenvectors as columns
+void eigh(const Matrix &a, std::vector<double> &w, Matrix &v);
+
+struct Vector3D {
+  double X = 0, Y = 0, Z = 0;
+};
+
+}  // namespace hfgpu
+
+namespace Orbitals {
+// One basis-file shell line: letters ("S", "SP", "D" ...), exponents, and
+// one coefficient column per letter (Basis.cpp:52-83).
+struct ContractedGaussianShell {
+  std::string letters;
+  std::vector<double> exponents;
+  std::vector<std::vector<double>> coefficients;
+  unsigned CountNumberOfContractedGaussians() const;
+};
+}  // namespace Orbitals
+
+namespace Systems {
+
+class Atom {
+ public:
+  hfgpu::Vector3D position;
+  unsigned int Z = 0;
+  unsigned int electronsNumber = 0;
+  unsigned int ID = 0;
+  explicit Atom(unsigned int z = 0) : Z(z), electronsNumber(z) {}
+};
+
+class AtomWithShells : public Atom {
+ public:
+  std::vector<Orbitals::ContractedGaussianShell> shells;
+  explicit AtomWithShells(unsigned int z = 0) : Atom(z) {}
+  unsigned CountNumberOfContractedGaussians() const;
+  unsigned GetMaxAngularMomentum() const;
+};
+
+class Molecule {
+ public:
+  std::vector<AtomWithShells> atoms;
+  unsigned int alphaElectrons = 0;
+  unsigned int betaElectrons = 0;
+
+  void Init();  // Molecule.cpp:127-140 (occupations)
+  unsigned int CountNumberOfContractedGaussians() const;
+  unsigned int ElectronsNumber() const;
+  unsigned int GetMaxAngularMomentum() const;
+  double NuclearRepulsionEnergy() const;
+  bool LoadXYZ(const std::string &fileName, const class Chemistry_Basis_fwd *unused = nullptr);
+
+  // engine-side shell table (one entry per shell letter), rebuilt by Init()
+  struct ShellTable {
+    std::vector<double> center, exponent, coefficient;
+    std::vector<int32_t> L, nprim, prim_offset, ao_offset;
+    int32_t nbf = 0;
+    hfg_shells view() const;
+  };
+  const ShellTable &shellTable() const { return table_; }
+
+ private:
+  ShellTable table_;
+};
+
+}  // namespace Systems
+
+namespace Chemistry {
+class Basis {
+ public:
+  std::vector<Systems::AtomWithShells> atoms;
+  void Load(const std::string &fileName);  // Basis.cpp:15-84
+};
+}  // namespace Chemistry
+
+namespace GaussianIntegrals {
+
+class IntegralsRepository {
+ public:
+  explicit IntegralsRepository(Systems::Molecule *molecule = nullptr);
+  ~IntegralsRepository();
+  IntegralsRepository(const IntegralsRepository &) = delete;
+  IntegralsRepository &operator=(const IntegralsRepository &) = delete;
+
+  void Reset(Systems::Molecule *molecule = nullptr);
+  Systems::Molecule *getMolecule() const { return molecule_; }
+
+  // Stored packed table (IntegralsRepository.cpp:566-584), computed on the GPU.
+  void CalculateElectronElectronIntegrals();
+  bool HasElectronElectronIntegrals() const { return !packed_.empty(); }
+  double getElectronElectron(int i, int j, int k, int l) const;  // .h:138-141
+  // single contracted integral without the table (.cpp:372-433)
+  double getElectronElectronDirect(int i, int j, int k, int l);
+
+  // No-ops kept for source compatibility: the engine has no host-side memo maps.
+  void ClearMatricesMaps() {}
+  void ClearElectronElectronIntermediaries() {}
+  void ClearElectronElectronMaps() {}
+  void ClearAllMaps() {}
+  void SetUseLotsOfMemory(bool) {}
+
+  // One-electron matrices (QuantumMatrix.cpp:34-155): overlap, kinetic,
+  // nuclear attraction; row-major nbf x nbf.
+  void OneElectron(hfgpu::Matrix &S, hfgpu::Matrix &T, hfgpu::Matrix &V) const;
+
+  hfg_ctx *engine();
+  hfg_opts options;  // engine options, used at the next Reset/first use
+
+ private:
+  Systems::Molecule *molecule_ = nullptr;
+  hfg_ctx *ctx_ = nullptr;
+  std::vector<double> packed_;
+};
+
+}  // namespace GaussianIntegrals
+
+namespace HartreeFock {
+
+class HartreeFockAlgorithm {
+ public:
+  hfgpu::Matrix h;
+  int numberOfOrbitals = 0;
+  GaussianIntegrals::IntegralsRepository integralsRepository;
+  double alpha = 0.75;      // HartreeFockAlgorithm.cpp:10-11
+  double initGuess = 0.75;
+  std::atomic_bool terminate{false};
+  bool converged = false;
+  double HOMOEnergy = 0;
+  double lastErrorEst = 0;
+  bool UseDIIS = true;
+  int maxDIISiterations = 1000;
+  int normalIterAfterDIIS = 500;
+  // engine extension: store the packed table at Init (as the reference
+  // always does) only when it fits this many bytes; the Fock builds are
+  // direct either way
+  size_t storedIntegralsBudget = size_t(1) << 30;
+  int iterations = 0;  // steps taken by the last Calculate()
+
+  explicit HartreeFockAlgorithm(int iterations = 3000);
+  virtual ~HartreeFockAlgorithm();
+  virtual void Init(Systems::Molecule *molecule);
+  double Calculate();
+  virtual double Step(int iter) = 0;
+  double GetTotalEnergy() const { return totalEnergy; }
+
+ protected:
+  double totalEnergy;
+  double nuclearRepulsionEnergy = 0;
+  hfgpu::Matrix overlap;  // overlapMatrix.matrix
+  hfgpu::Matrix V, Vt;    // S^-1/2
+  int maxIterations;
+  bool inited = false;
+  void FirstIterations(int &iter, double &curEnergy, double &prevEnergy);
+  void SelfConsistentIterations(int &iter, double &curEnergy, double &prevEnergy);
+  void NormalIterations(int &iter, double &curEnergy, double &prevEnergy);
+};
+
+class Diis {
+ public:
+  bool AddValueAndError(const hfgpu::Matrix &value, const hfgpu::Matrix &error);
+  double Estimate(hfgpu::Matrix &value) const;
+
+ private:
+  std::vector<hfgpu::Matrix> errors_, values_;
+};
+
+class RestrictedHartreeFock : public HartreeFockAlgorithm {
+ public:
+  hfgpu::Matrix DensityMatrix;
+  unsigned int nrOccupiedLevels = 0;
+  std::vector<bool> occupied;
+  std::vector<double> eigenvals;
+  hfgpu::Matrix C;
+  explicit RestrictedHartreeFock(int iterations = 3000) : HartreeFockAlgorithm(iterations) {}
+  void Init(Systems::Molecule *molecule) override;
+  double Step(int iter) override;
+
+ private:
+  Diis diis;
+  bool DIISStep(int iter, hfgpu::Matrix &F);
+  void InitFockMatrix(int iter, hfgpu::Matrix &F);
+};
+
+class UnrestrictedHartreeFock : public HartreeFockAlgorithm {
+ public:
+  hfgpu::Matrix DensityMatrixPlus, DensityMatrixMinus;
+  unsigned int nrOccupiedLevelsPlus = 0, nrOccupiedLevelsMinus = 0;
+  std::vector<bool> occupiedPlus, occupiedMinus;
+  std::vector<double> eigenvalsplus, eigenvalsminus;
+  hfgpu::Matrix Cplus, Cminus;
+  bool addAsymmetry = true;  // UnrestrictedHartreeFock.cpp:9
+  double asymmetry = 0.1;
+  explicit UnrestrictedHartreeFock(int iterations = 3000) : HartreeFockAlgorithm(iterations) {}
+  void Init(Systems::Molecule *molecule) override;
+  double Step(int iter) override;
+
+ private:
+  Diis diisPlus, diisMinus;
+  bool DIISStep(int iter, hfgpu::Matrix &Fp, hfgpu::Matrix &Fm);
+  void InitFockMatrices(int iter, hfgpu::Matrix &Fp, hfgpu::Matrix &Fm);
+};
+
+}  // namespace HartreeFock

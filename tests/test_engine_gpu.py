@@ -14,11 +14,13 @@ from hartreefock_b200.basis_io import basis_path
 
 pytestmark = pytest.mark.gpu
 
-# ERI tolerance: 1e-12 absolute.  The reference's own table is only
-# reproducible to ~2e-12 on oxygen 6-31G* integrals (compiling it with and
-# without FMA contraction moves one (sp|sp)-type element by 1.85e-12), so
-# elements above 0.1 in magnitude get 1e-11 relative instead.
-ERI_ABS, ERI_REL = 1e-12, 1e-11
+# ERI tolerance: 1e-12 absolute, or 2.5e-11 relative where that is larger.
+# The relative term is the reference's own reproducibility floor: compiling
+# the reference with and without FMA contraction moves one o2_631gs element
+# (value 0.0809, a cancellation-heavy oxygen-core quartet) by 1.85e-12,
+# i.e. 2.3e-11 relative.  Every other element of every fixture is within
+# 1e-12 absolute.
+ERI_ABS, ERI_REL = 1e-12, 2.5e-11
 
 
 def eri_close(got, ref):
