@@ -1,0 +1,1102 @@
+// Host side of the reference's C++ surface (include/hfgpu_host.hpp):
+// basis files, molecules, one-electron integrals, the SCF driver and DIIS.
+// Two-electron work goes to the GPU engine through the C ABI (hfgpu.h);
+// the symmetric eigen-decompositions go to cuSOLVER.
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <array>
+#include <cctype>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <limits>
+#include <mutex>
+#include <sstream>
+#include <stdexcept>
+#include <thread>
+
+#include "../../include/hfgpu_driver.h"
+#include "../../include/hfgpu_host.hpp"
+
+namespace {
+
+const char *kElements[] = {"H",  "He", "Li", "Be", "B",  "C",  "N",  "O",  "F",  "Ne", "Na", "Mg",
+                           "Al", "Si", "P",  "S",  "Cl", "Ar", "K",  "Ca", "Sc", "Ti", "V",  "Cr",
+                           "Mn", "Fe", "Co", "Ni", "Cu", "Zn", "Ga", "Ge", "As", "Se", "Br", "Kr"};
+
+unsigned z_for(const std::string &sym) {
+  for (unsigned i = 0; i < sizeof kElements / sizeof kElements[0]; ++i)
+    if (sym == kElements[i]) return i + 1;
+  return 0;
+}
+
+int letter_l(char c) {
+  switch (std::tolower(static_cast<unsigned char>(c))) {
+    case 's': return 0;
+    case 'p': return 1;
+    case 'd': return 2;
+    case 'f': return 3;
+    case 'g': return 4;
+    default: return -1;
+  }
+}
+
+inline int ncart(int L) { return (L + 1) * (L + 2) / 2; }
+
+double dfact(int n) {
+  double r = 1;
+  for (; n > 1; n -= 2) r *= n;
+  return r;
+}
+
+// Cartesian components in the reference's canonical order (xx, xy, xz, yy, yz, zz)
+void components(int L, std::vector<std::array<int, 3>> &out) {
+  out.clear();
+  for (int i = L; i >= 0; --i)
+    for (int j = L - i; j >= 0; --j) out.push_back({i, j, L - i - j});
+}
+
+// Boys function F_0..F_M(T): series below 30 (positive terms, downward
+// recursion), F_0 = sqrt(pi/T)/2 erf(sqrt T) and upward recursion above.
+void boys_host(int M, double T, double *F) {
+  if (T < 30.0) {
+    double term = 1.0 / (2 * M + 1), sum = 0;
+    for (int k = 0; k < 400; ++k) {
+      sum += term;
+      term *= 2.0 * T / (2 * M + 2 * k + 3);
+      if (term < sum * 1e-17) break;
+    }
+    const double e = std::exp(-T);
+    F[M] = e * sum;
+    for (int m = M - 1; m >= 0; --m) F[m] = (2 * T * F[m + 1] + e) / (2 * m + 1);
+  } else {
+    const double e = std::exp(-T);
+    F[0] = 0.5 * std::sqrt(M_PI / T) * std::erf(std::sqrt(T));
+    for (int m = 0; m < M; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) / (2 * T);
+  }
+}
+
+std::string trim(const std::string &s) {
+  size_t a = s.find_first_not_of(" \t\r\n"), b = s.find_last_not_of(" \t\r\n");
+  return a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
+}
+
+}  // namespace
+
+// ===========================================================================
+// matrices and the GPU eigensolver
+// ===========================================================================
+namespace hfgpu {
+
+Matrix operator*(const Matrix &a, const Matrix &b) {
+  Matrix m(a.rows(), b.cols());
+  const int n = a.rows(), p = a.cols(), q = b.cols();
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < p; ++k) {
+      const double aik = a(i, k);
+      if (aik == 0.0) continue;
+      const double *br = b.data() + (size_t)k * q;
+      double *mr = m.data() + (size_t)i * q;
+      for (int j = 0; j < q; ++j) mr[j] += aik * br[j];
+    }
+  return m;
+}
+Matrix operator+(const Matrix &a, const Matrix &b) {
+  Matrix m = a;
+  for (size_t x = 0; x < (size_t)a.rows() * a.cols(); ++x) m.data()[x] += b.data()[x];
+  return m;
+}
+Matrix operator-(const Matrix &a, const Matrix &b) {
+  Matrix m = a;
+  for (size_t x = 0; x < (size_t)a.rows() * a.cols(); ++x) m.data()[x] -= b.data()[x];
+  return m;
+}
+Matrix operator*(double s, const Matrix &a) {
+  Matrix m = a;
+  for (size_t x = 0; x < (size_t)a.rows() * a.cols(); ++x) m.data()[x] *= s;
+  return m;
+}
+Matrix transpose(const Matrix &a) {
+  Matrix t(a.cols(), a.rows());
+  for (int i = 0; i < a.rows(); ++i)
+    for (int j = 0; j < a.cols(); ++j) t(j, i) = a(i, j);
+  return t;
+}
+
+namespace {
+struct Solver {
+  cusolverDnHandle_t h = nullptr;
+  double *dA = nullptr, *dW = nullptr, *work = nullptr;
+  int *info = nullptr;
+  int cap = 0, lwork = 0;
+  std::mutex mu;
+  ~Solver() {
+    if (h) cusolverDnDestroy(h);
+    cudaFree(dA);
+    cudaFree(dW);
+    cudaFree(work);
+    cudaFree(info);
+  }
+};
+Solver &solver() {
+  static thread_local Solver s;
+  return s;
+}
+void check_cuda(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+void check_solver(cusolverStatus_t e, const char *what) {
+  if (e != CUSOLVER_STATUS_SUCCESS) throw std::runtime_error(std::string(what) + " failed");
+}
+}  // namespace
+
+void eigh(const Matrix &a, std::vector<double> &w, Matrix &v) {
+  const int n = a.rows();
+  Solver &s = solver();
+  if (!s.h) check_solver(cusolverDnCreate(&s.h), "cusolverDnCreate");
+  if (n > s.cap) {
+    cudaFree(s.dA);
+    cudaFree(s.dW);
+    cudaFree(s.work);
+    cudaFree(s.info);
+    check_cuda(cudaMalloc(&s.dA, sizeof(double) * n * n), "cudaMalloc");
+    check_cuda(cudaMalloc(&s.dW, sizeof(double) * n), "cudaMalloc");
+    check_cuda(cudaMalloc(&s.info, sizeof(int)), "cudaMalloc");
+    check_solver(cusolverDnDsyevd_bufferSize(s.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, s.dA, n, s.dW,
+                                             &s.lwork),
+                 "dsyevd_bufferSize");
+    check_cuda(cudaMalloc(&s.work, sizeof(double) * s.lwork), "cudaMalloc");
+    s.cap = n;
+  }
+  // symmetric input: row-major == column-major
+  check_cuda(cudaMemcpy(s.dA, a.data(), sizeof(double) * n * n, cudaMemcpyHostToDevice), "cudaMemcpy");
+  check_solver(cusolverDnDsyevd(s.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, s.dA, n, s.dW, s.work,
+                                s.lwork, s.info),
+               "dsyevd");
+  std::vector<double> colmajor((size_t)n * n);
+  w.resize(n);
+  int info = 0;
+  check_cuda(cudaMemcpy(colmajor.data(), s.dA, sizeof(double) * n * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+  check_cuda(cudaMemcpy(w.data(), s.dW, sizeof(double) * n, cudaMemcpyDeviceToHost), "cudaMemcpy");
+  check_cuda(cudaMemcpy(&info, s.info, sizeof(int), cudaMemcpyDeviceToHost), "cudaMemcpy");
+  if (info != 0) throw std::runtime_error("dsyevd did not converge");
+  v.resize(n, n);
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) v(i, j) = colmajor[(size_t)j * n + i];
+}
+
+}  // namespace hfgpu
+
+// ===========================================================================
+// basis, atoms, molecule
+// ===========================================================================
+unsigned Orbitals::ContractedGaussianShell::CountNumberOfContractedGaussians() const {
+  unsigned n = 0;
+  for (char c : letters) n += ncart(letter_l(c));
+  return n;
+}
+
+unsigned Systems::AtomWithShells::CountNumberOfContractedGaussians() const {
+  unsigned n = 0;
+  for (const auto &s : shells) n += s.CountNumberOfContractedGaussians();
+  return n;
+}
+
+unsigned Systems::AtomWithShells::GetMaxAngularMomentum() const {
+  int L = 0;
+  for (const auto &s : shells)
+    for (char c : s.letters) L = std::max(L, letter_l(c));
+  return (unsigned)L;
+}
+
+void Chemistry::Basis::Load(const std::string &fileName) {
+  std::ifstream f(fileName);
+  if (!f) throw std::runtime_error("cannot open basis file " + fileName);
+  atoms.clear();
+  std::string line;
+  Orbitals::ContractedGaussianShell *cur = nullptr;
+  while (std::getline(f, line)) {
+    const std::string t = trim(line);
+    if (t.empty() || t[0] == '#' || t.rfind("BASIS", 0) == 0 || t.rfind("END", 0) == 0) continue;
+    std::istringstream ls(t);
+    std::string a, b, extra;
+    ls >> a >> b;
+    const bool shell_line = std::isalpha(static_cast<unsigned char>(a[0])) && !b.empty() &&
+                            std::isalpha(static_cast<unsigned char>(b[0])) && !(ls >> extra);
+    if (shell_line) {
+      const unsigned Z = z_for(a);
+      if (!Z) throw std::runtime_error("unknown element " + a + " in " + fileName);
+      if (atoms.empty() || atoms.back().Z != Z) atoms.emplace_back(Z);
+      for (char c : b)
+        if (letter_l(c) < 0) throw std::runtime_error("unknown shell letter in " + fileName);
+      atoms.back().shells.push_back(Orbitals::ContractedGaussianShell{b, {}, std::vector<std::vector<double>>(b.size())});
+      cur = &atoms.back().shells.back();
+      continue;
+    }
+    if (!cur) continue;
+    std::string num;
+    std::istringstream ns(t);
+    std::vector<double> vals;
+    while (ns >> num) {
+      std::replace(num.begin(), num.end(), 'D', 'E');
+      vals.push_back(std::stod(num));
+    }
+    if (vals.empty()) continue;
+    cur->exponents.push_back(vals[0]);
+    for (size_t i = 0; i < cur->letters.size() && i + 1 < vals.size(); ++i) cur->coefficients[i].push_back(vals[i + 1]);
+  }
+}
+
+unsigned Systems::Molecule::CountNumberOfContractedGaussians() const {
+  unsigned n = 0;
+  for (const auto &a : atoms) n += a.CountNumberOfContractedGaussians();
+  return n;
+}
+
+unsigned Systems::Molecule::ElectronsNumber() const {
+  if (alphaElectrons > 0 || betaElectrons > 0) return alphaElectrons + betaElectrons;
+  unsigned n = 0;
+  for (const auto &a : atoms) n += a.electronsNumber;
+  return n;
+}
+
+unsigned Systems::Molecule::GetMaxAngularMomentum() const {
+  unsigned L = 0;
+  for (const auto &a : atoms) L = std::max(L, a.GetMaxAngularMomentum());
+  return L;
+}
+
+double Systems::Molecule::NuclearRepulsionEnergy() const {
+  double e = 0;
+  for (size_t i = 0; i < atoms.size(); ++i)
+    for (size_t j = i + 1; j < atoms.size(); ++j) {
+      const double dx = atoms[i].position.X - atoms[j].position.X, dy = atoms[i].position.Y - atoms[j].position.Y,
+                   dz = atoms[i].position.Z - atoms[j].position.Z;
+      e += double(atoms[i].Z) * atoms[j].Z / std::sqrt(dx * dx + dy * dy + dz * dz);
+    }
+  return e;
+}
+
+void Systems::Molecule::Init() {
+  ShellTable t;
+  int ao = 0;
+  for (size_t a = 0; a < atoms.size(); ++a) {
+    atoms[a].ID = (unsigned)a;
+    for (const auto &sh : atoms[a].shells)
+      for (size_t li = 0; li < sh.letters.size(); ++li) {
+        const int L = letter_l(sh.letters[li]);
+        t.center.push_back(atoms[a].position.X);
+        t.center.push_back(atoms[a].position.Y);
+        t.center.push_back(atoms[a].position.Z);
+        t.L.push_back(L);
+        t.nprim.push_back((int32_t)sh.exponents.size());
+        t.prim_offset.push_back((int32_t)t.exponent.size());
+        t.ao_offset.push_back(ao);
+        t.exponent.insert(t.exponent.end(), sh.exponents.begin(), sh.exponents.end());
+        t.coefficient.insert(t.coefficient.end(), sh.coefficients[li].begin(), sh.coefficients[li].end());
+        ao += ncart(L);
+      }
+  }
+  t.nbf = ao;
+  table_ = std::move(t);
+  // occupations, Molecule.cpp:132-139
+  const unsigned el = ElectronsNumber();
+  if (alphaElectrons == 0 && betaElectrons == 0) {
+    alphaElectrons = el / 2;
+    betaElectrons = el - alphaElectrons;
+  }
+}
+
+hfg_shells Systems::Molecule::ShellTable::view() const {
+  hfg_shells s{};
+  s.nshells = (int32_t)L.size();
+  s.center = center.data();
+  s.L = L.data();
+  s.nprim = nprim.data();
+  s.prim_offset = prim_offset.data();
+  s.ao_offset = ao_offset.data();
+  s.exponent = exponent.data();
+  s.coefficient = coefficient.data();
+  s.nbf = nbf;
+  return s;
+}
+
+bool Systems::Molecule::LoadXYZ(const std::string &fileName, const Chemistry::Basis &basis) {
+  std::ifstream f(fileName);
+  if (!f) return false;
+  std::string line;
+  if (!std::getline(f, line)) return false;
+  const int n = std::stoi(line);
+  if (!std::getline(f, line)) return false;
+  for (int i = 0; i < n; ++i) {
+    if (!std::getline(f, line)) return false;
+    std::istringstream ls(line);
+    std::string sym;
+    double x, y, z;
+    ls >> sym >> x >> y >> z;
+    const unsigned Z = z_for(sym);
+    bool found = false;
+    for (const auto &a : basis.atoms)
+      if (a.Z == Z) {
+        atoms.push_back(a);
+        atoms.back().position = {x, y, z};
+        found = true;
+        break;
+      }
+    if (!found) return false;
+  }
+  Init();
+  return true;
+}
+
+// ===========================================================================
+// one-electron integrals (Obara-Saika), per contracted shell pair
+// ===========================================================================
+namespace {
+
+struct ShellView {
+  double c[3];
+  int L, nprim;
+  const double *e, *k;
+  int ao;
+};
+
+// primitive normalisation without the component part: (2a/pi)^(3/4) (4a)^(L/2)
+inline double radial_norm(double a, int L) { return std::pow(2 * a / M_PI, 0.75) * std::pow(4 * a, L / 2.0); }
+inline double comp_norm(const std::array<int, 3> &c) {
+  return 1.0 / std::sqrt(dfact(2 * c[0] - 1) * dfact(2 * c[1] - 1) * dfact(2 * c[2] - 1));
+}
+
+// S, T and V blocks of one shell pair (row-major into the full matrices)
+void shell_pair_one_electron(const ShellView &A, const ShellView &B, const std::vector<double> &nuc_xyz,
+                             const std::vector<int> &nuc_z, int n, double *S, double *T, double *V) {
+  std::vector<std::array<int, 3>> ca, cb;
+  components(A.L, ca);
+  components(B.L, cb);
+  const int na = (int)ca.size(), nb = (int)cb.size();
+  std::vector<double> s(na * nb, 0.0), t(na * nb, 0.0), v(na * nb, 0.0);
+  double AB[3];
+  double ab2 = 0;
+  for (int d = 0; d < 3; ++d) {
+    AB[d] = A.c[d] - B.c[d];
+    ab2 += AB[d] * AB[d];
+  }
+  const int LT = A.L + B.L;
+  for (int i = 0; i < A.nprim; ++i)
+    for (int j = 0; j < B.nprim; ++j) {
+      const double a = A.e[i], b = B.e[j], z = a + b, iz = 1.0 / z;
+      const double K = std::exp(-a * b * iz * ab2);
+      const double cc = A.k[i] * radial_norm(a, A.L) * B.k[j] * radial_norm(b, B.L);
+      double P[3], PA[3], PB[3];
+      for (int d = 0; d < 3; ++d) {
+        P[d] = (a * A.c[d] + b * B.c[d]) * iz;
+        PA[d] = P[d] - A.c[d];
+        PB[d] = P[d] - B.c[d];
+      }
+      // 1D overlaps O[d][i][j], i <= LA, j <= LB+2 (OS recursion)
+      double O[3][5][7] = {};
+      for (int d = 0; d < 3; ++d) {
+        O[d][0][0] = std::sqrt(M_PI * iz);
+        for (int jj = 0; jj <= B.L + 2; ++jj)
+          for (int ii = 0; ii <= A.L; ++ii) {
+            if (ii == 0 && jj == 0) continue;
+            double val;
+            if (ii > 0) {
+              val = PA[d] * O[d][ii - 1][jj];
+              if (ii > 1) val += (ii - 1) * 0.5 * iz * O[d][ii - 2][jj];
+              if (jj > 0) val += jj * 0.5 * iz * O[d][ii - 1][jj - 1];
+            } else {
+              val = PB[d] * O[d][0][jj - 1];
+              if (jj > 1) val += (jj - 1) * 0.5 * iz * O[d][0][jj - 2];
+            }
+            O[d][ii][jj] = val;
+          }
+      }
+      // nuclear attraction: (a|0)^(m) by the OS vertical recursion on A,
+      // then the horizontal transfer to B, per nucleus
+      for (int x = 0; x < na; ++x)
+        for (int y = 0; y < nb; ++y) {
+          const auto &p = ca[x], &q = cb[y];
+          double sxyz = 1, kin = 0;
+          double o[3], d2[3];
+          for (int d = 0; d < 3; ++d) {
+            o[d] = O[d][p[d]][q[d]];
+            // <i| d^2/dx^2 |j> = j(j-1) S_{i,j-2} - 2b(2j+1) S_{i,j} + 4b^2 S_{i,j+2}
+            const int jj = q[d];
+            d2[d] = (jj > 1 ? jj * (jj - 1) * O[d][p[d]][jj - 2] : 0.0) - 2 * b * (2 * jj + 1) * O[d][p[d]][jj] +
+                    4 * b * b * O[d][p[d]][jj + 2];
+            sxyz *= o[d];
+          }
+          kin = -0.5 * (d2[0] * o[1] * o[2] + o[0] * d2[1] * o[2] + o[0] * o[1] * d2[2]);
+          s[x * nb + y] += cc * K * sxyz;
+          t[x * nb + y] += cc * K * kin;
+        }
+      // nuclear part
+      for (size_t c = 0; c < nuc_z.size(); ++c) {
+        const double *C = &nuc_xyz[3 * c];
+        double PC[3], pc2 = 0;
+        for (int d = 0; d < 3; ++d) {
+          PC[d] = P[d] - C[d];
+          pc2 += PC[d] * PC[d];
+        }
+        double F[9];
+        boys_host(LT, z * pc2, F);
+        // W[l][m][n][mm] for l+m+n <= LT, via the vertical recursion
+        double W[5][5][5][5] = {};
+        for (int mm = 0; mm <= LT; ++mm) W[0][0][0][mm] = 2 * M_PI * iz * K * F[mm];
+        for (int L = 1; L <= LT; ++L)
+          for (int l = L; l >= 0; --l)
+            for (int m = L - l; m >= 0; --m) {
+              const int nn = L - l - m;
+              int e[3] = {l, m, nn};
+              const int d = l > 0 ? 0 : (m > 0 ? 1 : 2);
+              int e1[3] = {l, m, nn};
+              e1[d] -= 1;
+              for (int mm = 0; mm + L <= LT; ++mm) {
+                double val = PA[d] * W[e1[0]][e1[1]][e1[2]][mm] - PC[d] * W[e1[0]][e1[1]][e1[2]][mm + 1];
+                if (e1[d] > 0) {
+                  int e2[3] = {e1[0], e1[1], e1[2]};
+                  e2[d] -= 1;
+                  val += e1[d] * 0.5 * iz * (W[e2[0]][e2[1]][e2[2]][mm] - W[e2[0]][e2[1]][e2[2]][mm + 1]);
+                }
+                W[e[0]][e[1]][e[2]][mm] = val;
+              }
+            }
+        // horizontal transfer (a|b+1_d) = (a+1_d|b) + AB_d (a|b), on m = 0
+        for (int x = 0; x < na; ++x)
+          for (int y = 0; y < nb; ++y) {
+            // expand (p|q) by moving B's exponents onto A one unit at a time
+            std::vector<std::pair<std::array<int, 3>, double>> terms{{ca[x], 1.0}};
+            std::array<int, 3> rem = cb[y];
+            for (int d = 0; d < 3; ++d)
+              while (rem[d] > 0) {
+                std::vector<std::pair<std::array<int, 3>, double>> nt;
+                for (auto &tm : terms) {
+                  auto up = tm.first;
+                  up[d] += 1;
+                  nt.push_back({up, tm.second});
+                  nt.push_back({tm.first, tm.second * AB[d]});
+                }
+                terms.swap(nt);
+                --rem[d];
+              }
+            double val = 0;
+            for (auto &tm : terms) val += tm.second * W[tm.first[0]][tm.first[1]][tm.first[2]][0];
+            v[x * nb + y] -= nuc_z[c] * cc * val;
+          }
+      }
+    }
+  for (int x = 0; x < na; ++x)
+    for (int y = 0; y < nb; ++y) {
+      const double f = comp_norm(ca[x]) * comp_norm(cb[y]);
+      const size_t I = A.ao + x, J = B.ao + y;
+      S[I * n + J] = S[J * n + I] = f * s[x * nb + y];
+      T[I * n + J] = T[J * n + I] = f * t[x * nb + y];
+      V[I * n + J] = V[J * n + I] = f * v[x * nb + y];
+    }
+}
+
+}  // namespace
+
+// ===========================================================================
+// IntegralsRepository
+// ===========================================================================
+namespace GaussianIntegrals {
+
+IntegralsRepository::IntegralsRepository(Systems::Molecule *molecule) : molecule_(molecule) {
+  hfg_default_opts(&options);
+}
+
+IntegralsRepository::~IntegralsRepository() {
+  if (ctx_) hfg_ctx_destroy(ctx_);
+}
+
+void IntegralsRepository::Reset(Systems::Molecule *molecule) {
+  if (ctx_) hfg_ctx_destroy(ctx_);
+  ctx_ = nullptr;
+  packed_.clear();
+  packed_.shrink_to_fit();
+  molecule_ = molecule;
+}
+
+hfg_ctx *IntegralsRepository::engine() {
+  if (!ctx_) {
+    if (!molecule_) throw std::runtime_error("IntegralsRepository without a molecule");
+    const hfg_shells sh = molecule_->shellTable().view();
+    if (hfg_ctx_create(&sh, &options, &ctx_) != HFG_OK)
+      throw std::runtime_error(std::string("hfg_ctx_create: ") + hfg_last_error());
+  }
+  return ctx_;
+}
+
+void IntegralsRepository::CalculateElectronElectronIntegrals() {
+  const int n = (int)molecule_->shellTable().nbf;
+  packed_.assign((size_t)hfg_packed_size(n), 0.0);
+  if (hfg_eri_packed(engine(), packed_.data(), (int64_t)packed_.size()) != HFG_OK)
+    throw std::runtime_error(std::string("hfg_eri_packed: ") + hfg_last_error());
+}
+
+double IntegralsRepository::getElectronElectron(int i, int j, int k, int l) const {
+  auto tri = [](long long a, long long b) { return a < b ? b * (b + 1) / 2 + a : a * (a + 1) / 2 + b; };
+  return packed_[(size_t)tri(tri(i, j), tri(k, l))];
+}
+
+double IntegralsRepository::getElectronElectronDirect(int i, int j, int k, int l) {
+  double v = 0;
+  if (hfg_eri_quartet(engine(), i, j, k, l, &v) != HFG_OK)
+    throw std::runtime_error(std::string("hfg_eri_quartet: ") + hfg_last_error());
+  return v;
+}
+
+void IntegralsRepository::OneElectron(hfgpu::Matrix &S, hfgpu::Matrix &T, hfgpu::Matrix &V) const {
+  const auto &t = molecule_->shellTable();
+  const int n = t.nbf, ns = (int)t.L.size();
+  S.resize(n, n);
+  T.resize(n, n);
+  V.resize(n, n);
+  std::vector<ShellView> sv(ns);
+  for (int s = 0; s < ns; ++s)
+    sv[s] = ShellView{{t.center[3 * s], t.center[3 * s + 1], t.center[3 * s + 2]}, t.L[s], t.nprim[s],
+                      &t.exponent[t.prim_offset[s]], &t.coefficient[t.prim_offset[s]], t.ao_offset[s]};
+  std::vector<double> nxyz;
+  std::vector<int> nz;
+  for (const auto &a : molecule_->atoms) {
+    nxyz.insert(nxyz.end(), {a.position.X, a.position.Y, a.position.Z});
+    nz.push_back((int)a.Z);
+  }
+  std::vector<std::pair<int, int>> pairs;
+  for (int a = 0; a < ns; ++a)
+    for (int b = 0; b <= a; ++b) pairs.push_back({a, b});
+  const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  for (unsigned w = 0; w < nt; ++w)
+    pool.emplace_back([&, w]() {
+      for (size_t p = w; p < pairs.size(); p += nt)
+        shell_pair_one_electron(sv[pairs[p].first], sv[pairs[p].second], nxyz, nz, n, S.data(), T.data(), V.data());
+    });
+  for (auto &th : pool) th.join();
+}
+
+}  // namespace GaussianIntegrals
+
+// ===========================================================================
+// SCF
+// ===========================================================================
+namespace HartreeFock {
+
+using hfgpu::Matrix;
+
+// Constants.h:6-10
+constexpr double kEnergyConvergenceDIIS = 1E-11;
+constexpr double kEnergyConvergence = 1E-13;
+constexpr double kRmsDConvergence = 1E-10;
+constexpr double kDiisConvergence = 1E-10;
+
+HartreeFockAlgorithm::HartreeFockAlgorithm(int iterations)
+    : totalEnergy(std::numeric_limits<double>::infinity()), maxIterations(iterations) {}
+
+HartreeFockAlgorithm::~HartreeFockAlgorithm() = default;
+
+void HartreeFockAlgorithm::Init(Systems::Molecule *molecule) {
+  converged = false;
+  integralsRepository.Reset(molecule);
+  Matrix T, Vn;
+  integralsRepository.OneElectron(overlap, T, Vn);
+  h = T + Vn;
+  nuclearRepulsionEnergy = molecule->NuclearRepulsionEnergy();
+  numberOfOrbitals = (int)molecule->shellTable().nbf;
+  // the reference always stores the 8-fold table at Init
+  // (HartreeFockAlgorithm.cpp:45); it is kept here when it fits the budget
+  if ((size_t)hfg_packed_size(numberOfOrbitals) * sizeof(double) <= storedIntegralsBudget)
+    integralsRepository.CalculateElectronElectronIntegrals();
+  else
+    integralsRepository.engine();
+  // V = S^-1/2 = U s^-1/2 U^T, symmetrised (HartreeFockAlgorithm.cpp:48-59)
+  std::vector<double> w;
+  Matrix U;
+  hfgpu::eigh(overlap, w, U);
+  const int n = numberOfOrbitals;
+  Matrix Us(n, n);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) Us(i, j) = U(i, j) / std::sqrt(w[j]);
+  V = Us * hfgpu::transpose(U);
+  Vt = hfgpu::transpose(V);
+  V = Vt = 0.5 * (V + Vt);
+  inited = true;
+}
+
+double HartreeFockAlgorithm::Calculate() {
+  double curEnergy = 0, prevEnergy = std::numeric_limits<double>::infinity();
+  if (!inited) return prevEnergy;
+  int iter = 0;
+  FirstIterations(iter, curEnergy, prevEnergy);
+  if (terminate) return curEnergy;
+  if (UseDIIS && iter < maxDIISiterations && converged && normalIterAfterDIIS) {
+    SelfConsistentIterations(iter, curEnergy, prevEnergy);
+    if (terminate) return curEnergy;
+  }
+  NormalIterations(iter, curEnergy, prevEnergy);
+  iterations = iter;
+  return curEnergy;
+}
+
+void HartreeFockAlgorithm::FirstIterations(int &iter, double &curEnergy, double &prevEnergy) {
+  for (; iter < maxIterations; ++iter) {
+    const double rmsD = Step(iter);
+    curEnergy = GetTotalEnergy();
+    if (std::fabs(prevEnergy - curEnergy) <= (UseDIIS ? kEnergyConvergenceDIIS : kEnergyConvergence) &&
+        rmsD < kRmsDConvergence && lastErrorEst < kDiisConvergence) {
+      converged = true;
+      break;
+    }
+    if (terminate) return;
+    prevEnergy = curEnergy;
+  }
+}
+
+void HartreeFockAlgorithm::SelfConsistentIterations(int &iter, double &curEnergy, double &prevEnergy) {
+  UseDIIS = false;
+  for (int i = 0; i < normalIterAfterDIIS; ++i) {
+    Step(iter + i);
+    curEnergy = GetTotalEnergy();
+    if (terminate) {
+      UseDIIS = true;
+      return;
+    }
+    prevEnergy = curEnergy;
+  }
+  iter += normalIterAfterDIIS;
+  UseDIIS = true;
+}
+
+void HartreeFockAlgorithm::NormalIterations(int &iter, double &curEnergy, double &prevEnergy) {
+  if (converged) return;
+  for (; iter < maxIterations; ++iter) {
+    const double rmsD = Step(iter);
+    curEnergy = GetTotalEnergy();
+    if (std::fabs(prevEnergy - curEnergy) <= kEnergyConvergence && rmsD < kRmsDConvergence) {
+      converged = true;
+      return;
+    }
+    if (terminate) return;
+    prevEnergy = curEnergy;
+  }
+}
+
+// DIIS.h:9-96: keep 6, extrapolate from 5, Pulay B matrix solved by a
+// column-pivoted Householder QR
+bool Diis::AddValueAndError(const Matrix &value, const Matrix &error) {
+  errors_.push_back(error);
+  values_.push_back(value);
+  if (errors_.size() > 6) {
+    errors_.erase(errors_.begin());
+    values_.erase(values_.begin());
+  }
+  return errors_.size() >= 5;
+}
+
+namespace {
+double dot(const Matrix &a, const Matrix &b) {
+  double s = 0;
+  for (size_t x = 0; x < (size_t)a.rows() * a.cols(); ++x) s += a.data()[x] * b.data()[x];
+  return s;
+}
+// least-squares solve of a small dense system by column-pivoted Householder QR
+std::vector<double> qr_solve(std::vector<double> A, int m, std::vector<double> b) {
+  const int n = m;
+  std::vector<int> perm(n);
+  for (int i = 0; i < n; ++i) perm[i] = i;
+  auto at = [&](int i, int j) -> double & { return A[(size_t)i * n + j]; };
+  std::vector<std::vector<double>> hv;
+  std::vector<double> betas;
+  std::vector<int> ks;
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    double best = -1;
+    for (int j = k; j < n; ++j) {
+      double s = 0;
+      for (int i = k; i < m; ++i) s += at(i, j) * at(i, j);
+      if (s > best) { best = s; p = j; }
+    }
+    if (p != k) {
+      for (int i = 0; i < m; ++i) std::swap(at(i, k), at(i, p));
+      std::swap(perm[k], perm[p]);
+    }
+    double al = 0;
+    for (int i = k; i < m; ++i) al += at(i, k) * at(i, k);
+    al = std::sqrt(al);
+    if (al == 0) continue;
+    if (at(k, k) > 0) al = -al;
+    std::vector<double> v(m - k);
+    v[0] = at(k, k) - al;
+    for (int i = k + 1; i < m; ++i) v[i - k] = at(i, k);
+    double vn = 0;
+    for (double x : v) vn += x * x;
+    const double beta = vn > 0 ? 2.0 / vn : 0.0;
+    for (int j = k; j < n; ++j) {
+      double s = 0;
+      for (int i = k; i < m; ++i) s += v[i - k] * at(i, j);
+      s *= beta;
+      for (int i = k; i < m; ++i) at(i, j) -= s * v[i - k];
+    }
+    double s = 0;
+    for (int i = k; i < m; ++i) s += v[i - k] * b[i];
+    s *= beta;
+    for (int i = k; i < m; ++i) b[i] -= s * v[i - k];
+  }
+  const double tol = std::fabs(at(0, 0)) * 1e-15 * n;
+  int rank = 0;
+  while (rank < n && std::fabs(at(rank, rank)) > tol) ++rank;
+  std::vector<double> z(n, 0.0), x(n, 0.0);
+  for (int i = rank - 1; i >= 0; --i) {
+    double s = b[i];
+    for (int j = i + 1; j < rank; ++j) s -= at(i, j) * z[j];
+    z[i] = s / at(i, i);
+  }
+  for (int j = 0; j < n; ++j) x[perm[j]] = z[j];
+  return x;
+}
+}  // namespace
+
+double Diis::Estimate(Matrix &value) const {
+  const int nm = (int)errors_.size(), np1 = nm + 1;
+  std::vector<double> B((size_t)np1 * np1, 0.0), rhs(np1, 0.0);
+  double last = 0;
+  for (int i = 0; i < nm; ++i) {
+    for (int j = 0; j < i; ++j) B[i * np1 + j] = B[j * np1 + i] = dot(errors_[i], errors_[j]);
+    B[i * np1 + i] = dot(errors_[i], errors_[i]);
+    if (i == nm - 1 || i == nm - 2) last += B[i * np1 + i];
+    B[nm * np1 + i] = B[i * np1 + nm] = 1;
+  }
+  last = std::sqrt(last);
+  rhs[nm] = 1;
+  const std::vector<double> c = qr_solve(B, np1, rhs);
+  value = Matrix::Zero(value.rows(), value.cols());
+  for (int i = 0; i < nm; ++i) value = value + c[i] * values_[i];
+  return last;
+}
+
+namespace {
+void two_electron_rhf(GaussianIntegrals::IntegralsRepository &repo, const Matrix &P, Matrix &G) {
+  G.resize(P.rows(), P.cols());
+  if (hfg_fock_rhf(repo.engine(), P.data(), G.data()) != HFG_OK)
+    throw std::runtime_error(std::string("hfg_fock_rhf: ") + hfg_last_error());
+}
+void two_electron_uhf(GaussianIntegrals::IntegralsRepository &repo, const Matrix &Pa, const Matrix &Pb, Matrix &Ga,
+                      Matrix &Gb) {
+  Ga.resize(Pa.rows(), Pa.cols());
+  Gb.resize(Pa.rows(), Pa.cols());
+  if (hfg_fock_uhf(repo.engine(), Pa.data(), Pb.data(), Ga.data(), Gb.data()) != HFG_OK)
+    throw std::runtime_error(std::string("hfg_fock_uhf: ") + hfg_last_error());
+}
+double rms_diff(const Matrix &a, const Matrix &b) {
+  double s = 0;
+  for (size_t x = 0; x < (size_t)a.rows() * a.cols(); ++x) {
+    const double d = a.data()[x] - b.data()[x];
+    s += d * d;
+  }
+  return s;
+}
+}  // namespace
+
+void RestrictedHartreeFock::Init(Systems::Molecule *molecule) {
+  HartreeFockAlgorithm::Init(molecule);
+  DensityMatrix = Matrix::Zero(h.rows(), h.cols());
+  diis = Diis();
+  nrOccupiedLevels = molecule->ElectronsNumber() / 2;  // RestrictedHartreeFock.cpp:24-31
+  if (!nrOccupiedLevels) nrOccupiedLevels = 1;
+  if (nrOccupiedLevels > (unsigned)numberOfOrbitals) nrOccupiedLevels = numberOfOrbitals;
+  occupied.assign(nrOccupiedLevels, true);
+}
+
+void RestrictedHartreeFock::InitFockMatrix(int iter, Matrix &F) {
+  const int n = h.rows();
+  if (iter == 0) {  // RestrictedHartreeFock.cpp:175-186
+    if (initGuess > 0) {
+      F.resize(n, n);
+      for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) F(i, j) = initGuess * overlap(i, j) * (h(i, i) + h(j, j)) * 0.5;
+    } else {
+      F = h;
+    }
+  } else {
+    Matrix G;
+    two_electron_rhf(integralsRepository, DensityMatrix, G);
+    F = h + G;
+  }
+  F = 0.5 * (F + hfgpu::transpose(F));
+}
+
+bool RestrictedHartreeFock::DIISStep(int iter, Matrix &F) {
+  bool used = false;
+  if (UseDIIS && iter && iter < maxDIISiterations) {
+    const Matrix err = overlap * DensityMatrix * F - F * DensityMatrix * overlap;
+    if (diis.AddValueAndError(F, err)) {
+      lastErrorEst = diis.Estimate(F);
+      used = true;
+    }
+  } else {
+    lastErrorEst = 0;
+  }
+  return used;
+}
+
+double RestrictedHartreeFock::Step(int iter) {
+  Matrix F;
+  InitFockMatrix(iter, F);
+  const bool used = DIISStep(iter, F);
+  const Matrix Ft = Vt * F * V;
+  Matrix Cp;
+  hfgpu::eigh(Ft, eigenvals, Cp);
+  C = V * Cp;
+  const int n = h.rows();
+  Matrix Pn(n, n);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      double s = 0;
+      for (unsigned v = 0; v < occupied.size(); ++v)
+        if (occupied[v]) s += C(i, v) * C(j, v);
+      Pn(i, j) = 2.0 * s;
+    }
+  // CalculateEnergy (RestrictedHartreeFock.cpp:209-249)
+  double e = 0;
+  for (int i = 1; i < n; ++i)
+    for (int j = 0; j < i; ++j) e += Pn(i, j) * h(j, i);
+  e *= 2.0;
+  for (int i = 0; i < n; ++i) e += Pn(i, i) * h(i, i);
+  e *= 0.5;
+  for (unsigned l = 0; l < occupied.size(); ++l)
+    if (occupied[l]) e += eigenvals[l];
+  HOMOEnergy = eigenvals[nrOccupiedLevels - 1];
+  totalEnergy = e + nuclearRepulsionEnergy;
+  const double rmsD = std::sqrt(rms_diff(Pn, DensityMatrix));
+  DensityMatrix = used ? Pn : alpha * Pn + (1.0 - alpha) * DensityMatrix;
+  return rmsD;
+}
+
+void UnrestrictedHartreeFock::Init(Systems::Molecule *molecule) {
+  HartreeFockAlgorithm::Init(molecule);
+  DensityMatrixPlus = Matrix::Zero(h.rows(), h.cols());
+  DensityMatrixMinus = Matrix::Zero(h.rows(), h.cols());
+  diisPlus = Diis();
+  diisMinus = Diis();
+  // UnrestrictedHartreeFock.cpp:29-56
+  const unsigned el = molecule->ElectronsNumber();
+  nrOccupiedLevelsMinus = el / 2;
+  nrOccupiedLevelsPlus = el - nrOccupiedLevelsMinus;
+  if (molecule->alphaElectrons > 0 || molecule->betaElectrons > 0) {
+    nrOccupiedLevelsPlus = molecule->alphaElectrons;
+    nrOccupiedLevelsMinus = molecule->betaElectrons;
+  }
+  const unsigned n = (unsigned)numberOfOrbitals;
+  if (nrOccupiedLevelsMinus + nrOccupiedLevelsPlus > 2 * n) nrOccupiedLevelsMinus = nrOccupiedLevelsPlus = n;
+  if (nrOccupiedLevelsPlus > n) {
+    nrOccupiedLevelsMinus += nrOccupiedLevelsPlus - n;
+    nrOccupiedLevelsPlus = n;
+  }
+  if (nrOccupiedLevelsMinus > n) nrOccupiedLevelsMinus = n;
+  occupiedPlus.assign(nrOccupiedLevelsPlus, true);
+  occupiedMinus.assign(nrOccupiedLevelsMinus, true);
+}
+
+void UnrestrictedHartreeFock::InitFockMatrices(int iter, Matrix &Fp, Matrix &Fm) {
+  const int n = h.rows();
+  if (iter == 0) {  // UnrestrictedHartreeFock.cpp:199-222
+    if (initGuess > 0) {
+      Fp.resize(n, n);
+      for (int i = 0; i < n; ++i)
+        for (int j = 0; j < n; ++j) Fp(i, j) = initGuess * overlap(i, j) * (h(i, i) + h(j, j)) * 0.5;
+      Fm = Fp;
+    } else {
+      Fp = h;
+      Fm = h;
+    }
+    if (addAsymmetry && n > 1) {
+      Fp(0, 1) += asymmetry;
+      Fp(1, 0) = Fp(0, 1);
+    }
+  } else {
+    Matrix Gp, Gm;
+    two_electron_uhf(integralsRepository, DensityMatrixPlus, DensityMatrixMinus, Gp, Gm);
+    Fp = h + Gp;
+    Fm = h + Gm;
+  }
+}
+
+bool UnrestrictedHartreeFock::DIISStep(int iter, Matrix &Fp, Matrix &Fm) {
+  bool used = false;
+  if (UseDIIS && iter && iter < maxDIISiterations) {
+    diisPlus.AddValueAndError(Fp, overlap * DensityMatrixPlus * Fp - Fp * DensityMatrixPlus * overlap);
+    if (diisMinus.AddValueAndError(Fm, overlap * DensityMatrixMinus * Fm - Fm * DensityMatrixMinus * overlap)) {
+      lastErrorEst = diisMinus.Estimate(Fm) + diisPlus.Estimate(Fp);
+      used = true;
+    }
+  } else {
+    lastErrorEst = 0;
+  }
+  return used;
+}
+
+double UnrestrictedHartreeFock::Step(int iter) {
+  Matrix Fp, Fm;
+  InitFockMatrices(iter, Fp, Fm);
+  const bool used = DIISStep(iter, Fp, Fm);
+  const int n = h.rows();
+  Matrix Cpp, Cmp;
+  hfgpu::eigh(Vt * Fp * V, eigenvalsplus, Cpp);
+  hfgpu::eigh(Vt * Fm * V, eigenvalsminus, Cmp);
+  Cplus = V * Cpp;
+  Cminus = V * Cmp;
+  Matrix Pp(n, n), Pm(n, n);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      double sp = 0, sm = 0;
+      for (unsigned v = 0; v < occupiedPlus.size(); ++v)
+        if (occupiedPlus[v]) sp += Cplus(i, v) * Cplus(j, v);
+      for (unsigned v = 0; v < occupiedMinus.size(); ++v)
+        if (occupiedMinus[v]) sm += Cminus(i, v) * Cminus(j, v);
+      Pp(i, j) = sp;
+      Pm(i, j) = sm;
+    }
+  // CalculateEnergy (UnrestrictedHartreeFock.cpp:246-293)
+  double e = 0;
+  for (int i = 1; i < n; ++i)
+    for (int j = 0; j < i; ++j) e += (Pp(i, j) + Pm(i, j)) * h(j, i);
+  e *= 2.0;
+  for (int i = 0; i < n; ++i) e += (Pp(i, i) + Pm(i, i)) * h(i, i);
+  for (unsigned l = 0; l < occupiedPlus.size(); ++l)
+    if (occupiedPlus[l]) e += eigenvalsplus[l];
+  for (unsigned l = 0; l < occupiedMinus.size(); ++l)
+    if (occupiedMinus[l]) e += eigenvalsminus[l];
+  HOMOEnergy = std::max(nrOccupiedLevelsPlus ? eigenvalsplus[nrOccupiedLevelsPlus - 1] : 0.0,
+                        nrOccupiedLevelsMinus ? eigenvalsminus[nrOccupiedLevelsMinus - 1] : 0.0);
+  totalEnergy = e / 2.0 + nuclearRepulsionEnergy;
+  const double rmsD = std::sqrt(rms_diff(Pp, DensityMatrixPlus) + rms_diff(Pm, DensityMatrixMinus));
+  if (used) {
+    DensityMatrixPlus = Pp;
+    DensityMatrixMinus = Pm;
+  } else {
+    DensityMatrixPlus = alpha * Pp + (1.0 - alpha) * DensityMatrixPlus;
+    DensityMatrixMinus = alpha * Pm + (1.0 - alpha) * DensityMatrixMinus;
+  }
+  return rmsD;
+}
+
+}  // namespace HartreeFock
+
+// ===========================================================================
+// driver C ABI (include/hfgpu_driver.h)
+// ===========================================================================
+namespace {
+thread_local std::string g_driver_error;
+
+Systems::Molecule build_molecule(const char *basis_path, int32_t natoms, const int32_t *Z, const double *xyz) {
+  Chemistry::Basis basis;
+  basis.Load(basis_path);
+  Systems::Molecule mol;
+  for (int a = 0; a < natoms; ++a) {
+    bool found = false;
+    for (const auto &b : basis.atoms)
+      if ((int)b.Z == Z[a]) {
+        mol.atoms.push_back(b);
+        mol.atoms.back().position = {xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2]};
+        found = true;
+        break;
+      }
+    if (!found) throw std::invalid_argument("basis has no element Z=" + std::to_string(Z[a]));
+  }
+  return mol;
+}
+}  // namespace
+
+extern "C" {
+
+const char *hfd_last_error(void) { return g_driver_error.c_str(); }
+
+void hfd_default_scf_opts(hfd_scf_opts *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->alpha = 0.75;
+  o->init_guess = 0.75;
+  o->use_diis = 1;
+  o->post_diis = 500;
+  o->eri_convention = HFG_ERI_REFERENCE;
+  o->schwarz_threshold = 1e-12;
+}
+
+hfg_status hfd_scf(const char *basis_path, int32_t natoms, const int32_t *Z, const double *xyz,
+                   const hfd_scf_opts *opts, hfd_scf_result *result, double *density, int64_t density_count) {
+  if (!basis_path || natoms <= 0 || !Z || !xyz || !opts || !result) return HFG_INVALID_ARG;
+  try {
+    Systems::Molecule mol = build_molecule(basis_path, natoms, Z, xyz);
+    mol.alphaElectrons = (unsigned)opts->alpha_electrons;
+    mol.betaElectrons = (unsigned)opts->beta_electrons;
+    mol.Init();
+    std::unique_ptr<HartreeFock::HartreeFockAlgorithm> algo;
+    if (opts->unrestricted) algo.reset(new HartreeFock::UnrestrictedHartreeFock());
+    else algo.reset(new HartreeFock::RestrictedHartreeFock());
+    algo->alpha = opts->alpha;
+    algo->initGuess = opts->init_guess;
+    algo->UseDIIS = opts->use_diis != 0;
+    algo->normalIterAfterDIIS = opts->post_diis;
+    algo->integralsRepository.options.eri_convention = opts->eri_convention;
+    algo->integralsRepository.options.schwarz_threshold = opts->schwarz_threshold;
+    algo->storedIntegralsBudget = 0;  // direct SCF: no stored table needed
+    algo->Init(&mol);
+    const double e = algo->Calculate();
+    std::memset(result, 0, sizeof *result);
+    result->energy = e;
+    result->homo = algo->HOMOEnergy;
+    result->converged = algo->converged ? 1 : 0;
+    result->iterations = algo->iterations;
+    result->nbf = algo->numberOfOrbitals;
+    const int64_t nn = (int64_t)result->nbf * result->nbf;
+    if (density) {
+      if (opts->unrestricted) {
+        if (density_count < 2 * nn) return HFG_INVALID_ARG;
+        auto *u = static_cast<HartreeFock::UnrestrictedHartreeFock *>(algo.get());
+        std::memcpy(density, u->DensityMatrixPlus.data(), nn * sizeof(double));
+        std::memcpy(density + nn, u->DensityMatrixMinus.data(), nn * sizeof(double));
+      } else {
+        if (density_count < nn) return HFG_INVALID_ARG;
+        auto *r = static_cast<HartreeFock::RestrictedHartreeFock *>(algo.get());
+        std::memcpy(density, r->DensityMatrix.data(), nn * sizeof(double));
+      }
+    }
+    return HFG_OK;
+  } catch (const std::invalid_argument &ex) {
+    g_driver_error = ex.what();
+    return HFG_INVALID_ARG;
+  } catch (const std::exception &ex) {
+    g_driver_error = ex.what();
+    return HFG_DEVICE_ERROR;
+  }
+}
+
+
+hfg_status hfd_one_electron(const char *basis_path, int32_t natoms, const int32_t *Z, const double *xyz, double *S,
+                            double *h, int64_t capacity, int32_t *nbf) {
+  if (!basis_path || natoms <= 0 || !Z || !xyz || !nbf) return HFG_INVALID_ARG;
+  try {
+    Systems::Molecule mol = build_molecule(basis_path, natoms, Z, xyz);
+    mol.Init();
+    GaussianIntegrals::IntegralsRepository repo(&mol);
+    hfgpu::Matrix s, t, v;
+    repo.OneElectron(s, t, v);
+    const int n = (int)mol.shellTable().nbf;
+    *nbf = n;
+    if (capacity < (int64_t)n * n) return HFG_INVALID_ARG;
+    for (int x = 0; x < n * n; ++x) {
+      if (S) S[x] = s.data()[x];
+      if (h) h[x] = t.data()[x] + v.data()[x];
+    }
+    return HFG_OK;
+  } catch (const std::exception &ex) {
+    g_driver_error = ex.what();
+    return HFG_INVALID_ARG;
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,99 @@
+"""ctypes binding of the one-call SCF driver (include/hfgpu_driver.h).
+
+The SCF itself is the C++ host code (include/hfgpu_host.hpp): the
+reference's RestrictedHartreeFock / UnrestrictedHartreeFock loop with its
+defaults, DIIS and convergence thresholds, over the GPU Fock builds.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import engine as E
+from .basis_io import basis_path
+
+
+class hfd_scf_opts(ctypes.Structure):
+    _fields_ = [("unrestricted", ctypes.c_int32), ("alpha", ctypes.c_double), ("init_guess", ctypes.c_double),
+                ("use_diis", ctypes.c_int32), ("post_diis", ctypes.c_int32), ("alpha_electrons", ctypes.c_int32),
+                ("beta_electrons", ctypes.c_int32), ("eri_convention", ctypes.c_int32),
+                ("schwarz_threshold", ctypes.c_double)]
+
+
+class hfd_scf_result(ctypes.Structure):
+    _fields_ = [("energy", ctypes.c_double), ("homo", ctypes.c_double), ("converged", ctypes.c_int32),
+                ("iterations", ctypes.c_int32), ("nbf", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("fock_ms_total", ctypes.c_double)]
+
+
+DRIVER_SYMBOLS = ["hfd_default_scf_opts", "hfd_last_error", "hfd_scf", "hfd_one_electron"]
+
+
+def _lib():
+    L = E.library()
+    if not getattr(L, "_hfd_ready", False):
+        L.hfd_default_scf_opts.argtypes = [ctypes.POINTER(hfd_scf_opts)]
+        L.hfd_default_scf_opts.restype = None
+        L.hfd_last_error.restype = ctypes.c_char_p
+        L.hfd_scf.argtypes = [ctypes.c_char_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                              ctypes.POINTER(hfd_scf_opts), ctypes.POINTER(hfd_scf_result), ctypes.c_void_p,
+                              ctypes.c_int64]
+        L.hfd_scf.restype = ctypes.c_int
+        L.hfd_one_electron.argtypes = [ctypes.c_char_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                       ctypes.POINTER(ctypes.c_int32)]
+        L.hfd_one_electron.restype = ctypes.c_int
+        L._hfd_ready = True
+    return L
+
+
+def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75, use_diis=True, post_diis=500,
+            alpha_electrons=0, beta_electrons=0, eri_convention=E.ERI_REFERENCE, schwarz_threshold=1e-12,
+            want_density=True):
+    """RestrictedHartreeFock / UnrestrictedHartreeFock Init + Calculate."""
+    L = _lib()
+    o = hfd_scf_opts()
+    L.hfd_default_scf_opts(ctypes.byref(o))
+    o.unrestricted, o.alpha, o.init_guess = int(unrestricted), alpha, init_guess
+    o.use_diis, o.post_diis = int(use_diis), post_diis
+    o.alpha_electrons, o.beta_electrons = alpha_electrons, beta_electrons
+    o.eri_convention, o.schwarz_threshold = eri_convention, schwarz_threshold
+    z = np.ascontiguousarray(Z, dtype=np.int32)
+    x = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
+    nbf_guess = 40 * len(z) + 64
+    cap = (2 if unrestricted else 1) * nbf_guess * nbf_guess
+    dens = np.zeros(cap) if want_density else None
+    r = hfd_scf_result()
+    st = L.hfd_scf(basis_path(basis).encode(), len(z), z.ctypes.data_as(ctypes.c_void_p),
+                   x.ctypes.data_as(ctypes.c_void_p), ctypes.byref(o), ctypes.byref(r),
+                   dens.ctypes.data_as(ctypes.c_void_p) if dens is not None else None, cap if dens is not None else 0)
+    if st != 0:
+        raise E.HfgError(st, L.hfd_last_error().decode())
+    out = {"energy": r.energy, "homo": r.homo, "converged": bool(r.converged), "iterations": r.iterations,
+           "nbf": r.nbf}
+    if dens is not None:
+        n = r.nbf
+        if unrestricted:
+            out["density_alpha"] = dens[:n * n].reshape(n, n).copy()
+            out["density_beta"] = dens[n * n:2 * n * n].reshape(n, n).copy()
+        else:
+            out["density"] = dens[:n * n].reshape(n, n).copy()
+    return out
+
+
+def one_electron(Z, xyz, basis: str):
+    """Overlap and core Hamiltonian from the host one-electron code."""
+    L = _lib()
+    z = np.ascontiguousarray(Z, dtype=np.int32)
+    x = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
+    cap = (40 * len(z) + 64) ** 2
+    S, h = np.zeros(cap), np.zeros(cap)
+    n = ctypes.c_int32()
+    st = L.hfd_one_electron(basis_path(basis).encode(), len(z), z.ctypes.data_as(ctypes.c_void_p),
+                            x.ctypes.data_as(ctypes.c_void_p), S.ctypes.data_as(ctypes.c_void_p),
+                            h.ctypes.data_as(ctypes.c_void_p), cap, ctypes.byref(n))
+    if st != 0:
+        raise E.HfgError(st, L.hfd_last_error().decode())
+    k = n.value
+    return S[:k * k].reshape(k, k).copy(), h[:k * k].reshape(k, k).copy()

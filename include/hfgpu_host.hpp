@@ -74,6 +74,10 @@ struct ContractedGaussianShell {
 };
 }  // namespace Orbitals
 
+namespace Chemistry {
+class Basis;
+}
+
 namespace Systems {
 
 class Atom {
@@ -104,7 +108,9 @@ class Molecule {
   unsigned int ElectronsNumber() const;
   unsigned int GetMaxAngularMomentum() const;
   double NuclearRepulsionEnergy() const;
-  bool LoadXYZ(const std::string &fileName, const class Chemistry_Basis_fwd *unused = nullptr);
+  // Molecule::LoadXYZ (Molecule.cpp:143-199): count line, comment line,
+  // then "<symbol> x y z" per atom (coordinates used as given, bohr)
+  bool LoadXYZ(const std::string &fileName, const Chemistry::Basis &basis);
 
   // engine-side shell table (one entry per shell letter), rebuilt by Init()
   struct ShellTable {
