@@ -745,3 +745,74 @@ hfg_status hfg_ctx_stats(const hfg_ctx *c, hfg_stats *out) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free direct RHF build (hfg_fock_rhf_noalloc)
+// ===========================================================================
+// Serving loops and other callers that must not allocate device memory once
+// they are running (a fixed HBM budget, no allocator on the hot path, no
+// implicit synchronisation from cudaMalloc/cudaFree) get this variant of the
+// direct build: its J and K accumulators live in a file-scope device array
+// instead of context buffers.  The array exists once per GPU that loads the
+// library and stays resident until the process exits.
+namespace hfg {
+
+constexpr int kNoAllocMaxNbf = 1024;
+// J then K, each nbf x nbf: 2 * 1024 * 1024 doubles = 16 MiB
+static __device__ __align__(256) double g_noalloc_scratch[2 * kNoAllocMaxNbf * kNoAllocMaxNbf];
+
+constexpr int kNoAllocMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static double *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on `device` (current).  The host-side
+// name g_noalloc_scratch is only a stand-in, so the address is looked up once
+// per device with that device current, and cached.
+static hfg_status noalloc_scratch(int device, double **out) {
+  if (device < 0 || device >= kNoAllocMaxDevices) return fail(HFG_INVALID_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return fail(HFG_DEVICE_ERROR, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+    g_noalloc_ptr[device] = static_cast<double *>(p);
+  }
+  *out = g_noalloc_ptr[device];
+  return HFG_OK;
+}
+
+}  // namespace hfg
+
+extern "C" hfg_status hfg_fock_rhf_noalloc(hfg_ctx *c, const double *dP, double *dG, void *stream) {
+  using namespace hfg;
+  if (!c || !dP || !dG) return fail(HFG_INVALID_ARG, "null argument");
+  if (c->nbf > kNoAllocMaxNbf)
+    return fail(HFG_INVALID_ARG, "hfg_fock_rhf_noalloc: " + std::to_string(c->nbf) +
+                                     " basis functions exceed its fixed scratch of " +
+                                     std::to_string(kNoAllocMaxNbf) + " (use hfg_fock_rhf_device)");
+  HFG_CUDA(cudaSetDevice(c->device));
+  double *scratch = nullptr;
+  hfg_status st = noalloc_scratch(c->device, &scratch);
+  if (st != HFG_OK) return st;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  const int n = c->nbf;
+  const size_t nn = (size_t)n * n;
+  double *J = scratch, *K = scratch + nn;
+  // the array keeps the previous call's sums: clear both accumulators
+  HFG_CUDA(cudaMemsetAsync(J, 0, 2 * nn * sizeof(double), s));
+  const EngineView v = c->view();
+  const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
+  for (const auto &q : c->qclasses) {
+    ClassLaunch cl = base_launch(c, q);
+    cl.Da = dP;
+    cl.Dt = dP;
+    cl.J = J;
+    cl.Ka = K;
+    kClasses[q.cls].launch(v, cl, kJkRhf, ref, grid_for(c, cl.ntasks), s);
+  }
+  const int fg = std::max(1, std::min(1024, (int)((nn + 255) / 256)));
+  finalize_rhf<<<fg, 256, 0, s>>>(J, K, dG, n);
+  HFG_CUDA(cudaGetLastError());
+  return HFG_OK;
+}

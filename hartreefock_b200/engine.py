@@ -24,7 +24,8 @@ ERI_REFERENCE, ERI_EXACT = 0, 1
 EXPORTED = ["hfg_default_opts", "hfg_last_error", "hfg_device_count", "hfg_ctx_create", "hfg_ctx_destroy",
             "hfg_ctx_nbf", "hfg_packed_size", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet",
             "hfg_fock_rhf", "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz",
-            "hfg_ctx_stats", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak"]
+            "hfg_ctx_stats", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak",
+            "hfg_fock_rhf_noalloc"]
 
 
 class HfgError(RuntimeError):
@@ -91,6 +92,8 @@ def library(path: str = LIB_PATH):
     L.hfg_fock_uhf_device.argtypes = [vp, dp, dp, dp, dp, vp]
     L.hfg_schwarz.argtypes = [vp, dp, i64]
     L.hfg_ctx_stats.argtypes = [vp, ctypes.POINTER(hfg_stats)]
+    L.hfg_fock_rhf_noalloc.argtypes = [vp, dp, dp, vp]
+    L.hfg_fock_rhf_noalloc.restype = ctypes.c_int
     L.hfg_set_profiling.argtypes = [vp, i32]
     L.hfg_class_profile.argtypes = [vp, ctypes.POINTER(hfg_class_time), i32, ctypes.POINTER(i32)]
     L.hfg_measure_fp64_peak.argtypes = [i32, ctypes.POINTER(ctypes.c_double)]
@@ -189,6 +192,11 @@ class Engine:
     def fock_rhf_device(self, P_ptr: int, G_ptr: int, stream: int = 0):
         _check(library().hfg_fock_rhf_device(self._h, ctypes.c_void_p(P_ptr), ctypes.c_void_p(G_ptr),
                                              ctypes.c_void_p(stream)))
+
+    def fock_rhf_noalloc(self, P_ptr: int, G_ptr: int, stream: int = 0):
+        """Allocation-free direct RHF build (fixed 1024-function scratch)."""
+        _check(library().hfg_fock_rhf_noalloc(self._h, ctypes.c_void_p(P_ptr), ctypes.c_void_p(G_ptr),
+                                              ctypes.c_void_p(stream)))
 
     def fock_uhf_device(self, Pa_ptr, Pb_ptr, Ga_ptr, Gb_ptr, stream: int = 0):
         _check(library().hfg_fock_uhf_device(self._h, ctypes.c_void_p(Pa_ptr), ctypes.c_void_p(Pb_ptr),

@@ -131,6 +131,22 @@ hfg_status hfg_fock_rhf_device(hfg_ctx *ctx, const double *dP, double *dG, void 
 hfg_status hfg_fock_uhf_device(hfg_ctx *ctx, const double *dPa, const double *dPb, double *dGa, double *dGb,
                                void *stream);
 
+/* Allocation-free variant of hfg_fock_rhf_device, for callers that must not
+ * allocate device memory while they run: a serving loop under a fixed HBM
+ * budget, code that cannot afford the implicit synchronisation of
+ * cudaMalloc/cudaFree, or a host without allocator access on that path.
+ * No counterpart in the reference (its Fock build, RestrictedHartreeFock.cpp
+ * :168-207, allocates freely).  The J/K accumulators live in a file-scope
+ * device array of 2 x 1024 x 1024 doubles (16 MiB) that every GPU loading
+ * the library keeps until exit; contexts above 1024 basis functions are
+ * rejected with HFG_INVALID_ARG.  The context (created beforehand with
+ * hfg_ctx_create, which does allocate) and the caller's device buffers dP, dG
+ * are the only other memory used.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * (different streams or contexts at the same time) race on it. */
+hfg_status hfg_fock_rhf_noalloc(hfg_ctx *ctx, const double *dP, double *dG, void *stream);
+
 /* Schwarz bounds sqrt(max (ij|ij)) per shell pair (a >= b), in pair order
  * a*(a+1)/2 + b; `count` = nshells*(nshells+1)/2. */
 hfg_status hfg_schwarz(hfg_ctx *ctx, double *host_out, int64_t count);
