@@ -147,6 +147,7 @@ def run_reference_arm(args, rank, world):
 
 
 def main():
+    global WATERS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -154,8 +155,11 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--ref-sample", type=int, default=30000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--waters", type=int, default=16,
+                    help="cluster size; the benchmark workload is 16 (smaller values size profiler captures)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    WATERS = args.waters
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -12,6 +12,7 @@
 
 #include "../../include/hfgpu.h"
 #include "eri_dispatch.cuh"
+#include "eri_split_dispatch.cuh"
 
 namespace hfg {
 
@@ -39,7 +40,7 @@ static const std::vector<double> &boys_table_host() {
   static std::vector<double> tab;
   static std::once_flag once;
   std::call_once(once, [] {
-    tab.resize((size_t)kBoysGrid * kBoysOrders);
+    tab.resize((size_t)kBoysGrid * kBoysOrders + kBoysGrid);
     for (int i = 0; i < kBoysGrid; ++i) {
       const long double T = (long double)i * (long double)kBoysStep;
       for (int m = 0; m < kBoysOrders; ++m) {
@@ -51,6 +52,7 @@ static const std::vector<double> &boys_table_host() {
         }
         tab[(size_t)i * kBoysOrders + m] = (double)(expl(-T) * sum);
       }
+      tab[(size_t)kBoysGrid * kBoysOrders + i] = (double)expl(-T);  // e^-T_i
     }
   });
   return tab;
@@ -64,17 +66,21 @@ struct HostShell {
   int L, nprim, prim_off, ao;
 };
 
+// Pairs of one class, grouped into buckets of similar primitive-pair count
+// (so that the 32 kets of a warp run equal primitive loops), each bucket
+// sorted by Schwarz bound descending (so that screening cuts a prefix).
+constexpr int kBuckets = 6;
+static inline int prim_bucket(int np) { return np <= 1 ? 0 : np <= 3 ? 1 : np <= 6 ? 2 : np <= 12 ? 3 : np <= 24 ? 4 : 5; }
 struct PairClassList {
-  std::vector<int> pairs;  // pair indices sorted by Q descending
+  std::vector<int> pairs;  // concatenated buckets
+  int bucket_start[kBuckets + 1] = {};
   int *d_pairs = nullptr;
 };
 
 struct QuartetClass {
   int cls;       // index into kClasses
   int bra_pc, ket_pc;
-  std::vector<int> ket_count;
   std::vector<Task> tasks;
-  int *d_ket_count = nullptr;
   Task *d_tasks = nullptr;
   int64_t shell_quartets = 0, function_quartets = 0, prim_quartets = 0;
   double flops = 0;
@@ -101,7 +107,7 @@ struct hfg_ctx {
   int nbf = 0;
   std::vector<HostShell> shells;
   int npairs = 0;
-  std::vector<int> pair_sa, pair_sb, pair_cls;
+  std::vector<int> pair_sa, pair_sb, pair_cls, pair_nprim;
   std::vector<double> pair_Q;
   PairClassList pclass[kNumPairClasses];
   std::vector<QuartetClass> qclasses;
@@ -117,6 +123,9 @@ struct hfg_ctx {
   // work buffers
   double *d_J = nullptr, *d_Ka = nullptr, *d_Kb = nullptr, *d_P = nullptr, *d_Pb = nullptr, *d_Pt = nullptr;
   double *d_G = nullptr, *d_Gb = nullptr, *d_block = nullptr;
+  double *d_scratch = nullptr;  // split-path [e0|f0] blocks
+  size_t scratch_doubles = 0;
+  size_t scratch_budget_bytes = size_t(512) << 20;
   hfg_stats stats{};
   bool profiling = false;
   EngineView view() const {
@@ -139,14 +148,14 @@ struct hfg_ctx {
   ~hfg_ctx() {
     cudaSetDevice(device);
     for (auto &q : qclasses) {
-      cudaFree(q.d_ket_count);
       cudaFree(q.d_tasks);
       if (q.ev_a) cudaEventDestroy(q.ev_a);
       if (q.ev_b) cudaEventDestroy(q.ev_b);
     }
     for (auto &p : pclass) cudaFree(p.d_pairs);
     void *bufs[] = {d_prim, d_pair_prim_off, d_pair_nprim, d_pair_sa, d_pair_sb, d_pair_ao_a, d_pair_ao_b,
-                    d_pair_AB, d_pair_Q, d_boys, d_pair_Dmax, d_J, d_Ka, d_Kb, d_P, d_Pb, d_Pt, d_G, d_Gb, d_block};
+                    d_pair_AB, d_pair_Q, d_boys, d_pair_Dmax, d_J, d_Ka, d_Kb, d_P, d_Pb, d_Pt, d_G, d_Gb, d_block,
+                    d_scratch};
     for (void *b : bufs) cudaFree(b);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -195,6 +204,9 @@ static inline int64_t pair_functions(const hfg_ctx *c, int p) {
 }
 
 // Build per-class quartet task lists with Schwarz screening at `threshold`.
+// Every unordered pair of pairs appears once: for different classes all
+// (bra, ket) combinations, for the same class the kets at positions <= the
+// bra's position in the concatenated bucket list.
 static void build_quartet_classes(hfg_ctx *c, double threshold) {
   c->qclasses.clear();
   for (int ci = 0; ci < kNumClasses; ++ci) {
@@ -203,52 +215,50 @@ static void build_quartet_classes(hfg_ctx *c, double threshold) {
     q.cls = ci;
     q.bra_pc = pair_class_index(ce.la, ce.lb);
     q.ket_pc = pair_class_index(ce.lc, ce.ld);
-    const auto &bras = c->pclass[q.bra_pc].pairs;
-    const auto &kets = c->pclass[q.ket_pc].pairs;
+    const PairClassList &BL = c->pclass[q.bra_pc], &KL = c->pclass[q.ket_pc];
+    const auto &bras = BL.pairs;
+    const auto &kets = KL.pairs;
     if (bras.empty() || kets.empty()) continue;
     const bool same = q.bra_pc == q.ket_pc;
-    // prefix sums over the ket list for quartet accounting
     std::vector<int64_t> kfun(kets.size() + 1, 0), kprim(kets.size() + 1, 0);
     std::vector<double> kq(kets.size());
     for (size_t k = 0; k < kets.size(); ++k) {
       kfun[k + 1] = kfun[k] + pair_functions(c, kets[k]);
-      const HostShell &sa = c->shells[c->pair_sa[kets[k]]], &sb = c->shells[c->pair_sb[kets[k]]];
-      kprim[k + 1] = kprim[k] + (int64_t)sa.nprim * sb.nprim;
+      kprim[k + 1] = kprim[k] + c->pair_nprim[kets[k]];
       kq[k] = c->pair_Q[kets[k]];
     }
-    q.ket_count.resize(bras.size());
     const double pf = prim_flops(ci, c->opts.eri_convention == HFG_ERI_REFERENCE);
     const double hf = hrr_flops(ci);
     const int ltot = ce.la + ce.lb + ce.lc + ce.ld;
     for (size_t b = 0; b < bras.size(); ++b) {
       const double qb = c->pair_Q[bras[b]];
-      // kets sorted by Q descending: count those with qb * qk >= threshold
-      int64_t lo = 0, hi = (int64_t)kets.size();
-      if (qb <= 0) hi = 0;
-      else {
-        const double need = threshold / qb;
+      if (!(qb > 0)) continue;
+      const double need = threshold / qb;
+      const int64_t bf = pair_functions(c, bras[b]);
+      const int64_t bprim = c->pair_nprim[bras[b]];
+      for (int k = 0; k < kBuckets; ++k) {
+        const int64_t s0 = KL.bucket_start[k], s1 = KL.bucket_start[k + 1];
+        // kets of the bucket with qb * qk >= threshold form a prefix
+        int64_t lo = s0, hi = s1;
         while (lo < hi) {
           const int64_t mid = (lo + hi) / 2;
           if (kq[mid] >= need) lo = mid + 1;
           else hi = mid;
         }
-        hi = lo;
+        int64_t end = lo;
+        if (same) end = std::min<int64_t>(end, (int64_t)b + 1);
+        if (end <= s0) continue;
+        for (int64_t st = s0; st < end; st += 32)
+          q.tasks.push_back(Task{(int)b, (int)st, (int)std::min<int64_t>(st + 32, end)});
+        q.shell_quartets += end - s0;
+        if (same && end == (int64_t)b + 1) {
+          // the diagonal quartet (bra == ket) counts its unique half
+          q.function_quartets += bf * (kfun[end - 1] - kfun[s0]) + bf * (bf + 1) / 2;
+        } else {
+          q.function_quartets += bf * (kfun[end] - kfun[s0]);
+        }
+        q.prim_quartets += bprim * (kprim[end] - kprim[s0]);
       }
-      int64_t cnt = hi;
-      if (same) cnt = std::min<int64_t>(cnt, (int64_t)b + 1);
-      q.ket_count[b] = (int)cnt;
-      for (int64_t s = 0; s < cnt; s += 32) q.tasks.push_back(Task{(int)b, (int)s});
-      q.shell_quartets += cnt;
-      const int64_t bf = pair_functions(c, bras[b]);
-      const HostShell &sa = c->shells[c->pair_sa[bras[b]]], &sb = c->shells[c->pair_sb[bras[b]]];
-      const int64_t bprim = (int64_t)sa.nprim * sb.nprim;
-      if (same && cnt == (int64_t)b + 1) {
-        // diagonal quartet (bra == ket) counts its unique half
-        q.function_quartets += bf * kfun[cnt - 1] + bf * (bf + 1) / 2;
-      } else {
-        q.function_quartets += bf * kfun[cnt];
-      }
-      q.prim_quartets += bprim * kprim[cnt];
     }
     q.flops = (double)q.prim_quartets * (pf + boys_geom_flops(ltot)) + (double)q.shell_quartets * hf;
     if (!q.tasks.empty()) c->qclasses.push_back(std::move(q));
@@ -260,9 +270,7 @@ static void build_quartet_classes(hfg_ctx *c, double threshold) {
 
 static hfg_status upload_classes(hfg_ctx *c) {
   for (auto &q : c->qclasses) {
-    hfg_status st = upload(&q.d_ket_count, q.ket_count);
-    if (st != HFG_OK) return st;
-    st = upload(&q.d_tasks, q.tasks);
+    const hfg_status st = upload(&q.d_tasks, q.tasks);
     if (st != HFG_OK) return st;
   }
   return HFG_OK;
@@ -277,7 +285,6 @@ static ClassLaunch base_launch(const hfg_ctx *c, const QuartetClass &q) {
   ClassLaunch cl{};
   cl.bra_list = c->pclass[q.bra_pc].d_pairs;
   cl.ket_list = c->pclass[q.ket_pc].d_pairs;
-  cl.ket_count = q.d_ket_count;
   cl.tasks = q.d_tasks;
   cl.ntasks = (int)q.tasks.size();
   cl.same_class = q.bra_pc == q.ket_pc;
@@ -312,6 +319,49 @@ static hfg_status ensure(double **p, size_t count) {
   return HFG_OK;
 }
 
+// Launch one class: the fused kernel, or for the large classes the split
+// primitive + HRR/digest kernels over chunks of tasks sized to the scratch
+// budget.  Counts the kernel launches in *launches.
+static int ncomp_range(int lo, int hi) {
+  int s = 0;
+  for (int L = lo; L <= hi; ++L) s += ncart_h(L);
+  return s;
+}
+
+static hfg_status launch_class(hfg_ctx *c, const QuartetClass &q, const ClassLaunch &cl, int mode, bool ref,
+                               cudaStream_t s, int *launches) {
+  const ClassEntry &e = kClasses[q.cls];
+  if (!kSplit[q.cls]) {
+    e.launch(c->view(), cl, mode, ref, grid_for(c, cl.ntasks), s);
+    ++*launches;
+    return HFG_OK;
+  }
+  const size_t acc = (size_t)ncomp_range(e.la, e.la + e.lb) * ncomp_range(e.lc, e.lc + e.ld);
+  const bool two = ref && e.la == 2 && e.lb == 2 && e.lc == 2 && e.ld == 2;
+  const size_t per_task = 32 * acc * (two ? 2 : 1);
+  const int max_tasks = (int)std::max<size_t>(1, c->scratch_budget_bytes / (per_task * sizeof(double)));
+  const int chunk_tasks = std::min(cl.ntasks, max_tasks);
+  const size_t need = (size_t)chunk_tasks * per_task;
+  if (need > c->scratch_doubles) {
+    cudaFree(c->d_scratch);
+    c->d_scratch = nullptr;
+    c->scratch_doubles = 0;
+    HFG_CUDA(cudaMalloc((void **)&c->d_scratch, need * sizeof(double)));
+    c->scratch_doubles = need;
+  }
+  for (int t0 = 0; t0 < cl.ntasks; t0 += chunk_tasks) {
+    SplitChunk ch{};
+    ch.ntasks = std::min(chunk_tasks, cl.ntasks - t0);
+    ch.task0 = t0;
+    ch.stride = (long long)ch.ntasks * 32;
+    ch.scr_fwd = c->d_scratch;
+    ch.scr_rev = c->d_scratch + acc * (size_t)ch.stride;
+    kSplit[q.cls](c->view(), cl, ch, mode, ref, s);
+    *launches += 2;
+  }
+  return HFG_OK;
+}
+
 // Direct J/K build: all classes on `s`, then G.
 static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const double *dPb, double *dGa, double *dGb,
                                cudaStream_t s) {
@@ -328,7 +378,6 @@ static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const do
     launches += 2;
   }
   HFG_CUDA(cudaEventRecord(c->ev0, s));
-  const EngineView v = c->view();
   const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
   c->stats = hfg_stats{};
   for (auto &q : c->qclasses) {
@@ -340,9 +389,9 @@ static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const do
     cl.J = c->d_J;
     cl.Ka = c->d_Ka;
     cl.Kb = c->d_Kb;
-    kClasses[q.cls].launch(v, cl, uhf ? kJkUhf : kJkRhf, ref, grid_for(c, cl.ntasks), s);
+    st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, s, &launches);
+    if (st != HFG_OK) return st;
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_b, s));
-    ++launches;
     c->stats.shell_quartets += q.shell_quartets;
     c->stats.function_quartets += q.function_quartets;
     c->stats.primitive_quartets += q.prim_quartets;
@@ -374,7 +423,6 @@ static hfg_status finish_timing(hfg_ctx *c) {
 static hfg_status stored_build(hfg_ctx *c, double *d_out, int64_t count, cudaStream_t s) {
   HFG_CUDA(cudaMemsetAsync(d_out, 0, (size_t)count * sizeof(double), s));
   HFG_CUDA(cudaEventRecord(c->ev0, s));
-  const EngineView v = c->view();
   const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
   c->stats = hfg_stats{};
   int launches = 1;
@@ -382,9 +430,9 @@ static hfg_status stored_build(hfg_ctx *c, double *d_out, int64_t count, cudaStr
     ClassLaunch cl = base_launch(c, q);
     cl.packed = d_out;
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_a, s));
-    kClasses[q.cls].launch(v, cl, kStorePacked, ref, grid_for(c, cl.ntasks), s);
+    const hfg_status st = launch_class(c, q, cl, kStorePacked, ref, s, &launches);
+    if (st != HFG_OK) return st;
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_b, s));
-    ++launches;
     c->stats.shell_quartets += q.shell_quartets;
     c->stats.function_quartets += q.function_quartets;
     c->stats.primitive_quartets += q.prim_quartets;
@@ -522,6 +570,29 @@ hfg_status hfg_ctx_create(const hfg_shells *sh, const hfg_opts *opts, hfg_ctx **
         }
       pn[p] = (int)prim.size() - poff[p];
     }
+  // Primitive-pair screening: drop primitive pairs whose largest possible
+  // quartet contribution, |K_ab| max|K| / sqrt(zeta_ab + min zeta), is below
+  // 1e-21 (recursion factors cannot lift that to the 1e-15 level).  Mostly
+  // tight-exponent pairs on distant atoms, about 60% of all for water clusters.
+  {
+    double kmax = 0, zmin = 1e300;
+    for (const PrimPair &pp : prim) {
+      kmax = std::max(kmax, std::fabs(pp.K));
+      zmin = std::min(zmin, pp.zeta);
+    }
+    std::vector<PrimPair> kept;
+    kept.reserve(prim.size());
+    for (int p = 0; p < np; ++p) {
+      const int o = poff[p], cnt = pn[p];
+      poff[p] = (int)kept.size();
+      for (int x = o; x < o + cnt; ++x)
+        if (std::fabs(prim[x].K) * kmax / std::sqrt(prim[x].zeta + zmin) >= 1e-21) kept.push_back(prim[x]);
+      pn[p] = (int)kept.size() - poff[p];
+    }
+    prim.swap(kept);
+    if (prim.empty()) prim.push_back(PrimPair{});  // keep a valid device allocation
+  }
+  ctx->pair_nprim = pn;
   hfg_status st;
   if ((st = upload(&ctx->d_prim, prim)) != HFG_OK || (st = upload(&ctx->d_pair_prim_off, poff)) != HFG_OK ||
       (st = upload(&ctx->d_pair_nprim, pn)) != HFG_OK || (st = upload(&ctx->d_pair_sa, psa)) != HFG_OK ||
@@ -553,12 +624,20 @@ hfg_status hfg_ctx_create(const hfg_shells *sh, const hfg_opts *opts, hfg_ctx **
   ctx->pair_Q.resize(np);
   HFG_CUDA(cudaMemcpy(ctx->pair_Q.data(), ctx->d_pair_Q, (size_t)np * sizeof(double), cudaMemcpyDeviceToHost));
 
-  // ---- class lists sorted by Q descending (ties by pair index)
+  // ---- class lists: primitive-count buckets, each sorted by Q descending
   for (int pc = 0; pc < kNumPairClasses; ++pc) {
-    auto &lst = ctx->pclass[pc].pairs;
-    lst = by_class[pc];
-    std::stable_sort(lst.begin(), lst.end(), [&](int x, int y) { return ctx->pair_Q[x] > ctx->pair_Q[y]; });
-    if ((st = upload(&ctx->pclass[pc].d_pairs, lst)) != HFG_OK) return st;
+    PairClassList &L = ctx->pclass[pc];
+    L.pairs.clear();
+    for (int k = 0; k < kBuckets; ++k) {
+      L.bucket_start[k] = (int)L.pairs.size();
+      std::vector<int> bk;
+      for (int p : by_class[pc])
+        if (prim_bucket(pn[p]) == k) bk.push_back(p);
+      std::stable_sort(bk.begin(), bk.end(), [&](int x, int y) { return ctx->pair_Q[x] > ctx->pair_Q[y]; });
+      L.pairs.insert(L.pairs.end(), bk.begin(), bk.end());
+    }
+    L.bucket_start[kBuckets] = (int)L.pairs.size();
+    if ((st = upload(&L.d_pairs, L.pairs)) != HFG_OK) return st;
   }
   build_quartet_classes(ctx.get(), ctx->opts.schwarz_threshold);
   if ((st = upload_classes(ctx.get())) != HFG_OK) return st;
@@ -674,20 +753,19 @@ hfg_status hfg_eri_quartet(hfg_ctx *c, int32_t i, int32_t j, int32_t k, int32_t 
   const int cls = class_index(kPairClasses[cb][0], kPairClasses[cb][1], kPairClasses[ck][0], kPairClasses[ck][1]);
   if (cls < 0) return fail(HFG_INVALID_ARG, "no class for quartet");
   // one-task launch over two one-element lists
-  std::vector<int> bl{bra}, kl{ket}, kc{1};
-  std::vector<Task> tk{Task{0, 0}};
-  int *d_bl = nullptr, *d_kl = nullptr, *d_kc = nullptr;
+  std::vector<int> bl{bra}, kl{ket};
+  std::vector<Task> tk{Task{0, 0, 1}};
+  int *d_bl = nullptr, *d_kl = nullptr;
   Task *d_tk = nullptr;
   hfg_status st;
-  if ((st = upload(&d_bl, bl)) != HFG_OK || (st = upload(&d_kl, kl)) != HFG_OK || (st = upload(&d_kc, kc)) != HFG_OK ||
-      (st = upload(&d_tk, tk)) != HFG_OK || (st = ensure(&c->d_block, 1296)) != HFG_OK) {
-    cudaFree(d_bl); cudaFree(d_kl); cudaFree(d_kc); cudaFree(d_tk);
+  if ((st = upload(&d_bl, bl)) != HFG_OK || (st = upload(&d_kl, kl)) != HFG_OK || (st = upload(&d_tk, tk)) != HFG_OK ||
+      (st = ensure(&c->d_block, 1296)) != HFG_OK) {
+    cudaFree(d_bl); cudaFree(d_kl); cudaFree(d_tk);
     return st;
   }
   ClassLaunch cl{};
   cl.bra_list = d_bl;
   cl.ket_list = d_kl;
-  cl.ket_count = d_kc;
   cl.tasks = d_tk;
   cl.ntasks = 1;
   cl.packed = c->d_block;
@@ -696,7 +774,7 @@ hfg_status hfg_eri_quartet(hfg_ctx *c, int32_t i, int32_t j, int32_t k, int32_t 
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(blk, c->d_block, sizeof blk, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  cudaFree(d_bl); cudaFree(d_kl); cudaFree(d_kc); cudaFree(d_tk);
+  cudaFree(d_bl); cudaFree(d_kl); cudaFree(d_tk);
   if (e != cudaSuccess) return fail(HFG_DEVICE_ERROR, cudaGetErrorString(e));
   // locate (i j | k l) in the (first second | first second) block
   const int fa = c->pair_sa[bra], fb = c->pair_sb[bra], fc = c->pair_sa[ket], fd = c->pair_sb[ket];

@@ -22,9 +22,10 @@ __device__ __forceinline__ double inv_factorial(int k) {
 
 template <int LTOT>
 __device__ __forceinline__ void stage_boys(double *tab, const double *__restrict__ g) {
-  for (int x = threadIdx.x; x < kBoysGrid * kBoysTaylor; x += blockDim.x) {
-    const int i = x / kBoysTaylor, k = x - i * kBoysTaylor;
-    tab[x] = g[i * kBoysOrders + LTOT + k] * inv_factorial(k);
+  for (int x = threadIdx.x; x < kBoysGrid * kBoysRow; x += blockDim.x) {
+    const int i = x / kBoysRow, k = x - i * kBoysRow;
+    // Taylor coefficients F_{LTOT+k}(T_i)/k!, then e^-T_i from the table's tail
+    tab[x] = k < kBoysTaylor ? g[i * kBoysOrders + LTOT + k] * inv_factorial(k) : g[kBoysGrid * kBoysOrders + i];
   }
   __syncthreads();
 }
@@ -50,12 +51,13 @@ __device__ __forceinline__ void quartet_block(const EngineView &v, const double 
     const PrimPair pk = v.prim[offk + ik];
     for (int ib = 0; ib < npb; ++ib) {
       const PrimPair pb = v.prim[offb + ib];
-      const double inv_zpe = 1.0 / (pb.zeta + pk.zeta);
+      const double rs = rsqrt(pb.zeta + pk.zeta);
+      const double inv_zpe = rs * rs;
       const double rho = pb.zeta * pk.zeta * inv_zpe;
       const double PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;
       const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
       double F[LTOT + 1];
-      boys_eval<LTOT, double>(F, T, pb.K * pk.K * sqrt(inv_zpe), tab);
+      boys_eval<LTOT, double>(F, T, pb.K * pk.K * rs, tab);
       const double roz = rho * pb.inv_zeta;
       const double ie = pk.inv_zeta;
       Cls::template prim<double>(acc, F, pb.PAx, pb.PAy, pb.PAz, -roz * PQx, -roz * PQy, -roz * PQz,
@@ -131,7 +133,7 @@ template <int LA, int LB, int LC, int LD, int MODE, bool REF>
 __global__ void __launch_bounds__(kThreads) eri_class_kernel(const EngineView v, const ClassLaunch cl) {
   constexpr int LTOT = LA + LB + LC + LD;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-  __shared__ double tab[kBoysGrid * kBoysTaylor];
+  __shared__ double tab[kBoysGrid * kBoysRow];
   stage_boys<LTOT>(tab, v.boys_table);
 
   const int lane = threadIdx.x & 31;
@@ -141,7 +143,7 @@ __global__ void __launch_bounds__(kThreads) eri_class_kernel(const EngineView v,
     const Task task = cl.tasks[t];
     const int bp = cl.bra_list[task.bra_pos];
     const int kpos = task.ket_start + lane;
-    const bool active = kpos < cl.ket_count[task.bra_pos];
+    const bool active = kpos < task.ket_end;
     const int kp = active ? cl.ket_list[kpos] : bp;
     const int npk = active ? v.pair_nprim[kp] : 0;
 
@@ -290,7 +292,7 @@ template <int LA, int LB>
 __global__ void __launch_bounds__(kThreads) schwarz_kernel(const EngineView v, const int *pairs, int npairs,
                                                            double *Q) {
   constexpr int NA = ncart(LA), NB = ncart(LB);
-  __shared__ double tab[kBoysGrid * kBoysTaylor];
+  __shared__ double tab[kBoysGrid * kBoysRow];
   stage_boys<2 * (LA + LB)>(tab, v.boys_table);
   for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < npairs; x += gridDim.x * blockDim.x) {
     const int p = pairs[x];

@@ -1,0 +1,215 @@
+// Split path for the large classes (more than 81 integrals per shell
+// quartet): the fused kernel's per-thread state (the contracted [e0|f0]
+// block plus the full (ab|cd) block plus the J/K partials) does not fit the
+// register file there and spills heavily.  Here
+//   1. eri_prim_split_kernel: thread per shell quartet runs the primitive
+//      loops (Boys, vertical recursion, electron transfer, contraction) and
+//      streams the contracted [e0|f0] block to scratch, column-major across
+//      the quartets of a chunk so that a warp's stores coalesce;
+//   2. eri_hrr_digest_kernel: thread per (shell quartet, bra row ab) expands
+//      the row with the linear horizontal recursion (<= 4 terms per output),
+//      then stores it (packed table) or digests it into J/K.
+// The 32 quartets of a warp share the bra pair (one task), so in step 2 the
+// J_ab partial of a warp reduces across lanes before its atomic.
+#pragma once
+
+#include "eri_kernels.cuh"
+#include "eri_split_gen.cuh"
+
+namespace hfg {
+
+// contracted [e0|f0] of one shell quartet, written to scr[x * stride]
+template <int LA, int LB, int LC, int LD, bool REF>
+__device__ __forceinline__ void prim_block_to_scratch(const EngineView &v, const double *tab, int bp, int kp, int npk,
+                                                      double *scr, long long stride) {
+  constexpr int LTOT = LA + LB + LC + LD;
+  using Cls = EriClass<LA, LB, LC, LD, REF>;
+  double acc[Cls::kAcc];
+#pragma unroll
+  for (int x = 0; x < Cls::kAcc; ++x) acc[x] = 0.0;
+  const int offb = v.pair_prim_off[bp], npb = v.pair_nprim[bp];
+  const int offk = v.pair_prim_off[kp];
+  for (int ik = 0; ik < npk; ++ik) {
+    const PrimPair pk = v.prim[offk + ik];
+    for (int ib = 0; ib < npb; ++ib) {
+      const PrimPair pb = v.prim[offb + ib];
+      const double rs = rsqrt(pb.zeta + pk.zeta);
+      const double inv_zpe = rs * rs;
+      const double rho = pb.zeta * pk.zeta * inv_zpe;
+      const double PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;
+      const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+      double F[LTOT + 1];
+      boys_eval<LTOT, double>(F, T, pb.K * pk.K * rs, tab);
+      const double roz = rho * pb.inv_zeta;
+      const double ie = pk.inv_zeta;
+      Cls::template prim<double>(acc, F, pb.PAx, pb.PAy, pb.PAz, -roz * PQx, -roz * PQy, -roz * PQz,
+                                 0.5 * pb.inv_zeta, roz, -(pb.bABx + pk.bABx) * ie, -(pb.bABy + pk.bABy) * ie,
+                                 -(pb.bABz + pk.bABz) * ie, pb.zeta * ie, 0.5 * ie);
+    }
+  }
+#pragma unroll
+  for (int x = 0; x < Cls::kAcc; ++x) scr[x * stride] = acc[x];
+}
+
+template <int LA, int LB, int LC, int LD, bool REF>
+__global__ void __launch_bounds__(kThreads) eri_prim_split_kernel(const EngineView v, const ClassLaunch cl,
+                                                                  const SplitChunk ch) {
+  constexpr int LTOT = LA + LB + LC + LD;
+  __shared__ double tab[kBoysGrid * kBoysRow];
+  stage_boys<LTOT>(tab, v.boys_table);
+  const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= (long long)ch.ntasks * 32) return;
+  const Task task = cl.tasks[ch.task0 + (int)(slot >> 5)];
+  const int kpos = task.ket_start + (int)(slot & 31);
+  if (kpos >= task.ket_end) return;
+  const int bp = cl.bra_list[task.bra_pos], kp = cl.ket_list[kpos];
+  constexpr bool kOrient = REF && LA == 2 && LB == 2 && LC == 2 && LD == 2;
+  if constexpr (kOrient) {
+    // bra/ket orientation the reference picks (see dddd_reference_values)
+    const int sab = v.pair_sa[bp], skt = v.pair_sa[kp];
+    if (sab >= skt)
+      prim_block_to_scratch<LA, LB, LC, LD, true>(v, tab, bp, kp, v.pair_nprim[kp], ch.scr_fwd + slot, ch.stride);
+    if (sab <= skt)
+      prim_block_to_scratch<LA, LB, LC, LD, true>(v, tab, kp, bp, v.pair_nprim[bp], ch.scr_rev + slot, ch.stride);
+  } else {
+    prim_block_to_scratch<LA, LB, LC, LD, REF>(v, tab, bp, kp, v.pair_nprim[kp], ch.scr_fwd + slot, ch.stride);
+  }
+}
+
+template <int LA, int LB, int LC, int LD, int MODE, bool REF>
+__global__ void __launch_bounds__(kThreads) eri_hrr_digest_kernel(const EngineView v, const ClassLaunch cl,
+                                                                  const SplitChunk ch) {
+  constexpr int NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+  constexpr bool kOrient = REF && LA == 2 && LB == 2 && LC == 2 && LD == 2;
+  const int ab = blockIdx.y;
+  const int a = ab / NB, b = ab - a * NB;
+  const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= (long long)ch.ntasks * 32) return;  // whole warps: slots come in tasks of 32
+  const int lane = threadIdx.x & 31;
+  const Task task = cl.tasks[ch.task0 + (int)(slot >> 5)];
+  const int kpos = task.ket_start + lane;
+  const bool active = kpos < task.ket_end;
+  const int bp = cl.bra_list[task.bra_pos];
+  const int kp = active ? cl.ket_list[kpos] : bp;
+  const int n = v.nbf;
+
+  double out[NC * ND];
+#pragma unroll
+  for (int x = 0; x < NC * ND; ++x) out[x] = 0.0;
+  const double X0 = v.pair_AB[3 * bp], X1 = v.pair_AB[3 * bp + 1], X2 = v.pair_AB[3 * bp + 2];
+  const double Y0 = v.pair_AB[3 * kp], Y1 = v.pair_AB[3 * kp + 1], Y2 = v.pair_AB[3 * kp + 2];
+  const int aoa = v.pair_ao_a[bp], aob = v.pair_ao_b[bp], aoc = v.pair_ao_a[kp], aod = v.pair_ao_b[kp];
+  const bool bdiag = v.pair_sa[bp] == v.pair_sb[bp], kdiag = v.pair_sa[kp] == v.pair_sb[kp];
+  if (active) {
+    if constexpr (kOrient) {
+      const int sab = v.pair_sa[bp], skt = v.pair_sa[kp];
+      if (sab > skt) {
+        EriRows<LA, LB, LC, LD>::template row<double>(out, ab, ch.scr_fwd + slot, ch.stride, X0, X1, X2, Y0, Y1, Y2);
+      } else if (sab < skt) {
+        EriRows<LA, LB, LC, LD>::template col<double>(out, ab, ch.scr_rev + slot, ch.stride, Y0, Y1, Y2, X0, X1, X2);
+      } else {
+        double sw[NC * ND];
+        EriRows<LA, LB, LC, LD>::template row<double>(out, ab, ch.scr_fwd + slot, ch.stride, X0, X1, X2, Y0, Y1, Y2);
+        EriRows<LA, LB, LC, LD>::template col<double>(sw, ab, ch.scr_rev + slot, ch.stride, Y0, Y1, Y2, X0, X1, X2);
+        const int I = aoa + a, J = aob + b;
+        const int o1 = bdiag ? max(I, J) : I, o2 = bdiag ? min(I, J) : J;
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+#pragma unroll
+          for (int d = 0; d < ND; ++d) {
+            const int K = aoc + c, L = aod + d;
+            const int o3 = kdiag ? max(K, L) : K, o4 = kdiag ? min(K, L) : L;
+            if (!(o1 > o3 || (o1 == o3 && o2 >= o4))) out[c * ND + d] = sw[c * ND + d];
+          }
+      }
+    } else {
+      EriRows<LA, LB, LC, LD>::template row<double>(out, ab, ch.scr_fwd + slot, ch.stride, X0, X1, X2, Y0, Y1, Y2);
+    }
+    const double nab = comp_norm<LA>(a) * comp_norm<LB>(b);
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int d = 0; d < ND; ++d) out[c * ND + d] *= nab * comp_norm<LC>(c) * comp_norm<LD>(d);
+  }
+  const int I = aoa + a, J = aob + b;
+  const bool same = bp == kp;
+
+  if constexpr (MODE == kStorePacked) {
+    if (!active) return;
+    if (bdiag && I < J) return;
+    const long long ij = tri(I, J);
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        const int K = aoc + c, L = aod + d;
+        if (kdiag && K < L) continue;
+        const long long kl = tri(K, L);
+        if (same && ij < kl) continue;
+        cl.packed[tri(ij, kl)] = out[c * ND + d];
+      }
+  } else {
+    constexpr bool kUhf = MODE == kJkUhf;
+    const double *DJ = kUhf ? cl.Dt : cl.Da;
+    const double s = (bdiag ? 0.5 : 1.0) * (kdiag ? 0.5 : 1.0) * (same ? 0.5 : 1.0);
+    double jab = 0.0;
+    if (active) {
+      const double dij = 2.0 * s * __ldg(&DJ[I * n + J]);
+      double kac[NC], kbc[NC], kad[ND], kbd[ND];
+      double kac2[kUhf ? NC : 1], kbc2[kUhf ? NC : 1], kad2[kUhf ? ND : 1], kbd2[kUhf ? ND : 1];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) kac[c] = kbc[c] = 0.0;
+#pragma unroll
+      for (int d = 0; d < ND; ++d) kad[d] = kbd[d] = 0.0;
+      if constexpr (kUhf) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) kac2[c] = kbc2[c] = 0.0;
+#pragma unroll
+        for (int d = 0; d < ND; ++d) kad2[d] = kbd2[d] = 0.0;
+      }
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+          const int K = aoc + c, L = aod + d;
+          const double val = s * out[c * ND + d];
+          jab += 2.0 * val * __ldg(&DJ[K * n + L]);
+          atomicAdd(&cl.J[K * n + L], dij * out[c * ND + d]);
+          kac[c] += val * __ldg(&cl.Da[J * n + L]);
+          kad[d] += val * __ldg(&cl.Da[J * n + K]);
+          kbc[c] += val * __ldg(&cl.Da[I * n + L]);
+          kbd[d] += val * __ldg(&cl.Da[I * n + K]);
+          if constexpr (kUhf) {
+            kac2[c] += val * __ldg(&cl.Db[J * n + L]);
+            kad2[d] += val * __ldg(&cl.Db[J * n + K]);
+            kbc2[c] += val * __ldg(&cl.Db[I * n + L]);
+            kbd2[d] += val * __ldg(&cl.Db[I * n + K]);
+          }
+        }
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        atomicAdd(&cl.Ka[I * n + aoc + c], kac[c]);
+        atomicAdd(&cl.Ka[J * n + aoc + c], kbc[c]);
+        if constexpr (kUhf) {
+          atomicAdd(&cl.Kb[I * n + aoc + c], kac2[c]);
+          atomicAdd(&cl.Kb[J * n + aoc + c], kbc2[c]);
+        }
+      }
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        atomicAdd(&cl.Ka[I * n + aod + d], kad[d]);
+        atomicAdd(&cl.Ka[J * n + aod + d], kbd[d]);
+        if constexpr (kUhf) {
+          atomicAdd(&cl.Kb[I * n + aod + d], kad2[d]);
+          atomicAdd(&cl.Kb[J * n + aod + d], kbd2[d]);
+        }
+      }
+    }
+    // the warp's 32 quartets share the bra pair and this (a b) row
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) jab += __shfl_xor_sync(0xffffffffu, jab, o);
+    if (lane == 0) atomicAdd(&cl.J[I * n + J], jab);
+  }
+}
+
+}  // namespace hfg

@@ -357,8 +357,257 @@ def emit_launchers(out_dir):
         fh.write("\n".join(lines))
 
 
+# ---------------------------------------------------------------------------
+# Row-wise horizontal recursion for the split (primitive kernel + HRR/digest
+# kernel) path of the large classes.  The HRR is linear, so (a b| expands to
+# a short sum over (e| with polynomial coefficients in A-B:
+#   (a, b) = (a + 1_i, b - 1_i) + AB_i (a, b - 1_i)
+# For one bra row (a, b) this gives <= 4 terms per ket column f; the ket
+# recursion expands the same way in C-D.
+# ---------------------------------------------------------------------------
+def poly_mul_x(p, i):
+    out = {}
+    for mono, c in p.items():
+        m = list(mono)
+        m[i] += 1
+        out[tuple(m)] = out.get(tuple(m), 0) + c
+    return out
+
+
+def poly_add(p, q):
+    out = dict(p)
+    for mono, c in q.items():
+        out[mono] = out.get(mono, 0) + c
+    return {m: c for m, c in out.items() if c != 0}
+
+
+def hrr_expansion(a, b, memo=None):
+    """{e: poly} with (a b| = sum_e poly(X) (e 0|, e on the first centre."""
+    if memo is None:
+        memo = {}
+    key = (a, b)
+    if key in memo:
+        return memo[key]
+    if tot(b) == 0:
+        r = {a: {(0, 0, 0): 1}}
+    else:
+        i = direction(b)
+        b1 = add(b, i, -1)
+        r = {}
+        for e, p in hrr_expansion(add(a, i, 1), b1, memo).items():
+            r[e] = poly_add(r.get(e, {}), p)
+        for e, p in hrr_expansion(a, b1, memo).items():
+            r[e] = poly_add(r.get(e, {}), poly_mul_x(p, i))
+    memo[key] = r
+    return r
+
+
+def poly_expr(p, var):
+    """C expression of a polynomial in var0..var2 (monomials precomputed as
+    {var}_{k0}{k1}{k2})."""
+    terms = []
+    for mono, c in sorted(p.items()):
+        name = None if mono == (0, 0, 0) else f"{var}_{mono[0]}{mono[1]}{mono[2]}"
+        if name is None:
+            terms.append(f"R({c})")
+        elif c == 1:
+            terms.append(name)
+        else:
+            terms.append(f"R({c}) * {name}")
+    return " + ".join(terms) if terms else "R(0)"
+
+
+def monomials(maxdeg):
+    out = []
+    for d in range(1, maxdeg + 1):
+        for k0 in range(d, -1, -1):
+            for k1 in range(d - k0, -1, -1):
+                out.append((k0, k1, d - k0 - k1))
+    return out
+
+
+def emit_monomials(var, maxdeg):
+    lines = []
+    for m in monomials(maxdeg):
+        name = f"{var}_{m[0]}{m[1]}{m[2]}"
+        i = 0 if m[0] else (1 if m[1] else 2)
+        lower = list(m)
+        lower[i] -= 1
+        if sum(lower) == 0:
+            lines.append(f"const R {name} = {var}{i};")
+        else:
+            lines.append(f"const R {name} = {var}_{lower[0]}{lower[1]}{lower[2]} * {var}{i};")
+    return lines
+
+
+def hrr_row_code(la, lb, lc, ld):
+    """One bra row (a b | c d), all c d, from the contracted [e0|f0] block
+    stored column-major in scratch: acc(e, f) = scr[(e * NF + f) * stride]."""
+    E = comps_range(la, la + lb)
+    Fc = comps_range(lc, lc + ld)
+    eidx = {c: i for i, c in enumerate(E)}
+    fidx = {c: i for i, c in enumerate(Fc)}
+    NF = len(Fc)
+    A, B, C, D = comps(la), comps(lb), comps(lc), comps(ld)
+    lines = emit_monomials("X", lb) + emit_monomials("Y", ld)
+    lines.append("R vf[%d];" % NF)
+    lines.append("switch (ab) {")
+    memo = {}
+    for ia, a in enumerate(A):
+        for ib, b in enumerate(B):
+            lines.append(f"  case {ia * len(B) + ib}: {{")
+            ex = hrr_expansion(a, b, memo)
+            for jf in range(NF):
+                terms = [f"({poly_expr(p, 'X')}) * R(scr[({eidx[e]} * {NF} + {jf}) * stride])"
+                         for e, p in sorted(ex.items(), key=lambda kv: eidx[kv[0]])]
+                lines.append(f"    vf[{jf}] = " + " + ".join(terms) + ";")
+            lines.append("  } break;")
+    lines.append("  default: break;")
+    lines.append("}")
+    memo2 = {}
+    k = 0
+    for c in C:
+        for d in D:
+            ex = hrr_expansion(c, d, memo2)
+            terms = [f"({poly_expr(p, 'Y')}) * vf[{fidx[f]}]" for f, p in sorted(ex.items(), key=lambda kv: fidx[kv[0]])]
+            lines.append(f"out[{k}] = " + " + ".join(terms) + ";")
+            k += 1
+    return lines
+
+
+def hrr_col_code(la, lb, lc, ld):
+    """One ket column (c d | a b), all c d, of a block stored with bra (c d)
+    (components C, D, HRR variable X) and ket (a b) (variable Y); `ab`
+    selects the ket pair.  Used for the reference convention's swapped
+    (dd|dd) orientation."""
+    E = comps_range(la, la + lb)
+    Fc = comps_range(lc, lc + ld)
+    eidx = {c: i for i, c in enumerate(E)}
+    fidx = {c: i for i, c in enumerate(Fc)}
+    NF = len(Fc)
+    A, B, C, D = comps(la), comps(lb), comps(lc), comps(ld)
+    lines = emit_monomials("X", lb) + emit_monomials("Y", ld)
+    lines.append("R we[%d];" % len(E))
+    lines.append("switch (ab) {")
+    memo = {}
+    for ic, c in enumerate(C):
+        for id_, d in enumerate(D):
+            lines.append(f"  case {ic * len(D) + id_}: {{")
+            ex = hrr_expansion(c, d, memo)
+            for ie in range(len(E)):
+                terms = [f"({poly_expr(p, 'Y')}) * R(scr[({ie} * {NF} + {fidx[f]}) * stride])"
+                         for f, p in sorted(ex.items(), key=lambda kv: fidx[kv[0]])]
+                lines.append(f"    we[{ie}] = " + " + ".join(terms) + ";")
+            lines.append("  } break;")
+    lines.append("  default: break;")
+    lines.append("}")
+    memo2 = {}
+    k = 0
+    for a in A:
+        for b in B:
+            ex = hrr_expansion(a, b, memo2)
+            terms = [f"({poly_expr(p, 'X')}) * we[{eidx[e]}]" for e, p in sorted(ex.items(), key=lambda kv: eidx[kv[0]])]
+            lines.append(f"out[{k}] = " + " + ".join(terms) + ";")
+            k += 1
+    return lines
+
+
+def is_split_class(la, lb, lc, ld):
+    n = lambda L: (L + 1) * (L + 2) // 2
+    return n(la) * n(lb) * n(lc) * n(ld) > 81
+
+
+def emit_split(out_dir):
+    """eri_split_gen.cuh (row/column HRR functions of the split classes),
+    one launcher TU per split class, and the split dispatch table."""
+    pairs, quartets = canonical_classes()
+    hdr = ["// Generated by gen_eri.py -- do not edit.", "#pragma once", ""]
+    for (la, lb, lc, ld) in quartets:
+        if not is_split_class(la, lb, lc, ld):
+            continue
+        tag = f"{la}{lb}{lc}{ld}"
+        hdr.append(f"// ({la}{lb}|{lc}{ld}): bra row `ab` of the block, all ket (c d)")
+        hdr.append(f"template <class R> __device__ __forceinline__ void eri_hrr_row_{tag}(R* __restrict__ out, int ab,")
+        hdr.append("    const double* __restrict__ scr, long long stride, R X0, R X1, R X2, R Y0, R Y1, R Y2) {")
+        hdr += ["  " + l for l in hrr_row_code(la, lb, lc, ld)]
+        hdr.append("}")
+        if (la, lb, lc, ld) == (2, 2, 2, 2):
+            hdr.append(f"// ({la}{lb}|{lc}{ld}): ket column `ab` of a block stored with bra/ket exchanged")
+            hdr.append(f"template <class R> __device__ __forceinline__ void eri_hrr_col_{tag}(R* __restrict__ out, int ab,")
+            hdr.append("    const double* __restrict__ scr, long long stride, R X0, R X1, R X2, R Y0, R Y1, R Y2) {")
+            hdr += ["  " + l for l in hrr_col_code(la, lb, lc, ld)]
+            hdr.append("}")
+        hdr.append("")
+    hdr.append("template <int LA, int LB, int LC, int LD> struct EriRows;")
+    for (la, lb, lc, ld) in quartets:
+        if not is_split_class(la, lb, lc, ld):
+            continue
+        tag = f"{la}{lb}{lc}{ld}"
+        hdr.append(f"template <> struct EriRows<{la}, {lb}, {lc}, {ld}> {{")
+        hdr.append("  template <class R> static __device__ __forceinline__ void row(R* out, int ab, const double* scr,")
+        hdr.append("      long long stride, R X0, R X1, R X2, R Y0, R Y1, R Y2) {")
+        hdr.append(f"    eri_hrr_row_{tag}<R>(out, ab, scr, stride, X0, X1, X2, Y0, Y1, Y2);")
+        hdr.append("  }")
+        hdr.append("  template <class R> static __device__ __forceinline__ void col(R* out, int ab, const double* scr,")
+        hdr.append("      long long stride, R X0, R X1, R X2, R Y0, R Y1, R Y2) {")
+        if (la, lb, lc, ld) == (2, 2, 2, 2):
+            hdr.append(f"    eri_hrr_col_{tag}<R>(out, ab, scr, stride, X0, X1, X2, Y0, Y1, Y2);")
+        hdr.append("  }")
+        hdr.append("};")
+    with open(os.path.join(out_dir, "eri_split_gen.cuh"), "w") as fh:
+        fh.write("\n".join(hdr) + "\n")
+    modes = ("kStorePacked", "kJkRhf", "kJkUhf")
+    for (a, b, c, d) in quartets:
+        if not is_split_class(a, b, c, d):
+            continue
+        ref = (c + d) >= a + 2
+        lines = [f"// Generated by gen_eri.py: split-path launchers for the ({a}{b}|{c}{d}) class.",
+                 '#include "eri_split.cuh"', "", "namespace hfg {", "",
+                 f"void launch_split_{a}{b}{c}{d}(const EngineView &v, const ClassLaunch &cl, const SplitChunk &ch, int mode,",
+                 "                        bool ref, cudaStream_t s) {",
+                 "  const int slots = ch.ntasks * 32;",
+                 "  const int gridA = (slots + kThreads - 1) / kThreads;",
+                 f"  const dim3 gridB((slots + kThreads - 1) / kThreads, {((a + 1) * (a + 2) // 2) * ((b + 1) * (b + 2) // 2)});"]
+        if ref:
+            lines.append(f"  if (ref) eri_prim_split_kernel<{a}, {b}, {c}, {d}, true><<<gridA, kThreads, 0, s>>>(v, cl, ch);")
+            lines.append(f"  else eri_prim_split_kernel<{a}, {b}, {c}, {d}, false><<<gridA, kThreads, 0, s>>>(v, cl, ch);")
+        else:
+            lines.append(f"  eri_prim_split_kernel<{a}, {b}, {c}, {d}, false><<<gridA, kThreads, 0, s>>>(v, cl, ch);")
+        lines.append("  switch (mode) {")
+        for mode in modes:
+            lines.append(f"    case {mode}:")
+            k = f"eri_hrr_digest_kernel<{a}, {b}, {c}, {d}, {mode}"
+            if ref:
+                lines.append(f"      if (ref) {k}, true><<<gridB, kThreads, 0, s>>>(v, cl, ch);")
+                lines.append(f"      else {k}, false><<<gridB, kThreads, 0, s>>>(v, cl, ch);")
+            else:
+                lines.append(f"      {k}, false><<<gridB, kThreads, 0, s>>>(v, cl, ch);")
+            lines.append("      break;")
+        lines += ["    default:", "      break;", "  }"]
+        if not ref:
+            lines.append("  (void)ref;")
+        lines += ["}", "", "}  // namespace hfg", ""]
+        with open(os.path.join(out_dir, f"eri_split_{a}{b}{c}{d}.cu"), "w") as fh:
+            fh.write("\n".join(lines))
+    lines = ["// Generated by gen_eri.py: split-path launcher table.", "#pragma once", '#include "hfg_internal.cuh"', "",
+             "namespace hfg {", "",
+             "using SplitLauncher = void (*)(const EngineView &, const ClassLaunch &, const SplitChunk &, int, bool, cudaStream_t);"]
+    for (a, b, c, d) in quartets:
+        if is_split_class(a, b, c, d):
+            lines.append(f"void launch_split_{a}{b}{c}{d}(const EngineView &v, const ClassLaunch &cl, const SplitChunk &ch, int mode, bool ref, cudaStream_t s);")
+    lines.append("")
+    lines.append("// split launcher per class (same order as kClasses), nullptr for fused-only classes")
+    lines.append("static const SplitLauncher kSplit[] = {")
+    for (a, b, c, d) in quartets:
+        lines.append(f"    {'launch_split_%d%d%d%d' % (a, b, c, d) if is_split_class(a, b, c, d) else 'nullptr'},")
+    lines += ["};", "", "}  // namespace hfg", ""]
+    with open(os.path.join(out_dir, "eri_split_dispatch.cuh"), "w") as fh:
+        fh.write("\n".join(lines))
+
+
 if __name__ == "__main__":
     here = os.path.dirname(os.path.abspath(__file__))
     out_dir = sys.argv[1] if len(sys.argv) > 1 else here
     main(os.path.join(out_dir, "eri_gen.cuh"))
     emit_launchers(out_dir)
+    emit_split(out_dir)

@@ -13,6 +13,7 @@ constexpr double kBoysStep = 0.05;            // grid spacing in T
 constexpr double kBoysTmax = 36.0;            // above: asymptotic F_0 + upward recursion
 constexpr int kBoysGrid = 721;                // 36 / 0.05 + 1 grid points
 constexpr int kBoysOrders = kMaxLtot + kBoysTaylor;  // orders 0 .. 14 tabulated
+constexpr int kBoysRow = kBoysTaylor + 1;             // staged row: 7 Taylor terms + exp(-T_i)
 
 constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = 32 * kWarpsPerBlock;
@@ -45,17 +46,17 @@ struct EngineView {
   int reference_convention;   // 1: reproduce the reference's (dd|dd) ET rows
 };
 
-// One unit of work: a bra pair position in the class's bra list and the
-// first ket position of a 32-wide ket chunk.
+// One unit of work: a bra pair position in the class's pair list and a
+// range of at most 32 ket positions (kets of one primitive-count bucket).
 struct Task {
   int bra_pos;
   int ket_start;
+  int ket_end;
 };
 
 struct ClassLaunch {
   const int *bra_list;   // pair indices of the bra class, sorted by Q desc
   const int *ket_list;   // pair indices of the ket class, sorted by Q desc
-  const int *ket_count;  // valid kets per bra position
   const Task *tasks;
   int ntasks;
   int same_class;        // bra class == ket class
@@ -67,6 +68,16 @@ struct ClassLaunch {
   double *J, *Ka, *Kb;   // accumulators (n x n)
   double *Qout;          // kSchwarz: per pair
   int *fp32_counter;     // unused in FP64 kernels
+};
+
+// One chunk of a split-path class launch (see eri_split.cuh): scratch for
+// the contracted [e0|f0] blocks of `ntasks` tasks starting at `task0`.
+struct SplitChunk {
+  double *scr_fwd;   // [kAcc][slots]: block with bra = task's bra pair
+  double *scr_rev;   // [kAcc][slots]: reference-convention (dd|dd) only, bra = ket pair
+  long long stride;  // slots in the chunk (ntasks * 32)
+  int task0;         // first task of the chunk
+  int ntasks;
 };
 
 // component normalisation f(l,m,n) = 1/sqrt((2l-1)!!(2m-1)!!(2n-1)!!) in the
@@ -93,8 +104,10 @@ __device__ __forceinline__ long long tri(long long a, long long b) {
 
 // Boys function F_0..F_M at T.  Below kBoysTmax: 7-term Taylor expansion of
 // F_M about the nearest grid point, F_M(T) = sum_k F_{M+k}(T_i) (-dT)^k / k!,
-// from the shared-memory slice tab[i][k] = F_{M+k}(T_i)/k!, then the downward
-// recursion F_m = (2T F_{m+1} + e^-T) / (2m+1) (BoysFunctions.cpp:17-20).
+// from the shared-memory slice tab[i][k] = F_{M+k}(T_i)/k! (k < 7), then the
+// downward recursion F_m = (2T F_{m+1} + e^-T) / (2m+1) (BoysFunctions.cpp:17-20)
+// with e^-T = e^-T_i * e^(T_i - T), tab[i][7] = e^-T_i and the second factor
+// from its 8-term Taylor series (|T_i - T| <= 0.025: truncation < 4e-18).
 // Above: F_0 = sqrt(pi/T)/2 (erfc(sqrt T) < 3e-17 there) and the upward
 // recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T).  The scale folds the
 // quartet prefactor into every order.
@@ -103,14 +116,22 @@ __device__ __forceinline__ void boys_eval(R *F, double T, double scale, const do
   if (T < kBoysTmax) {
     const int i = __double2int_rn(T * (1.0 / kBoysStep));
     const double dt = i * kBoysStep - T;  // -(T - T_i)
-    const double *t = tab + i * kBoysTaylor;
+    const double *t = tab + i * kBoysRow;
     double f = t[6];
 #pragma unroll
     for (int k = 5; k >= 0; --k) f = fma(f, dt, t[k]);
     double fm[M + 1];
     fm[M] = f;
     if (M > 0) {
-      const double e = exp(-T);
+      double x = 1.0 / 5040.0;
+      x = fma(x, dt, 1.0 / 720.0);
+      x = fma(x, dt, 1.0 / 120.0);
+      x = fma(x, dt, 1.0 / 24.0);
+      x = fma(x, dt, 1.0 / 6.0);
+      x = fma(x, dt, 0.5);
+      x = fma(x, dt, 1.0);
+      x = fma(x, dt, 1.0);
+      const double e = t[7] * x;
       const double t2 = 2.0 * T;
 #pragma unroll
       for (int m = M - 1; m >= 0; --m) fm[m] = fma(t2, fm[m + 1], e) * (1.0 / (2 * m + 1));
