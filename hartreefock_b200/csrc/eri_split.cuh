@@ -76,139 +76,172 @@ __global__ void __launch_bounds__(kThreads) eri_prim_split_kernel(const EngineVi
   }
 }
 
+// One block per task (32 quartets sharing the bra pair); warp w of the block
+// expands rows ab = w, w + 4, ... of all 32 quartets.  The J_cd partials of a
+// quartet accumulate in registers across a warp's rows and across the
+// block's warps in shared memory before one atomic per element; J_ab reduces
+// across the warp; the K partials go out per row.
 template <int LA, int LB, int LC, int LD, int MODE, bool REF>
 __global__ void __launch_bounds__(kThreads) eri_hrr_digest_kernel(const EngineView v, const ClassLaunch cl,
                                                                   const SplitChunk ch) {
-  constexpr int NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+  constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+  constexpr int NAB = NA * NB, NCD = NC * ND;
   constexpr bool kOrient = REF && LA == 2 && LB == 2 && LC == 2 && LD == 2;
-  const int ab = blockIdx.y;
-  const int a = ab / NB, b = ab - a * NB;
-  const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (slot >= (long long)ch.ntasks * 32) return;  // whole warps: slots come in tasks of 32
-  const int lane = threadIdx.x & 31;
-  const Task task = cl.tasks[ch.task0 + (int)(slot >> 5)];
+  constexpr bool kJk = MODE != kStorePacked;
+  constexpr bool kUhf = MODE == kJkUhf;
+  __shared__ double jcd_sh[kJk ? kWarpsPerBlock * 32 * NCD : 1];
+  const int tloc = blockIdx.x;
+  if (tloc >= ch.ntasks) return;  // whole block
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long slot = (long long)tloc * 32 + lane;
+  const Task task = cl.tasks[ch.task0 + tloc];
   const int kpos = task.ket_start + lane;
   const bool active = kpos < task.ket_end;
   const int bp = cl.bra_list[task.bra_pos];
   const int kp = active ? cl.ket_list[kpos] : bp;
   const int n = v.nbf;
-
-  double out[NC * ND];
-#pragma unroll
-  for (int x = 0; x < NC * ND; ++x) out[x] = 0.0;
   const double X0 = v.pair_AB[3 * bp], X1 = v.pair_AB[3 * bp + 1], X2 = v.pair_AB[3 * bp + 2];
   const double Y0 = v.pair_AB[3 * kp], Y1 = v.pair_AB[3 * kp + 1], Y2 = v.pair_AB[3 * kp + 2];
   const int aoa = v.pair_ao_a[bp], aob = v.pair_ao_b[bp], aoc = v.pair_ao_a[kp], aod = v.pair_ao_b[kp];
   const bool bdiag = v.pair_sa[bp] == v.pair_sb[bp], kdiag = v.pair_sa[kp] == v.pair_sb[kp];
-  if (active) {
-    if constexpr (kOrient) {
-      const int sab = v.pair_sa[bp], skt = v.pair_sa[kp];
-      if (sab > skt) {
-        EriRows<LA, LB, LC, LD>::template row<double>(out, ab, ch.scr_fwd + slot, ch.stride, X0, X1, X2, Y0, Y1, Y2);
-      } else if (sab < skt) {
-        EriRows<LA, LB, LC, LD>::template col<double>(out, ab, ch.scr_rev + slot, ch.stride, Y0, Y1, Y2, X0, X1, X2);
+  const bool same = bp == kp;
+  const double s = (bdiag ? 0.5 : 1.0) * (kdiag ? 0.5 : 1.0) * (same ? 0.5 : 1.0);
+  const double *DJ = kUhf ? cl.Dt : cl.Da;
+
+  double jcd[kJk ? NCD : 1];
+#pragma unroll
+  for (int x = 0; x < (kJk ? NCD : 1); ++x) jcd[x] = 0.0;
+
+  for (int ab = warp; ab < NAB; ab += kWarpsPerBlock) {
+    const int a = ab / NB, b = ab - a * NB;
+    const int I = aoa + a, J = aob + b;
+    double out[NCD];
+#pragma unroll
+    for (int x = 0; x < NCD; ++x) out[x] = 0.0;
+    if (active) {
+      if constexpr (kOrient) {
+        const int sab = v.pair_sa[bp], skt = v.pair_sa[kp];
+        if (sab > skt) {
+          EriRows<LA, LB, LC, LD>::template row<double>(out, ab, ch.scr_fwd + slot, ch.stride, X0, X1, X2, Y0, Y1,
+                                                        Y2);
+        } else if (sab < skt) {
+          EriRows<LA, LB, LC, LD>::template col<double>(out, ab, ch.scr_rev + slot, ch.stride, Y0, Y1, Y2, X0, X1,
+                                                        X2);
+        } else {
+          double sw[NCD];
+          EriRows<LA, LB, LC, LD>::template row<double>(out, ab, ch.scr_fwd + slot, ch.stride, X0, X1, X2, Y0, Y1,
+                                                        Y2);
+          EriRows<LA, LB, LC, LD>::template col<double>(sw, ab, ch.scr_rev + slot, ch.stride, Y0, Y1, Y2, X0, X1,
+                                                        X2);
+          const int o1 = bdiag ? max(I, J) : I, o2 = bdiag ? min(I, J) : J;
+#pragma unroll
+          for (int c = 0; c < NC; ++c)
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+              const int K = aoc + c, L = aod + d;
+              const int o3 = kdiag ? max(K, L) : K, o4 = kdiag ? min(K, L) : L;
+              if (!(o1 > o3 || (o1 == o3 && o2 >= o4))) out[c * ND + d] = sw[c * ND + d];
+            }
+        }
       } else {
-        double sw[NC * ND];
         EriRows<LA, LB, LC, LD>::template row<double>(out, ab, ch.scr_fwd + slot, ch.stride, X0, X1, X2, Y0, Y1, Y2);
-        EriRows<LA, LB, LC, LD>::template col<double>(sw, ab, ch.scr_rev + slot, ch.stride, Y0, Y1, Y2, X0, X1, X2);
-        const int I = aoa + a, J = aob + b;
-        const int o1 = bdiag ? max(I, J) : I, o2 = bdiag ? min(I, J) : J;
+      }
+      const double nab = comp_norm<LA>(a) * comp_norm<LB>(b);
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+#pragma unroll
+        for (int d = 0; d < ND; ++d) out[c * ND + d] *= nab * comp_norm<LC>(c) * comp_norm<LD>(d);
+    }
+
+    if constexpr (!kJk) {
+      if (active && !(bdiag && I < J)) {
+        const long long ij = tri(I, J);
 #pragma unroll
         for (int c = 0; c < NC; ++c)
 #pragma unroll
           for (int d = 0; d < ND; ++d) {
             const int K = aoc + c, L = aod + d;
-            const int o3 = kdiag ? max(K, L) : K, o4 = kdiag ? min(K, L) : L;
-            if (!(o1 > o3 || (o1 == o3 && o2 >= o4))) out[c * ND + d] = sw[c * ND + d];
+            if (kdiag && K < L) continue;
+            const long long kl = tri(K, L);
+            if (same && ij < kl) continue;
+            cl.packed[tri(ij, kl)] = out[c * ND + d];
           }
       }
     } else {
-      EriRows<LA, LB, LC, LD>::template row<double>(out, ab, ch.scr_fwd + slot, ch.stride, X0, X1, X2, Y0, Y1, Y2);
-    }
-    const double nab = comp_norm<LA>(a) * comp_norm<LB>(b);
+      double jab = 0.0;
+      if (active) {
+        const double dij = 2.0 * s * __ldg(&DJ[I * n + J]);
+        double kac[NC], kbc[NC], kad[ND], kbd[ND];
+        double kac2[kUhf ? NC : 1], kbc2[kUhf ? NC : 1], kad2[kUhf ? ND : 1], kbd2[kUhf ? ND : 1];
 #pragma unroll
-    for (int c = 0; c < NC; ++c)
+        for (int c = 0; c < NC; ++c) kac[c] = kbc[c] = 0.0;
 #pragma unroll
-      for (int d = 0; d < ND; ++d) out[c * ND + d] *= nab * comp_norm<LC>(c) * comp_norm<LD>(d);
-  }
-  const int I = aoa + a, J = aob + b;
-  const bool same = bp == kp;
-
-  if constexpr (MODE == kStorePacked) {
-    if (!active) return;
-    if (bdiag && I < J) return;
-    const long long ij = tri(I, J);
+        for (int d = 0; d < ND; ++d) kad[d] = kbd[d] = 0.0;
+        if constexpr (kUhf) {
 #pragma unroll
-    for (int c = 0; c < NC; ++c)
+          for (int c = 0; c < NC; ++c) kac2[c] = kbc2[c] = 0.0;
 #pragma unroll
-      for (int d = 0; d < ND; ++d) {
-        const int K = aoc + c, L = aod + d;
-        if (kdiag && K < L) continue;
-        const long long kl = tri(K, L);
-        if (same && ij < kl) continue;
-        cl.packed[tri(ij, kl)] = out[c * ND + d];
-      }
-  } else {
-    constexpr bool kUhf = MODE == kJkUhf;
-    const double *DJ = kUhf ? cl.Dt : cl.Da;
-    const double s = (bdiag ? 0.5 : 1.0) * (kdiag ? 0.5 : 1.0) * (same ? 0.5 : 1.0);
-    double jab = 0.0;
-    if (active) {
-      const double dij = 2.0 * s * __ldg(&DJ[I * n + J]);
-      double kac[NC], kbc[NC], kad[ND], kbd[ND];
-      double kac2[kUhf ? NC : 1], kbc2[kUhf ? NC : 1], kad2[kUhf ? ND : 1], kbd2[kUhf ? ND : 1];
+          for (int d = 0; d < ND; ++d) kad2[d] = kbd2[d] = 0.0;
+        }
 #pragma unroll
-      for (int c = 0; c < NC; ++c) kac[c] = kbc[c] = 0.0;
+        for (int c = 0; c < NC; ++c)
 #pragma unroll
-      for (int d = 0; d < ND; ++d) kad[d] = kbd[d] = 0.0;
-      if constexpr (kUhf) {
+          for (int d = 0; d < ND; ++d) {
+            const int K = aoc + c, L = aod + d;
+            const double val = s * out[c * ND + d];
+            jab += 2.0 * val * __ldg(&DJ[K * n + L]);
+            jcd[c * ND + d] += dij * out[c * ND + d];
+            kac[c] += val * __ldg(&cl.Da[J * n + L]);
+            kad[d] += val * __ldg(&cl.Da[J * n + K]);
+            kbc[c] += val * __ldg(&cl.Da[I * n + L]);
+            kbd[d] += val * __ldg(&cl.Da[I * n + K]);
+            if constexpr (kUhf) {
+              kac2[c] += val * __ldg(&cl.Db[J * n + L]);
+              kad2[d] += val * __ldg(&cl.Db[J * n + K]);
+              kbc2[c] += val * __ldg(&cl.Db[I * n + L]);
+              kbd2[d] += val * __ldg(&cl.Db[I * n + K]);
+            }
+          }
 #pragma unroll
-        for (int c = 0; c < NC; ++c) kac2[c] = kbc2[c] = 0.0;
-#pragma unroll
-        for (int d = 0; d < ND; ++d) kad2[d] = kbd2[d] = 0.0;
-      }
-#pragma unroll
-      for (int c = 0; c < NC; ++c)
-#pragma unroll
-        for (int d = 0; d < ND; ++d) {
-          const int K = aoc + c, L = aod + d;
-          const double val = s * out[c * ND + d];
-          jab += 2.0 * val * __ldg(&DJ[K * n + L]);
-          atomicAdd(&cl.J[K * n + L], dij * out[c * ND + d]);
-          kac[c] += val * __ldg(&cl.Da[J * n + L]);
-          kad[d] += val * __ldg(&cl.Da[J * n + K]);
-          kbc[c] += val * __ldg(&cl.Da[I * n + L]);
-          kbd[d] += val * __ldg(&cl.Da[I * n + K]);
+        for (int c = 0; c < NC; ++c) {
+          atomicAdd(&cl.Ka[I * n + aoc + c], kac[c]);
+          atomicAdd(&cl.Ka[J * n + aoc + c], kbc[c]);
           if constexpr (kUhf) {
-            kac2[c] += val * __ldg(&cl.Db[J * n + L]);
-            kad2[d] += val * __ldg(&cl.Db[J * n + K]);
-            kbc2[c] += val * __ldg(&cl.Db[I * n + L]);
-            kbd2[d] += val * __ldg(&cl.Db[I * n + K]);
+            atomicAdd(&cl.Kb[I * n + aoc + c], kac2[c]);
+            atomicAdd(&cl.Kb[J * n + aoc + c], kbc2[c]);
           }
         }
 #pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        atomicAdd(&cl.Ka[I * n + aoc + c], kac[c]);
-        atomicAdd(&cl.Ka[J * n + aoc + c], kbc[c]);
-        if constexpr (kUhf) {
-          atomicAdd(&cl.Kb[I * n + aoc + c], kac2[c]);
-          atomicAdd(&cl.Kb[J * n + aoc + c], kbc2[c]);
+        for (int d = 0; d < ND; ++d) {
+          atomicAdd(&cl.Ka[I * n + aod + d], kad[d]);
+          atomicAdd(&cl.Ka[J * n + aod + d], kbd[d]);
+          if constexpr (kUhf) {
+            atomicAdd(&cl.Kb[I * n + aod + d], kad2[d]);
+            atomicAdd(&cl.Kb[J * n + aod + d], kbd2[d]);
+          }
         }
       }
+      // the warp's 32 quartets share the bra pair and this (a b) row
 #pragma unroll
-      for (int d = 0; d < ND; ++d) {
-        atomicAdd(&cl.Ka[I * n + aod + d], kad[d]);
-        atomicAdd(&cl.Ka[J * n + aod + d], kbd[d]);
-        if constexpr (kUhf) {
-          atomicAdd(&cl.Kb[I * n + aod + d], kad2[d]);
-          atomicAdd(&cl.Kb[J * n + aod + d], kbd2[d]);
-        }
+      for (int o = 16; o > 0; o >>= 1) jab += __shfl_xor_sync(0xffffffffu, jab, o);
+      if (lane == 0) atomicAdd(&cl.J[I * n + J], jab);
+    }
+  }
+
+  if constexpr (kJk) {
+    // sum the J_cd partials of the block's warps, one atomic per element
+#pragma unroll
+    for (int x = 0; x < NCD; ++x) jcd_sh[(warp * NCD + x) * 32 + lane] = jcd[x];
+    __syncthreads();
+    if (active) {
+      for (int x = warp; x < NCD; x += kWarpsPerBlock) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < kWarpsPerBlock; ++w) t += jcd_sh[(w * NCD + x) * 32 + lane];
+        const int c = x / ND, d = x - c * ND;
+        atomicAdd(&cl.J[(aoc + c) * n + aod + d], t);
       }
     }
-    // the warp's 32 quartets share the bra pair and this (a b) row
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) jab += __shfl_xor_sync(0xffffffffu, jab, o);
-    if (lane == 0) atomicAdd(&cl.J[I * n + J], jab);
   }
 }
 

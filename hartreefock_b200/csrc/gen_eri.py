@@ -513,8 +513,11 @@ def hrr_col_code(la, lb, lc, ld):
 
 
 def is_split_class(la, lb, lc, ld):
+    """Classes whose fused kernel spills most: more than 150 integrals per
+    shell quartet.  Below that ((dp|ds), (dd|ps) at 108) the fused kernel's
+    single digestion beats the split path's per-row atomics."""
     n = lambda L: (L + 1) * (L + 2) // 2
-    return n(la) * n(lb) * n(lc) * n(ld) > 81
+    return n(la) * n(lb) * n(lc) * n(ld) > 150
 
 
 def emit_split(out_dir):
@@ -567,7 +570,7 @@ def emit_split(out_dir):
                  "                        bool ref, cudaStream_t s) {",
                  "  const int slots = ch.ntasks * 32;",
                  "  const int gridA = (slots + kThreads - 1) / kThreads;",
-                 f"  const dim3 gridB((slots + kThreads - 1) / kThreads, {((a + 1) * (a + 2) // 2) * ((b + 1) * (b + 2) // 2)});"]
+                 "  const int gridB = ch.ntasks;  // one block per task"]
         if ref:
             lines.append(f"  if (ref) eri_prim_split_kernel<{a}, {b}, {c}, {d}, true><<<gridA, kThreads, 0, s>>>(v, cl, ch);")
             lines.append(f"  else eri_prim_split_kernel<{a}, {b}, {c}, {d}, false><<<gridA, kThreads, 0, s>>>(v, cl, ch);")

@@ -3,6 +3,7 @@
 // Two-electron work goes to the GPU engine through the C ABI (hfgpu.h);
 // the symmetric eigen-decompositions go to cuSOLVER.
 #include <cuda_runtime.h>
+#include <cublas_v2.h>
 #include <cusolverDn.h>
 
 #include <algorithm>
@@ -90,9 +91,53 @@ std::string trim(const std::string &s) {
 // ===========================================================================
 namespace hfgpu {
 
+namespace {
+// cuBLAS handle and device buffers for the SCF's large matrix products
+struct Gemm {
+  cublasHandle_t h = nullptr;
+  double *dA = nullptr, *dB = nullptr, *dC = nullptr;
+  size_t capA = 0, capB = 0, capC = 0;
+  ~Gemm() {
+    if (h) cublasDestroy(h);
+    cudaFree(dA);
+    cudaFree(dB);
+    cudaFree(dC);
+  }
+};
+Gemm &gemm_state() {
+  static thread_local Gemm g;
+  return g;
+}
+void grow(double **p, size_t *cap, size_t need) {
+  if (need <= *cap) return;
+  cudaFree(*p);
+  *p = nullptr;
+  if (cudaMalloc(p, need * sizeof(double)) != cudaSuccess) throw std::runtime_error("cudaMalloc (gemm)");
+  *cap = need;
+}
+}  // namespace
+
 Matrix operator*(const Matrix &a, const Matrix &b) {
   Matrix m(a.rows(), b.cols());
   const int n = a.rows(), p = a.cols(), q = b.cols();
+  if ((double)n * p * q > 2.0e6) {
+    // FP64 DGEMM on the GPU; row-major C = A B is column-major C^T = B^T A^T
+    Gemm &g = gemm_state();
+    if (!g.h && cublasCreate(&g.h) != CUBLAS_STATUS_SUCCESS) throw std::runtime_error("cublasCreate");
+    grow(&g.dA, &g.capA, (size_t)n * p);
+    grow(&g.dB, &g.capB, (size_t)p * q);
+    grow(&g.dC, &g.capC, (size_t)n * q);
+    if (cudaMemcpy(g.dA, a.data(), sizeof(double) * n * p, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(g.dB, b.data(), sizeof(double) * p * q, cudaMemcpyHostToDevice) != cudaSuccess)
+      throw std::runtime_error("cudaMemcpy (gemm)");
+    const double one = 1.0, zero = 0.0;
+    if (cublasDgemm(g.h, CUBLAS_OP_N, CUBLAS_OP_N, q, n, p, &one, g.dB, q, g.dA, p, &zero, g.dC, q) !=
+        CUBLAS_STATUS_SUCCESS)
+      throw std::runtime_error("cublasDgemm");
+    if (cudaMemcpy(m.data(), g.dC, sizeof(double) * n * q, cudaMemcpyDeviceToHost) != cudaSuccess)
+      throw std::runtime_error("cudaMemcpy (gemm)");
+    return m;
+  }
   for (int i = 0; i < n; ++i)
     for (int k = 0; k < p; ++k) {
       const double aik = a(i, k);
