@@ -6,6 +6,15 @@ A step is one two-electron Fock build G[P] over every Schwarz-significant
 shell quartet (threshold 1e-12).  The metric is ERI quartets/s: 8-fold
 unique contracted function quartets evaluated per second.
 
+The same line carries "scf": complete RHF runs of (H2O)_32 / 6-31G* (608
+functions) through the C++ host API (the one-call driver, hfd_scf), once in
+the plain FP64 form (the reference's convergence thresholds) and once in the
+precision form (FP32 below a density-weighted bound of 1e-4, incremental
+builds from the density difference, two all-FP64 iterations at the end),
+with wall time, iterations, seconds per iteration, and the precision form's
+energy and density error against the FP64 run; plus the plain form stopped
+by the precision form's rule, for a comparison at equal criteria.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 With N > 1 (torchrun, one rank per GPU) every rank builds the same molecule's
@@ -119,6 +128,53 @@ def cpu_baseline(sample_per_thread: int, threads: int):
     return out
 
 
+SCF_WATERS = 32
+
+
+def scf_comparison(waters: int):
+    """Plain FP64 vs precision-form RHF of (H2O)_waters / 6-31G*, through the
+    one-call driver (C++ host API: device-resident SCF over the engine)."""
+    from hartreefock_b200 import molecules, scf
+    Z, xyz = molecules.water_cluster(waters, seed=SEED)
+    kw = dict(alpha=0.75, init_guess=0.75, post_diis=0, schwarz_threshold=THRESHOLD)
+    runs = {}
+    for name, extra in (("fp64", {}), ("mixed", {"mixed_cutoff": 1e-4}),
+                        ("fp64_same_criteria", {"stop_at_precision_test": True})):
+        t0 = time.perf_counter()
+        r = scf.run_scf(Z, xyz, BASIS, **kw, **extra)
+        wall = time.perf_counter() - t0
+        runs[name] = (wall, r)
+    ref_wall, ref = runs["fp64"]
+
+    def summary(name):
+        wall, r = runs[name]
+        out = {"wall_s": wall, "init_s": r["seconds_init"], "scf_s": r["seconds_total"],
+               "iterations": r["iterations"], "converged": r["converged"],
+               "s_per_iter": r["seconds_total"] / max(1, r["iterations"]), "energy": r["energy"],
+               "fock_s": r["fock_ms_total"] / 1e3, "eigen_s": r["seconds_eigen"], "diis_s": r["seconds_diis"],
+               "fock_builds": r["fock_builds"]}
+        if name != "fp64":
+            out["dE_vs_fp64"] = r["energy"] - ref["energy"]
+            out["max_dD_vs_fp64"] = float(np.abs(r["density"] - ref["density"]).max())
+        q = r["fp32_quartets"] + r["fp64_quartets"]
+        if r["fp32_quartets"]:
+            out["fp32_quartet_fraction"] = r["fp32_quartets"] / q
+            out["incremental_builds"] = r["mixed_steps"]
+        return out
+
+    return {
+        "workload": f"(H2O)_{waters} {BASIS} RHF, direct SCF, seed {SEED}; initGuess 0.75, alpha 0.75, DIIS 6/5, "
+                    "no post-DIIS steps",
+        "nbf": runs["fp64"][1]["nbf"],
+        "fp64": dict(summary("fp64"), criteria="reference: |dE|<=1e-11, rmsD<1e-10, DIIS error<1e-10"),
+        "mixed": dict(summary("mixed"), criteria="|dE|<1e-7 and rmsD<1e-7 in the incremental FP32/FP64 phase, "
+                                                 "then 2 full FP64 iterations"),
+        "fp64_same_criteria": dict(summary("fp64_same_criteria"), criteria="plain FP64 builds, the mixed run's rule"),
+        "speedup_wall": ref_wall / runs["mixed"][0],
+        "speedup_wall_same_criteria": runs["fp64_same_criteria"][0] / runs["mixed"][0],
+    }
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -157,6 +213,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--waters", type=int, default=16,
                     help="cluster size; the benchmark workload is 16 (smaller values size profiler captures)")
+    ap.add_argument("--scf-waters", type=int, default=SCF_WATERS, help="cluster of the SCF comparison (0: skip)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     WATERS = args.waters
@@ -262,6 +319,8 @@ def main():
                      "tflops": round(c["flops"] / max(c["ms"], 1e-9) / 1e9, 3)} for c in prof],
         "clocks": clocks.summary(),
     }
+    if rank == 0 and world == 1 and args.scf_waters > 0:
+        line["scf"] = scf_comparison(args.scf_waters)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = 1
         cb = cpu_baseline(args.ref_sample, threads)

@@ -119,15 +119,28 @@ struct hfg_ctx {
   int *d_pair_prim_off = nullptr, *d_pair_nprim = nullptr, *d_pair_sa = nullptr, *d_pair_sb = nullptr;
   int *d_pair_ao_a = nullptr, *d_pair_ao_b = nullptr;
   double *d_pair_AB = nullptr, *d_pair_Q = nullptr, *d_boys = nullptr;
-  float *d_pair_Dmax = nullptr;
   // work buffers
   double *d_J = nullptr, *d_Ka = nullptr, *d_Kb = nullptr, *d_P = nullptr, *d_Pb = nullptr, *d_Pt = nullptr;
   double *d_G = nullptr, *d_Gb = nullptr, *d_block = nullptr;
   double *d_scratch = nullptr;  // split-path [e0|f0] blocks
   size_t scratch_doubles = 0;
   size_t scratch_budget_bytes = size_t(512) << 20;
+  // precision form: density screening, FP32 cutoff, incremental history
+  int nshells = 0;
+  int *d_shell_ao = nullptr, *d_shell_nf = nullptr;
+  float *d_shell_dmax = nullptr;                 // [nshells][nshells]
+  unsigned long long *d_counters = nullptr;      // FP64 / FP32 quartets of the last build
+  double *d_prev_P[2] = {}, *d_prev_G[2] = {};   // incremental history (alpha, beta)
+  double *d_dP[2] = {};                          // density difference of the build
+  bool inc_valid = false, inc_uhf = false;
+  double mixed_cutoff = 0;
+  bool counted = false;                          // d_counters hold the last build's counts
   hfg_stats stats{};
   bool profiling = false;
+  bool precision_form() const { return opts.density_screening || opts.incremental || mixed_cutoff > 0; }
+  double density_threshold() const {
+    return opts.density_threshold > 0 ? opts.density_threshold : opts.schwarz_threshold;
+  }
   EngineView view() const {
     EngineView v{};
     v.prim = d_prim;
@@ -139,7 +152,8 @@ struct hfg_ctx {
     v.pair_ao_b = d_pair_ao_b;
     v.pair_AB = d_pair_AB;
     v.pair_Q = d_pair_Q;
-    v.pair_Dmax = d_pair_Dmax;
+    v.shell_dmax = d_shell_dmax;
+    v.nshells = nshells;
     v.boys_table = d_boys;
     v.nbf = nbf;
     v.reference_convention = opts.eri_convention == HFG_ERI_REFERENCE;
@@ -153,9 +167,11 @@ struct hfg_ctx {
       if (q.ev_b) cudaEventDestroy(q.ev_b);
     }
     for (auto &p : pclass) cudaFree(p.d_pairs);
-    void *bufs[] = {d_prim, d_pair_prim_off, d_pair_nprim, d_pair_sa, d_pair_sb, d_pair_ao_a, d_pair_ao_b,
-                    d_pair_AB, d_pair_Q, d_boys, d_pair_Dmax, d_J, d_Ka, d_Kb, d_P, d_Pb, d_Pt, d_G, d_Gb, d_block,
-                    d_scratch};
+    void *bufs[] = {d_prim,       d_pair_prim_off, d_pair_nprim, d_pair_sa,  d_pair_sb,    d_pair_ao_a, d_pair_ao_b,
+                    d_pair_AB,    d_pair_Q,        d_boys,       d_J,        d_Ka,         d_Kb,        d_P,
+                    d_Pb,         d_Pt,            d_G,          d_Gb,       d_block,      d_scratch,   d_shell_ao,
+                    d_shell_nf,   d_shell_dmax,    d_counters,   d_prev_P[0], d_prev_P[1], d_prev_G[0], d_prev_G[1],
+                    d_dP[0],      d_dP[1]};
     for (void *b : bufs) cudaFree(b);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -276,8 +292,11 @@ static hfg_status upload_classes(hfg_ctx *c) {
   return HFG_OK;
 }
 
-static int grid_for(const hfg_ctx *c, int ntasks) {
-  const int blocks = (ntasks + kWarpsPerBlock - 1) / kWarpsPerBlock;
+// blocks of a fused class launch: one warp per task, fused_warps() per block
+static int grid_for(const hfg_ctx *c, int ntasks, int cls) {
+  const ClassEntry &e = kClasses[cls];
+  const int w = fused_warps(e.la, e.lb, e.lc, e.ld);
+  const int blocks = (ntasks + w - 1) / w;
   return std::max(1, std::min(blocks, c->num_sms * 16));
 }
 
@@ -313,6 +332,58 @@ __global__ void add_densities(const double *a, const double *b, double *t, int n
   for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < nn; x += gridDim.x * blockDim.x) t[x] = a[x] + b[x];
 }
 
+// Incremental builds: dP = P - P_prev (P_prev taken as 0 when `fresh`), then
+// P_prev = P.
+__global__ void density_difference(const double *P, double *prev, double *dP, int nn, int fresh) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < nn; x += gridDim.x * blockDim.x) {
+    const double p = P[x];
+    dP[x] = fresh ? p : p - prev[x];
+    prev[x] = p;
+  }
+}
+
+// max |A| (+ |B| when B is given) over each shell block, thread per block
+__global__ void shell_block_max(const double *A, const double *B, const int *ao, const int *nf, int ns, int n,
+                                float *out) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < ns * ns; x += gridDim.x * blockDim.x) {
+    const int sa = x / ns, sb = x - sa * ns;
+    const int i0 = ao[sa], j0 = ao[sb], ni = nf[sa], nj = nf[sb];
+    double m = 0.0;
+    for (int i = i0; i < i0 + ni; ++i)
+      for (int j = j0; j < j0 + nj; ++j) {
+        const double a = fabs(A[(size_t)i * n + j]) + (B ? fabs(B[(size_t)i * n + j]) : 0.0);
+        m = fmax(m, a);
+      }
+    // round up so that the float bound never undercuts the double one
+    out[x] = __double2float_ru(m);
+  }
+}
+
+// G = (accumulate ? G_prev : 0) + (J + J^T) - (K + K^T)/2, G_prev = G
+__global__ void finalize_rhf_incremental(const double *J, const double *K, double *Gprev, double *G, int n,
+                                         int accumulate) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n * n; x += gridDim.x * blockDim.x) {
+    const int i = x / n, j = x - i * n;
+    const double g = (accumulate ? Gprev[x] : 0.0) + (J[i * n + j] + J[j * n + i]) - 0.5 * (K[i * n + j] + K[j * n + i]);
+    G[x] = g;
+    Gprev[x] = g;
+  }
+}
+
+__global__ void finalize_uhf_incremental(const double *J, const double *Ka, const double *Kb, double *Gaprev,
+                                         double *Gbprev, double *Ga, double *Gb, int n, int accumulate) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n * n; x += gridDim.x * blockDim.x) {
+    const int i = x / n, j = x - i * n;
+    const double jv = J[i * n + j] + J[j * n + i];
+    const double ga = (accumulate ? Gaprev[x] : 0.0) + jv - (Ka[i * n + j] + Ka[j * n + i]);
+    const double gb = (accumulate ? Gbprev[x] : 0.0) + jv - (Kb[i * n + j] + Kb[j * n + i]);
+    Ga[x] = ga;
+    Gb[x] = gb;
+    Gaprev[x] = ga;
+    Gbprev[x] = gb;
+  }
+}
+
 static hfg_status ensure(double **p, size_t count) {
   if (*p) return HFG_OK;
   HFG_CUDA(cudaMalloc((void **)p, count * sizeof(double)));
@@ -328,12 +399,14 @@ static int ncomp_range(int lo, int hi) {
   return s;
 }
 
+// `prec`: 0 plain FP64, 1 density-screened FP64, 2 density-screened FP64 +
+// FP32 halves (the precision form).
 static hfg_status launch_class(hfg_ctx *c, const QuartetClass &q, const ClassLaunch &cl, int mode, bool ref,
-                               cudaStream_t s, int *launches) {
+                               int prec, cudaStream_t s, int *launches) {
   const ClassEntry &e = kClasses[q.cls];
   if (!kSplit[q.cls]) {
-    e.launch(c->view(), cl, mode, ref, grid_for(c, cl.ntasks), s);
-    ++*launches;
+    e.launch(c->view(), cl, mode, ref, prec, grid_for(c, cl.ntasks, q.cls), s);
+    *launches += prec == 2 ? 2 : 1;
     return HFG_OK;
   }
   const size_t acc = (size_t)ncomp_range(e.la, e.la + e.lb) * ncomp_range(e.lc, e.lc + e.ld);
@@ -356,40 +429,76 @@ static hfg_status launch_class(hfg_ctx *c, const QuartetClass &q, const ClassLau
     ch.stride = (long long)ch.ntasks * 32;
     ch.scr_fwd = c->d_scratch;
     ch.scr_rev = c->d_scratch + acc * (size_t)ch.stride;
-    kSplit[q.cls](c->view(), cl, ch, mode, ref, s);
-    *launches += 2;
+    kSplit[q.cls](c->view(), cl, ch, mode, ref, prec, s);
+    *launches += prec == 2 ? 3 : 2;
   }
   return HFG_OK;
 }
 
-// Direct J/K build: all classes on `s`, then G.
+// Direct J/K build: all classes on `s`, then G.  The plain form reads the
+// full density; the precision form (see hfg_opts) first forms the density
+// difference (incremental), the shell-block maxima for the density
+// screening, and accumulates G onto the previous one.
 static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const double *dPb, double *dGa, double *dGb,
                                cudaStream_t s) {
   const size_t nn = (size_t)c->nbf * c->nbf;
+  const int n = c->nbf;
   hfg_status st;
   if ((st = ensure(&c->d_J, nn)) != HFG_OK || (st = ensure(&c->d_Ka, nn)) != HFG_OK) return st;
   if (uhf && ((st = ensure(&c->d_Kb, nn)) != HFG_OK || (st = ensure(&c->d_Pt, nn)) != HFG_OK)) return st;
+  const bool precise = c->precision_form();
+  const bool incremental = precise && c->opts.incremental;
+  const bool fresh = !c->inc_valid || c->inc_uhf != uhf;
+  const int eg = std::max(1, std::min(1024, (int)((nn + 255) / 256)));
+  int launches = 2;
+  const double *Da = dPa, *Db = dPb;
+  if (precise) {
+    const int ns = c->nshells;
+    if (!c->d_shell_dmax) HFG_CUDA(cudaMalloc((void **)&c->d_shell_dmax, (size_t)ns * ns * sizeof(float)));
+    if (!c->d_counters) HFG_CUDA(cudaMalloc((void **)&c->d_counters, 2 * sizeof(unsigned long long)));
+    HFG_CUDA(cudaMemsetAsync(c->d_counters, 0, 2 * sizeof(unsigned long long), s));
+    if (incremental) {
+      for (int k = 0; k < (uhf ? 2 : 1); ++k)
+        if ((st = ensure(&c->d_prev_P[k], nn)) != HFG_OK || (st = ensure(&c->d_prev_G[k], nn)) != HFG_OK ||
+            (st = ensure(&c->d_dP[k], nn)) != HFG_OK)
+          return st;
+      density_difference<<<eg, 256, 0, s>>>(dPa, c->d_prev_P[0], c->d_dP[0], (int)nn, fresh);
+      Da = c->d_dP[0];
+      ++launches;
+      if (uhf) {
+        density_difference<<<eg, 256, 0, s>>>(dPb, c->d_prev_P[1], c->d_dP[1], (int)nn, fresh);
+        Db = c->d_dP[1];
+        ++launches;
+      }
+    }
+    const int sg = std::max(1, std::min(4096, (ns * ns + 255) / 256));
+    shell_block_max<<<sg, 256, 0, s>>>(Da, uhf ? Db : nullptr, c->d_shell_ao, c->d_shell_nf, ns, n, c->d_shell_dmax);
+    launches += 2;
+  }
   HFG_CUDA(cudaMemsetAsync(c->d_J, 0, nn * sizeof(double), s));
   HFG_CUDA(cudaMemsetAsync(c->d_Ka, 0, nn * sizeof(double), s));
-  int launches = 2;
   if (uhf) {
     HFG_CUDA(cudaMemsetAsync(c->d_Kb, 0, nn * sizeof(double), s));
-    add_densities<<<256, 256, 0, s>>>(dPa, dPb, c->d_Pt, (int)nn);
+    add_densities<<<256, 256, 0, s>>>(Da, Db, c->d_Pt, (int)nn);
     launches += 2;
   }
   HFG_CUDA(cudaEventRecord(c->ev0, s));
   const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
+  const int prec = !precise ? 0 : c->mixed_cutoff > 0 ? 2 : 1;
   c->stats = hfg_stats{};
   for (auto &q : c->qclasses) {
     ClassLaunch cl = base_launch(c, q);
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_a, s));
-    cl.Da = dPa;
-    cl.Db = dPb;
-    cl.Dt = uhf ? c->d_Pt : dPa;
+    cl.Da = Da;
+    cl.Db = Db;
+    cl.Dt = uhf ? c->d_Pt : Da;
     cl.J = c->d_J;
     cl.Ka = c->d_Ka;
     cl.Kb = c->d_Kb;
-    st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, s, &launches);
+    cl.dens_threshold = (float)c->density_threshold();
+    cl.mixed_cutoff = (float)c->mixed_cutoff;
+    cl.counters = precise ? c->d_counters : nullptr;
+    st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, prec, s, &launches);
     if (st != HFG_OK) return st;
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_b, s));
     c->stats.shell_quartets += q.shell_quartets;
@@ -399,14 +508,26 @@ static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const do
   }
   HFG_CUDA(cudaGetLastError());
   HFG_CUDA(cudaEventRecord(c->ev1, s));
-  const int n = c->nbf;
   const int fg = std::max(1, std::min(1024, (int)((nn + 255) / 256)));
-  if (uhf) finalize_uhf<<<fg, 256, 0, s>>>(c->d_J, c->d_Ka, c->d_Kb, dGa, dGb, n);
-  else finalize_rhf<<<fg, 256, 0, s>>>(c->d_J, c->d_Ka, dGa, n);
+  if (incremental) {
+    if (uhf)
+      finalize_uhf_incremental<<<fg, 256, 0, s>>>(c->d_J, c->d_Ka, c->d_Kb, c->d_prev_G[0], c->d_prev_G[1], dGa, dGb,
+                                                  n, !fresh);
+    else
+      finalize_rhf_incremental<<<fg, 256, 0, s>>>(c->d_J, c->d_Ka, c->d_prev_G[0], dGa, n, !fresh);
+    c->inc_valid = true;
+    c->inc_uhf = uhf;
+  } else if (uhf) {
+    finalize_uhf<<<fg, 256, 0, s>>>(c->d_J, c->d_Ka, c->d_Kb, dGa, dGb, n);
+  } else {
+    finalize_rhf<<<fg, 256, 0, s>>>(c->d_J, c->d_Ka, dGa, n);
+  }
   ++launches;
   HFG_CUDA(cudaGetLastError());
   c->stats.kernel_launches = launches;
   c->stats.shell_pairs = c->npairs;
+  c->counted = precise;
+  if (!precise) c->stats.fp64_shell_quartets = c->stats.shell_quartets;
   return HFG_OK;
 }
 
@@ -430,7 +551,7 @@ static hfg_status stored_build(hfg_ctx *c, double *d_out, int64_t count, cudaStr
     ClassLaunch cl = base_launch(c, q);
     cl.packed = d_out;
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_a, s));
-    const hfg_status st = launch_class(c, q, cl, kStorePacked, ref, s, &launches);
+    const hfg_status st = launch_class(c, q, cl, kStorePacked, ref, 0, s, &launches);
     if (st != HFG_OK) return st;
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_b, s));
     c->stats.shell_quartets += q.shell_quartets;
@@ -442,6 +563,8 @@ static hfg_status stored_build(hfg_ctx *c, double *d_out, int64_t count, cudaStr
   HFG_CUDA(cudaEventRecord(c->ev1, s));
   c->stats.kernel_launches = launches;
   c->stats.shell_pairs = c->npairs;
+  c->stats.fp64_shell_quartets = c->stats.shell_quartets;
+  c->counted = false;
   return HFG_OK;
 }
 
@@ -512,6 +635,19 @@ hfg_status hfg_ctx_create(const hfg_shells *sh, const hfg_opts *opts, hfg_ctx **
     funcs += ncart_h(h.L);
   }
   if (funcs != sh->nbf) return fail(HFG_INVALID_ARG, "shell functions do not sum to nbf");
+  if (!(ctx->opts.mixed_cutoff >= 0) || !(ctx->opts.mixed_cutoff < 1e300) || !(ctx->opts.density_threshold >= 0))
+    return fail(HFG_INVALID_ARG, "mixed cutoff and density threshold must be finite and >= 0");
+  ctx->mixed_cutoff = ctx->opts.mixed_cutoff;
+  ctx->nshells = ns;
+  {
+    std::vector<int> sao(ns), snf(ns);
+    for (int s = 0; s < ns; ++s) {
+      sao[s] = ctx->shells[s].ao;
+      snf[s] = ncart_h(ctx->shells[s].L);
+    }
+    hfg_status st0;
+    if ((st0 = upload(&ctx->d_shell_ao, sao)) != HFG_OK || (st0 = upload(&ctx->d_shell_nf, snf)) != HFG_OK) return st0;
+  }
 
   // ---- shell pairs and primitive pairs (pair index a*(a+1)/2 + b, a >= b)
   const int np = ns * (ns + 1) / 2;
@@ -769,7 +905,7 @@ hfg_status hfg_eri_quartet(hfg_ctx *c, int32_t i, int32_t j, int32_t k, int32_t 
   cl.tasks = d_tk;
   cl.ntasks = 1;
   cl.packed = c->d_block;
-  kClasses[cls].launch(c->view(), cl, kBlock, c->opts.eri_convention == HFG_ERI_REFERENCE, 1, c->stream);
+  kClasses[cls].launch(c->view(), cl, kBlock, c->opts.eri_convention == HFG_ERI_REFERENCE, 0, 1, c->stream);
   double blk[1296];
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(blk, c->d_block, sizeof blk, cudaMemcpyDeviceToHost, c->stream);
@@ -819,6 +955,34 @@ hfg_status hfg_class_profile(const hfg_ctx *c, hfg_class_time *out, int32_t cap,
 hfg_status hfg_ctx_stats(const hfg_ctx *c, hfg_stats *out) {
   if (!c || !out) return hfg::fail(HFG_INVALID_ARG, "null argument");
   *out = c->stats;
+  if (c->counted) {
+    // quartets the density screening kept, per precision (waits for the build)
+    unsigned long long cnt[2] = {0, 0};
+    HFG_CUDA(cudaSetDevice(c->device));
+    HFG_CUDA(cudaMemcpy(cnt, c->d_counters, sizeof cnt, cudaMemcpyDeviceToHost));
+    out->fp64_shell_quartets = (int64_t)cnt[0];
+    out->fp32_shell_quartets = (int64_t)cnt[1];
+  }
+  return HFG_OK;
+}
+
+hfg_status hfg_fock_reset(hfg_ctx *c) {
+  if (!c) return hfg::fail(HFG_INVALID_ARG, "null context");
+  c->inc_valid = false;
+  return HFG_OK;
+}
+
+hfg_status hfg_set_mixed_cutoff(hfg_ctx *c, double cutoff) {
+  if (!c) return hfg::fail(HFG_INVALID_ARG, "null context");
+  if (!(cutoff >= 0) || !(cutoff < 1e300)) return hfg::fail(HFG_INVALID_ARG, "mixed cutoff must be finite and >= 0");
+  c->mixed_cutoff = cutoff;
+  return HFG_OK;
+}
+
+hfg_status hfg_set_incremental(hfg_ctx *c, int32_t on) {
+  if (!c) return hfg::fail(HFG_INVALID_ARG, "null context");
+  c->opts.incremental = on != 0;
+  c->inc_valid = false;
   return HFG_OK;
 }
 
@@ -887,7 +1051,7 @@ extern "C" hfg_status hfg_fock_rhf_noalloc(hfg_ctx *c, const double *dP, double 
     cl.Dt = dP;
     cl.J = J;
     cl.Ka = K;
-    kClasses[q.cls].launch(v, cl, kJkRhf, ref, grid_for(c, cl.ntasks), s);
+    kClasses[q.cls].launch(v, cl, kJkRhf, ref, 0, grid_for(c, cl.ntasks, q.cls), s);
   }
   const int fg = std::max(1, std::min(1024, (int)((nn + 255) / 256)));
   finalize_rhf<<<fg, 256, 0, s>>>(J, K, dG, n);

@@ -5,6 +5,8 @@
 // needs is staged into shared memory once per block.
 #pragma once
 
+#include <type_traits>
+
 #include "eri_gen.cuh"
 #include "hfg_internal.cuh"
 
@@ -15,33 +17,37 @@ template <int N>
 constexpr int kUnrollBlock = N <= 81 ? 64 : 1;
 
 __device__ __forceinline__ double inv_factorial(int k) {
-  // 1/k! for k = 0..6
-  const double t[7] = {1.0, 1.0, 0.5, 1.0 / 6.0, 1.0 / 24.0, 1.0 / 120.0, 1.0 / 720.0};
-  return t[k];
+  // 1/k! for k = 0..6 as a select chain (an indexed array would live in
+  // local memory and be rebuilt on every call)
+  return k <= 1 ? 1.0 : k == 2 ? 0.5 : k == 3 ? 1.0 / 6.0 : k == 4 ? 1.0 / 24.0 : k == 5 ? 1.0 / 120.0 : 1.0 / 720.0;
 }
 
 template <int LTOT>
 __device__ __forceinline__ void stage_boys(double *tab, const double *__restrict__ g) {
   for (int x = threadIdx.x; x < kBoysGrid * kBoysRow; x += blockDim.x) {
     const int i = x / kBoysRow, k = x - i * kBoysRow;
-    // Taylor coefficients F_{LTOT+k}(T_i)/k!, then e^-T_i from the table's tail
-    tab[x] = k < kBoysTaylor ? g[i * kBoysOrders + LTOT + k] * inv_factorial(k) : g[kBoysGrid * kBoysOrders + i];
+    // Taylor coefficients F_{LTOT+k}(T_i)/k!, then e^-T_i from the table's
+    // tail, each at its swizzled place in the row
+    tab[boys_swizzle(i, k)] =
+        k < kBoysTaylor ? g[i * kBoysOrders + LTOT + k] * inv_factorial(k) : g[kBoysGrid * kBoysOrders + i];
   }
   __syncthreads();
 }
 
 // Contracted (ab|cd) block of one shell quartet, bra pair `bp`, ket pair
 // `kp`, components in canonical order, normalisation applied.  `npk` = 0
-// yields an all-zero block (inactive lanes).
-template <int LA, int LB, int LC, int LD, bool REF>
+// yields an all-zero block (inactive lanes).  R is the type of the
+// recursions and the contraction; the Boys function, T and the prefactor
+// are always evaluated in FP64.
+template <int LA, int LB, int LC, int LD, bool REF, class R = double>
 __device__ __forceinline__ void quartet_block(const EngineView &v, const double *tab, int bp, int kp, int npk,
-                                              double *out) {
+                                              R *out) {
   constexpr int LTOT = LA + LB + LC + LD;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   using Cls = EriClass<LA, LB, LC, LD, REF>;
-  double acc[Cls::kAcc];
+  R acc[Cls::kAcc];
 #pragma unroll
-  for (int x = 0; x < Cls::kAcc; ++x) acc[x] = 0.0;
+  for (int x = 0; x < Cls::kAcc; ++x) acc[x] = R(0);
 
   const int offb = v.pair_prim_off[bp], npb = v.pair_nprim[bp];
   const int offk = v.pair_prim_off[kp];
@@ -56,17 +62,17 @@ __device__ __forceinline__ void quartet_block(const EngineView &v, const double 
       const double rho = pb.zeta * pk.zeta * inv_zpe;
       const double PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;
       const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
-      double F[LTOT + 1];
-      boys_eval<LTOT, double>(F, T, pb.K * pk.K * rs, tab);
+      R F[LTOT + 1];
+      boys_eval<LTOT, R>(F, T, pb.K * pk.K * rs, tab);
       const double roz = rho * pb.inv_zeta;
       const double ie = pk.inv_zeta;
-      Cls::template prim<double>(acc, F, pb.PAx, pb.PAy, pb.PAz, -roz * PQx, -roz * PQy, -roz * PQz,
-                                 0.5 * pb.inv_zeta, roz, -(pb.bABx + pk.bABx) * ie, -(pb.bABy + pk.bABy) * ie,
-                                 -(pb.bABz + pk.bABz) * ie, pb.zeta * ie, 0.5 * ie);
+      Cls::template prim<R>(acc, F, R(pb.PAx), R(pb.PAy), R(pb.PAz), R(-roz * PQx), R(-roz * PQy), R(-roz * PQz),
+                            R(0.5 * pb.inv_zeta), R(roz), R(-(pb.bABx + pk.bABx) * ie), R(-(pb.bABy + pk.bABy) * ie),
+                            R(-(pb.bABz + pk.bABz) * ie), R(pb.zeta * ie), R(0.5 * ie));
     }
   }
-  Cls::template hrr<double>(out, acc, v.pair_AB[3 * bp], v.pair_AB[3 * bp + 1], v.pair_AB[3 * bp + 2],
-                            v.pair_AB[3 * kp], v.pair_AB[3 * kp + 1], v.pair_AB[3 * kp + 2]);
+  Cls::template hrr<R>(out, acc, R(v.pair_AB[3 * bp]), R(v.pair_AB[3 * bp + 1]), R(v.pair_AB[3 * bp + 2]),
+                       R(v.pair_AB[3 * kp]), R(v.pair_AB[3 * kp + 1]), R(v.pair_AB[3 * kp + 2]));
   constexpr int U = kUnrollBlock<NA * NB * NC * ND>;
 #pragma unroll U
   for (int a = 0; a < NA; ++a)
@@ -76,8 +82,43 @@ __device__ __forceinline__ void quartet_block(const EngineView &v, const double 
       for (int c = 0; c < NC; ++c)
 #pragma unroll U
         for (int d = 0; d < ND; ++d)
-          out[((a * NB + b) * NC + c) * ND + d] *= comp_norm<LA>(a) * comp_norm<LB>(b) * comp_norm<LC>(c) *
-                                                   comp_norm<LD>(d);
+          out[((a * NB + b) * NC + c) * ND + d] *= R(comp_norm<LA>(a) * comp_norm<LB>(b) * comp_norm<LC>(c) *
+                                                     comp_norm<LD>(d));
+}
+
+// Density-weighted Schwarz bound of the quartet (bp|kp): Q_ab Q_cd times the
+// largest |D| over the six shell blocks a J/K digestion reads (ab, cd for J;
+// ac, ad, bc, bd for K).
+__device__ __forceinline__ float density_bound(const EngineView &v, int bp, int kp) {
+  const int a = v.pair_sa[bp], b = v.pair_sb[bp], c = v.pair_sa[kp], d = v.pair_sb[kp];
+  const float *S = v.shell_dmax;
+  const int ns = v.nshells;
+  const float m = fmaxf(fmaxf(fmaxf(S[a * ns + b], S[c * ns + d]), fmaxf(S[a * ns + c], S[a * ns + d])),
+                        fmaxf(S[b * ns + c], S[b * ns + d]));
+  return (float)(v.pair_Q[bp] * v.pair_Q[kp]) * m;
+}
+
+// Warp-level density screening of one task.  Sets *keep for the lane's
+// quartet (active and bound >= threshold) and returns whether this launch
+// (SCR = kScreenFp64 or kScreenFp32) takes the task: the warp's largest kept
+// bound against the mixed cutoff, identical in every lane and in both
+// kernels, so each task with a kept quartet is taken by exactly one of them.
+template <int SCR>
+__device__ __forceinline__ bool screen_task(const EngineView &v, const ClassLaunch &cl, int bp, int kp, bool active,
+                                            bool *keep) {
+  const float bnd = active ? density_bound(v, bp, kp) : 0.0f;
+  const bool k = active && bnd >= cl.dens_threshold;
+  *keep = k;
+  const unsigned kept = __ballot_sync(0xffffffffu, k);
+  if (!kept) return false;
+  float m = k ? bnd : 0.0f;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  const bool hi = m >= cl.mixed_cutoff;
+  const bool take = SCR == kScreenFp64 ? hi : !hi;
+  if (take && (threadIdx.x & 31) == 0 && cl.counters)
+    atomicAdd(&cl.counters[SCR == kScreenFp64 ? 0 : 1], (unsigned long long)__popc(kept));
+  return take;
 }
 
 // The reference evaluates each function quartet of a (dd|dd) shell quartet
@@ -86,16 +127,17 @@ __device__ __forceinline__ void quartet_block(const EngineView &v, const double 
 // row range the orientation changes the value.  This reproduces the choice
 // per element (AO index == function ID).  Kept out of line: it holds three
 // (dd|dd) blocks and is only reached by the rare two-d-shell quartets.
-static __device__ __noinline__ void dddd_reference_values(const EngineView &v, const double *tab, int bp, int kp, int npk,
-                                                   double *out) {
+template <class R>
+static __device__ __noinline__ void dddd_reference_values(const EngineView &v, const double *tab, int bp, int kp,
+                                                          int npk, R *out) {
   constexpr int N = 6;
   const int sab = v.pair_sa[bp], skt = v.pair_sa[kp];
   if (sab > skt || npk == 0) {
-    quartet_block<2, 2, 2, 2, true>(v, tab, bp, kp, npk, out);
+    quartet_block<2, 2, 2, 2, true, R>(v, tab, bp, kp, npk, out);
     return;
   }
-  double sw[N * N * N * N];
-  quartet_block<2, 2, 2, 2, true>(v, tab, kp, bp, v.pair_nprim[bp], sw);
+  R sw[N * N * N * N];
+  quartet_block<2, 2, 2, 2, true, R>(v, tab, kp, bp, v.pair_nprim[bp], sw);
   if (sab < skt) {
     for (int a = 0; a < N; ++a)
       for (int b = 0; b < N; ++b)
@@ -104,7 +146,7 @@ static __device__ __noinline__ void dddd_reference_values(const EngineView &v, c
     return;
   }
   // same first shell: per-element orientation
-  quartet_block<2, 2, 2, 2, true>(v, tab, bp, kp, npk, out);
+  quartet_block<2, 2, 2, 2, true, R>(v, tab, bp, kp, npk, out);
   const int aoa = v.pair_ao_a[bp], aob = v.pair_ao_b[bp], aoc = v.pair_ao_a[kp], aod = v.pair_ao_b[kp];
   const bool bdiag = v.pair_sa[bp] == v.pair_sb[bp], kdiag = v.pair_sa[kp] == v.pair_sb[kp];
   for (int a = 0; a < N; ++a)
@@ -119,36 +161,47 @@ static __device__ __noinline__ void dddd_reference_values(const EngineView &v, c
         }
 }
 
-template <int LA, int LB, int LC, int LD, bool REF>
+template <int LA, int LB, int LC, int LD, bool REF, class R>
 __device__ __forceinline__ void quartet_values(const EngineView &v, const double *tab, int bp, int kp, int npk,
-                                               double *out) {
+                                               R *out) {
   if constexpr (REF && LA == 2 && LB == 2 && LC == 2 && LD == 2) {
-    dddd_reference_values(v, tab, bp, kp, npk, out);
+    dddd_reference_values<R>(v, tab, bp, kp, npk, out);
   } else {
-    quartet_block<LA, LB, LC, LD, REF>(v, tab, bp, kp, npk, out);
+    quartet_block<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, npk, out);
   }
 }
 
-template <int LA, int LB, int LC, int LD, int MODE, bool REF>
-__global__ void __launch_bounds__(kThreads) eri_class_kernel(const EngineView v, const ClassLaunch cl) {
+// SCR (enum Screen) selects plain FP64, or the density-screened FP64 / FP32
+// halves of a mixed-precision J/K build (kJkRhf, kJkUhf only).
+template <int LA, int LB, int LC, int LD, int MODE, bool REF, int SCR = kScreenNone>
+__global__ void __launch_bounds__(32 * fused_warps(LA, LB, LC, LD))
+    eri_class_kernel(const EngineView v, const ClassLaunch cl) {
+  constexpr int kW = fused_warps(LA, LB, LC, LD);
   constexpr int LTOT = LA + LB + LC + LD;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
+  using R = typename std::conditional<SCR == kScreenFp32, float, double>::type;
+  static_assert(SCR == kScreenNone || MODE == kJkRhf || MODE == kJkUhf, "screening applies to J/K builds");
   __shared__ double tab[kBoysGrid * kBoysRow];
   stage_boys<LTOT>(tab, v.boys_table);
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int n = v.nbf;
-  for (int t = blockIdx.x * kWarpsPerBlock + warp; t < cl.ntasks; t += gridDim.x * kWarpsPerBlock) {
+  for (int t = blockIdx.x * kW + warp; t < cl.ntasks; t += gridDim.x * kW) {
     const Task task = cl.tasks[t];
     const int bp = cl.bra_list[task.bra_pos];
     const int kpos = task.ket_start + lane;
-    const bool active = kpos < task.ket_end;
+    bool active = kpos < task.ket_end;
     const int kp = active ? cl.ket_list[kpos] : bp;
+    if constexpr (SCR != kScreenNone) {
+      bool keep;
+      if (!screen_task<SCR>(v, cl, bp, kp, active, &keep)) continue;  // warp-uniform
+      active = keep;
+    }
     const int npk = active ? v.pair_nprim[kp] : 0;
 
-    double out[NA * NB * NC * ND];
-    quartet_values<LA, LB, LC, LD, REF>(v, tab, bp, kp, npk, out);
+    R out[NA * NB * NC * ND];
+    quartet_values<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, npk, out);
     // blocks above 81 integrals live in local memory anyway: keep their
     // epilogue loops rolled (code size, compile time)
     constexpr int U = kUnrollBlock<NA * NB * NC * ND>;

@@ -1,4 +1,4 @@
-// Split path for the large classes (more than 81 integrals per shell
+// Split path for the large classes (more than 150 integrals per shell
 // quartet): the fused kernel's per-thread state (the contracted [e0|f0]
 // block plus the full (ab|cd) block plus the J/K partials) does not fit the
 // register file there and spills heavily.  Here
@@ -6,11 +6,12 @@
 //      loops (Boys, vertical recursion, electron transfer, contraction) and
 //      streams the contracted [e0|f0] block to scratch, column-major across
 //      the quartets of a chunk so that a warp's stores coalesce;
-//   2. eri_hrr_digest_kernel: thread per (shell quartet, bra row ab) expands
-//      the row with the linear horizontal recursion (<= 4 terms per output),
-//      then stores it (packed table) or digests it into J/K.
-// The 32 quartets of a warp share the bra pair (one task), so in step 2 the
-// J_ab partial of a warp reduces across lanes before its atomic.
+//   2. eri_hrr_digest_kernel: one block per task (32 quartets sharing the
+//      bra pair); each warp expands bra rows (a b) of all 32 quartets with the
+//      linear horizontal recursion (<= 4 terms per output), then stores them
+//      (packed table) or digests them into J/K.
+// Density-screened builds run step 1 twice (FP64 and FP32 halves, each
+// taking its own tasks) and step 2 once over the quartets either kept.
 #pragma once
 
 #include "eri_kernels.cuh"
@@ -19,14 +20,14 @@
 namespace hfg {
 
 // contracted [e0|f0] of one shell quartet, written to scr[x * stride]
-template <int LA, int LB, int LC, int LD, bool REF>
+template <int LA, int LB, int LC, int LD, bool REF, class R>
 __device__ __forceinline__ void prim_block_to_scratch(const EngineView &v, const double *tab, int bp, int kp, int npk,
                                                       double *scr, long long stride) {
   constexpr int LTOT = LA + LB + LC + LD;
   using Cls = EriClass<LA, LB, LC, LD, REF>;
-  double acc[Cls::kAcc];
+  R acc[Cls::kAcc];
 #pragma unroll
-  for (int x = 0; x < Cls::kAcc; ++x) acc[x] = 0.0;
+  for (int x = 0; x < Cls::kAcc; ++x) acc[x] = R(0);
   const int offb = v.pair_prim_off[bp], npb = v.pair_nprim[bp];
   const int offk = v.pair_prim_off[kp];
   for (int ik = 0; ik < npk; ++ik) {
@@ -38,41 +39,50 @@ __device__ __forceinline__ void prim_block_to_scratch(const EngineView &v, const
       const double rho = pb.zeta * pk.zeta * inv_zpe;
       const double PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;
       const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
-      double F[LTOT + 1];
-      boys_eval<LTOT, double>(F, T, pb.K * pk.K * rs, tab);
+      R F[LTOT + 1];
+      boys_eval<LTOT, R>(F, T, pb.K * pk.K * rs, tab);
       const double roz = rho * pb.inv_zeta;
       const double ie = pk.inv_zeta;
-      Cls::template prim<double>(acc, F, pb.PAx, pb.PAy, pb.PAz, -roz * PQx, -roz * PQy, -roz * PQz,
-                                 0.5 * pb.inv_zeta, roz, -(pb.bABx + pk.bABx) * ie, -(pb.bABy + pk.bABy) * ie,
-                                 -(pb.bABz + pk.bABz) * ie, pb.zeta * ie, 0.5 * ie);
+      Cls::template prim<R>(acc, F, R(pb.PAx), R(pb.PAy), R(pb.PAz), R(-roz * PQx), R(-roz * PQy), R(-roz * PQz),
+                            R(0.5 * pb.inv_zeta), R(roz), R(-(pb.bABx + pk.bABx) * ie), R(-(pb.bABy + pk.bABy) * ie),
+                            R(-(pb.bABz + pk.bABz) * ie), R(pb.zeta * ie), R(0.5 * ie));
     }
   }
 #pragma unroll
-  for (int x = 0; x < Cls::kAcc; ++x) scr[x * stride] = acc[x];
+  for (int x = 0; x < Cls::kAcc; ++x) scr[x * stride] = (double)acc[x];
 }
 
-template <int LA, int LB, int LC, int LD, bool REF>
+// SCR (enum Screen): plain FP64, or the density-screened FP64 / FP32 half.
+// A warp is one task (blockDim and the slot count are multiples of 32).
+template <int LA, int LB, int LC, int LD, bool REF, int SCR = kScreenNone>
 __global__ void __launch_bounds__(kThreads) eri_prim_split_kernel(const EngineView v, const ClassLaunch cl,
                                                                   const SplitChunk ch) {
   constexpr int LTOT = LA + LB + LC + LD;
+  using R = typename std::conditional<SCR == kScreenFp32, float, double>::type;
   __shared__ double tab[kBoysGrid * kBoysRow];
   stage_boys<LTOT>(tab, v.boys_table);
   const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (slot >= (long long)ch.ntasks * 32) return;
+  if (slot >= (long long)ch.ntasks * 32) return;  // whole warps
   const Task task = cl.tasks[ch.task0 + (int)(slot >> 5)];
   const int kpos = task.ket_start + (int)(slot & 31);
-  if (kpos >= task.ket_end) return;
-  const int bp = cl.bra_list[task.bra_pos], kp = cl.ket_list[kpos];
+  bool active = kpos < task.ket_end;
+  const int bp = cl.bra_list[task.bra_pos], kp = active ? cl.ket_list[kpos] : bp;
+  if constexpr (SCR != kScreenNone) {
+    bool keep;
+    if (!screen_task<SCR>(v, cl, bp, kp, active, &keep)) return;  // warp-uniform
+    active = keep;
+  }
+  if (!active) return;
   constexpr bool kOrient = REF && LA == 2 && LB == 2 && LC == 2 && LD == 2;
   if constexpr (kOrient) {
     // bra/ket orientation the reference picks (see dddd_reference_values)
     const int sab = v.pair_sa[bp], skt = v.pair_sa[kp];
     if (sab >= skt)
-      prim_block_to_scratch<LA, LB, LC, LD, true>(v, tab, bp, kp, v.pair_nprim[kp], ch.scr_fwd + slot, ch.stride);
+      prim_block_to_scratch<LA, LB, LC, LD, true, R>(v, tab, bp, kp, v.pair_nprim[kp], ch.scr_fwd + slot, ch.stride);
     if (sab <= skt)
-      prim_block_to_scratch<LA, LB, LC, LD, true>(v, tab, kp, bp, v.pair_nprim[bp], ch.scr_rev + slot, ch.stride);
+      prim_block_to_scratch<LA, LB, LC, LD, true, R>(v, tab, kp, bp, v.pair_nprim[bp], ch.scr_rev + slot, ch.stride);
   } else {
-    prim_block_to_scratch<LA, LB, LC, LD, REF>(v, tab, bp, kp, v.pair_nprim[kp], ch.scr_fwd + slot, ch.stride);
+    prim_block_to_scratch<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, v.pair_nprim[kp], ch.scr_fwd + slot, ch.stride);
   }
 }
 
@@ -80,8 +90,9 @@ __global__ void __launch_bounds__(kThreads) eri_prim_split_kernel(const EngineVi
 // expands rows ab = w, w + 4, ... of all 32 quartets.  The J_cd partials of a
 // quartet accumulate in registers across a warp's rows and across the
 // block's warps in shared memory before one atomic per element; J_ab reduces
-// across the warp; the K partials go out per row.
-template <int LA, int LB, int LC, int LD, int MODE, bool REF>
+// across the warp; the K partials go out per row.  SCREENED: only the
+// quartets the density screening kept (the same test as step 1).
+template <int LA, int LB, int LC, int LD, int MODE, bool REF, bool SCREENED = false>
 __global__ void __launch_bounds__(kThreads) eri_hrr_digest_kernel(const EngineView v, const ClassLaunch cl,
                                                                   const SplitChunk ch) {
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
@@ -96,9 +107,14 @@ __global__ void __launch_bounds__(kThreads) eri_hrr_digest_kernel(const EngineVi
   const long long slot = (long long)tloc * 32 + lane;
   const Task task = cl.tasks[ch.task0 + tloc];
   const int kpos = task.ket_start + lane;
-  const bool active = kpos < task.ket_end;
+  bool active = kpos < task.ket_end;
   const int bp = cl.bra_list[task.bra_pos];
   const int kp = active ? cl.ket_list[kpos] : bp;
+  if constexpr (SCREENED) {
+    // every warp of the block sees the same task: block-uniform return
+    active = active && density_bound(v, bp, kp) >= cl.dens_threshold;
+    if (!__any_sync(0xffffffffu, active)) return;
+  }
   const int n = v.nbf;
   const double X0 = v.pair_AB[3 * bp], X1 = v.pair_AB[3 * bp + 1], X2 = v.pair_AB[3 * bp + 2];
   const double Y0 = v.pair_AB[3 * kp], Y1 = v.pair_AB[3 * kp + 1], Y2 = v.pair_AB[3 * kp + 2];

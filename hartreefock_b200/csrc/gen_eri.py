@@ -304,31 +304,66 @@ def main(out_path):
 
 
 def emit_launchers(out_dir):
-    """One translation unit per quartet class (they compile in parallel), the
-    Schwarz launcher and the dispatch table."""
+    """One translation unit per quartet class (they compile in parallel), a
+    second one with the density-screened FP64/FP32 J/K kernels of the fused
+    classes, the Schwarz launcher and the dispatch table.  `prec` of a
+    launcher: 0 plain FP64, 1 screened FP64, 2 screened FP64 + FP32 halves."""
     pairs, quartets = canonical_classes()
     modes = ("kStorePacked", "kJkRhf", "kJkUhf", "kBlock")
+
+    def launch(lines, ind, k, ref, tail="<<<grid, kFusedBlock, 0, s>>>(v, cl);"):
+        if ref:
+            lines.append(f"{ind}if (ref) {k.format(r='true')}{tail}")
+            lines.append(f"{ind}else {k.format(r='false')}{tail}")
+        else:
+            lines.append(f"{ind}{k.format(r='false')}{tail}")
+
     for (a, b, c, d) in quartets:
         ref = (c + d) >= a + 2  # classes whose reference variant differs
+        split = is_split_class(a, b, c, d)
+        tag = f"{a}{b}{c}{d}"
         lines = [f"// Generated by gen_eri.py: launcher for the ({a}{b}|{c}{d}) class kernels.",
                  '#include "eri_dispatch.cuh"', "", "namespace hfg {", "",
-                 f"void launch_class_{a}{b}{c}{d}(const EngineView &v, const ClassLaunch &cl, int mode, bool ref, int grid,",
-                 "                       cudaStream_t s) {",
-                 "  switch (mode) {"]
+                 f"void launch_class_{tag}(const EngineView &v, const ClassLaunch &cl, int mode, bool ref, int prec,",
+                 "                       int grid, cudaStream_t s) {",
+                 f"  constexpr int kFusedBlock = 32 * fused_warps({a}, {b}, {c}, {d});"]
+        if not split:
+            lines += ["  if (prec != 0 && (mode == kJkRhf || mode == kJkUhf)) {",
+                      f"    launch_class_{tag}_scr(v, cl, mode, ref, prec, grid, s);",
+                      "    return;", "  }"]
+        lines.append("  switch (mode) {")
         for mode in modes:
             lines.append(f"    case {mode}:")
-            k = f"eri_class_kernel<{a}, {b}, {c}, {d}, {mode}"
-            if ref:
-                lines.append(f"      if (ref) {k}, true><<<grid, kThreads, 0, s>>>(v, cl);")
-                lines.append(f"      else {k}, false><<<grid, kThreads, 0, s>>>(v, cl);")
-            else:
-                lines.append(f"      {k}, false><<<grid, kThreads, 0, s>>>(v, cl);")
+            launch(lines, "      ", f"eri_class_kernel<{a}, {b}, {c}, {d}, {mode}, {{r}}>", ref)
+            lines.append("      break;")
+        lines += ["    default:", "      break;", "  }"]
+        if not ref:
+            lines.append("  (void)ref;")
+        if split:
+            lines.append("  (void)prec;")
+        lines += ["}", "", "}  // namespace hfg", ""]
+        with open(os.path.join(out_dir, f"eri_class_{tag}.cu"), "w") as fh:
+            fh.write("\n".join(lines))
+        if split:
+            continue
+        lines = [f"// Generated by gen_eri.py: density-screened J/K kernels of the ({a}{b}|{c}{d}) class.",
+                 '#include "eri_dispatch.cuh"', "", "namespace hfg {", "",
+                 f"void launch_class_{tag}_scr(const EngineView &v, const ClassLaunch &cl, int mode, bool ref, int prec,",
+                 "                           int grid, cudaStream_t s) {",
+                 f"  constexpr int kFusedBlock = 32 * fused_warps({a}, {b}, {c}, {d});",
+                 "  switch (mode) {"]
+        for mode in ("kJkRhf", "kJkUhf"):
+            lines.append(f"    case {mode}:")
+            launch(lines, "      ", f"eri_class_kernel<{a}, {b}, {c}, {d}, {mode}, {{r}}, kScreenFp64>", ref)
+            lines.append("      if (prec == 2) {")
+            launch(lines, "        ", f"eri_class_kernel<{a}, {b}, {c}, {d}, {mode}, {{r}}, kScreenFp32>", ref)
+            lines.append("      }")
             lines.append("      break;")
         lines += ["    default:", "      break;", "  }"]
         if not ref:
             lines.append("  (void)ref;")
         lines += ["}", "", "}  // namespace hfg", ""]
-        with open(os.path.join(out_dir, f"eri_class_{a}{b}{c}{d}.cu"), "w") as fh:
+        with open(os.path.join(out_dir, f"eri_class_{tag}_scr.cu"), "w") as fh:
             fh.write("\n".join(lines))
     lines = ["// Generated by gen_eri.py: Schwarz-bound kernels, one per pair class.", '#include "eri_dispatch.cuh"', "",
              "namespace hfg {", "",
@@ -342,9 +377,11 @@ def emit_launchers(out_dir):
         fh.write("\n".join(lines))
     lines = ["// Generated by gen_eri.py: launch wrappers for the class kernels.", "#pragma once",
              '#include "eri_kernels.cuh"', "", "namespace hfg {", "",
-             "using ClassLauncher = void (*)(const EngineView &, const ClassLaunch &, int, bool, int, cudaStream_t);"]
+             "using ClassLauncher = void (*)(const EngineView &, const ClassLaunch &, int, bool, int, int, cudaStream_t);"]
     for (a, b, c, d) in quartets:
-        lines.append(f"void launch_class_{a}{b}{c}{d}(const EngineView &v, const ClassLaunch &cl, int mode, bool ref, int grid, cudaStream_t s);")
+        lines.append(f"void launch_class_{a}{b}{c}{d}(const EngineView &v, const ClassLaunch &cl, int mode, bool ref, int prec, int grid, cudaStream_t s);")
+        if not is_split_class(a, b, c, d):
+            lines.append(f"void launch_class_{a}{b}{c}{d}_scr(const EngineView &v, const ClassLaunch &cl, int mode, bool ref, int prec, int grid, cudaStream_t s);")
     lines += ["void launch_schwarz(int la, int lb, const EngineView &v, const int *pairs, int npairs, double *Q, cudaStream_t s);",
               "", "struct ClassEntry {", "  int la, lb, lc, ld;", "  ClassLauncher launch;", "};",
               "static const ClassEntry kClasses[] = {"]
@@ -560,44 +597,68 @@ def emit_split(out_dir):
     with open(os.path.join(out_dir, "eri_split_gen.cuh"), "w") as fh:
         fh.write("\n".join(hdr) + "\n")
     modes = ("kStorePacked", "kJkRhf", "kJkUhf")
+
+    def launch(lines, ind, k, ref, grid):
+        tail = f"<<<{grid}, kThreads, 0, s>>>(v, cl, ch);"
+        if ref:
+            lines.append(f"{ind}if (ref) {k.format(r='true')}{tail}")
+            lines.append(f"{ind}else {k.format(r='false')}{tail}")
+        else:
+            lines.append(f"{ind}{k.format(r='false')}{tail}")
+
+    head = ["  const int slots = ch.ntasks * 32;",
+            "  const int gridA = (slots + kThreads - 1) / kThreads;",
+            "  const int gridB = ch.ntasks;  // one block per task"]
     for (a, b, c, d) in quartets:
         if not is_split_class(a, b, c, d):
             continue
         ref = (c + d) >= a + 2
+        tag = f"{a}{b}{c}{d}"
         lines = [f"// Generated by gen_eri.py: split-path launchers for the ({a}{b}|{c}{d}) class.",
-                 '#include "eri_split.cuh"', "", "namespace hfg {", "",
-                 f"void launch_split_{a}{b}{c}{d}(const EngineView &v, const ClassLaunch &cl, const SplitChunk &ch, int mode,",
-                 "                        bool ref, cudaStream_t s) {",
-                 "  const int slots = ch.ntasks * 32;",
-                 "  const int gridA = (slots + kThreads - 1) / kThreads;",
-                 "  const int gridB = ch.ntasks;  // one block per task"]
-        if ref:
-            lines.append(f"  if (ref) eri_prim_split_kernel<{a}, {b}, {c}, {d}, true><<<gridA, kThreads, 0, s>>>(v, cl, ch);")
-            lines.append(f"  else eri_prim_split_kernel<{a}, {b}, {c}, {d}, false><<<gridA, kThreads, 0, s>>>(v, cl, ch);")
-        else:
-            lines.append(f"  eri_prim_split_kernel<{a}, {b}, {c}, {d}, false><<<gridA, kThreads, 0, s>>>(v, cl, ch);")
+                 '#include "eri_split.cuh"', '#include "eri_split_dispatch.cuh"', "", "namespace hfg {", "",
+                 f"void launch_split_{tag}(const EngineView &v, const ClassLaunch &cl, const SplitChunk &ch, int mode,",
+                 "                        bool ref, int prec, cudaStream_t s) {",
+                 "  if (prec != 0 && (mode == kJkRhf || mode == kJkUhf)) {",
+                 f"    launch_split_{tag}_scr(v, cl, ch, mode, ref, prec, s);",
+                 "    return;", "  }"] + head
+        launch(lines, "  ", f"eri_prim_split_kernel<{a}, {b}, {c}, {d}, {{r}}>", ref, "gridA")
         lines.append("  switch (mode) {")
         for mode in modes:
             lines.append(f"    case {mode}:")
-            k = f"eri_hrr_digest_kernel<{a}, {b}, {c}, {d}, {mode}"
-            if ref:
-                lines.append(f"      if (ref) {k}, true><<<gridB, kThreads, 0, s>>>(v, cl, ch);")
-                lines.append(f"      else {k}, false><<<gridB, kThreads, 0, s>>>(v, cl, ch);")
-            else:
-                lines.append(f"      {k}, false><<<gridB, kThreads, 0, s>>>(v, cl, ch);")
+            launch(lines, "      ", f"eri_hrr_digest_kernel<{a}, {b}, {c}, {d}, {mode}, {{r}}>", ref, "gridB")
             lines.append("      break;")
         lines += ["    default:", "      break;", "  }"]
         if not ref:
             lines.append("  (void)ref;")
         lines += ["}", "", "}  // namespace hfg", ""]
-        with open(os.path.join(out_dir, f"eri_split_{a}{b}{c}{d}.cu"), "w") as fh:
+        with open(os.path.join(out_dir, f"eri_split_{tag}.cu"), "w") as fh:
+            fh.write("\n".join(lines))
+        lines = [f"// Generated by gen_eri.py: density-screened split-path launchers for the ({a}{b}|{c}{d}) class.",
+                 '#include "eri_split.cuh"', '#include "eri_split_dispatch.cuh"', "", "namespace hfg {", "",
+                 f"void launch_split_{tag}_scr(const EngineView &v, const ClassLaunch &cl, const SplitChunk &ch, int mode,",
+                 "                            bool ref, int prec, cudaStream_t s) {"] + head
+        launch(lines, "  ", f"eri_prim_split_kernel<{a}, {b}, {c}, {d}, {{r}}, kScreenFp64>", ref, "gridA")
+        lines.append("  if (prec == 2) {")
+        launch(lines, "    ", f"eri_prim_split_kernel<{a}, {b}, {c}, {d}, {{r}}, kScreenFp32>", ref, "gridA")
+        lines.append("  }")
+        lines.append("  switch (mode) {")
+        for mode in ("kJkRhf", "kJkUhf"):
+            lines.append(f"    case {mode}:")
+            launch(lines, "      ", f"eri_hrr_digest_kernel<{a}, {b}, {c}, {d}, {mode}, {{r}}, true>", ref, "gridB")
+            lines.append("      break;")
+        lines += ["    default:", "      break;", "  }"]
+        if not ref:
+            lines.append("  (void)ref;")
+        lines += ["}", "", "}  // namespace hfg", ""]
+        with open(os.path.join(out_dir, f"eri_split_{tag}_scr.cu"), "w") as fh:
             fh.write("\n".join(lines))
     lines = ["// Generated by gen_eri.py: split-path launcher table.", "#pragma once", '#include "hfg_internal.cuh"', "",
              "namespace hfg {", "",
-             "using SplitLauncher = void (*)(const EngineView &, const ClassLaunch &, const SplitChunk &, int, bool, cudaStream_t);"]
+             "using SplitLauncher = void (*)(const EngineView &, const ClassLaunch &, const SplitChunk &, int, bool, int, cudaStream_t);"]
     for (a, b, c, d) in quartets:
         if is_split_class(a, b, c, d):
-            lines.append(f"void launch_split_{a}{b}{c}{d}(const EngineView &v, const ClassLaunch &cl, const SplitChunk &ch, int mode, bool ref, cudaStream_t s);")
+            for suf in ("", "_scr"):
+                lines.append(f"void launch_split_{a}{b}{c}{d}{suf}(const EngineView &v, const ClassLaunch &cl, const SplitChunk &ch, int mode, bool ref, int prec, cudaStream_t s);")
     lines.append("")
     lines.append("// split launcher per class (same order as kClasses), nullptr for fused-only classes")
     lines.append("static const SplitLauncher kSplit[] = {")

@@ -13,12 +13,37 @@ constexpr double kBoysStep = 0.05;            // grid spacing in T
 constexpr double kBoysTmax = 36.0;            // above: asymptotic F_0 + upward recursion
 constexpr int kBoysGrid = 721;                // 36 / 0.05 + 1 grid points
 constexpr int kBoysOrders = kMaxLtot + kBoysTaylor;  // orders 0 .. 14 tabulated
-constexpr int kBoysRow = kBoysTaylor + 1;             // staged row: 7 Taylor terms + exp(-T_i)
+// staged row: 7 Taylor terms and exp(-T_i), 8 doubles.  Word k of row i is
+// stored at k ^ ((i >> 1) & 7) within the row: rows start on bank 0 or 16
+// only, and the swizzle spreads one column of 16 consecutive rows over all
+// 32 banks (plain rows put a whole warp's column on one bank pair).
+constexpr int kBoysRow = kBoysTaylor + 1;
+__host__ __device__ constexpr int boys_swizzle(int i, int k) { return i * kBoysRow + (k ^ ((i >> 1) & 7)); }
 
 constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = 32 * kWarpsPerBlock;
+__host__ __device__ constexpr int ncart(int L) { return (L + 1) * (L + 2) / 2; }
+
+// Warps per block of the fused class kernel.  The staged Boys table (46 KB)
+// admits 4 blocks per SM: the light classes (<= 9 integrals per quartet,
+// <= ~120 registers) run 8 warps per block so that the table is shared by
+// more warps; the register-heavy ones keep 4, where the register file, not
+// the table, sets the residency.
+__host__ __device__ constexpr int fused_warps(int la, int lb, int lc, int ld) {
+  return ncart(la) * ncart(lb) * ncart(lc) * ncart(ld) <= 9 ? 8 : 4;
+}
 
 enum Mode { kStorePacked = 0, kJkRhf = 1, kJkUhf = 2, kSchwarz = 3, kBlock = 4 };
+
+// Density screening and precision of a J/K launch.  kScreenNone: every
+// Schwarz-surviving quartet in FP64.  kScreenFp64 / kScreenFp32: quartets
+// whose density-weighted bound Q_ab Q_cd max|D| falls below the launch's
+// density threshold are skipped; of the rest, a task (one bra pair, <= 32
+// kets) whose largest bound reaches the mixed cutoff runs in the FP64
+// kernel, any other in the FP32 kernel (FP64 Boys function, FP32
+// recursions, FP64 J/K accumulation).  The two kernels split the tasks
+// between them by the same warp-uniform test.
+enum Screen { kScreenNone = 0, kScreenFp64 = 1, kScreenFp32 = 2 };
 
 // One primitive pair of a shell pair (first shell A with exponent a, second
 // B with exponent b): zeta = a+b, P = (aA+bB)/zeta, PA = P-A,
@@ -40,7 +65,8 @@ struct EngineView {
   const int *pair_ao_b;
   const double *pair_AB;      // [3*npairs] A - B
   const double *pair_Q;       // Schwarz bound
-  const float *pair_Dmax;     // max |D| over the pair's AO block (density screening)
+  const float *shell_dmax;    // [nshells][nshells] max |D| over each shell block (density screening)
+  int nshells;
   const double *boys_table;   // [kBoysGrid][kBoysOrders] F_m(T_i)
   int nbf;
   int reference_convention;   // 1: reproduce the reference's (dd|dd) ET rows
@@ -67,7 +93,10 @@ struct ClassLaunch {
   const double *Dt;      // total density for J in UHF
   double *J, *Ka, *Kb;   // accumulators (n x n)
   double *Qout;          // kSchwarz: per pair
-  int *fp32_counter;     // unused in FP64 kernels
+  // density screening (kScreenFp64 / kScreenFp32 launches)
+  float dens_threshold;  // skip quartets whose density-weighted bound is below
+  float mixed_cutoff;    // tasks whose largest bound is below run in FP32
+  unsigned long long *counters;  // [0] FP64, [1] FP32 quartets evaluated
 };
 
 // One chunk of a split-path class launch (see eri_split.cuh): scratch for
@@ -95,8 +124,6 @@ __device__ __forceinline__ double comp_norm<2>(int c) {
   return (c == 0 || c == 3 || c == 5) ? 0.57735026918962576451 : 1.0;
 }
 
-__host__ __device__ constexpr int ncart(int L) { return (L + 1) * (L + 2) / 2; }
-
 // Packed 8-fold index (IntegralsRepository.h:151-162)
 __device__ __forceinline__ long long tri(long long a, long long b) {
   return a < b ? b * (b + 1) / 2 + a : a * (a + 1) / 2 + b;
@@ -117,9 +144,10 @@ __device__ __forceinline__ void boys_eval(R *F, double T, double scale, const do
     const int i = __double2int_rn(T * (1.0 / kBoysStep));
     const double dt = i * kBoysStep - T;  // -(T - T_i)
     const double *t = tab + i * kBoysRow;
-    double f = t[6];
+    const int sw = (i >> 1) & 7;
+    double f = t[6 ^ sw];
 #pragma unroll
-    for (int k = 5; k >= 0; --k) f = fma(f, dt, t[k]);
+    for (int k = 5; k >= 0; --k) f = fma(f, dt, t[k ^ sw]);
     double fm[M + 1];
     fm[M] = f;
     if (M > 0) {
@@ -131,7 +159,7 @@ __device__ __forceinline__ void boys_eval(R *F, double T, double scale, const do
       x = fma(x, dt, 0.5);
       x = fma(x, dt, 1.0);
       x = fma(x, dt, 1.0);
-      const double e = t[7] * x;
+      const double e = t[7 ^ sw] * x;
       const double t2 = 2.0 * T;
 #pragma unroll
       for (int m = M - 1; m >= 0; --m) fm[m] = fma(t2, fm[m + 1], e) * (1.0 / (2 * m + 1));

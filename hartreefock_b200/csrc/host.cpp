@@ -7,6 +7,8 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
 #include <array>
 #include <cctype>
 #include <cmath>
@@ -20,6 +22,7 @@
 
 #include "../../include/hfgpu_driver.h"
 #include "../../include/hfgpu_host.hpp"
+#include "scf_device.h"
 
 namespace {
 
@@ -429,6 +432,32 @@ void shell_pair_one_electron(const ShellView &A, const ShellView &B, const std::
     ab2 += AB[d] * AB[d];
   }
   const int LT = A.L + B.L;
+  // horizontal transfer (a|b+1_d) = (a+1_d|b) + AB_d (a|b): each (x|y) is a
+  // fixed combination of (e|0) with e on A, the same for every primitive
+  // pair and nucleus
+  struct Term {
+    int l, m, nn;
+    double c;
+  };
+  std::vector<std::vector<Term>> hrr(na * nb);
+  for (int x = 0; x < na; ++x)
+    for (int y = 0; y < nb; ++y) {
+      std::vector<std::pair<std::array<int, 3>, double>> terms{{ca[x], 1.0}};
+      std::array<int, 3> rem = cb[y];
+      for (int d = 0; d < 3; ++d)
+        while (rem[d] > 0) {
+          std::vector<std::pair<std::array<int, 3>, double>> nt;
+          for (auto &tm : terms) {
+            auto up = tm.first;
+            up[d] += 1;
+            nt.push_back({up, tm.second});
+            nt.push_back({tm.first, tm.second * AB[d]});
+          }
+          terms.swap(nt);
+          --rem[d];
+        }
+      for (auto &tm : terms) hrr[x * nb + y].push_back(Term{tm.first[0], tm.first[1], tm.first[2], tm.second});
+    }
   for (int i = 0; i < A.nprim; ++i)
     for (int j = 0; j < B.nprim; ++j) {
       const double a = A.e[i], b = B.e[j], z = a + b, iz = 1.0 / z;
@@ -509,28 +538,12 @@ void shell_pair_one_electron(const ShellView &A, const ShellView &B, const std::
                 W[e[0]][e[1]][e[2]][mm] = val;
               }
             }
-        // horizontal transfer (a|b+1_d) = (a+1_d|b) + AB_d (a|b), on m = 0
-        for (int x = 0; x < na; ++x)
-          for (int y = 0; y < nb; ++y) {
-            // expand (p|q) by moving B's exponents onto A one unit at a time
-            std::vector<std::pair<std::array<int, 3>, double>> terms{{ca[x], 1.0}};
-            std::array<int, 3> rem = cb[y];
-            for (int d = 0; d < 3; ++d)
-              while (rem[d] > 0) {
-                std::vector<std::pair<std::array<int, 3>, double>> nt;
-                for (auto &tm : terms) {
-                  auto up = tm.first;
-                  up[d] += 1;
-                  nt.push_back({up, tm.second});
-                  nt.push_back({tm.first, tm.second * AB[d]});
-                }
-                terms.swap(nt);
-                --rem[d];
-              }
-            double val = 0;
-            for (auto &tm : terms) val += tm.second * W[tm.first[0]][tm.first[1]][tm.first[2]][0];
-            v[x * nb + y] -= nuc_z[c] * cc * val;
-          }
+        // horizontal transfer to B, on m = 0
+        for (int x = 0; x < na * nb; ++x) {
+          double val = 0;
+          for (const Term &tm : hrr[x]) val += tm.c * W[tm.l][tm.m][tm.nn][0];
+          v[x] -= nuc_z[c] * cc * val;
+        }
       }
     }
   for (int x = 0; x < na; ++x)
@@ -595,6 +608,8 @@ double IntegralsRepository::getElectronElectronDirect(int i, int j, int k, int l
   return v;
 }
 
+// QuantumMatrix.cpp:34-155 (overlap, kinetic, nuclear attraction), shell
+// pair by shell pair on the host's threads
 void IntegralsRepository::OneElectron(hfgpu::Matrix &S, hfgpu::Matrix &T, hfgpu::Matrix &V) const {
   const auto &t = molecule_->shellTable();
   const int n = t.nbf, ns = (int)t.L.size();
@@ -645,7 +660,13 @@ HartreeFockAlgorithm::HartreeFockAlgorithm(int iterations)
 HartreeFockAlgorithm::~HartreeFockAlgorithm() = default;
 
 void HartreeFockAlgorithm::Init(Systems::Molecule *molecule) {
+  const auto t_init = std::chrono::steady_clock::now();
   converged = false;
+  if (PrecisionForm()) {
+    integralsRepository.options.incremental = 1;
+    integralsRepository.options.density_screening = 1;
+    integralsRepository.options.mixed_cutoff = std::max(0.0, mixedCutoff);
+  }
   integralsRepository.Reset(molecule);
   Matrix T, Vn;
   integralsRepository.OneElectron(overlap, T, Vn);
@@ -670,29 +691,113 @@ void HartreeFockAlgorithm::Init(Systems::Molecule *molecule) {
   Vt = hfgpu::transpose(V);
   V = Vt = 0.5 * (V + Vt);
   inited = true;
+  secondsInit = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_init).count();
 }
 
 double HartreeFockAlgorithm::Calculate() {
   double curEnergy = 0, prevEnergy = std::numeric_limits<double>::infinity();
   if (!inited) return prevEnergy;
+  const auto t0 = std::chrono::steady_clock::now();
+  fockMilliseconds = 0;
+  fockBuilds = mixedSteps = 0;
+  fp32Quartets = fp64Quartets = 0;
+  secondsFock = secondsEigen = secondsDiis = secondsTotal = 0;
+  fp64Phase = !PrecisionCriteria();
+  fp64Steps = 0;
+  if (PrecisionForm()) {
+    hfg_ctx *ctx = integralsRepository.engine();
+    if (hfg_set_mixed_cutoff(ctx, std::max(0.0, mixedCutoff)) != HFG_OK || hfg_set_incremental(ctx, 1) != HFG_OK)
+      throw std::runtime_error(std::string("precision form: ") + hfg_last_error());
+  }
+  struct TotalTimer {
+    double &out;
+    std::chrono::steady_clock::time_point t0;
+    ~TotalTimer() { out = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+  } total_timer{secondsTotal, t0};
+  // the iterations run on the device; the public fields are synced around them
+  Device().reset_timers();
+  SyncToDevice();
+  struct CalcScope {
+    HartreeFockAlgorithm *a;
+    bool done = false;
+    ~CalcScope() {
+      a->inCalculate = false;
+      a->secondsEigen = a->device_ ? a->device_->eigen_seconds() : 0.0;
+      if (!done) {
+        try {
+          a->SyncFromDevice();
+        } catch (...) {
+        }
+      }
+    }
+  } scope{this};
+  inCalculate = true;
   int iter = 0;
   FirstIterations(iter, curEnergy, prevEnergy);
   if (terminate) return curEnergy;
-  if (UseDIIS && iter < maxDIISiterations && converged && normalIterAfterDIIS) {
+  // the reference's post-DIIS plain iterations (HartreeFockAlgorithm.cpp:117-121);
+  // the precision form ends with its FP64 iterations instead
+  const bool postDiis = !PrecisionCriteria() || fp64FinalConverge;
+  if (postDiis && UseDIIS && iter < maxDIISiterations && converged && normalIterAfterDIIS) {
     SelfConsistentIterations(iter, curEnergy, prevEnergy);
     if (terminate) return curEnergy;
   }
   NormalIterations(iter, curEnergy, prevEnergy);
   iterations = iter;
+  SyncFromDevice();
+  scope.done = true;
   return curEnergy;
+}
+
+// Plain form: the reference's test.  Precision form: leave the incremental
+// phase on its own (looser) test; from then on every build is a full FP64
+// build from the whole density, and the SCF is done after
+// fp64FinalIterations of them (or, with fp64FinalConverge, once the
+// reference's test passes as well).
+bool HartreeFockAlgorithm::ConvergedAfterStep(bool test, double dE, double rmsD) {
+  if (!PrecisionCriteria()) return test;
+  if (fp64Phase) return fp64Steps >= fp64FinalIterations && (test || !fp64FinalConverge);
+  // a small step alone is not enough: a stalled DIIS also takes small steps
+  if (test || (dE < mixedSwitchEnergy && rmsD < mixedSwitchDensity && lastErrorEst < mixedSwitchDiis)) {
+    if (PrecisionForm()) {
+      hfg_ctx *ctx = integralsRepository.engine();
+      if (hfg_set_mixed_cutoff(ctx, 0.0) != HFG_OK || hfg_set_incremental(ctx, 0) != HFG_OK)
+        throw std::runtime_error(std::string("precision form: ") + hfg_last_error());
+    }
+    fp64Phase = true;
+    fp64Steps = 0;
+  }
+  return false;
+}
+
+void HartreeFockAlgorithm::TraceStep(int iter, double energy, double dE, double rmsD) const {
+  if (!traceIterations) return;
+  std::fprintf(stderr, "scf iter %4d E %.12f dE %.3e rmsD %.3e diis %.3e phase %s build_ms %.3f\n", iter, energy, dE,
+               rmsD, lastErrorEst, fp64Phase ? "fp64" : (mixedCutoff > 0 ? "mixed" : "inc64"),
+               fockBuilds ? fockMilliseconds / fockBuilds : 0.0);
+}
+
+void HartreeFockAlgorithm::AccountFockBuild() {
+  hfg_stats st{};
+  if (hfg_ctx_stats(integralsRepository.engine(), &st) != HFG_OK)
+    throw std::runtime_error(std::string("hfg_ctx_stats: ") + hfg_last_error());
+  fockMilliseconds += st.last_build_ms;
+  ++fockBuilds;
+  fp32Quartets += st.fp32_shell_quartets;
+  fp64Quartets += st.fp64_shell_quartets;
+  if (fp64Phase) ++fp64Steps;
+  else ++mixedSteps;
 }
 
 void HartreeFockAlgorithm::FirstIterations(int &iter, double &curEnergy, double &prevEnergy) {
   for (; iter < maxIterations; ++iter) {
     const double rmsD = Step(iter);
     curEnergy = GetTotalEnergy();
-    if (std::fabs(prevEnergy - curEnergy) <= (UseDIIS ? kEnergyConvergenceDIIS : kEnergyConvergence) &&
-        rmsD < kRmsDConvergence && lastErrorEst < kDiisConvergence) {
+    const double dE = std::fabs(prevEnergy - curEnergy);
+    TraceStep(iter, curEnergy, dE, rmsD);
+    const bool test = dE <= (UseDIIS ? kEnergyConvergenceDIIS : kEnergyConvergence) && rmsD < kRmsDConvergence &&
+                      lastErrorEst < kDiisConvergence;
+    if (ConvergedAfterStep(test, dE, rmsD)) {
       converged = true;
       break;
     }
@@ -721,7 +826,10 @@ void HartreeFockAlgorithm::NormalIterations(int &iter, double &curEnergy, double
   for (; iter < maxIterations; ++iter) {
     const double rmsD = Step(iter);
     curEnergy = GetTotalEnergy();
-    if (std::fabs(prevEnergy - curEnergy) <= kEnergyConvergence && rmsD < kRmsDConvergence) {
+    const double dE = std::fabs(prevEnergy - curEnergy);
+    TraceStep(iter, curEnergy, dE, rmsD);
+    const bool test = dE <= kEnergyConvergence && rmsD < kRmsDConvergence;
+    if (ConvergedAfterStep(test, dE, rmsD)) {
       converged = true;
       return;
     }
@@ -748,8 +856,11 @@ double dot(const Matrix &a, const Matrix &b) {
   for (size_t x = 0; x < (size_t)a.rows() * a.cols(); ++x) s += a.data()[x] * b.data()[x];
   return s;
 }
+}  // namespace
+}  // namespace HartreeFock
+
 // least-squares solve of a small dense system by column-pivoted Householder QR
-std::vector<double> qr_solve(std::vector<double> A, int m, std::vector<double> b) {
+std::vector<double> hfgpu::detail::pulay_solve(std::vector<double> A, int m, std::vector<double> b) {
   const int n = m;
   std::vector<int> perm(n);
   for (int i = 0; i < n; ++i) perm[i] = i;
@@ -803,7 +914,8 @@ std::vector<double> qr_solve(std::vector<double> A, int m, std::vector<double> b
   for (int j = 0; j < n; ++j) x[perm[j]] = z[j];
   return x;
 }
-}  // namespace
+
+namespace HartreeFock {
 
 double Diis::Estimate(Matrix &value) const {
   const int nm = (int)errors_.size(), np1 = nm + 1;
@@ -817,34 +929,52 @@ double Diis::Estimate(Matrix &value) const {
   }
   last = std::sqrt(last);
   rhs[nm] = 1;
-  const std::vector<double> c = qr_solve(B, np1, rhs);
+  const std::vector<double> c = hfgpu::detail::pulay_solve(B, np1, rhs);
   value = Matrix::Zero(value.rows(), value.cols());
   for (int i = 0; i < nm; ++i) value = value + c[i] * values_[i];
   return last;
 }
 
 namespace {
-void two_electron_rhf(GaussianIntegrals::IntegralsRepository &repo, const Matrix &P, Matrix &G) {
-  G.resize(P.rows(), P.cols());
-  if (hfg_fock_rhf(repo.engine(), P.data(), G.data()) != HFG_OK)
-    throw std::runtime_error(std::string("hfg_fock_rhf: ") + hfg_last_error());
+struct ScopedSeconds {
+  double &acc;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  explicit ScopedSeconds(double &a) : acc(a) {}
+  ~ScopedSeconds() { acc += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+};
+void check_engine(hfg_status st, const char *what) {
+  if (st != HFG_OK) throw std::runtime_error(std::string(what) + ": " + hfg_last_error());
 }
-void two_electron_uhf(GaussianIntegrals::IntegralsRepository &repo, const Matrix &Pa, const Matrix &Pb, Matrix &Ga,
-                      Matrix &Gb) {
-  Ga.resize(Pa.rows(), Pa.cols());
-  Gb.resize(Pa.rows(), Pa.cols());
-  if (hfg_fock_uhf(repo.engine(), Pa.data(), Pb.data(), Ga.data(), Gb.data()) != HFG_OK)
-    throw std::runtime_error(std::string("hfg_fock_uhf: ") + hfg_last_error());
+// iteration-0 Fock matrix (RestrictedHartreeFock.cpp:175-186): the extended
+// Hueckel-like guess initGuess S_ij (h_ii + h_jj)/2, or h when initGuess = 0
+Matrix guess_fock(const Matrix &h, const Matrix &S, double initGuess) {
+  if (!(initGuess > 0)) return h;
+  const int n = h.rows();
+  Matrix F(n, n);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) F(i, j) = initGuess * S(i, j) * (h(i, i) + h(j, j)) * 0.5;
+  return F;
 }
-double rms_diff(const Matrix &a, const Matrix &b) {
-  double s = 0;
-  for (size_t x = 0; x < (size_t)a.rows() * a.cols(); ++x) {
-    const double d = a.data()[x] - b.data()[x];
-    s += d * d;
-  }
-  return s;
+double occupied_sum(const std::vector<double> &w, const std::vector<bool> &occupied) {
+  double e = 0;
+  for (size_t l = 0; l < occupied.size() && l < w.size(); ++l)
+    if (occupied[l]) e += w[l];
+  return e;
 }
 }  // namespace
+
+hfgpu::detail::DeviceScf &HartreeFockAlgorithm::Device() {
+  if (!device_) {
+    device_.reset(new hfgpu::detail::DeviceScf(numberOfOrbitals, integralsRepository.options.device));
+    device_->SetMatrices(h.data(), overlap.data(), V.data());
+  }
+  return *device_;
+}
+
+void HartreeFockAlgorithm::AccountDevice(double fock_wall_seconds) {
+  secondsFock += fock_wall_seconds;
+  AccountFockBuild();
+}
 
 void RestrictedHartreeFock::Init(Systems::Molecule *molecule) {
   HartreeFockAlgorithm::Init(molecule);
@@ -854,71 +984,59 @@ void RestrictedHartreeFock::Init(Systems::Molecule *molecule) {
   if (!nrOccupiedLevels) nrOccupiedLevels = 1;
   if (nrOccupiedLevels > (unsigned)numberOfOrbitals) nrOccupiedLevels = numberOfOrbitals;
   occupied.assign(nrOccupiedLevels, true);
+  device_.reset();
+  Device().ResetDiis();
 }
 
-void RestrictedHartreeFock::InitFockMatrix(int iter, Matrix &F) {
-  const int n = h.rows();
-  if (iter == 0) {  // RestrictedHartreeFock.cpp:175-186
-    if (initGuess > 0) {
-      F.resize(n, n);
-      for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j) F(i, j) = initGuess * overlap(i, j) * (h(i, i) + h(j, j)) * 0.5;
-    } else {
-      F = h;
-    }
+void RestrictedHartreeFock::SyncToDevice() { Device().SetDensity(0, DensityMatrix.data()); }
+
+void RestrictedHartreeFock::SyncFromDevice() {
+  const int n = numberOfOrbitals;
+  DensityMatrix.resize(n, n);
+  C.resize(n, n);
+  Device().CopyOut(0, DensityMatrix.data(), C.data());
+}
+
+// RestrictedHartreeFock::Step (RestrictedHartreeFock.cpp:61-166) with the
+// matrices on the device: F (guess, or h + G from the direct build, then
+// symmetrised), DIIS, F' = V F V, eigen-decomposition, C = V C', the new
+// density 2 C_occ C_occ^T, the energy, the density change and the mixing.
+double RestrictedHartreeFock::Step(int iter) {
+  hfgpu::detail::DeviceScf &d = Device();
+  if (!inCalculate) SyncToDevice();
+  const int n = numberOfOrbitals;
+  if (iter == 0) {
+    Matrix F = guess_fock(h, overlap, initGuess);
+    F = 0.5 * (F + hfgpu::transpose(F));
+    d.SetFock(0, F.data());
   } else {
-    Matrix G;
-    two_electron_rhf(integralsRepository, DensityMatrix, G);
-    F = h + G;
+    const auto t0 = std::chrono::steady_clock::now();
+    check_engine(hfg_fock_rhf_device(integralsRepository.engine(), d.density(0), d.g_buffer(0), d.stream()),
+                 "hfg_fock_rhf_device");
+    AccountDevice(std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+    d.FockFromG(0, d.g_buffer(0), true);
   }
-  F = 0.5 * (F + hfgpu::transpose(F));
-}
-
-bool RestrictedHartreeFock::DIISStep(int iter, Matrix &F) {
   bool used = false;
-  if (UseDIIS && iter && iter < maxDIISiterations) {
-    const Matrix err = overlap * DensityMatrix * F - F * DensityMatrix * overlap;
-    if (diis.AddValueAndError(F, err)) {
-      lastErrorEst = diis.Estimate(F);
+  if (UseDIIS && iter && iter < maxDIISiterations) {  // RestrictedHartreeFock.cpp:35-58
+    ScopedSeconds t(secondsDiis);
+    double est = 0;
+    if (d.DiisStep(0, &est)) {
+      lastErrorEst = est;
       used = true;
     }
   } else {
     lastErrorEst = 0;
   }
-  return used;
-}
-
-double RestrictedHartreeFock::Step(int iter) {
-  Matrix F;
-  InitFockMatrix(iter, F);
-  const bool used = DIISStep(iter, F);
-  const Matrix Ft = Vt * F * V;
-  Matrix Cp;
-  hfgpu::eigh(Ft, eigenvals, Cp);
-  C = V * Cp;
-  const int n = h.rows();
-  Matrix Pn(n, n);
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j < n; ++j) {
-      double s = 0;
-      for (unsigned v = 0; v < occupied.size(); ++v)
-        if (occupied[v]) s += C(i, v) * C(j, v);
-      Pn(i, j) = 2.0 * s;
-    }
+  eigenvals.resize(n);
+  d.Diagonalize(0, occupied, 2.0, eigenvals.data());
+  double trace_ph = 0, change2 = 0;
+  d.EnergyAndChange(0, &trace_ph, &change2);
   // CalculateEnergy (RestrictedHartreeFock.cpp:209-249)
-  double e = 0;
-  for (int i = 1; i < n; ++i)
-    for (int j = 0; j < i; ++j) e += Pn(i, j) * h(j, i);
-  e *= 2.0;
-  for (int i = 0; i < n; ++i) e += Pn(i, i) * h(i, i);
-  e *= 0.5;
-  for (unsigned l = 0; l < occupied.size(); ++l)
-    if (occupied[l]) e += eigenvals[l];
   HOMOEnergy = eigenvals[nrOccupiedLevels - 1];
-  totalEnergy = e + nuclearRepulsionEnergy;
-  const double rmsD = std::sqrt(rms_diff(Pn, DensityMatrix));
-  DensityMatrix = used ? Pn : alpha * Pn + (1.0 - alpha) * DensityMatrix;
-  return rmsD;
+  totalEnergy = 0.5 * trace_ph + occupied_sum(eigenvals, occupied) + nuclearRepulsionEnergy;
+  d.UpdateDensity(0, used, alpha);
+  if (!inCalculate) SyncFromDevice();
+  return std::sqrt(change2);
 }
 
 void UnrestrictedHartreeFock::Init(Systems::Molecule *molecule) {
@@ -944,89 +1062,77 @@ void UnrestrictedHartreeFock::Init(Systems::Molecule *molecule) {
   if (nrOccupiedLevelsMinus > n) nrOccupiedLevelsMinus = n;
   occupiedPlus.assign(nrOccupiedLevelsPlus, true);
   occupiedMinus.assign(nrOccupiedLevelsMinus, true);
+  device_.reset();
+  Device().ResetDiis();
 }
 
-void UnrestrictedHartreeFock::InitFockMatrices(int iter, Matrix &Fp, Matrix &Fm) {
-  const int n = h.rows();
+void UnrestrictedHartreeFock::SyncToDevice() {
+  Device().SetDensity(0, DensityMatrixPlus.data());
+  Device().SetDensity(1, DensityMatrixMinus.data());
+}
+
+void UnrestrictedHartreeFock::SyncFromDevice() {
+  const int n = numberOfOrbitals;
+  DensityMatrixPlus.resize(n, n);
+  DensityMatrixMinus.resize(n, n);
+  Cplus.resize(n, n);
+  Cminus.resize(n, n);
+  Device().CopyOut(0, DensityMatrixPlus.data(), Cplus.data());
+  Device().CopyOut(1, DensityMatrixMinus.data(), Cminus.data());
+}
+
+// UnrestrictedHartreeFock::Step (UnrestrictedHartreeFock.cpp:87-191) on the
+// device; the Fock matrices are not symmetrised, as in the reference.
+double UnrestrictedHartreeFock::Step(int iter) {
+  hfgpu::detail::DeviceScf &d = Device();
+  if (!inCalculate) SyncToDevice();
+  const int n = numberOfOrbitals;
   if (iter == 0) {  // UnrestrictedHartreeFock.cpp:199-222
-    if (initGuess > 0) {
-      Fp.resize(n, n);
-      for (int i = 0; i < n; ++i)
-        for (int j = 0; j < n; ++j) Fp(i, j) = initGuess * overlap(i, j) * (h(i, i) + h(j, j)) * 0.5;
-      Fm = Fp;
-    } else {
-      Fp = h;
-      Fm = h;
-    }
+    Matrix Fp = guess_fock(h, overlap, initGuess);
+    Matrix Fm = Fp;
     if (addAsymmetry && n > 1) {
       Fp(0, 1) += asymmetry;
       Fp(1, 0) = Fp(0, 1);
     }
+    d.SetFock(0, Fp.data());
+    d.SetFock(1, Fm.data());
   } else {
-    Matrix Gp, Gm;
-    two_electron_uhf(integralsRepository, DensityMatrixPlus, DensityMatrixMinus, Gp, Gm);
-    Fp = h + Gp;
-    Fm = h + Gm;
+    const auto t0 = std::chrono::steady_clock::now();
+    check_engine(hfg_fock_uhf_device(integralsRepository.engine(), d.density(0), d.density(1), d.g_buffer(0),
+                                     d.g_buffer(1), d.stream()),
+                 "hfg_fock_uhf_device");
+    AccountDevice(std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+    d.FockFromG(0, d.g_buffer(0), false);
+    d.FockFromG(1, d.g_buffer(1), false);
   }
-}
-
-bool UnrestrictedHartreeFock::DIISStep(int iter, Matrix &Fp, Matrix &Fm) {
   bool used = false;
-  if (UseDIIS && iter && iter < maxDIISiterations) {
-    diisPlus.AddValueAndError(Fp, overlap * DensityMatrixPlus * Fp - Fp * DensityMatrixPlus * overlap);
-    if (diisMinus.AddValueAndError(Fm, overlap * DensityMatrixMinus * Fm - Fm * DensityMatrixMinus * overlap)) {
-      lastErrorEst = diisMinus.Estimate(Fm) + diisPlus.Estimate(Fp);
+  if (UseDIIS && iter && iter < maxDIISiterations) {  // UnrestrictedHartreeFock.cpp:62-84
+    ScopedSeconds t(secondsDiis);
+    double ep = 0, em = 0;
+    const bool plus = d.DiisStep(0, &ep);
+    if (d.DiisStep(1, &em) && plus) {
+      lastErrorEst = em + ep;
       used = true;
     }
   } else {
     lastErrorEst = 0;
   }
-  return used;
-}
-
-double UnrestrictedHartreeFock::Step(int iter) {
-  Matrix Fp, Fm;
-  InitFockMatrices(iter, Fp, Fm);
-  const bool used = DIISStep(iter, Fp, Fm);
-  const int n = h.rows();
-  Matrix Cpp, Cmp;
-  hfgpu::eigh(Vt * Fp * V, eigenvalsplus, Cpp);
-  hfgpu::eigh(Vt * Fm * V, eigenvalsminus, Cmp);
-  Cplus = V * Cpp;
-  Cminus = V * Cmp;
-  Matrix Pp(n, n), Pm(n, n);
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j < n; ++j) {
-      double sp = 0, sm = 0;
-      for (unsigned v = 0; v < occupiedPlus.size(); ++v)
-        if (occupiedPlus[v]) sp += Cplus(i, v) * Cplus(j, v);
-      for (unsigned v = 0; v < occupiedMinus.size(); ++v)
-        if (occupiedMinus[v]) sm += Cminus(i, v) * Cminus(j, v);
-      Pp(i, j) = sp;
-      Pm(i, j) = sm;
-    }
+  eigenvalsplus.resize(n);
+  eigenvalsminus.resize(n);
+  d.Diagonalize(0, occupiedPlus, 1.0, eigenvalsplus.data());
+  d.Diagonalize(1, occupiedMinus, 1.0, eigenvalsminus.data());
+  double tp = 0, tm = 0, cp = 0, cm = 0;
+  d.EnergyAndChange(0, &tp, &cp);
+  d.EnergyAndChange(1, &tm, &cm);
   // CalculateEnergy (UnrestrictedHartreeFock.cpp:246-293)
-  double e = 0;
-  for (int i = 1; i < n; ++i)
-    for (int j = 0; j < i; ++j) e += (Pp(i, j) + Pm(i, j)) * h(j, i);
-  e *= 2.0;
-  for (int i = 0; i < n; ++i) e += (Pp(i, i) + Pm(i, i)) * h(i, i);
-  for (unsigned l = 0; l < occupiedPlus.size(); ++l)
-    if (occupiedPlus[l]) e += eigenvalsplus[l];
-  for (unsigned l = 0; l < occupiedMinus.size(); ++l)
-    if (occupiedMinus[l]) e += eigenvalsminus[l];
+  const double e = tp + tm + occupied_sum(eigenvalsplus, occupiedPlus) + occupied_sum(eigenvalsminus, occupiedMinus);
   HOMOEnergy = std::max(nrOccupiedLevelsPlus ? eigenvalsplus[nrOccupiedLevelsPlus - 1] : 0.0,
                         nrOccupiedLevelsMinus ? eigenvalsminus[nrOccupiedLevelsMinus - 1] : 0.0);
   totalEnergy = e / 2.0 + nuclearRepulsionEnergy;
-  const double rmsD = std::sqrt(rms_diff(Pp, DensityMatrixPlus) + rms_diff(Pm, DensityMatrixMinus));
-  if (used) {
-    DensityMatrixPlus = Pp;
-    DensityMatrixMinus = Pm;
-  } else {
-    DensityMatrixPlus = alpha * Pp + (1.0 - alpha) * DensityMatrixPlus;
-    DensityMatrixMinus = alpha * Pm + (1.0 - alpha) * DensityMatrixMinus;
-  }
-  return rmsD;
+  d.UpdateDensity(0, used, alpha);
+  d.UpdateDensity(1, used, alpha);
+  if (!inCalculate) SyncFromDevice();
+  return std::sqrt(cp + cm);
 }
 
 }  // namespace HartreeFock
@@ -1069,6 +1175,14 @@ void hfd_default_scf_opts(hfd_scf_opts *o) {
   o->post_diis = 500;
   o->eri_convention = HFG_ERI_REFERENCE;
   o->schwarz_threshold = 1e-12;
+  o->mixed_cutoff = 0;
+  o->mixed_switch_energy = 1e-7;
+  o->mixed_switch_density = 1e-7;
+  o->mixed_switch_diis = 1e-6;
+  o->fp64_final_iterations = 2;
+  o->fp64_final_converge = 0;
+  o->incremental = 0;
+  o->trace = 0;
 }
 
 hfg_status hfd_scf(const char *basis_path, int32_t natoms, const int32_t *Z, const double *xyz,
@@ -1089,6 +1203,15 @@ hfg_status hfd_scf(const char *basis_path, int32_t natoms, const int32_t *Z, con
     algo->integralsRepository.options.eri_convention = opts->eri_convention;
     algo->integralsRepository.options.schwarz_threshold = opts->schwarz_threshold;
     algo->storedIntegralsBudget = 0;  // direct SCF: no stored table needed
+    algo->mixedCutoff = opts->mixed_cutoff;
+    algo->mixedSwitchEnergy = opts->mixed_switch_energy;
+    algo->fp64FinalIterations = opts->fp64_final_iterations;
+    algo->mixedSwitchDensity = opts->mixed_switch_density;
+    algo->mixedSwitchDiis = opts->mixed_switch_diis;
+    algo->fp64FinalConverge = opts->fp64_final_converge != 0;
+    algo->stopAtPrecisionTest = opts->stop_at_precision_test != 0;
+    algo->incrementalFock = opts->incremental != 0;
+    algo->traceIterations = opts->trace != 0;
     algo->Init(&mol);
     const double e = algo->Calculate();
     std::memset(result, 0, sizeof *result);
@@ -1097,6 +1220,16 @@ hfg_status hfd_scf(const char *basis_path, int32_t natoms, const int32_t *Z, con
     result->converged = algo->converged ? 1 : 0;
     result->iterations = algo->iterations;
     result->nbf = algo->numberOfOrbitals;
+    result->fock_builds = algo->fockBuilds;
+    result->fock_ms_total = algo->fockMilliseconds;
+    result->fp32_quartets = algo->fp32Quartets;
+    result->fp64_quartets = algo->fp64Quartets;
+    result->mixed_steps = algo->mixedSteps;
+    result->seconds_fock = algo->secondsFock;
+    result->seconds_eigen = algo->secondsEigen;
+    result->seconds_diis = algo->secondsDiis;
+    result->seconds_total = algo->secondsTotal;
+    result->seconds_init = algo->secondsInit;
     const int64_t nn = (int64_t)result->nbf * result->nbf;
     if (density) {
       if (opts->unrestricted) {

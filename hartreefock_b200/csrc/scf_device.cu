@@ -1,0 +1,283 @@
+// Device-resident SCF iteration for the host API (include/hfgpu_host.hpp):
+// the steps of RestrictedHartreeFock::Step (RestrictedHartreeFock.cpp:61-166)
+// and UnrestrictedHartreeFock::Step (UnrestrictedHartreeFock.cpp:87-191)
+// with every matrix in HBM.  F = h + G comes straight from the engine's
+// direct build on the same stream, DIIS (DIIS.h:34-96) keeps its Fock and
+// error matrices on the device (Pulay B matrix from one Gram product, the
+// small (m+1)x(m+1) solve on the host), the orthogonalised Fock matrix is
+// diagonalised by cuSOLVER (dsyevd) and the density is one product of the
+// occupied coefficients.  Per step only scalars (energy terms, norms, the
+// B matrix, eigenvalues) cross to the host.  All arithmetic is FP64.
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "scf_device.h"
+
+namespace hfgpu {
+namespace detail {
+
+namespace {
+
+void ck(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+void ck(cublasStatus_t e, const char *what) {
+  if (e != CUBLAS_STATUS_SUCCESS) throw std::runtime_error(std::string(what) + ": cuBLAS status " + std::to_string((int)e));
+}
+void ck(cusolverStatus_t e, const char *what) {
+  if (e != CUSOLVER_STATUS_SUCCESS)
+    throw std::runtime_error(std::string(what) + ": cuSOLVER status " + std::to_string((int)e));
+}
+
+// F = h + G (G may be null: F = h), then F = (F + F^T)/2 when `sym`
+__global__ void fock_from_g(const double *h, const double *G, double *F, int n, int sym) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n * n; x += gridDim.x * blockDim.x) {
+    const int i = x / n, j = x - i * n;
+    const double a = h[x] + (G ? G[x] : 0.0);
+    if (sym) {
+      const double b = h[j * n + i] + (G ? G[j * n + i] : 0.0);
+      F[x] = 0.5 * (a + b);
+    } else {
+      F[x] = a;
+    }
+  }
+}
+
+// C_w = C with the columns of unoccupied levels zeroed (occ[k] = 0/1)
+__global__ void mask_columns(const double *C, const int *occ, double *Cw, int n) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n * n; x += gridDim.x * blockDim.x) {
+    const int k = x % n;
+    Cw[x] = occ[k] ? C[x] : 0.0;
+  }
+}
+
+int grid_of(size_t nn) { return (int)std::max<size_t>(1, std::min<size_t>(2048, (nn + 255) / 256)); }
+
+}  // namespace
+
+DeviceScf::DeviceScf(int n, int device) : n_(n), device_(device) {
+  ck(cudaSetDevice(device), "cudaSetDevice");
+  ck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  ck(cublasCreate(&blas_), "cublasCreate");
+  ck(cublasSetStream(blas_, stream_), "cublasSetStream");
+  ck(cusolverDnCreate(&solver_), "cusolverDnCreate");
+  ck(cusolverDnSetStream(solver_, stream_), "cusolverDnSetStream");
+  const size_t nn = (size_t)n * n;
+  for (double **p : {&h_, &S_, &V_, &T1_, &T2_, &Ft_, &W_, &err_})
+    ck(cudaMalloc((void **)p, nn * sizeof(double)), "cudaMalloc");
+  for (int s = 0; s < 2; ++s)
+    for (double **p : {&P_[s], &Pn_[s], &F_[s], &G_[s], &C_[s]}) ck(cudaMalloc((void **)p, nn * sizeof(double)), "cudaMalloc");
+  ck(cudaMalloc((void **)&w_, 2 * (size_t)n * sizeof(double)), "cudaMalloc");
+  ck(cudaMalloc((void **)&info_, sizeof(int)), "cudaMalloc");
+  ck(cudaMalloc((void **)&occ_dev_, (size_t)n * sizeof(int)), "cudaMalloc");
+  ck(cudaMalloc((void **)&scalars_, 64 * sizeof(double)), "cudaMalloc");
+  ck(cudaMalloc((void **)&coef_, 16 * sizeof(double)), "cudaMalloc");
+  ck(cudaMallocHost((void **)&host_scalars_, 64 * sizeof(double)), "cudaMallocHost");
+  ck(cudaMallocHost((void **)&host_info_, sizeof(int)), "cudaMallocHost");
+  ck(cudaMallocHost((void **)&host_w_, 2 * (size_t)n * sizeof(double)), "cudaMallocHost");
+  ck(cusolverDnDsyevd_bufferSize(solver_, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, Ft_, n, w_, &lwork_),
+     "dsyevd_bufferSize");
+  ck(cudaMalloc((void **)&work_, (size_t)std::max(lwork_, 1) * sizeof(double)), "cudaMalloc");
+  for (int s = 0; s < 2; ++s) {
+    ck(cudaMalloc((void **)&diis_F_[s], kDiisKeep * nn * sizeof(double)), "cudaMalloc");
+    ck(cudaMalloc((void **)&diis_E_[s], kDiisKeep * nn * sizeof(double)), "cudaMalloc");
+  }
+  for (auto &e : ev_) ck(cudaEventCreate(&e), "cudaEventCreate");
+}
+
+DeviceScf::~DeviceScf() {
+  cudaSetDevice(device_);
+  if (stream_) cudaStreamSynchronize(stream_);
+  for (double *p : {h_, S_, V_, T1_, T2_, Ft_, W_, err_, w_, scalars_, coef_, work_}) cudaFree(p);
+  for (int s = 0; s < 2; ++s) {
+    for (double *p : {P_[s], Pn_[s], F_[s], G_[s], C_[s], diis_F_[s], diis_E_[s]}) cudaFree(p);
+  }
+  cudaFree(info_);
+  cudaFree(occ_dev_);
+  cudaFreeHost(host_scalars_);
+  cudaFreeHost(host_w_);
+  cudaFreeHost(host_info_);
+  for (auto &e : ev_)
+    if (e) cudaEventDestroy(e);
+  if (solver_) cusolverDnDestroy(solver_);
+  if (blas_) cublasDestroy(blas_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void DeviceScf::upload(double *dst, const double *src) {
+  ck(cudaMemcpyAsync(dst, src, (size_t)n_ * n_ * sizeof(double), cudaMemcpyHostToDevice, stream_), "upload");
+}
+void DeviceScf::download(double *dst, const double *src) {
+  ck(cudaMemcpyAsync(dst, src, (size_t)n_ * n_ * sizeof(double), cudaMemcpyDeviceToHost, stream_), "download");
+}
+
+void DeviceScf::SetMatrices(const double *h, const double *S, const double *V) {
+  upload(h_, h);
+  upload(S_, S);
+  upload(V_, V);
+  ck(cudaStreamSynchronize(stream_), "SetMatrices");
+}
+
+void DeviceScf::SetDensity(int spin, const double *P) {
+  upload(P_[spin], P);
+  ck(cudaStreamSynchronize(stream_), "SetDensity");
+}
+
+void DeviceScf::ResetDiis() { diis_count_[0] = diis_count_[1] = diis_head_[0] = diis_head_[1] = 0; }
+
+// row-major C(MxN) = alpha op(A) op(B) + beta C: the column-major product
+// C^T = op(B)^T op(A)^T, so the operands swap and keep their op flags
+void DeviceScf::gemm(bool ta, bool tb, int M, int N, int K, double alpha, const double *A, int lda, const double *B,
+                     int ldb, double beta, double *C, int ldc) {
+  ck(cublasDgemm(blas_, tb ? CUBLAS_OP_T : CUBLAS_OP_N, ta ? CUBLAS_OP_T : CUBLAS_OP_N, N, M, K, &alpha, B, ldb, A,
+                 lda, &beta, C, ldc),
+     "cublasDgemm");
+}
+
+void DeviceScf::FockFromG(int spin, const double *G, bool symmetrize) {
+  fock_from_g<<<grid_of((size_t)n_ * n_), 256, 0, stream_>>>(h_, G, F_[spin], n_, symmetrize ? 1 : 0);
+  ck(cudaGetLastError(), "fock_from_g");
+}
+
+void DeviceScf::SetFock(int spin, const double *F) { upload(F_[spin], F); }
+
+// DIIS.h:9-96 on the device: ring of the last kDiisKeep (F, error) pairs;
+// error = S P F - F P S = Z - Z^T with Z = S P F (S, P, F symmetric).
+// Returns true once kDiisFirst pairs are held and extrapolates F in place;
+// *err_est = sqrt of the two newest errors' squared norms.
+bool DeviceScf::DiisStep(int spin, double *err_est) {
+  const int n = n_;
+  const size_t nn = (size_t)n * n;
+  gemm(false, false, n, n, n, 1.0, S_, n, P_[spin], n, 0.0, T1_, n);
+  gemm(false, false, n, n, n, 1.0, T1_, n, F_[spin], n, 0.0, T2_, n);
+  const int slot = diis_head_[spin];
+  double *E = diis_E_[spin] + (size_t)slot * nn;
+  const double one = 1.0, mone = -1.0;
+  ck(cublasDgeam(blas_, CUBLAS_OP_N, CUBLAS_OP_T, n, n, &one, T2_, n, &mone, T2_, n, E, n), "cublasDgeam");
+  ck(cudaMemcpyAsync(diis_F_[spin] + (size_t)slot * nn, F_[spin], nn * sizeof(double), cudaMemcpyDeviceToDevice,
+                     stream_),
+     "diis copy");
+  diis_head_[spin] = (slot + 1) % kDiisKeep;
+  diis_count_[spin] = std::min(diis_count_[spin] + 1, kDiisKeep);
+  const int m = diis_count_[spin];
+  if (m < kDiisFirst) {
+    *err_est = 0;
+    return false;
+  }
+  // Gram matrix of the error ring (slot order): row-major m x m = E E^T
+  gemm(false, true, m, m, (int)nn, 1.0, diis_E_[spin], (int)nn, diis_E_[spin], (int)nn, 0.0, scalars_, m);
+  ck(cudaMemcpyAsync(host_scalars_, scalars_, (size_t)m * m * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+     "gram");
+  ck(cudaStreamSynchronize(stream_), "gram sync");
+  // logical order oldest .. newest, as the reference's list
+  std::vector<int> order(m);
+  const int oldest = (diis_head_[spin] - m + kDiisKeep) % kDiisKeep;
+  for (int i = 0; i < m; ++i) order[i] = (oldest + i) % kDiisKeep;
+  const int np1 = m + 1;
+  std::vector<double> B((size_t)np1 * np1, 0.0), rhs(np1, 0.0);
+  double last = 0;
+  for (int i = 0; i < m; ++i) {
+    for (int j = 0; j < m; ++j) B[(size_t)i * np1 + j] = host_scalars_[order[i] * m + order[j]];
+    if (i == m - 1 || i == m - 2) last += B[(size_t)i * np1 + i];
+    B[(size_t)m * np1 + i] = B[(size_t)i * np1 + m] = 1;
+  }
+  *err_est = std::sqrt(last);
+  rhs[m] = 1;
+  const std::vector<double> c = pulay_solve(B, np1, rhs);
+  double cs[kDiisKeep] = {0};
+  for (int i = 0; i < m; ++i) cs[order[i]] = c[i];
+  ck(cudaMemcpyAsync(coef_, cs, sizeof cs, cudaMemcpyHostToDevice, stream_), "coef");
+  // F = sum_slot c_slot F_slot: (1 x m) (m x nn) row-major
+  gemm(false, false, 1, (int)nn, m, 1.0, coef_, m, diis_F_[spin], (int)nn, 0.0, F_[spin], (int)nn);
+  ck(cudaStreamSynchronize(stream_), "diis sync");  // cs lives on this frame
+  return true;
+}
+
+// Ft = V F V, eigen-decomposition, C = V Cp, Pn = factor * C_occ C_occ^T.
+void DeviceScf::Diagonalize(int spin, const std::vector<bool> &occupied, double factor, double *eigenvalues) {
+  const int n = n_;
+  gemm(false, false, n, n, n, 1.0, V_, n, F_[spin], n, 0.0, T1_, n);
+  gemm(false, false, n, n, n, 1.0, T1_, n, V_, n, 0.0, Ft_, n);
+  ck(cudaEventRecord(ev_[2], stream_), "event");
+  // symmetric input: row-major == column-major; on return column k of the
+  // column-major array is eigenvector k, i.e. row k of the row-major view
+  ck(cusolverDnDsyevd(solver_, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, Ft_, n, w_ + spin * n, work_,
+                      lwork_, info_),
+     "dsyevd");
+  ck(cudaEventRecord(ev_[3], stream_), "event");
+  // C = V Cp = V X^T with X the row-major eigenvector rows
+  gemm(false, true, n, n, n, 1.0, V_, n, Ft_, n, 0.0, C_[spin], n);
+  int nocc = 0;
+  bool prefix = true;
+  for (size_t k = 0; k < occupied.size(); ++k) {
+    if (occupied[k]) {
+      if ((int)k != nocc) prefix = false;
+      ++nocc;
+    }
+  }
+  if (prefix) {
+    if (nocc > 0)
+      gemm(false, true, n, n, nocc, factor, C_[spin], n, C_[spin], n, 0.0, Pn_[spin], n);
+    else
+      ck(cudaMemsetAsync(Pn_[spin], 0, (size_t)n * n * sizeof(double), stream_), "memset");
+  } else {
+    std::vector<int> occ(n, 0);
+    for (size_t k = 0; k < occupied.size() && (int)k < n; ++k) occ[k] = occupied[k] ? 1 : 0;
+    ck(cudaMemcpyAsync(occ_dev_, occ.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, stream_), "occ");
+    mask_columns<<<grid_of((size_t)n * n), 256, 0, stream_>>>(C_[spin], occ_dev_, W_, n);
+    gemm(false, true, n, n, n, factor, W_, n, W_, n, 0.0, Pn_[spin], n);
+    ck(cudaStreamSynchronize(stream_), "occ sync");
+  }
+  ck(cudaMemcpyAsync(host_w_ + spin * n, w_ + spin * n, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+     "w");
+  ck(cudaMemcpyAsync(host_info_, info_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "info");
+  ck(cudaStreamSynchronize(stream_), "diag sync");
+  const int info = *host_info_;
+  if (info != 0) throw std::runtime_error("dsyevd did not converge (info " + std::to_string(info) + ")");
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, ev_[2], ev_[3]) == cudaSuccess) eigen_seconds_ += ms * 1e-3;
+  std::copy(host_w_ + spin * n, host_w_ + (spin + 1) * n, eigenvalues);
+}
+
+// sum_ij Pn_ij h_ij (symmetric h), and ||Pn - P||_F^2
+void DeviceScf::EnergyAndChange(int spin, double *trace_ph, double *change2) {
+  const int n = n_;
+  const int nn = n * n;
+  ck(cublasSetPointerMode(blas_, CUBLAS_POINTER_MODE_DEVICE), "pointer mode");
+  ck(cublasDdot(blas_, nn, Pn_[spin], 1, h_, 1, scalars_), "ddot");
+  const double one = 1.0, mone = -1.0;
+  ck(cublasSetPointerMode(blas_, CUBLAS_POINTER_MODE_HOST), "pointer mode");
+  ck(cublasDgeam(blas_, CUBLAS_OP_N, CUBLAS_OP_N, n, n, &one, Pn_[spin], n, &mone, P_[spin], n, W_, n), "geam");
+  ck(cublasSetPointerMode(blas_, CUBLAS_POINTER_MODE_DEVICE), "pointer mode");
+  ck(cublasDdot(blas_, nn, W_, 1, W_, 1, scalars_ + 1), "ddot");
+  ck(cublasSetPointerMode(blas_, CUBLAS_POINTER_MODE_HOST), "pointer mode");
+  ck(cudaMemcpyAsync(host_scalars_, scalars_, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream_), "scalars");
+  ck(cudaStreamSynchronize(stream_), "scalars sync");
+  *trace_ph = host_scalars_[0];
+  *change2 = host_scalars_[1];
+}
+
+// P = Pn (DIIS step) or alpha Pn + (1 - alpha) P (mixing)
+void DeviceScf::UpdateDensity(int spin, bool take_new, double alpha) {
+  const int n = n_;
+  const double a = take_new ? 1.0 : alpha, b = take_new ? 0.0 : 1.0 - alpha;
+  ck(cublasDgeam(blas_, CUBLAS_OP_N, CUBLAS_OP_N, n, n, &a, Pn_[spin], n, &b, P_[spin], n, P_[spin], n), "geam");
+}
+
+void DeviceScf::Sync() { ck(cudaStreamSynchronize(stream_), "sync"); }
+
+void DeviceScf::CopyOut(int spin, double *P, double *C) {
+  if (P) download(P, P_[spin]);
+  if (C) download(C, C_[spin]);
+  Sync();
+}
+
+}  // namespace detail
+}  // namespace hfgpu

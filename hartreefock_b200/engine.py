@@ -25,7 +25,7 @@ EXPORTED = ["hfg_default_opts", "hfg_last_error", "hfg_device_count", "hfg_ctx_c
             "hfg_ctx_nbf", "hfg_packed_size", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet",
             "hfg_fock_rhf", "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz",
             "hfg_ctx_stats", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak",
-            "hfg_fock_rhf_noalloc"]
+            "hfg_fock_rhf_noalloc", "hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental"]
 
 
 class HfgError(RuntimeError):
@@ -43,13 +43,15 @@ class hfg_shells(ctypes.Structure):
 class hfg_opts(ctypes.Structure):
     _fields_ = [("schwarz_threshold", ctypes.c_double), ("mixed_cutoff", ctypes.c_double),
                 ("eri_convention", ctypes.c_int32), ("device", ctypes.c_int32),
-                ("density_screening", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5)]
+                ("density_screening", ctypes.c_int32), ("incremental", ctypes.c_int32),
+                ("density_threshold", ctypes.c_double), ("reserved", ctypes.c_int32 * 2)]
 
 
 class hfg_stats(ctypes.Structure):
     _fields_ = [("shell_pairs", ctypes.c_int64), ("shell_quartets", ctypes.c_int64),
                 ("function_quartets", ctypes.c_int64), ("primitive_quartets", ctypes.c_int64),
-                ("fp32_shell_quartets", ctypes.c_int64), ("flops", ctypes.c_double),
+                ("fp32_shell_quartets", ctypes.c_int64), ("fp64_shell_quartets", ctypes.c_int64),
+                ("flops", ctypes.c_double),
                 ("last_build_ms", ctypes.c_double), ("kernel_launches", ctypes.c_int32),
                 ("reserved", ctypes.c_int32)]
 
@@ -97,7 +99,10 @@ def library(path: str = LIB_PATH):
     L.hfg_set_profiling.argtypes = [vp, i32]
     L.hfg_class_profile.argtypes = [vp, ctypes.POINTER(hfg_class_time), i32, ctypes.POINTER(i32)]
     L.hfg_measure_fp64_peak.argtypes = [i32, ctypes.POINTER(ctypes.c_double)]
-    for name in ("hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak", "hfg_ctx_create", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet", "hfg_fock_rhf",
+    L.hfg_fock_reset.argtypes = [vp]
+    L.hfg_set_mixed_cutoff.argtypes = [vp, ctypes.c_double]
+    L.hfg_set_incremental.argtypes = [vp, i32]
+    for name in ("hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak", "hfg_ctx_create", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet", "hfg_fock_rhf",
                  "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz", "hfg_ctx_stats"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
@@ -129,7 +134,8 @@ class Engine:
     """One molecule's ERI / Fock-build context on one GPU."""
 
     def __init__(self, Z, xyz, basis: str, schwarz_threshold: float = 1e-12, eri_convention: int = ERI_REFERENCE,
-                 device: int = 0, mixed_cutoff: float = 0.0, density_screening: bool = False):
+                 device: int = 0, mixed_cutoff: float = 0.0, density_screening: bool = False,
+                 incremental: bool = False, density_threshold: float = 0.0):
         self.table: ShellTable = shell_table(Z, xyz, basis)
         self.Z, self.xyz, self.basis = list(Z), np.asarray(xyz, dtype=np.float64).reshape(-1, 3), basis
         t = self.table
@@ -142,6 +148,8 @@ class Engine:
         o.device = device
         o.mixed_cutoff = mixed_cutoff
         o.density_screening = int(density_screening)
+        o.incremental = int(incremental)
+        o.density_threshold = density_threshold
         self.opts = o
         h = ctypes.c_void_p()
         _check(library().hfg_ctx_create(ctypes.byref(sh), ctypes.byref(o), ctypes.byref(h)))
@@ -202,6 +210,16 @@ class Engine:
         _check(library().hfg_fock_uhf_device(self._h, ctypes.c_void_p(Pa_ptr), ctypes.c_void_p(Pb_ptr),
                                              ctypes.c_void_p(Ga_ptr), ctypes.c_void_p(Gb_ptr),
                                              ctypes.c_void_p(stream)))
+
+    def fock_reset(self):
+        """Drop the incremental history: the next build starts from the full density."""
+        _check(library().hfg_fock_reset(self._h))
+
+    def set_mixed_cutoff(self, cutoff: float):
+        _check(library().hfg_set_mixed_cutoff(self._h, float(cutoff)))
+
+    def set_incremental(self, on: bool):
+        _check(library().hfg_set_incremental(self._h, int(on)))
 
     def schwarz(self) -> np.ndarray:
         n = len(self.table.L)

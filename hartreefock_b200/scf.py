@@ -18,13 +18,22 @@ class hfd_scf_opts(ctypes.Structure):
     _fields_ = [("unrestricted", ctypes.c_int32), ("alpha", ctypes.c_double), ("init_guess", ctypes.c_double),
                 ("use_diis", ctypes.c_int32), ("post_diis", ctypes.c_int32), ("alpha_electrons", ctypes.c_int32),
                 ("beta_electrons", ctypes.c_int32), ("eri_convention", ctypes.c_int32),
-                ("schwarz_threshold", ctypes.c_double)]
+                ("schwarz_threshold", ctypes.c_double), ("mixed_cutoff", ctypes.c_double),
+                ("mixed_switch_energy", ctypes.c_double), ("mixed_switch_density", ctypes.c_double),
+                ("mixed_switch_diis", ctypes.c_double),
+                ("fp64_final_iterations", ctypes.c_int32), ("fp64_final_converge", ctypes.c_int32),
+                ("incremental", ctypes.c_int32), ("trace", ctypes.c_int32),
+                ("stop_at_precision_test", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class hfd_scf_result(ctypes.Structure):
     _fields_ = [("energy", ctypes.c_double), ("homo", ctypes.c_double), ("converged", ctypes.c_int32),
-                ("iterations", ctypes.c_int32), ("nbf", ctypes.c_int32), ("reserved", ctypes.c_int32),
-                ("fock_ms_total", ctypes.c_double)]
+                ("iterations", ctypes.c_int32), ("nbf", ctypes.c_int32), ("fock_builds", ctypes.c_int32),
+                ("fock_ms_total", ctypes.c_double), ("fp32_quartets", ctypes.c_int64),
+                ("fp64_quartets", ctypes.c_int64), ("mixed_steps", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("seconds_fock", ctypes.c_double), ("seconds_eigen", ctypes.c_double),
+                ("seconds_diis", ctypes.c_double), ("seconds_total", ctypes.c_double),
+                ("seconds_init", ctypes.c_double)]
 
 
 DRIVER_SYMBOLS = ["hfd_default_scf_opts", "hfd_last_error", "hfd_scf", "hfd_one_electron"]
@@ -50,8 +59,15 @@ def _lib():
 
 def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75, use_diis=True, post_diis=500,
             alpha_electrons=0, beta_electrons=0, eri_convention=E.ERI_REFERENCE, schwarz_threshold=1e-12,
-            want_density=True):
-    """RestrictedHartreeFock / UnrestrictedHartreeFock Init + Calculate."""
+            want_density=True, mixed_cutoff=0.0, mixed_switch_energy=1e-7, mixed_switch_density=1e-7,
+            mixed_switch_diis=1e-6,
+            fp64_final_iterations=2, fp64_final_converge=False, incremental=False, trace=False,
+            stop_at_precision_test=False):
+    """RestrictedHartreeFock / UnrestrictedHartreeFock Init + Calculate.
+
+    mixed_cutoff > 0 selects the precision form of the Fock builds (FP32
+    below the cutoff, incremental from the density difference, all-FP64
+    final iterations); incremental=True alone gives FP64 incremental builds."""
     L = _lib()
     o = hfd_scf_opts()
     L.hfd_default_scf_opts(ctypes.byref(o))
@@ -59,6 +75,12 @@ def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75,
     o.use_diis, o.post_diis = int(use_diis), post_diis
     o.alpha_electrons, o.beta_electrons = alpha_electrons, beta_electrons
     o.eri_convention, o.schwarz_threshold = eri_convention, schwarz_threshold
+    o.mixed_cutoff, o.mixed_switch_energy = mixed_cutoff, mixed_switch_energy
+    o.fp64_final_iterations, o.incremental = fp64_final_iterations, int(incremental)
+    o.mixed_switch_density, o.fp64_final_converge = mixed_switch_density, int(fp64_final_converge)
+    o.mixed_switch_diis = mixed_switch_diis
+    o.trace = int(trace)
+    o.stop_at_precision_test = int(stop_at_precision_test)
     z = np.ascontiguousarray(Z, dtype=np.int32)
     x = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
     nbf_guess = 40 * len(z) + 64
@@ -71,7 +93,10 @@ def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75,
     if st != 0:
         raise E.HfgError(st, L.hfd_last_error().decode())
     out = {"energy": r.energy, "homo": r.homo, "converged": bool(r.converged), "iterations": r.iterations,
-           "nbf": r.nbf}
+           "nbf": r.nbf, "fock_builds": r.fock_builds, "fock_ms_total": r.fock_ms_total,
+           "fp32_quartets": r.fp32_quartets, "fp64_quartets": r.fp64_quartets, "mixed_steps": r.mixed_steps,
+           "seconds_fock": r.seconds_fock, "seconds_eigen": r.seconds_eigen, "seconds_diis": r.seconds_diis,
+           "seconds_total": r.seconds_total, "seconds_init": r.seconds_init}
     if dens is not None:
         n = r.nbf
         if unrestricted:

@@ -62,26 +62,43 @@ typedef struct {
   int32_t nbf;               /* number of Cartesian basis functions */
 } hfg_shells;
 
+/* Direct Fock builds come in two forms.  The plain form (all fields below
+ * at their defaults) evaluates every quartet that survives the Schwarz test
+ * in FP64 from the full density, as the reference does.  The precision form
+ * is switched on by any of density_screening, incremental or a positive
+ * mixed_cutoff:
+ *   - density screening: a quartet is skipped when its density-weighted
+ *     bound Q_ab Q_cd max|D| (max over the six shell blocks of D that its
+ *     J/K digestion reads) is below density_threshold;
+ *   - mixed precision: of the kept quartets, those of a task (one bra shell
+ *     pair and up to 32 ket pairs) whose largest density-weighted bound is
+ *     below mixed_cutoff are evaluated with FP32 recursions (FP64 Boys
+ *     function, prefactor and J/K accumulation); the others in FP64;
+ *   - incremental: the context keeps the previous density and two-electron
+ *     matrix; each build evaluates G[P - P_prev] and returns
+ *     G_prev + G[P - P_prev].  hfg_fock_reset() starts over from P_prev = 0. */
 typedef struct {
   double schwarz_threshold; /* skip quartets with Q_ab*Q_cd below this (1e-12) */
-  double mixed_cutoff;      /* direct Fock: quartets whose density-weighted
-                               Schwarz bound is below this run in FP32 with
-                               FP64 accumulation; 0 = all FP64 (default 0) */
+  double mixed_cutoff;      /* FP32 below this density-weighted bound; 0 = all
+                               FP64 (default 0; the precision form uses 1e-4) */
   int32_t eri_convention;   /* hfg_eri_convention, default HFG_ERI_REFERENCE */
   int32_t device;           /* CUDA ordinal, default 0 */
-  int32_t density_screening;/* 1: direct Fock skips quartets whose
-                               Q_ab*Q_cd*max|D| block bound < threshold */
-  int32_t reserved[5];
+  int32_t density_screening;/* 1: skip quartets below density_threshold */
+  int32_t incremental;      /* 1: build from the density difference */
+  double density_threshold; /* density screening cutoff; 0 = schwarz_threshold */
+  int32_t reserved[2];
 } hfg_opts;
 
 typedef struct hfg_ctx hfg_ctx;
 
 typedef struct {
   int64_t shell_pairs;         /* significant shell pairs */
-  int64_t shell_quartets;      /* quartets evaluated by the last build */
+  int64_t shell_quartets;      /* Schwarz-surviving quartets of the last build */
   int64_t function_quartets;   /* 8-fold unique function quartets, same build */
   int64_t primitive_quartets;  /* primitive quartets, same build */
-  int64_t fp32_shell_quartets; /* of which evaluated in FP32 (mixed mode) */
+  int64_t fp32_shell_quartets; /* precision form: quartets evaluated in FP32 */
+  int64_t fp64_shell_quartets; /* precision form: quartets evaluated in FP64
+                                  (plain form: = shell_quartets) */
   double flops;                /* algorithmic flops of the last build */
   double last_build_ms;        /* device time of the last build (events) */
   int32_t kernel_launches;     /* kernels launched by the last build */
@@ -130,6 +147,19 @@ hfg_status hfg_fock_uhf(hfg_ctx *ctx, const double *Pa, const double *Pb, double
 hfg_status hfg_fock_rhf_device(hfg_ctx *ctx, const double *dP, double *dG, void *stream);
 hfg_status hfg_fock_uhf_device(hfg_ctx *ctx, const double *dPa, const double *dPb, double *dGa, double *dGb,
                                void *stream);
+
+/* Precision form controls (see hfg_opts).  No reference counterpart: the
+ * reference rebuilds the full two-electron matrix in FP64 every iteration
+ * (RestrictedHartreeFock.cpp:168-207).
+ * hfg_fock_reset: drop the incremental history, so that the next build
+ * evaluates G from the full density (P_prev = 0, G_prev = 0).
+ * hfg_set_mixed_cutoff: FP32 cutoff of the following builds (0 = all FP64);
+ * an SCF driver finishes with hfg_set_mixed_cutoff(ctx, 0) plus
+ * hfg_fock_reset(ctx), so that its last iterations run all-FP64.
+ * hfg_set_incremental: switch incremental builds on or off (resets). */
+hfg_status hfg_fock_reset(hfg_ctx *ctx);
+hfg_status hfg_set_mixed_cutoff(hfg_ctx *ctx, double cutoff);
+hfg_status hfg_set_incremental(hfg_ctx *ctx, int32_t on);
 
 /* Allocation-free variant of hfg_fock_rhf_device, for callers that must not
  * allocate device memory while they run: a serving loop under a fixed HBM

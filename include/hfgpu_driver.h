@@ -24,6 +24,18 @@ typedef struct {
   int32_t beta_electrons;
   int32_t eri_convention;    /* hfg_eri_convention */
   double schwarz_threshold;
+  /* precision form of the Fock builds (HartreeFockAlgorithm::mixedCutoff
+   * and friends in hfgpu_host.hpp); all 0 = the plain FP64 form */
+  double mixed_cutoff;       /* FP32 below this density-weighted bound */
+  double mixed_switch_energy;/* leave the incremental phase below this |dE| ... */
+  double mixed_switch_density;/* ... and this rms density change ... */
+  double mixed_switch_diis;  /* ... and this DIIS error estimate */
+  int32_t fp64_final_iterations;
+  int32_t fp64_final_converge;/* 1: the FP64 phase also meets the reference's test */
+  int32_t incremental;       /* FP64 incremental builds (implied by mixed_cutoff > 0) */
+  int32_t trace;             /* 1: one line per SCF step on stderr */
+  int32_t stop_at_precision_test; /* plain builds, precision form's stopping rule */
+  int32_t reserved;
 } hfd_scf_opts;
 
 typedef struct {
@@ -32,8 +44,15 @@ typedef struct {
   int32_t converged;
   int32_t iterations;
   int32_t nbf;
-  int32_t reserved;
+  int32_t fock_builds;       /* two-electron builds (iterations after the first) */
   double fock_ms_total;      /* device time spent in two-electron builds */
+  int64_t fp32_quartets;     /* shell quartets evaluated in FP32, all builds */
+  int64_t fp64_quartets;     /* shell quartets evaluated in FP64, all builds */
+  int32_t mixed_steps;       /* builds of the incremental (first) phase */
+  int32_t reserved;
+  /* wall-clock split of the SCF (seconds) */
+  double seconds_fock, seconds_eigen, seconds_diis, seconds_total;
+  double seconds_init;       /* Init: one-electron matrices, engine context, S^-1/2 */
 } hfd_scf_result;
 
 void hfd_default_scf_opts(hfd_scf_opts *o);

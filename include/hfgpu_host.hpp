@@ -11,10 +11,14 @@
 //   double e = hf.Calculate();
 //
 // The two-electron work (Fock builds, stored integral table, single
-// integrals) runs on the GPU through the C ABI of hfgpu.h; one-electron
-// matrices, DIIS and the orthogonalisation stay in host FP64 as in the
-// reference.  Matrices are row-major (hfgpu::Matrix) instead of
-// Eigen::MatrixXd; element access M(i, j) is the same.
+// integrals) runs on the GPU through the C ABI of hfgpu.h.  The SCF
+// iterations run on the same GPU in FP64 (Fock assembly, DIIS,
+// orthogonalisation, cuSOLVER eigensolves, densities), with the public
+// fields (DensityMatrix, C, eigenvalues, energies) brought back to the host
+// at the end of Calculate() or of a Step() called on its own.  One-electron
+// matrices and S^-1/2 are formed on the host at Init.  Matrices are
+// row-major (hfgpu::Matrix) instead of Eigen::MatrixXd; element access
+// M(i, j) is the same.
 #pragma once
 
 #include <atomic>
@@ -25,6 +29,9 @@
 #include "hfgpu.h"
 
 namespace hfgpu {
+namespace detail {
+class DeviceScf;  // device-resident SCF matrices (internal)
+}
 
 class Matrix {
  public:
@@ -198,6 +205,42 @@ class HartreeFockAlgorithm {
   size_t storedIntegralsBudget = size_t(1) << 30;
   int iterations = 0;  // steps taken by the last Calculate()
 
+  // Engine extension, no reference counterpart: the precision form of the
+  // direct Fock builds (hfgpu.h, hfg_opts).  mixedCutoff > 0 (FP32 below the
+  // cutoff) or incrementalFock (FP64) switches it on.  First phase:
+  // incremental builds from the density difference with density screening,
+  // until |dE| < mixedSwitchEnergy, the density change (rms, as the
+  // reference measures it) < mixedSwitchDensity and the DIIS error estimate
+  // < mixedSwitchDiis, or the reference's own convergence test passes.  Second phase: fp64FinalIterations full FP64
+  // builds from the whole density (density-screened, no history: F is a
+  // function of D alone, as in the plain form), after which the SCF counts
+  // as converged.  With fp64FinalConverge the second phase instead runs on
+  // until the reference's convergence test (Constants.h:6-10) passes too.
+  // The incremental phase cannot meet that test itself: every increment
+  // adds its screening and FP32 errors to G, which the test's 1e-10-level
+  // thresholds resolve.
+  double mixedCutoff = 0;
+  double mixedSwitchEnergy = 1e-7;
+  double mixedSwitchDensity = 1e-7;
+  double mixedSwitchDiis = 1e-6;
+  int fp64FinalIterations = 2;
+  bool fp64FinalConverge = false;
+  bool incrementalFock = false;
+  // measurement aid: plain FP64 builds throughout, but stopped by the
+  // precision form's test (its switch point + fp64FinalIterations steps), for
+  // comparing the two forms at equal convergence criteria
+  bool stopAtPrecisionTest = false;
+  // per-Calculate accounting of the two-electron builds
+  double fockMilliseconds = 0;   // device time of all builds
+  int fockBuilds = 0;
+  int64_t fp32Quartets = 0, fp64Quartets = 0;  // shell quartets evaluated per precision
+  int mixedSteps = 0;            // builds of the first (incremental) phase
+  // wall-clock split of Calculate (seconds): two-electron builds, the
+  // eigensolves, DIIS (error matrices and extrapolation), everything else
+  double secondsFock = 0, secondsEigen = 0, secondsDiis = 0, secondsTotal = 0;
+  double secondsInit = 0;        // the last Init(): one-electron matrices, engine context, S^-1/2
+  bool traceIterations = false;  // one line per step on stderr
+
   explicit HartreeFockAlgorithm(int iterations = 3000);
   virtual ~HartreeFockAlgorithm();
   virtual void Init(Systems::Molecule *molecule);
@@ -212,6 +255,21 @@ class HartreeFockAlgorithm {
   hfgpu::Matrix V, Vt;    // S^-1/2
   int maxIterations;
   bool inited = false;
+  bool fp64Phase = true;  // precision form: the FP32 part is over
+  int fp64Steps = 0;      // builds since the switch to FP64
+  bool inCalculate = false;  // Step() called from Calculate(): public fields synced at its end
+  std::unique_ptr<hfgpu::detail::DeviceScf> device_;
+  hfgpu::detail::DeviceScf &Device();
+  void AccountDevice(double fock_wall_seconds);
+  // copy the public density fields to the device / the device state back
+  virtual void SyncToDevice() = 0;
+  virtual void SyncFromDevice() = 0;
+  bool PrecisionForm() const { return mixedCutoff > 0 || incrementalFock; }
+  bool PrecisionCriteria() const { return PrecisionForm() || stopAtPrecisionTest; }
+  // convergence decision after a step: `test` is the reference's test
+  bool ConvergedAfterStep(bool test, double dE, double rmsD);
+  void AccountFockBuild();
+  void TraceStep(int iter, double energy, double dE, double rmsD) const;
   void FirstIterations(int &iter, double &curEnergy, double &prevEnergy);
   void SelfConsistentIterations(int &iter, double &curEnergy, double &prevEnergy);
   void NormalIterations(int &iter, double &curEnergy, double &prevEnergy);
@@ -237,10 +295,12 @@ class RestrictedHartreeFock : public HartreeFockAlgorithm {
   void Init(Systems::Molecule *molecule) override;
   double Step(int iter) override;
 
+ protected:
+  void SyncToDevice() override;
+  void SyncFromDevice() override;
+
  private:
-  Diis diis;
-  bool DIISStep(int iter, hfgpu::Matrix &F);
-  void InitFockMatrix(int iter, hfgpu::Matrix &F);
+  Diis diis;  // host DIIS object kept for source compatibility; the SCF's DIIS runs on the device
 };
 
 class UnrestrictedHartreeFock : public HartreeFockAlgorithm {
@@ -256,10 +316,12 @@ class UnrestrictedHartreeFock : public HartreeFockAlgorithm {
   void Init(Systems::Molecule *molecule) override;
   double Step(int iter) override;
 
+ protected:
+  void SyncToDevice() override;
+  void SyncFromDevice() override;
+
  private:
-  Diis diisPlus, diisMinus;
-  bool DIISStep(int iter, hfgpu::Matrix &Fp, hfgpu::Matrix &Fm);
-  void InitFockMatrices(int iter, hfgpu::Matrix &Fp, hfgpu::Matrix &Fm);
+  Diis diisPlus, diisMinus;  // kept for source compatibility, see RestrictedHartreeFock
 };
 
 }  // namespace HartreeFock
