@@ -7,6 +7,7 @@
 #include <memory>
 #include <mutex>
 #include <numeric>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -116,6 +117,7 @@ struct hfg_ctx {
   int num_sms = 148;
   // device tables
   PrimPair *d_prim = nullptr;
+  PrimPairF *d_primf = nullptr;
   int *d_pair_prim_off = nullptr, *d_pair_nprim = nullptr, *d_pair_sa = nullptr, *d_pair_sb = nullptr;
   int *d_pair_ao_a = nullptr, *d_pair_ao_b = nullptr;
   double *d_pair_AB = nullptr, *d_pair_Q = nullptr, *d_boys = nullptr;
@@ -144,6 +146,7 @@ struct hfg_ctx {
   EngineView view() const {
     EngineView v{};
     v.prim = d_prim;
+    v.primf = d_primf;
     v.pair_prim_off = d_pair_prim_off;
     v.pair_nprim = d_pair_nprim;
     v.pair_sa = d_pair_sa;
@@ -171,7 +174,7 @@ struct hfg_ctx {
                     d_pair_AB,    d_pair_Q,        d_boys,       d_J,        d_Ka,         d_Kb,        d_P,
                     d_Pb,         d_Pt,            d_G,          d_Gb,       d_block,      d_scratch,   d_shell_ao,
                     d_shell_nf,   d_shell_dmax,    d_counters,   d_prev_P[0], d_prev_P[1], d_prev_G[0], d_prev_G[1],
-                    d_dP[0],      d_dP[1]};
+                    d_dP[0],      d_dP[1],         d_primf};
     for (void *b : bufs) cudaFree(b);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -399,14 +402,14 @@ static int ncomp_range(int lo, int hi) {
   return s;
 }
 
-// `prec`: 0 plain FP64, 1 density-screened FP64, 2 density-screened FP64 +
-// FP32 halves (the precision form).
+// `prec`: 0 plain FP64, 1 density-screened FP64, 2 density-screened with
+// the per-task FP64/FP32 choice (the precision form).
 static hfg_status launch_class(hfg_ctx *c, const QuartetClass &q, const ClassLaunch &cl, int mode, bool ref,
                                int prec, cudaStream_t s, int *launches) {
   const ClassEntry &e = kClasses[q.cls];
   if (!kSplit[q.cls]) {
     e.launch(c->view(), cl, mode, ref, prec, grid_for(c, cl.ntasks, q.cls), s);
-    *launches += prec == 2 ? 2 : 1;
+    ++*launches;
     return HFG_OK;
   }
   const size_t acc = (size_t)ncomp_range(e.la, e.la + e.lb) * ncomp_range(e.lc, e.lc + e.ld);
@@ -430,7 +433,7 @@ static hfg_status launch_class(hfg_ctx *c, const QuartetClass &q, const ClassLau
     ch.scr_fwd = c->d_scratch;
     ch.scr_rev = c->d_scratch + acc * (size_t)ch.stride;
     kSplit[q.cls](c->view(), cl, ch, mode, ref, prec, s);
-    *launches += prec == 2 ? 3 : 2;
+    *launches += 2;
   }
   return HFG_OK;
 }
@@ -729,8 +732,15 @@ hfg_status hfg_ctx_create(const hfg_shells *sh, const hfg_opts *opts, hfg_ctx **
     if (prim.empty()) prim.push_back(PrimPair{});  // keep a valid device allocation
   }
   ctx->pair_nprim = pn;
+  std::vector<PrimPairF> primf(prim.size());
+  for (size_t x = 0; x < prim.size(); ++x) {
+    const PrimPair &d = prim[x];
+    primf[x] = PrimPairF{(float)d.zeta, (float)d.Px,   (float)d.Py,   (float)d.Pz, (float)d.PAx,     (float)d.PAy,
+                         (float)d.PAz,  (float)d.bABx, (float)d.bABy, (float)d.bABz, (float)d.K, (float)d.inv_zeta};
+  }
   hfg_status st;
-  if ((st = upload(&ctx->d_prim, prim)) != HFG_OK || (st = upload(&ctx->d_pair_prim_off, poff)) != HFG_OK ||
+  if ((st = upload(&ctx->d_prim, prim)) != HFG_OK || (st = upload(&ctx->d_primf, primf)) != HFG_OK ||
+      (st = upload(&ctx->d_pair_prim_off, poff)) != HFG_OK ||
       (st = upload(&ctx->d_pair_nprim, pn)) != HFG_OK || (st = upload(&ctx->d_pair_sa, psa)) != HFG_OK ||
       (st = upload(&ctx->d_pair_sb, psb)) != HFG_OK || (st = upload(&ctx->d_pair_ao_a, paoa)) != HFG_OK ||
       (st = upload(&ctx->d_pair_ao_b, paob)) != HFG_OK || (st = upload(&ctx->d_pair_AB, pab)) != HFG_OK ||

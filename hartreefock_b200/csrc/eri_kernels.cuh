@@ -34,43 +34,160 @@ __device__ __forceinline__ void stage_boys(double *tab, const double *__restrict
   __syncthreads();
 }
 
+// FP64 Boys function for the two edges the FP32 paths do not serve:
+// T < kBoysStep (series F_M(T) = sum_k (-T)^k / (k! (2M+2k+1)), 9 terms,
+// truncation below 1e-17 there, then the downward recursion) and the band
+// just above the asymptotic switch (asymptotic F_0 and the upward
+// recursion, as boys_eval).
+template <int M>
+__device__ __noinline__ void boys_edges_fp64(double *F, double T, double scale) {
+  if (T < kBoysStep) {
+    double term = 1.0, f = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      f += term / (2 * M + 2 * k + 1);
+      term *= -T / (k + 1);
+    }
+    double fm[M + 1];
+    fm[M] = f;
+    const double e = exp(-T), t2 = 2.0 * T;
+#pragma unroll
+    for (int m = M - 1; m >= 0; --m) fm[m] = fma(t2, fm[m + 1], e) * (1.0 / (2 * m + 1));
+#pragma unroll
+    for (int m = 0; m <= M; ++m) F[m] = fm[m] * scale;
+  } else {
+    double f = 0.88622692545275801365 * rsqrt(T);
+    F[0] = f * scale;
+    const double e = exp(-T), h = 0.5 / T;
+#pragma unroll
+    for (int m = 0; m < M; ++m) {
+      f = ((2 * m + 1) * f - e) * h;
+      F[m + 1] = f * scale;
+    }
+  }
+}
+
+// FP32 Boys function: the 7-term Taylor expansion and the downward recursion
+// of boys_eval in single precision on [kBoysStep, kBoysTmax) (coefficients
+// rounded from the staged FP64 table), the asymptotic form in single
+// precision from kBoysTmax + kBoysF32Band on, FP64 near T = 0 and in the band
+// at the switch.  (The far, small quartets that run in FP32 are mostly at
+// large T: the asymptotic branch is their common case.)
+constexpr float kBoysF32Band = 4.0f;
+template <int M>
+__device__ __forceinline__ void boys_eval_f32(float *F, float T, float scale, const double *__restrict__ tab) {
+  if (T >= (float)kBoysTmax + kBoysF32Band) {
+    float f = 0.88622692545275801365f * rsqrtf(T);  // sqrt(pi)/2 / sqrt(T)
+    F[0] = f * scale;
+    if (M > 0) {
+      const float e = __expf(-T), h = 0.5f / T;
+#pragma unroll
+      for (int m = 0; m < M; ++m) {
+        f = ((2 * m + 1) * f - e) * h;
+        F[m + 1] = f * scale;
+      }
+    }
+  } else if (T >= (float)kBoysStep && T < (float)kBoysTmax) {
+    const int i = __float2int_rn(T * (float)(1.0 / kBoysStep));
+    const float dt = (float)i * (float)kBoysStep - T;
+    const double *t = tab + i * kBoysRow;
+    const int sw = (i >> 1) & 7;
+    float f = (float)t[6 ^ sw];
+#pragma unroll
+    for (int k = 5; k >= 0; --k) f = fmaf(f, dt, (float)t[k ^ sw]);
+    float fm[M + 1];
+    fm[M] = f;
+    if (M > 0) {
+      // e^(T_i - T), |dt| <= 0.025: five terms reach float precision
+      float x = 1.0f / 120.0f;
+      x = fmaf(x, dt, 1.0f / 24.0f);
+      x = fmaf(x, dt, 1.0f / 6.0f);
+      x = fmaf(x, dt, 0.5f);
+      x = fmaf(x, dt, 1.0f);
+      x = fmaf(x, dt, 1.0f);
+      const float e = (float)t[7 ^ sw] * x, t2 = 2.0f * T;
+#pragma unroll
+      for (int m = M - 1; m >= 0; --m) fm[m] = fmaf(t2, fm[m + 1], e) * (1.0f / (2 * m + 1));
+    }
+#pragma unroll
+    for (int m = 0; m <= M; ++m) F[m] = fm[m] * scale;
+  } else {
+    double Fd[M + 1];
+    boys_edges_fp64<M>(Fd, (double)T, (double)scale);
+#pragma unroll
+    for (int m = 0; m <= M; ++m) F[m] = (float)Fd[m];
+  }
+}
+
+// Contracted [e0|f0] of one shell quartet (bra pair `bp`, ket pair `kp`)
+// accumulated into acc: the primitive loops.  R = double: FP64 throughout;
+// R = float: the FP32 primitive pairs and FP32 arithmetic (mixed
+// precision), with the Boys function's edges in FP64.
+template <int LA, int LB, int LC, int LD, bool REF, class R>
+__device__ __forceinline__ void accumulate_primitives(const EngineView &v, const double *tab, int bp, int kp, int npk,
+                                                      R *acc) {
+  constexpr int LTOT = LA + LB + LC + LD;
+  using Cls = EriClass<LA, LB, LC, LD, REF>;
+  const int offb = v.pair_prim_off[bp], npb = v.pair_nprim[bp];
+  const int offk = v.pair_prim_off[kp];
+  // ket primitive pairs differ across the warp's lanes: load each once; the
+  // bra primitive pairs are shared by the warp (broadcast loads).  Staging
+  // them in shared memory per task was measured slower (generic loads).
+  if constexpr (std::is_same<R, float>::value) {
+    const PrimPairF *bsrc = v.primf + offb;
+    for (int ik = 0; ik < npk; ++ik) {
+      const PrimPairF pk = v.primf[offk + ik];
+      for (int ib = 0; ib < npb; ++ib) {
+        const PrimPairF pb = bsrc[ib];
+        const float rs = rsqrtf(pb.zeta + pk.zeta);
+        const float rho = pb.zeta * pk.zeta * (rs * rs);
+        const float PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;
+        const float T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+        float F[LTOT + 1];
+        boys_eval_f32<LTOT>(F, T, pb.K * pk.K * rs, tab);
+        const float roz = rho * pb.inv_zeta;
+        const float ie = pk.inv_zeta;
+        Cls::template prim<float>(acc, F, pb.PAx, pb.PAy, pb.PAz, -roz * PQx, -roz * PQy, -roz * PQz,
+                                  0.5f * pb.inv_zeta, roz, -(pb.bABx + pk.bABx) * ie, -(pb.bABy + pk.bABy) * ie,
+                                  -(pb.bABz + pk.bABz) * ie, pb.zeta * ie, 0.5f * ie);
+      }
+    }
+  } else {
+    const PrimPair *bsrc = v.prim + offb;
+    for (int ik = 0; ik < npk; ++ik) {
+      const PrimPair pk = v.prim[offk + ik];
+#pragma unroll kPrimUnroll
+      for (int ib = 0; ib < npb; ++ib) {
+        const PrimPair pb = bsrc[ib];
+        const double rs = rsqrt(pb.zeta + pk.zeta);
+        const double inv_zpe = rs * rs;
+        const double rho = pb.zeta * pk.zeta * inv_zpe;
+        const double PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;
+        const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+        double F[LTOT + 1];
+        boys_eval<LTOT, double>(F, T, pb.K * pk.K * rs, tab);
+        const double roz = rho * pb.inv_zeta;
+        const double ie = pk.inv_zeta;
+        Cls::template prim<double>(acc, F, pb.PAx, pb.PAy, pb.PAz, -roz * PQx, -roz * PQy, -roz * PQz,
+                                   0.5 * pb.inv_zeta, roz, -(pb.bABx + pk.bABx) * ie, -(pb.bABy + pk.bABy) * ie,
+                                   -(pb.bABz + pk.bABz) * ie, pb.zeta * ie, 0.5 * ie);
+      }
+    }
+  }
+}
+
 // Contracted (ab|cd) block of one shell quartet, bra pair `bp`, ket pair
 // `kp`, components in canonical order, normalisation applied.  `npk` = 0
-// yields an all-zero block (inactive lanes).  R is the type of the
-// recursions and the contraction; the Boys function, T and the prefactor
-// are always evaluated in FP64.
+// yields an all-zero block (inactive lanes).  R is the arithmetic type
+// (see accumulate_primitives).
 template <int LA, int LB, int LC, int LD, bool REF, class R = double>
-__device__ __forceinline__ void quartet_block(const EngineView &v, const double *tab, int bp, int kp, int npk,
-                                              R *out) {
-  constexpr int LTOT = LA + LB + LC + LD;
+__device__ __forceinline__ void quartet_block(const EngineView &v, const double *tab, int bp, int kp, int npk, R *out) {
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   using Cls = EriClass<LA, LB, LC, LD, REF>;
   R acc[Cls::kAcc];
 #pragma unroll
   for (int x = 0; x < Cls::kAcc; ++x) acc[x] = R(0);
-
-  const int offb = v.pair_prim_off[bp], npb = v.pair_nprim[bp];
-  const int offk = v.pair_prim_off[kp];
-  // ket primitive pairs differ across the warp's lanes: load each once; the
-  // bra primitive pairs are shared by the warp (broadcast loads)
-  for (int ik = 0; ik < npk; ++ik) {
-    const PrimPair pk = v.prim[offk + ik];
-    for (int ib = 0; ib < npb; ++ib) {
-      const PrimPair pb = v.prim[offb + ib];
-      const double rs = rsqrt(pb.zeta + pk.zeta);
-      const double inv_zpe = rs * rs;
-      const double rho = pb.zeta * pk.zeta * inv_zpe;
-      const double PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;
-      const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
-      R F[LTOT + 1];
-      boys_eval<LTOT, R>(F, T, pb.K * pk.K * rs, tab);
-      const double roz = rho * pb.inv_zeta;
-      const double ie = pk.inv_zeta;
-      Cls::template prim<R>(acc, F, R(pb.PAx), R(pb.PAy), R(pb.PAz), R(-roz * PQx), R(-roz * PQy), R(-roz * PQz),
-                            R(0.5 * pb.inv_zeta), R(roz), R(-(pb.bABx + pk.bABx) * ie), R(-(pb.bABy + pk.bABy) * ie),
-                            R(-(pb.bABz + pk.bABz) * ie), R(pb.zeta * ie), R(0.5 * ie));
-    }
-  }
+  accumulate_primitives<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, npk, acc);
   Cls::template hrr<R>(out, acc, R(v.pair_AB[3 * bp]), R(v.pair_AB[3 * bp + 1]), R(v.pair_AB[3 * bp + 2]),
                        R(v.pair_AB[3 * kp]), R(v.pair_AB[3 * kp + 1]), R(v.pair_AB[3 * kp + 2]));
   constexpr int U = kUnrollBlock<NA * NB * NC * ND>;
@@ -99,26 +216,28 @@ __device__ __forceinline__ float density_bound(const EngineView &v, int bp, int 
 }
 
 // Warp-level density screening of one task.  Sets *keep for the lane's
-// quartet (active and bound >= threshold) and returns whether this launch
-// (SCR = kScreenFp64 or kScreenFp32) takes the task: the warp's largest kept
-// bound against the mixed cutoff, identical in every lane and in both
-// kernels, so each task with a kept quartet is taken by exactly one of them.
+// quartet (active and bound >= threshold) and *fp64 for the task (the warp's
+// largest kept bound reaches the mixed cutoff; always true for kScreenFp64),
+// identically in every lane; returns false when no quartet is kept.  Counts
+// the kept quartets per precision.
 template <int SCR>
 __device__ __forceinline__ bool screen_task(const EngineView &v, const ClassLaunch &cl, int bp, int kp, bool active,
-                                            bool *keep) {
+                                            bool *keep, bool *fp64) {
   const float bnd = active ? density_bound(v, bp, kp) : 0.0f;
   const bool k = active && bnd >= cl.dens_threshold;
   *keep = k;
   const unsigned kept = __ballot_sync(0xffffffffu, k);
   if (!kept) return false;
-  float m = k ? bnd : 0.0f;
+  bool hi = true;
+  if constexpr (SCR == kScreenMixed) {
+    float m = k ? bnd : 0.0f;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  const bool hi = m >= cl.mixed_cutoff;
-  const bool take = SCR == kScreenFp64 ? hi : !hi;
-  if (take && (threadIdx.x & 31) == 0 && cl.counters)
-    atomicAdd(&cl.counters[SCR == kScreenFp64 ? 0 : 1], (unsigned long long)__popc(kept));
-  return take;
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    hi = m >= cl.mixed_cutoff;
+  }
+  *fp64 = hi;
+  if ((threadIdx.x & 31) == 0 && cl.counters) atomicAdd(&cl.counters[hi ? 0 : 1], (unsigned long long)__popc(kept));
+  return true;
 }
 
 // The reference evaluates each function quartet of a (dd|dd) shell quartet
@@ -171,15 +290,15 @@ __device__ __forceinline__ void quartet_values(const EngineView &v, const double
   }
 }
 
-// SCR (enum Screen) selects plain FP64, or the density-screened FP64 / FP32
-// halves of a mixed-precision J/K build (kJkRhf, kJkUhf only).
+// SCR (enum Screen) selects plain FP64, or a density-screened FP64 or mixed
+// FP64/FP32 J/K build (kJkRhf, kJkUhf only).
 template <int LA, int LB, int LC, int LD, int MODE, bool REF, int SCR = kScreenNone>
-__global__ void __launch_bounds__(32 * fused_warps(LA, LB, LC, LD))
+__global__ void __launch_bounds__(32 * fused_warps(LA, LB, LC, LD), fused_min_blocks(LA, LB, LC, LD))
     eri_class_kernel(const EngineView v, const ClassLaunch cl) {
   constexpr int kW = fused_warps(LA, LB, LC, LD);
   constexpr int LTOT = LA + LB + LC + LD;
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
-  using R = typename std::conditional<SCR == kScreenFp32, float, double>::type;
+  constexpr int N = NA * NB * NC * ND;
   static_assert(SCR == kScreenNone || MODE == kJkRhf || MODE == kJkUhf, "screening applies to J/K builds");
   __shared__ double tab[kBoysGrid * kBoysRow];
   stage_boys<LTOT>(tab, v.boys_table);
@@ -193,15 +312,24 @@ __global__ void __launch_bounds__(32 * fused_warps(LA, LB, LC, LD))
     const int kpos = task.ket_start + lane;
     bool active = kpos < task.ket_end;
     const int kp = active ? cl.ket_list[kpos] : bp;
+    bool fp64 = true;
     if constexpr (SCR != kScreenNone) {
       bool keep;
-      if (!screen_task<SCR>(v, cl, bp, kp, active, &keep)) continue;  // warp-uniform
+      if (!screen_task<SCR>(v, cl, bp, kp, active, &keep, &fp64)) continue;  // warp-uniform
       active = keep;
     }
     const int npk = active ? v.pair_nprim[kp] : 0;
 
-    R out[NA * NB * NC * ND];
-    quartet_values<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, npk, out);
+    double out[N];
+    if (SCR != kScreenMixed || fp64) {
+      quartet_values<LA, LB, LC, LD, REF, double>(v, tab, bp, kp, npk, out);
+    } else if constexpr (SCR == kScreenMixed) {
+      // FP32 evaluation, FP64 from here on (digestion, accumulation)
+      float o32[N];
+      quartet_values<LA, LB, LC, LD, REF, float>(v, tab, bp, kp, npk, o32);
+#pragma unroll kUnrollBlock<N>
+      for (int x = 0; x < N; ++x) out[x] = (double)o32[x];
+    }
     // blocks above 81 integrals live in local memory anyway: keep their
     // epilogue loops rolled (code size, compile time)
     constexpr int U = kUnrollBlock<NA * NB * NC * ND>;
@@ -358,6 +486,12 @@ __global__ void __launch_bounds__(kThreads) schwarz_kernel(const EngineView v, c
       for (int b = 0; b < NB; ++b) m = fmax(m, fabs(out[((a * NB + b) * NA + a) * NB + b]));
     Q[p] = sqrt(m);
   }
+}
+
+// Host: launch one fused class kernel (block size per class).
+template <int LA, int LB, int LC, int LD, int MODE, bool REF, int SCR = kScreenNone>
+void launch_fused(const EngineView &v, const ClassLaunch &cl, int grid, cudaStream_t s) {
+  eri_class_kernel<LA, LB, LC, LD, MODE, REF, SCR><<<grid, 32 * fused_warps(LA, LB, LC, LD), 0, s>>>(v, cl);
 }
 
 }  // namespace hfg

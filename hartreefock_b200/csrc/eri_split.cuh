@@ -23,56 +23,19 @@ namespace hfg {
 template <int LA, int LB, int LC, int LD, bool REF, class R>
 __device__ __forceinline__ void prim_block_to_scratch(const EngineView &v, const double *tab, int bp, int kp, int npk,
                                                       double *scr, long long stride) {
-  constexpr int LTOT = LA + LB + LC + LD;
   using Cls = EriClass<LA, LB, LC, LD, REF>;
   R acc[Cls::kAcc];
 #pragma unroll
   for (int x = 0; x < Cls::kAcc; ++x) acc[x] = R(0);
-  const int offb = v.pair_prim_off[bp], npb = v.pair_nprim[bp];
-  const int offk = v.pair_prim_off[kp];
-  for (int ik = 0; ik < npk; ++ik) {
-    const PrimPair pk = v.prim[offk + ik];
-    for (int ib = 0; ib < npb; ++ib) {
-      const PrimPair pb = v.prim[offb + ib];
-      const double rs = rsqrt(pb.zeta + pk.zeta);
-      const double inv_zpe = rs * rs;
-      const double rho = pb.zeta * pk.zeta * inv_zpe;
-      const double PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;
-      const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
-      R F[LTOT + 1];
-      boys_eval<LTOT, R>(F, T, pb.K * pk.K * rs, tab);
-      const double roz = rho * pb.inv_zeta;
-      const double ie = pk.inv_zeta;
-      Cls::template prim<R>(acc, F, R(pb.PAx), R(pb.PAy), R(pb.PAz), R(-roz * PQx), R(-roz * PQy), R(-roz * PQz),
-                            R(0.5 * pb.inv_zeta), R(roz), R(-(pb.bABx + pk.bABx) * ie), R(-(pb.bABy + pk.bABy) * ie),
-                            R(-(pb.bABz + pk.bABz) * ie), R(pb.zeta * ie), R(0.5 * ie));
-    }
-  }
+  accumulate_primitives<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, npk, acc);
 #pragma unroll
   for (int x = 0; x < Cls::kAcc; ++x) scr[x * stride] = (double)acc[x];
 }
 
-// SCR (enum Screen): plain FP64, or the density-screened FP64 / FP32 half.
-// A warp is one task (blockDim and the slot count are multiples of 32).
-template <int LA, int LB, int LC, int LD, bool REF, int SCR = kScreenNone>
-__global__ void __launch_bounds__(kThreads) eri_prim_split_kernel(const EngineView v, const ClassLaunch cl,
-                                                                  const SplitChunk ch) {
-  constexpr int LTOT = LA + LB + LC + LD;
-  using R = typename std::conditional<SCR == kScreenFp32, float, double>::type;
-  __shared__ double tab[kBoysGrid * kBoysRow];
-  stage_boys<LTOT>(tab, v.boys_table);
-  const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (slot >= (long long)ch.ntasks * 32) return;  // whole warps
-  const Task task = cl.tasks[ch.task0 + (int)(slot >> 5)];
-  const int kpos = task.ket_start + (int)(slot & 31);
-  bool active = kpos < task.ket_end;
-  const int bp = cl.bra_list[task.bra_pos], kp = active ? cl.ket_list[kpos] : bp;
-  if constexpr (SCR != kScreenNone) {
-    bool keep;
-    if (!screen_task<SCR>(v, cl, bp, kp, active, &keep)) return;  // warp-uniform
-    active = keep;
-  }
-  if (!active) return;
+// One quartet's contracted [e0|f0] block(s) in precision R, to its slot.
+template <int LA, int LB, int LC, int LD, bool REF, class R>
+__device__ __forceinline__ void prim_to_scratch(const EngineView &v, const double *tab, int bp, int kp,
+                                                const SplitChunk &ch, long long slot) {
   constexpr bool kOrient = REF && LA == 2 && LB == 2 && LC == 2 && LD == 2;
   if constexpr (kOrient) {
     // bra/ket orientation the reference picks (see dddd_reference_values)
@@ -84,6 +47,43 @@ __global__ void __launch_bounds__(kThreads) eri_prim_split_kernel(const EngineVi
   } else {
     prim_block_to_scratch<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, v.pair_nprim[kp], ch.scr_fwd + slot, ch.stride);
   }
+}
+
+// SCR (enum Screen): plain FP64, density-screened FP64, or density-screened
+// with the per-task FP64/FP32 choice.  A warp is one task (blockDim and the
+// slot count are multiples of 32).
+template <int LA, int LB, int LC, int LD, bool REF, int SCR = kScreenNone>
+__global__ void __launch_bounds__(kThreads) eri_prim_split_kernel(const EngineView v, const ClassLaunch cl,
+                                                                  const SplitChunk ch) {
+  constexpr int LTOT = LA + LB + LC + LD;
+  __shared__ double tab[kBoysGrid * kBoysRow];
+  stage_boys<LTOT>(tab, v.boys_table);
+  const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= (long long)ch.ntasks * 32) return;  // whole warps
+  const Task task = cl.tasks[ch.task0 + (int)(slot >> 5)];
+  const int kpos = task.ket_start + (int)(slot & 31);
+  bool active = kpos < task.ket_end;
+  const int bp = cl.bra_list[task.bra_pos], kp = active ? cl.ket_list[kpos] : bp;
+  bool fp64 = true;
+  if constexpr (SCR != kScreenNone) {
+    bool keep;
+    if (!screen_task<SCR>(v, cl, bp, kp, active, &keep, &fp64)) return;  // warp-uniform
+    active = keep;
+  }
+  if (!active) return;
+  if constexpr (SCR == kScreenMixed) {
+    if (!fp64) {
+      prim_to_scratch<LA, LB, LC, LD, REF, float>(v, tab, bp, kp, ch, slot);
+      return;
+    }
+  }
+  prim_to_scratch<LA, LB, LC, LD, REF, double>(v, tab, bp, kp, ch, slot);
+}
+
+// Host: launch one primitive-split kernel.
+template <int LA, int LB, int LC, int LD, bool REF, int SCR = kScreenNone>
+void launch_prim_split(const EngineView &v, const ClassLaunch &cl, const SplitChunk &ch, int grid, cudaStream_t s) {
+  eri_prim_split_kernel<LA, LB, LC, LD, REF, SCR><<<grid, kThreads, 0, s>>>(v, cl, ch);
 }
 
 // One block per task (32 quartets sharing the bra pair); warp w of the block

@@ -307,11 +307,12 @@ def emit_launchers(out_dir):
     """One translation unit per quartet class (they compile in parallel), a
     second one with the density-screened FP64/FP32 J/K kernels of the fused
     classes, the Schwarz launcher and the dispatch table.  `prec` of a
-    launcher: 0 plain FP64, 1 screened FP64, 2 screened FP64 + FP32 halves."""
+    launcher: 0 plain FP64, 1 screened FP64, 2 screened with the per-task
+    FP64/FP32 choice."""
     pairs, quartets = canonical_classes()
     modes = ("kStorePacked", "kJkRhf", "kJkUhf", "kBlock")
 
-    def launch(lines, ind, k, ref, tail="<<<grid, kFusedBlock, 0, s>>>(v, cl);"):
+    def launch(lines, ind, k, ref, tail="(v, cl, grid, s);"):
         if ref:
             lines.append(f"{ind}if (ref) {k.format(r='true')}{tail}")
             lines.append(f"{ind}else {k.format(r='false')}{tail}")
@@ -325,8 +326,7 @@ def emit_launchers(out_dir):
         lines = [f"// Generated by gen_eri.py: launcher for the ({a}{b}|{c}{d}) class kernels.",
                  '#include "eri_dispatch.cuh"', "", "namespace hfg {", "",
                  f"void launch_class_{tag}(const EngineView &v, const ClassLaunch &cl, int mode, bool ref, int prec,",
-                 "                       int grid, cudaStream_t s) {",
-                 f"  constexpr int kFusedBlock = 32 * fused_warps({a}, {b}, {c}, {d});"]
+                 "                       int grid, cudaStream_t s) {"]
         if not split:
             lines += ["  if (prec != 0 && (mode == kJkRhf || mode == kJkUhf)) {",
                       f"    launch_class_{tag}_scr(v, cl, mode, ref, prec, grid, s);",
@@ -334,7 +334,7 @@ def emit_launchers(out_dir):
         lines.append("  switch (mode) {")
         for mode in modes:
             lines.append(f"    case {mode}:")
-            launch(lines, "      ", f"eri_class_kernel<{a}, {b}, {c}, {d}, {mode}, {{r}}>", ref)
+            launch(lines, "      ", f"launch_fused<{a}, {b}, {c}, {d}, {mode}, {{r}}>", ref)
             lines.append("      break;")
         lines += ["    default:", "      break;", "  }"]
         if not ref:
@@ -350,13 +350,13 @@ def emit_launchers(out_dir):
                  '#include "eri_dispatch.cuh"', "", "namespace hfg {", "",
                  f"void launch_class_{tag}_scr(const EngineView &v, const ClassLaunch &cl, int mode, bool ref, int prec,",
                  "                           int grid, cudaStream_t s) {",
-                 f"  constexpr int kFusedBlock = 32 * fused_warps({a}, {b}, {c}, {d});",
                  "  switch (mode) {"]
         for mode in ("kJkRhf", "kJkUhf"):
             lines.append(f"    case {mode}:")
-            launch(lines, "      ", f"eri_class_kernel<{a}, {b}, {c}, {d}, {mode}, {{r}}, kScreenFp64>", ref)
             lines.append("      if (prec == 2) {")
-            launch(lines, "        ", f"eri_class_kernel<{a}, {b}, {c}, {d}, {mode}, {{r}}, kScreenFp32>", ref)
+            launch(lines, "        ", f"launch_fused<{a}, {b}, {c}, {d}, {mode}, {{r}}, kScreenMixed>", ref)
+            lines.append("      } else {")
+            launch(lines, "        ", f"launch_fused<{a}, {b}, {c}, {d}, {mode}, {{r}}, kScreenFp64>", ref)
             lines.append("      }")
             lines.append("      break;")
         lines += ["    default:", "      break;", "  }"]
@@ -599,7 +599,7 @@ def emit_split(out_dir):
     modes = ("kStorePacked", "kJkRhf", "kJkUhf")
 
     def launch(lines, ind, k, ref, grid):
-        tail = f"<<<{grid}, kThreads, 0, s>>>(v, cl, ch);"
+        tail = f"(v, cl, ch, {grid}, s);" if k.startswith("launch_prim_split") else f"<<<{grid}, kThreads, 0, s>>>(v, cl, ch);"
         if ref:
             lines.append(f"{ind}if (ref) {k.format(r='true')}{tail}")
             lines.append(f"{ind}else {k.format(r='false')}{tail}")
@@ -621,7 +621,7 @@ def emit_split(out_dir):
                  "  if (prec != 0 && (mode == kJkRhf || mode == kJkUhf)) {",
                  f"    launch_split_{tag}_scr(v, cl, ch, mode, ref, prec, s);",
                  "    return;", "  }"] + head
-        launch(lines, "  ", f"eri_prim_split_kernel<{a}, {b}, {c}, {d}, {{r}}>", ref, "gridA")
+        launch(lines, "  ", f"launch_prim_split<{a}, {b}, {c}, {d}, {{r}}>", ref, "gridA")
         lines.append("  switch (mode) {")
         for mode in modes:
             lines.append(f"    case {mode}:")
@@ -637,9 +637,10 @@ def emit_split(out_dir):
                  '#include "eri_split.cuh"', '#include "eri_split_dispatch.cuh"', "", "namespace hfg {", "",
                  f"void launch_split_{tag}_scr(const EngineView &v, const ClassLaunch &cl, const SplitChunk &ch, int mode,",
                  "                            bool ref, int prec, cudaStream_t s) {"] + head
-        launch(lines, "  ", f"eri_prim_split_kernel<{a}, {b}, {c}, {d}, {{r}}, kScreenFp64>", ref, "gridA")
         lines.append("  if (prec == 2) {")
-        launch(lines, "    ", f"eri_prim_split_kernel<{a}, {b}, {c}, {d}, {{r}}, kScreenFp32>", ref, "gridA")
+        launch(lines, "    ", f"launch_prim_split<{a}, {b}, {c}, {d}, {{r}}, kScreenMixed>", ref, "gridA")
+        lines.append("  } else {")
+        launch(lines, "    ", f"launch_prim_split<{a}, {b}, {c}, {d}, {{r}}, kScreenFp64>", ref, "gridA")
         lines.append("  }")
         lines.append("  switch (mode) {")
         for mode in ("kJkRhf", "kJkUhf"):

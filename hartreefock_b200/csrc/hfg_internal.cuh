@@ -32,18 +32,32 @@ __host__ __device__ constexpr int ncart(int L) { return (L + 1) * (L + 2) / 2; }
 __host__ __device__ constexpr int fused_warps(int la, int lb, int lc, int ld) {
   return ncart(la) * ncart(lb) * ncart(lc) * ncart(ld) <= 9 ? 8 : 4;
 }
+// Resident blocks per SM the compiler must allow for the light classes (the
+// register cap that follows: 65536 / (32 * warps * blocks)); 1 leaves the
+// register allocation free.
+#ifndef HFG_FUSED_MIN_BLOCKS
+#define HFG_FUSED_MIN_BLOCKS 1
+#endif
+__host__ __device__ constexpr int fused_min_blocks(int la, int lb, int lc, int ld) {
+  return ncart(la) * ncart(lb) * ncart(lc) * ncart(ld) <= 9 ? HFG_FUSED_MIN_BLOCKS : 1;
+}
+// unroll factor of the inner (bra) primitive loop
+#ifndef HFG_PRIM_UNROLL
+#define HFG_PRIM_UNROLL 1
+#endif
+constexpr int kPrimUnroll = HFG_PRIM_UNROLL;
 
 enum Mode { kStorePacked = 0, kJkRhf = 1, kJkUhf = 2, kSchwarz = 3, kBlock = 4 };
 
 // Density screening and precision of a J/K launch.  kScreenNone: every
-// Schwarz-surviving quartet in FP64.  kScreenFp64 / kScreenFp32: quartets
+// Schwarz-surviving quartet in FP64.  kScreenFp64 / kScreenMixed: quartets
 // whose density-weighted bound Q_ab Q_cd max|D| falls below the launch's
-// density threshold are skipped; of the rest, a task (one bra pair, <= 32
-// kets) whose largest bound reaches the mixed cutoff runs in the FP64
-// kernel, any other in the FP32 kernel (FP64 Boys function, FP32
-// recursions, FP64 J/K accumulation).  The two kernels split the tasks
-// between them by the same warp-uniform test.
-enum Screen { kScreenNone = 0, kScreenFp64 = 1, kScreenFp32 = 2 };
+// density threshold are skipped.  kScreenFp64 evaluates the rest in FP64;
+// kScreenMixed decides per task (one bra pair, <= 32 kets, a warp-uniform
+// test): FP64 when the task's largest bound reaches the mixed cutoff, else
+// FP32 primitive pairs, geometry, Boys interpolation and recursions (the
+// Boys function's edges in FP64) with the J/K digestion in FP64.
+enum Screen { kScreenNone = 0, kScreenFp64 = 1, kScreenMixed = 2 };
 
 // One primitive pair of a shell pair (first shell A with exponent a, second
 // B with exponent b): zeta = a+b, P = (aA+bB)/zeta, PA = P-A,
@@ -53,10 +67,15 @@ enum Screen { kScreenNone = 0, kScreenFp64 = 1, kScreenFp32 = 2 };
 struct __align__(16) PrimPair {
   double zeta, Px, Py, Pz, PAx, PAy, PAz, bABx, bABy, bABz, K, inv_zeta;
 };
+// FP32 copy of a PrimPair for the mixed-precision kernels (48 B)
+struct __align__(16) PrimPairF {
+  float zeta, Px, Py, Pz, PAx, PAy, PAz, bABx, bABy, bABz, K, inv_zeta;
+};
 
 // Device view of one context's tables.
 struct EngineView {
   const PrimPair *prim;       // all primitive pairs, pair-major
+  const PrimPairF *primf;     // the same in FP32
   const int *pair_prim_off;   // per pair
   const int *pair_nprim;
   const int *pair_sa;         // first shell (higher L; higher index on ties)
@@ -93,7 +112,7 @@ struct ClassLaunch {
   const double *Dt;      // total density for J in UHF
   double *J, *Ka, *Kb;   // accumulators (n x n)
   double *Qout;          // kSchwarz: per pair
-  // density screening (kScreenFp64 / kScreenFp32 launches)
+  // density screening (kScreenFp64 / kScreenMixed launches)
   float dens_threshold;  // skip quartets whose density-weighted bound is below
   float mixed_cutoff;    // tasks whose largest bound is below run in FP32
   unsigned long long *counters;  // [0] FP64, [1] FP32 quartets evaluated
