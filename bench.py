@@ -17,9 +17,10 @@ by the precision form's rule, for a comparison at equal criteria.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-With N > 1 (torchrun, one rank per GPU) every rank builds the same molecule's
-Fock matrix: the build is replicated, not sharded (scaling "weak"); the
-sharded multi-GPU build lives in hartreefock_b200.multi.
+With N > 1 (torchrun, one rank per GPU, NCCL) the one build is sharded: each
+rank evaluates every N-th task of each quartet class and one all-reduce sums
+the partial G (hartreefock_b200/shards.py); scaling "strong" (the molecule
+is fixed), value = the whole build's quartets / the slowest rank's time.
 `--impl reference` times the reference's own CPU ERI path (oracle/_ref,
 compiled headless from the reference sources) on a bounded sample of the
 same workload with all host threads.
@@ -243,13 +244,29 @@ def main():
     dG = torch.empty_like(dP)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
 
+    # the whole molecule's build (units of the metric; reference G for the check)
+    eng.fock_rhf_device(dP.data_ptr(), dG.data_ptr(), sptr)
+    torch.cuda.synchronize()
+    stats_full = eng.stats()
+    G_full = dG.clone()
+    # N > 1: every rank builds its shard of each class's tasks, one NCCL
+    # all-reduce of G per build (hartreefock_b200/shards.py)
+    sf = None
+    if dist:
+        from hartreefock_b200.shards import ShardedFock
+        sf = ShardedFock(eng)
+
     def step():
-        eng.fock_rhf_device(dP.data_ptr(), dG.data_ptr(), sptr)
+        if sf:
+            sf.fock_rhf(dP, dG)
+        else:
+            eng.fock_rhf_device(dP.data_ptr(), dG.data_ptr(), sptr)
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     stats = eng.stats()
+    assert torch.allclose(dG, G_full, atol=1e-9)
 
     # ---- device-timed value: per-step events, L2 flushed between steps
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
@@ -270,20 +287,33 @@ def main():
         t = torch.tensor([total_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    quartets = stats["function_quartets"] * world
+    quartets = stats_full["function_quartets"]
     value = quartets * args.steps / (total_ms / 1e3)
 
-    # ---- end to end through the public host-buffer entry point hfg_fock_rhf
-    # (H2D of P, build, D2H of G inside the call; the call is synchronous)
-    P_pin = torch.from_numpy(P_host).pin_memory().numpy()
-    G_pin = torch.empty(n, n, dtype=torch.float64).pin_memory().numpy()
-    eng.fock_rhf(P_pin, out=G_pin)
+    # ---- end to end from host buffers: N = 1 through the public host-buffer
+    # entry point hfg_fock_rhf (H2D of P, build, D2H of G inside the call);
+    # N > 1 the same by hand around the sharded build and its all-reduce
+    P_pin = torch.from_numpy(P_host).pin_memory()
+    G_pin = torch.empty(n, n, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        if sf:
+            dP.copy_(P_pin, non_blocking=True)
+            sf.fock_rhf(dP, dG)
+            G_pin.copy_(dG, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+        else:
+            eng.fock_rhf(P_pin.numpy(), out=G_pin.numpy())
+
+    e2e_step()
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        eng.fock_rhf(P_pin, out=G_pin)
+        e2e_step()
     e2e_ms = (time.perf_counter() - t0) * 1e3
-    assert np.allclose(G_pin, dG.cpu().numpy(), atol=1e-9)
+    assert np.allclose(G_pin.numpy(), G_full.cpu().numpy(), atol=1e-9)
     if dist:
         t = torch.tensor([e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -298,23 +328,26 @@ def main():
     eng.set_profiling(False)
     top = max(prof, key=lambda c: c["ms"])
     peak = E.measure_fp64_peak(local)
-    achieved = top["flops"] / (top["ms"] / 1e3) / 1e12
+    # class flops are whole-class figures; a shard runs 1/world of them
+    achieved = top["flops"] / world / (top["ms"] / 1e3) / 1e12
 
     line = {
         "metric": METRIC, "value": value, "unit": "quartets/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"(H2O)_{WATERS} {BASIS} direct RHF Fock build, seed {SEED}", "nbf": n,
-                   "schwarz_threshold": THRESHOLD, "shell_quartets": stats["shell_quartets"],
-                   "function_quartets": stats["function_quartets"], "l2": "flushed (256 MB write) between steps",
-                   "parallelism": f"replicated x{world}"},
+                   "schwarz_threshold": THRESHOLD, "shell_quartets": stats_full["shell_quartets"],
+                   "function_quartets": stats_full["function_quartets"],
+                   "l2": "flushed (256 MB write) between steps",
+                   "parallelism": f"task shards x{world}, one NCCL all-reduce of G per build" if world > 1
+                   else "single GPU"},
         "e2e": {"value": e2e, "unit": "quartets/s", "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": n * n * 8},
         "gpu_launches": stats["kernel_launches"] * args.steps,
         "roofline": {"bound": "fp64", "kernel": f"eri_class_kernel<{top['la']},{top['lb']},{top['lc']},{top['ld']}> (J/K)",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "peak_source": "measured in-run: FP64 FMA microbenchmark (hfg_measure_fp64_peak)",
                      "traffic": None},
-        "build_tflops": stats["flops"] / (total_ms / args.steps / 1e3) / 1e12,
+        "build_tflops": stats_full["flops"] / (total_ms / args.steps / 1e3) / 1e12,
         "classes": [{"class": f"({c['la']}{c['lb']}|{c['lc']}{c['ld']})", "ms": round(c["ms"], 4),
                      "tflops": round(c["flops"] / max(c["ms"], 1e-9) / 1e9, 3)} for c in prof],
         "clocks": clocks.summary(),

@@ -137,6 +137,7 @@ struct hfg_ctx {
   bool inc_valid = false, inc_uhf = false;
   double mixed_cutoff = 0;
   bool counted = false;                          // d_counters hold the last build's counts
+  int shard_rank = 0, shard_count = 1;           // direct builds: this shard of every class's tasks
   hfg_stats stats{};
   bool profiling = false;
   bool precision_form() const { return opts.density_screening || opts.incremental || mixed_cutoff > 0; }
@@ -303,12 +304,19 @@ static int grid_for(const hfg_ctx *c, int ntasks, int cls) {
   return std::max(1, std::min(blocks, c->num_sms * 16));
 }
 
-static ClassLaunch base_launch(const hfg_ctx *c, const QuartetClass &q) {
+// A class launch over all tasks, or with `sharded` over this context's
+// shard of them: every shard_count-th task from shard_rank (the tasks of a
+// class are in bucket, then Schwarz order, so the interleave spreads cheap
+// and expensive tasks evenly over the shards).
+static ClassLaunch base_launch(const hfg_ctx *c, const QuartetClass &q, bool sharded = false) {
   ClassLaunch cl{};
   cl.bra_list = c->pclass[q.bra_pc].d_pairs;
   cl.ket_list = c->pclass[q.ket_pc].d_pairs;
   cl.tasks = q.d_tasks;
-  cl.ntasks = (int)q.tasks.size();
+  const int total = (int)q.tasks.size();
+  cl.task_offset = sharded ? c->shard_rank : 0;
+  cl.task_stride = sharded ? c->shard_count : 1;
+  cl.ntasks = total > cl.task_offset ? (total - cl.task_offset + cl.task_stride - 1) / cl.task_stride : 0;
   cl.same_class = q.bra_pc == q.ket_pc;
   return cl;
 }
@@ -490,7 +498,7 @@ static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const do
   const int prec = !precise ? 0 : c->mixed_cutoff > 0 ? 2 : 1;
   c->stats = hfg_stats{};
   for (auto &q : c->qclasses) {
-    ClassLaunch cl = base_launch(c, q);
+    ClassLaunch cl = base_launch(c, q, true);
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_a, s));
     cl.Da = Da;
     cl.Db = Db;
@@ -501,13 +509,17 @@ static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const do
     cl.dens_threshold = (float)c->density_threshold();
     cl.mixed_cutoff = (float)c->mixed_cutoff;
     cl.counters = precise ? c->d_counters : nullptr;
-    st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, prec, s, &launches);
-    if (st != HFG_OK) return st;
+    if (cl.ntasks > 0) {
+      st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, prec, s, &launches);
+      if (st != HFG_OK) return st;
+    }
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_b, s));
-    c->stats.shell_quartets += q.shell_quartets;
-    c->stats.function_quartets += q.function_quartets;
-    c->stats.primitive_quartets += q.prim_quartets;
-    c->stats.flops += q.flops;
+    // a shard's share of the class, in proportion to its tasks
+    const double share = q.tasks.empty() ? 0.0 : (double)cl.ntasks / (double)q.tasks.size();
+    c->stats.shell_quartets += (int64_t)(share * (double)q.shell_quartets + 0.5);
+    c->stats.function_quartets += (int64_t)(share * (double)q.function_quartets + 0.5);
+    c->stats.primitive_quartets += (int64_t)(share * (double)q.prim_quartets + 0.5);
+    c->stats.flops += share * q.flops;
   }
   HFG_CUDA(cudaGetLastError());
   HFG_CUDA(cudaEventRecord(c->ev1, s));
@@ -986,6 +998,15 @@ hfg_status hfg_set_mixed_cutoff(hfg_ctx *c, double cutoff) {
   if (!c) return hfg::fail(HFG_INVALID_ARG, "null context");
   if (!(cutoff >= 0) || !(cutoff < 1e300)) return hfg::fail(HFG_INVALID_ARG, "mixed cutoff must be finite and >= 0");
   c->mixed_cutoff = cutoff;
+  return HFG_OK;
+}
+
+hfg_status hfg_set_shard(hfg_ctx *c, int32_t rank, int32_t count) {
+  if (!c) return hfg::fail(HFG_INVALID_ARG, "null context");
+  if (count < 1 || rank < 0 || rank >= count) return hfg::fail(HFG_INVALID_ARG, "shard rank outside [0, count)");
+  c->shard_rank = rank;
+  c->shard_count = count;
+  c->inc_valid = false;  // an incremental history belongs to one shard
   return HFG_OK;
 }
 

@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(32 * fused_warps(LA, LB, LC, LD), fused_min_bl
   const int warp = threadIdx.x >> 5;
   const int n = v.nbf;
   for (int t = blockIdx.x * kW + warp; t < cl.ntasks; t += gridDim.x * kW) {
-    const Task task = cl.tasks[t];
+    const Task task = launch_task(cl, t);
     const int bp = cl.bra_list[task.bra_pos];
     const int kpos = task.ket_start + lane;
     bool active = kpos < task.ket_end;

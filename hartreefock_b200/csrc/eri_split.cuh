@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(kThreads) eri_prim_split_kernel(const EngineVi
   stage_boys<LTOT>(tab, v.boys_table);
   const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= (long long)ch.ntasks * 32) return;  // whole warps
-  const Task task = cl.tasks[ch.task0 + (int)(slot >> 5)];
+  const Task task = launch_task(cl, ch.task0 + (int)(slot >> 5));
   const int kpos = task.ket_start + (int)(slot & 31);
   bool active = kpos < task.ket_end;
   const int bp = cl.bra_list[task.bra_pos], kp = active ? cl.ket_list[kpos] : bp;
@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(kThreads) eri_hrr_digest_kernel(const EngineVi
   if (tloc >= ch.ntasks) return;  // whole block
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const long long slot = (long long)tloc * 32 + lane;
-  const Task task = cl.tasks[ch.task0 + tloc];
+  const Task task = launch_task(cl, ch.task0 + tloc);
   const int kpos = task.ket_start + lane;
   bool active = kpos < task.ket_end;
   const int bp = cl.bra_list[task.bra_pos];

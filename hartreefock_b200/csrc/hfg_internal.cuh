@@ -103,7 +103,9 @@ struct ClassLaunch {
   const int *bra_list;   // pair indices of the bra class, sorted by Q desc
   const int *ket_list;   // pair indices of the ket class, sorted by Q desc
   const Task *tasks;
-  int ntasks;
+  int ntasks;            // tasks of this launch (of this shard)
+  int task_offset;       // shard: launch task t is tasks[task_offset + t * task_stride]
+  int task_stride;
   int same_class;        // bra class == ket class
   double threshold;
   // outputs by mode
@@ -117,6 +119,11 @@ struct ClassLaunch {
   float mixed_cutoff;    // tasks whose largest bound is below run in FP32
   unsigned long long *counters;  // [0] FP64, [1] FP32 quartets evaluated
 };
+
+// task t of a launch (shards take every task_stride-th task of the class)
+__device__ __forceinline__ Task launch_task(const ClassLaunch &cl, int t) {
+  return cl.tasks[cl.task_offset + (long long)t * cl.task_stride];
+}
 
 // One chunk of a split-path class launch (see eri_split.cuh): scratch for
 // the contracted [e0|f0] blocks of `ntasks` tasks starting at `task0`.

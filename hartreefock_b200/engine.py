@@ -25,7 +25,8 @@ EXPORTED = ["hfg_default_opts", "hfg_last_error", "hfg_device_count", "hfg_ctx_c
             "hfg_ctx_nbf", "hfg_packed_size", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet",
             "hfg_fock_rhf", "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz",
             "hfg_ctx_stats", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak",
-            "hfg_fock_rhf_noalloc", "hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental"]
+            "hfg_fock_rhf_noalloc", "hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental",
+            "hfg_set_shard"]
 
 
 class HfgError(RuntimeError):
@@ -102,7 +103,8 @@ def library(path: str = LIB_PATH):
     L.hfg_fock_reset.argtypes = [vp]
     L.hfg_set_mixed_cutoff.argtypes = [vp, ctypes.c_double]
     L.hfg_set_incremental.argtypes = [vp, i32]
-    for name in ("hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak", "hfg_ctx_create", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet", "hfg_fock_rhf",
+    L.hfg_set_shard.argtypes = [vp, i32, i32]
+    for name in ("hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental", "hfg_set_shard", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak", "hfg_ctx_create", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet", "hfg_fock_rhf",
                  "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz", "hfg_ctx_stats"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
@@ -201,6 +203,20 @@ class Engine:
         _check(library().hfg_fock_rhf_device(self._h, ctypes.c_void_p(P_ptr), ctypes.c_void_p(G_ptr),
                                              ctypes.c_void_p(stream)))
 
+    def fock_rhf_tensor(self, P, G):
+        """Direct build between torch CUDA tensors (contiguous n x n float64),
+        on torch's current stream."""
+        import torch
+        assert P.is_cuda and G.is_cuda and P.dtype == torch.float64 and P.is_contiguous() and G.is_contiguous()
+        self.fock_rhf_device(P.data_ptr(), G.data_ptr(), torch.cuda.current_stream().cuda_stream)
+
+    def fock_uhf_tensor(self, Pa, Pb, Ga, Gb):
+        import torch
+        for t in (Pa, Pb, Ga, Gb):
+            assert t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()
+        self.fock_uhf_device(Pa.data_ptr(), Pb.data_ptr(), Ga.data_ptr(), Gb.data_ptr(),
+                             torch.cuda.current_stream().cuda_stream)
+
     def fock_rhf_noalloc(self, P_ptr: int, G_ptr: int, stream: int = 0):
         """Allocation-free direct RHF build (fixed 1024-function scratch)."""
         _check(library().hfg_fock_rhf_noalloc(self._h, ctypes.c_void_p(P_ptr), ctypes.c_void_p(G_ptr),
@@ -220,6 +236,10 @@ class Engine:
 
     def set_incremental(self, on: bool):
         _check(library().hfg_set_incremental(self._h, int(on)))
+
+    def set_shard(self, rank: int, count: int):
+        """Direct builds return shard `rank` of `count`'s partial G (hfg_set_shard)."""
+        _check(library().hfg_set_shard(self._h, int(rank), int(count)))
 
     def schwarz(self) -> np.ndarray:
         n = len(self.table.L)

@@ -161,6 +161,16 @@ hfg_status hfg_fock_reset(hfg_ctx *ctx);
 hfg_status hfg_set_mixed_cutoff(hfg_ctx *ctx, double cutoff);
 hfg_status hfg_set_incremental(hfg_ctx *ctx, int32_t on);
 
+/* Sharded direct builds (one molecule over several GPUs; no reference
+ * counterpart): with shard (rank, count) set, hfg_fock_rhf/uhf[_device]
+ * evaluate only every count-th task of each quartet class starting at rank,
+ * and return that shard's partial G.  The partial G of the `count` shards
+ * sum to the full G (G is linear in the J/K sums); the caller reduces them,
+ * e.g. with one NCCL all-reduce (hartreefock_b200/shards.py).  Incremental
+ * builds keep a per-shard history.  Stored builds (hfg_eri_packed) and
+ * hfg_fock_rhf_noalloc are not sharded.  Default (0, 1). */
+hfg_status hfg_set_shard(hfg_ctx *ctx, int32_t rank, int32_t count);
+
 /* Allocation-free variant of hfg_fock_rhf_device, for callers that must not
  * allocate device memory while they run: a serving loop under a fixed HBM
  * budget, code that cannot afford the implicit synchronisation of
