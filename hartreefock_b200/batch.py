@@ -1,0 +1,215 @@
+"""Batched SCF: many independent molecules of uneven size converged together.
+
+Every iteration runs one batched Fock build (engine.BatchEngine: one launch
+per quartet class over all molecules' tasks) and the reference's SCF step
+(RestrictedHartreeFock.cpp:61-166, UnrestrictedHartreeFock.cpp:87-191) for
+all molecules at once in torch on the device: F = h + G, DIIS (keep 6, start
+at 5; DIIS.h:9-96), F' = V F V, batched eigensolve, new density, energy,
+mixing, the reference's convergence test per molecule.  Molecules that have
+converged drop out of the following builds (the engine's `active` mask).
+Matrices are padded to the largest molecule: a padded block carries a large
+diagonal shift in F', so its levels sort above every real one and are never
+occupied.  All FP64.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import engine as E
+from . import scf
+
+E_CONV_DIIS, E_CONV, RMS_CONV, DIIS_CONV = 1e-11, 1e-13, 1e-10, 1e-10  # Constants.h:6-10
+PAD_SHIFT = 1.0e4
+
+
+class BatchSCF:
+    """molecules: sequence of dicts with Z, xyz (bohr), basis, and optionally
+    unrestricted (bool), alpha/beta electron counts (UHF)."""
+
+    def __init__(self, molecules, unrestricted=False, alpha=0.75, init_guess=0.75, max_iter=300,
+                 use_diis=True, schwarz_threshold=1e-12, device="cuda"):
+        self.mols = list(molecules)
+        self.uhf = unrestricted
+        self.alpha, self.init_guess, self.max_iter, self.use_diis = alpha, init_guess, max_iter, use_diis
+        self.dev = torch.device(device)
+        self.eng = E.BatchEngine([(m["Z"], m["xyz"], m["basis"]) for m in self.mols],
+                                 schwarz_threshold=schwarz_threshold)
+        M = len(self.mols)
+        self.M = M
+        self.nbf = self.eng.nbf.astype(np.int64)
+        self.nmax = int(self.nbf.max())
+        n = self.nmax
+        # flat (engine layout) <-> padded [M, n, n] index maps
+        rows, flat = [], []
+        for m in range(M):
+            k = int(self.nbf[m])
+            i, j = np.meshgrid(np.arange(k), np.arange(k), indexing="ij")
+            rows.append(m * n * n + i.ravel() * n + j.ravel())
+            flat.append(self.eng.offset[m] + i.ravel() * k + j.ravel())
+        self.pad_idx = torch.from_numpy(np.concatenate(rows)).to(self.dev)
+        self.flat_idx = torch.from_numpy(np.concatenate(flat)).to(self.dev)
+        # one-electron matrices, S^-1/2, occupations, nuclear repulsion
+        h = np.zeros((M, n, n))
+        S = np.zeros((M, n, n))
+        self.enuc = np.zeros(M)
+        self.nocc = np.zeros((2, M), dtype=np.int64)
+        for m, mol in enumerate(self.mols):
+            k = int(self.nbf[m])
+            Sm, hm = scf.one_electron(mol["Z"], mol["xyz"], mol["basis"])
+            h[m, :k, :k], S[m, :k, :k] = hm, Sm
+            self.enuc[m] = _nuclear_repulsion(mol["Z"], mol["xyz"])
+            ne = int(sum(mol["Z"]))
+            if unrestricted:
+                na = mol.get("alpha_electrons") or ne - ne // 2
+                nb = mol.get("beta_electrons") or ne // 2
+                self.nocc[:, m] = (na, nb)
+            else:
+                self.nocc[:, m] = (max(1, ne // 2), 0)
+        self.h = torch.from_numpy(h).to(self.dev)
+        self.S = torch.from_numpy(S).to(self.dev)
+        valid = torch.zeros(M, n, device=self.dev, dtype=torch.bool)
+        for m in range(M):
+            valid[m, : int(self.nbf[m])] = True
+        self.valid = valid
+        # V = S^-1/2 (HartreeFockAlgorithm.cpp:48-59); the padded block of S
+        # is set to the identity for the decomposition, then V's is zeroed
+        Spad = self.S + torch.diag_embed((~valid).double())
+        w, U = torch.linalg.eigh(Spad)
+        V = U @ torch.diag_embed(w.rsqrt()) @ U.transpose(1, 2)
+        mask2 = valid[:, :, None] & valid[:, None, :]
+        self.V = 0.5 * (V + V.transpose(1, 2)) * mask2
+        self.mask2 = mask2
+        self.shift = torch.diag_embed((~valid).double() * PAD_SHIFT)
+
+    # ---- flat <-> padded
+    def to_flat(self, X):
+        out = torch.zeros(self.eng.total, dtype=torch.float64, device=self.dev)
+        out[self.flat_idx] = X.reshape(-1)[self.pad_idx]
+        return out
+
+    def to_pad(self, flat):
+        out = torch.zeros(self.M * self.nmax * self.nmax, dtype=torch.float64, device=self.dev)
+        out[self.pad_idx] = flat[self.flat_idx]
+        return out.reshape(self.M, self.nmax, self.nmax)
+
+    def _guess_fock(self):
+        h = self.h
+        if self.init_guess > 0:
+            d = torch.diagonal(h, dim1=1, dim2=2)
+            F = self.init_guess * self.S * (d[:, :, None] + d[:, None, :]) * 0.5
+        else:
+            F = h.clone()
+        return F
+
+    def _occ_mask(self, spin):
+        return (torch.arange(self.nmax, device=self.dev)[None, :] <
+                torch.from_numpy(self.nocc[spin]).to(self.dev)[:, None]).double()
+
+    def run(self):
+        M, n, dev = self.M, self.nmax, self.dev
+        nspin = 2 if self.uhf else 1
+        P = [torch.zeros(M, n, n, dtype=torch.float64, device=dev) for _ in range(nspin)]
+        diisF = [[] for _ in range(nspin)]
+        diisE = [[] for _ in range(nspin)]
+        energy = torch.full((M,), float("inf"), dtype=torch.float64, device=dev)
+        prev = torch.full((M,), float("inf"), dtype=torch.float64, device=dev)
+        active = torch.ones(M, dtype=torch.bool, device=dev)
+        iters = torch.zeros(M, dtype=torch.int64, device=dev)
+        flatG = [torch.zeros(self.eng.total, dtype=torch.float64, device=dev) for _ in range(nspin)]
+        builds = 0
+        for it in range(self.max_iter):
+            act = active.clone()
+            if it == 0:
+                F0 = self._guess_fock()
+                F = [F0.clone() for _ in range(nspin)]
+                if self.uhf:  # UnrestrictedHartreeFock.cpp:214-219: asymmetry on the alpha guess
+                    F[0][:, 0, 1] += 0.1
+                    F[0][:, 1, 0] = F[0][:, 0, 1]
+            else:
+                flatP = [self.to_flat(p) for p in P]
+                active_np = act.cpu().numpy().astype(np.uint8)
+                if self.uhf:
+                    self.eng.fock_uhf(flatP[0], flatP[1], flatG[0], flatG[1], active=active_np)
+                else:
+                    self.eng.fock_rhf(flatP[0], flatG[0], active=active_np)
+                builds += 1
+                F = [self.h + self.to_pad(g) for g in flatG]
+            if not self.uhf:
+                F = [0.5 * (f + f.transpose(1, 2)) for f in F]
+            used = torch.zeros(M, dtype=torch.bool, device=dev)
+            err_est = torch.zeros(M, dtype=torch.float64, device=dev)
+            if self.use_diis and it > 0:
+                for s in range(nspin):
+                    err = self.S @ P[s] @ F[s] - F[s] @ P[s] @ self.S
+                    diisF[s].append(F[s].clone())
+                    diisE[s].append(err)
+                    if len(diisF[s]) > 6:
+                        diisF[s].pop(0)
+                        diisE[s].pop(0)
+                    if len(diisF[s]) >= 5:
+                        F[s], est = _diis_extrapolate(diisF[s], diisE[s])
+                        err_est = err_est + est
+                        used[:] = True
+            Pn, eps = [], []
+            for s in range(nspin):
+                Ft = self.V @ F[s] @ self.V + self.shift
+                w, Cp = torch.linalg.eigh(Ft)
+                C = self.V @ Cp
+                occ = self._occ_mask(s)
+                factor = 1.0 if self.uhf else 2.0
+                Co = C * occ[:, None, :]
+                Pn.append(factor * Co @ Co.transpose(1, 2))
+                eps.append((w * occ).sum(1))
+            if self.uhf:
+                e = 0.5 * (((Pn[0] + Pn[1]) * self.h).sum((1, 2)) + eps[0] + eps[1])
+            else:
+                e = 0.5 * (Pn[0] * self.h).sum((1, 2)) + eps[0]
+            e = e + torch.from_numpy(self.enuc).to(dev)
+            rms = torch.sqrt(sum(((pn - p) ** 2).sum((1, 2)) for pn, p in zip(Pn, P)))
+            for s in range(nspin):
+                mix = torch.where(used[:, None, None], Pn[s], self.alpha * Pn[s] + (1 - self.alpha) * P[s])
+                P[s] = torch.where(act[:, None, None], mix, P[s])
+            energy = torch.where(act, e, energy)
+            dE = (prev - e).abs()
+            econv = E_CONV_DIIS if self.use_diis else E_CONV
+            conv = (dE <= econv) & (rms < RMS_CONV) & (err_est < DIIS_CONV)
+            iters = torch.where(act, iters + 1, iters)
+            prev = torch.where(act, e, prev)
+            active = act & ~conv
+            if not bool(active.any()):
+                break
+        self.iterations = iters.cpu().numpy()
+        self.converged = (~active).cpu().numpy()
+        self.builds = builds
+        self.energies = energy.cpu().numpy()
+        self.densities = P
+        return self.energies
+
+
+def _diis_extrapolate(Fs, Es):
+    """Pulay extrapolation per molecule (DIIS.h:34-96): B_ij = <e_i, e_j>,
+    bordered by ones; returns sum_i c_i F_i and sqrt(|e_m|^2 + |e_m-1|^2)."""
+    m = len(Fs)
+    Ee = torch.stack(Es, 1)  # [M, m, n, n]
+    B = torch.einsum("aikl,ajkl->aij", Ee, Ee)
+    M = B.shape[0]
+    Bb = torch.zeros(M, m + 1, m + 1, dtype=B.dtype, device=B.device)
+    Bb[:, :m, :m] = B
+    Bb[:, m, :m] = 1
+    Bb[:, :m, m] = 1
+    rhs = torch.zeros(M, m + 1, 1, dtype=B.dtype, device=B.device)
+    rhs[:, m, 0] = 1
+    c = torch.linalg.lstsq(Bb, rhs).solution[:, :m, 0] if Bb.device.type == "cpu" else torch.linalg.solve(Bb, rhs)[:, :m, 0]
+    F = torch.einsum("ai,aikl->akl", c, torch.stack(Fs, 1))
+    est = torch.sqrt(torch.diagonal(B, dim1=1, dim2=2)[:, -2:].sum(1))
+    return F, est
+
+
+def _nuclear_repulsion(Z, xyz):
+    xyz = np.asarray(xyz, dtype=np.float64).reshape(-1, 3)
+    e = 0.0
+    for a in range(len(Z)):
+        for b in range(a):
+            e += Z[a] * Z[b] / np.linalg.norm(xyz[a] - xyz[b])
+    return e

@@ -74,7 +74,9 @@ constexpr int kBuckets = 6;
 static inline int prim_bucket(int np) { return np <= 1 ? 0 : np <= 3 ? 1 : np <= 6 ? 2 : np <= 12 ? 3 : np <= 24 ? 4 : 5; }
 struct PairClassList {
   std::vector<int> pairs;  // concatenated buckets
-  int bucket_start[kBuckets + 1] = {};
+  // segment starts in `pairs`, molecule-major then bucket: molecule m's
+  // bucket k is [seg_start[m * kBuckets + k], seg_start[m * kBuckets + k + 1])
+  std::vector<int> seg_start;
   int *d_pairs = nullptr;
 };
 
@@ -138,6 +140,16 @@ struct hfg_ctx {
   double mixed_cutoff = 0;
   bool counted = false;                          // d_counters hold the last build's counts
   int shard_rank = 0, shard_count = 1;           // direct builds: this shard of every class's tasks
+  // batched contexts: many molecules, shell pairs and quartets only within a
+  // molecule, each molecule's n x n matrices at mol_off[m] in flat buffers
+  bool batch = false;
+  int nmol = 1;
+  std::vector<int> pair_mol, mol_nbf;
+  std::vector<long long> mol_off;
+  long long batch_elems = 0;
+  int *d_pair_mol = nullptr, *d_mol_nbf = nullptr;
+  long long *d_mol_off = nullptr;
+  unsigned char *d_mol_active = nullptr;
   hfg_stats stats{};
   bool profiling = false;
   bool precision_form() const { return opts.density_screening || opts.incremental || mixed_cutoff > 0; }
@@ -161,6 +173,12 @@ struct hfg_ctx {
     v.boys_table = d_boys;
     v.nbf = nbf;
     v.reference_convention = opts.eri_convention == HFG_ERI_REFERENCE;
+    if (batch) {
+      v.pair_mol = d_pair_mol;
+      v.mol_nbf = d_mol_nbf;
+      v.mol_off = d_mol_off;
+      v.mol_active = d_mol_active;
+    }
     return v;
   }
   ~hfg_ctx() {
@@ -175,7 +193,7 @@ struct hfg_ctx {
                     d_pair_AB,    d_pair_Q,        d_boys,       d_J,        d_Ka,         d_Kb,        d_P,
                     d_Pb,         d_Pt,            d_G,          d_Gb,       d_block,      d_scratch,   d_shell_ao,
                     d_shell_nf,   d_shell_dmax,    d_counters,   d_prev_P[0], d_prev_P[1], d_prev_G[0], d_prev_G[1],
-                    d_dP[0],      d_dP[1],         d_primf};
+                    d_dP[0],      d_dP[1],         d_primf,      d_pair_mol, d_mol_nbf,    d_mol_off,   d_mol_active};
     for (void *b : bufs) cudaFree(b);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -256,8 +274,10 @@ static void build_quartet_classes(hfg_ctx *c, double threshold) {
       const double need = threshold / qb;
       const int64_t bf = pair_functions(c, bras[b]);
       const int64_t bprim = c->pair_nprim[bras[b]];
+      // kets come from the bra's own molecule only
+      const int mol = c->pair_mol.empty() ? 0 : c->pair_mol[bras[b]];
       for (int k = 0; k < kBuckets; ++k) {
-        const int64_t s0 = KL.bucket_start[k], s1 = KL.bucket_start[k + 1];
+        const int64_t s0 = KL.seg_start[mol * kBuckets + k], s1 = KL.seg_start[mol * kBuckets + k + 1];
         // kets of the bucket with qb * qk >= threshold form a prefix
         int64_t lo = s0, hi = s1;
         while (lo < hi) {
@@ -452,6 +472,7 @@ static hfg_status launch_class(hfg_ctx *c, const QuartetClass &q, const ClassLau
 // screening, and accumulates G onto the previous one.
 static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const double *dPb, double *dGa, double *dGb,
                                cudaStream_t s) {
+  if (c->batch) return fail(HFG_INVALID_ARG, "batched context: use hfg_fock_rhf/uhf_batch_device");
   const size_t nn = (size_t)c->nbf * c->nbf;
   const int n = c->nbf;
   hfg_status st;
@@ -546,6 +567,93 @@ static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const do
   return HFG_OK;
 }
 
+// Batched contexts: G of every active molecule, blockIdx.y = molecule.
+__global__ void finalize_rhf_batch(const double *J, const double *K, double *G, const int *nbf,
+                                   const long long *off, const unsigned char *active) {
+  const int m = blockIdx.y;
+  if (!active[m]) return;
+  const int n = nbf[m];
+  const long long b = off[m];
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n * n; x += gridDim.x * blockDim.x) {
+    const int i = x / n, j = x - i * n;
+    G[b + x] = (J[b + i * n + j] + J[b + j * n + i]) - 0.5 * (K[b + i * n + j] + K[b + j * n + i]);
+  }
+}
+
+__global__ void finalize_uhf_batch(const double *J, const double *Ka, const double *Kb, double *Ga, double *Gb,
+                                   const int *nbf, const long long *off, const unsigned char *active) {
+  const int m = blockIdx.y;
+  if (!active[m]) return;
+  const int n = nbf[m];
+  const long long b = off[m];
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < n * n; x += gridDim.x * blockDim.x) {
+    const int i = x / n, j = x - i * n;
+    const double jv = J[b + i * n + j] + J[b + j * n + i];
+    Ga[b + x] = jv - (Ka[b + i * n + j] + Ka[b + j * n + i]);
+    Gb[b + x] = jv - (Kb[b + i * n + j] + Kb[b + j * n + i]);
+  }
+}
+
+// Direct J/K build of a batched context: one launch per quartet class over
+// the tasks of all molecules (inactive molecules' tasks exit at once), then
+// G per active molecule.  `active`: host flags per molecule, or null = all.
+static hfg_status batch_build(hfg_ctx *c, bool uhf, const double *dPa, const double *dPb, double *dGa, double *dGb,
+                              const unsigned char *active, cudaStream_t s) {
+  const size_t tot = (size_t)c->batch_elems;
+  hfg_status st;
+  if ((st = ensure(&c->d_J, tot)) != HFG_OK || (st = ensure(&c->d_Ka, tot)) != HFG_OK) return st;
+  if (uhf && ((st = ensure(&c->d_Kb, tot)) != HFG_OK || (st = ensure(&c->d_Pt, tot)) != HFG_OK)) return st;
+  const std::vector<unsigned char> all(c->nmol, 1);
+  HFG_CUDA(cudaMemcpyAsync(c->d_mol_active, active ? active : all.data(), c->nmol, cudaMemcpyHostToDevice, s));
+  HFG_CUDA(cudaMemsetAsync(c->d_J, 0, tot * sizeof(double), s));
+  HFG_CUDA(cudaMemsetAsync(c->d_Ka, 0, tot * sizeof(double), s));
+  int launches = 2;
+  if (uhf) {
+    HFG_CUDA(cudaMemsetAsync(c->d_Kb, 0, tot * sizeof(double), s));
+    add_densities<<<std::max(1, std::min(1024, (int)((tot + 255) / 256))), 256, 0, s>>>(dPa, dPb, c->d_Pt, (int)tot);
+    launches += 2;
+  }
+  HFG_CUDA(cudaEventRecord(c->ev0, s));
+  const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
+  c->stats = hfg_stats{};
+  for (auto &q : c->qclasses) {
+    ClassLaunch cl = base_launch(c, q, true);
+    if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_a, s));
+    cl.Da = dPa;
+    cl.Db = dPb;
+    cl.Dt = uhf ? c->d_Pt : dPa;
+    cl.J = c->d_J;
+    cl.Ka = c->d_Ka;
+    cl.Kb = c->d_Kb;
+    if (cl.ntasks > 0) {
+      st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, 0, s, &launches);
+      if (st != HFG_OK) return st;
+    }
+    if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_b, s));
+    c->stats.shell_quartets += q.shell_quartets;
+    c->stats.function_quartets += q.function_quartets;
+    c->stats.primitive_quartets += q.prim_quartets;
+    c->stats.flops += q.flops;
+  }
+  HFG_CUDA(cudaGetLastError());
+  HFG_CUDA(cudaEventRecord(c->ev1, s));
+  int nmax = 0;
+  for (int n : c->mol_nbf) nmax = std::max(nmax, n);
+  const dim3 fg(std::max(1, std::min(64, (nmax * nmax + 255) / 256)), c->nmol);
+  if (uhf)
+    finalize_uhf_batch<<<fg, 256, 0, s>>>(c->d_J, c->d_Ka, c->d_Kb, dGa, dGb, c->d_mol_nbf, c->d_mol_off,
+                                          c->d_mol_active);
+  else
+    finalize_rhf_batch<<<fg, 256, 0, s>>>(c->d_J, c->d_Ka, dGa, c->d_mol_nbf, c->d_mol_off, c->d_mol_active);
+  ++launches;
+  HFG_CUDA(cudaGetLastError());
+  c->stats.kernel_launches = launches;
+  c->stats.shell_pairs = c->npairs;
+  c->stats.fp64_shell_quartets = c->stats.shell_quartets;
+  c->counted = false;
+  return HFG_OK;
+}
+
 static hfg_status finish_timing(hfg_ctx *c) {
   HFG_CUDA(cudaEventSynchronize(c->ev1));
   float ms = 0;
@@ -557,6 +665,7 @@ static hfg_status finish_timing(hfg_ctx *c) {
 }
 
 static hfg_status stored_build(hfg_ctx *c, double *d_out, int64_t count, cudaStream_t s) {
+  if (c->batch) return fail(HFG_INVALID_ARG, "batched context: no stored table");
   HFG_CUDA(cudaMemsetAsync(d_out, 0, (size_t)count * sizeof(double), s));
   HFG_CUDA(cudaEventRecord(c->ev0, s));
   const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
@@ -616,12 +725,19 @@ int64_t hfg_packed_size(int32_t n) {
 
 int32_t hfg_ctx_nbf(const hfg_ctx *c) { return c ? c->nbf : 0; }
 
-hfg_status hfg_ctx_create(const hfg_shells *sh, const hfg_opts *opts, hfg_ctx **out) {
+}  // extern "C"
+
+// Context over one molecule (shell_mol = nullptr) or over `nmol` molecules
+// whose shells `sh` lists one after another (shell_mol[s] = molecule of
+// shell s, AO offsets molecule-local, mol_nbf[m] its functions): shell pairs,
+// and hence quartets, only within a molecule.
+static hfg_status create_context(const hfg_shells *sh, const int *shell_mol, int nmol, const int *mol_nbf,
+                                 const hfg_opts *opts, hfg_ctx **out) {
   using namespace hfg;
   if (!out) return fail(HFG_INVALID_ARG, "out is null");
   *out = nullptr;
   if (!sh || sh->nshells <= 0 || !sh->center || !sh->L || !sh->nprim || !sh->prim_offset || !sh->ao_offset ||
-      !sh->exponent || !sh->coefficient || sh->nbf <= 0)
+      !sh->exponent || !sh->coefficient || (!shell_mol && sh->nbf <= 0))
     return fail(HFG_INVALID_ARG, "incomplete hfg_shells");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(HFG_NO_DEVICE, "no CUDA device");
@@ -633,10 +749,12 @@ hfg_status hfg_ctx_create(const hfg_shells *sh, const hfg_opts *opts, hfg_ctx **
   ctx->device = ctx->opts.device;
   HFG_CUDA(cudaSetDevice(ctx->device));
   HFG_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
-  ctx->nbf = sh->nbf;
+  ctx->batch = shell_mol != nullptr;
+  ctx->nmol = ctx->batch ? nmol : 1;
+  ctx->nbf = ctx->batch ? 0 : sh->nbf;
   const int ns = sh->nshells;
   ctx->shells.resize(ns);
-  int64_t funcs = 0;
+  std::vector<int64_t> funcs(ctx->nmol, 0);
   for (int s = 0; s < ns; ++s) {
     HostShell &h = ctx->shells[s];
     for (int d = 0; d < 3; ++d) h.c[d] = sh->center[3 * s + d];
@@ -644,12 +762,16 @@ hfg_status hfg_ctx_create(const hfg_shells *sh, const hfg_opts *opts, hfg_ctx **
     h.nprim = sh->nprim[s];
     h.prim_off = sh->prim_offset[s];
     h.ao = sh->ao_offset[s];
+    const int m = ctx->batch ? shell_mol[s] : 0;
+    const int mnbf = ctx->batch ? mol_nbf[m] : sh->nbf;
     if (h.L < 0 || h.L > kMaxL) return fail(HFG_UNSUPPORTED_L, "shell angular momentum above d");
     if (h.nprim <= 0 || h.prim_off < 0) return fail(HFG_INVALID_ARG, "shell without primitives");
-    if (h.ao < 0 || h.ao + ncart_h(h.L) > sh->nbf) return fail(HFG_INVALID_ARG, "AO offset outside nbf");
-    funcs += ncart_h(h.L);
+    if (h.ao < 0 || h.ao + ncart_h(h.L) > mnbf) return fail(HFG_INVALID_ARG, "AO offset outside nbf");
+    funcs[m] += ncart_h(h.L);
   }
-  if (funcs != sh->nbf) return fail(HFG_INVALID_ARG, "shell functions do not sum to nbf");
+  for (int m = 0; m < ctx->nmol; ++m)
+    if (funcs[m] != (ctx->batch ? mol_nbf[m] : sh->nbf))
+      return fail(HFG_INVALID_ARG, "shell functions do not sum to nbf");
   if (!(ctx->opts.mixed_cutoff >= 0) || !(ctx->opts.mixed_cutoff < 1e300) || !(ctx->opts.density_threshold >= 0))
     return fail(HFG_INVALID_ARG, "mixed cutoff and density threshold must be finite and >= 0");
   ctx->mixed_cutoff = ctx->opts.mixed_cutoff;
@@ -664,9 +786,18 @@ hfg_status hfg_ctx_create(const hfg_shells *sh, const hfg_opts *opts, hfg_ctx **
     if ((st0 = upload(&ctx->d_shell_ao, sao)) != HFG_OK || (st0 = upload(&ctx->d_shell_nf, snf)) != HFG_OK) return st0;
   }
 
-  // ---- shell pairs and primitive pairs (pair index a*(a+1)/2 + b, a >= b)
-  const int np = ns * (ns + 1) / 2;
+  // ---- shell pairs (a >= b, same molecule; one molecule: pair index
+  // a*(a+1)/2 + b) and their primitive pairs
+  std::vector<std::pair<int, int>> plist;
+  for (int a = 0; a < ns; ++a)
+    for (int b = 0; b <= a; ++b)
+      if (!ctx->batch || shell_mol[a] == shell_mol[b]) plist.emplace_back(a, b);
+  const int np = (int)plist.size();
   ctx->npairs = np;
+  if (ctx->batch) {
+    ctx->pair_mol.resize(np);
+    for (int p = 0; p < np; ++p) ctx->pair_mol[p] = shell_mol[plist[p].first];
+  }
   std::vector<PrimPair> prim;
   std::vector<int> poff(np), pn(np), psa(np), psb(np), paoa(np), paob(np);
   std::vector<double> pab(3 * (size_t)np);
@@ -674,9 +805,9 @@ hfg_status hfg_ctx_create(const hfg_shells *sh, const hfg_opts *opts, hfg_ctx **
   ctx->pair_sb.resize(np);
   ctx->pair_cls.resize(np);
   const double sqrt2pi54 = std::sqrt(2.0) * std::pow(M_PI, 1.25);
-  for (int a = 0; a < ns; ++a)
-    for (int b = 0; b <= a; ++b) {
-      const int p = a * (a + 1) / 2 + b;
+  for (int p = 0; p < np; ++p) {
+    {
+      const int a = plist[p].first, b = plist[p].second;
       int f = a, g = b;
       if (ctx->shells[b].L > ctx->shells[a].L) std::swap(f, g);  // first = higher L, else higher index
       const HostShell &A = ctx->shells[f], &B = ctx->shells[g];
@@ -721,6 +852,7 @@ hfg_status hfg_ctx_create(const hfg_shells *sh, const hfg_opts *opts, hfg_ctx **
         }
       pn[p] = (int)prim.size() - poff[p];
     }
+  }
   // Primitive-pair screening: drop primitive pairs whose largest possible
   // quartet contribution, |K_ab| max|K| / sqrt(zeta_ab + min zeta), is below
   // 1e-21 (recursion factors cannot lift that to the 1e-15 level).  Mostly
@@ -782,24 +914,101 @@ hfg_status hfg_ctx_create(const hfg_shells *sh, const hfg_opts *opts, hfg_ctx **
   ctx->pair_Q.resize(np);
   HFG_CUDA(cudaMemcpy(ctx->pair_Q.data(), ctx->d_pair_Q, (size_t)np * sizeof(double), cudaMemcpyDeviceToHost));
 
-  // ---- class lists: primitive-count buckets, each sorted by Q descending
+  // ---- class lists: per molecule, primitive-count buckets, each sorted by
+  // Q descending
+  const int nmols = ctx->nmol;
   for (int pc = 0; pc < kNumPairClasses; ++pc) {
     PairClassList &L = ctx->pclass[pc];
     L.pairs.clear();
-    for (int k = 0; k < kBuckets; ++k) {
-      L.bucket_start[k] = (int)L.pairs.size();
-      std::vector<int> bk;
-      for (int p : by_class[pc])
-        if (prim_bucket(pn[p]) == k) bk.push_back(p);
-      std::stable_sort(bk.begin(), bk.end(), [&](int x, int y) { return ctx->pair_Q[x] > ctx->pair_Q[y]; });
-      L.pairs.insert(L.pairs.end(), bk.begin(), bk.end());
+    L.seg_start.assign((size_t)nmols * kBuckets + 1, 0);
+    std::vector<std::vector<int>> seg((size_t)nmols * kBuckets);
+    for (int p : by_class[pc]) {
+      const int m = ctx->pair_mol.empty() ? 0 : ctx->pair_mol[p];
+      seg[(size_t)m * kBuckets + prim_bucket(pn[p])].push_back(p);
     }
-    L.bucket_start[kBuckets] = (int)L.pairs.size();
+    for (size_t x = 0; x < seg.size(); ++x) {
+      L.seg_start[x] = (int)L.pairs.size();
+      std::stable_sort(seg[x].begin(), seg[x].end(),
+                       [&](int a, int b) { return ctx->pair_Q[a] > ctx->pair_Q[b]; });
+      L.pairs.insert(L.pairs.end(), seg[x].begin(), seg[x].end());
+    }
+    L.seg_start[seg.size()] = (int)L.pairs.size();
     if ((st = upload(&L.d_pairs, L.pairs)) != HFG_OK) return st;
   }
   build_quartet_classes(ctx.get(), ctx->opts.schwarz_threshold);
   if ((st = upload_classes(ctx.get())) != HFG_OK) return st;
+  if (ctx->batch) {
+    ctx->mol_nbf.assign(mol_nbf, mol_nbf + nmol);
+    ctx->mol_off.resize(nmol);
+    long long off = 0;
+    for (int m = 0; m < nmol; ++m) {
+      ctx->mol_off[m] = off;
+      off += (long long)mol_nbf[m] * mol_nbf[m];
+    }
+    ctx->batch_elems = off;
+    const std::vector<unsigned char> all_active(nmol, 1);
+    if ((st = upload(&ctx->d_pair_mol, ctx->pair_mol)) != HFG_OK ||
+        (st = upload(&ctx->d_mol_nbf, ctx->mol_nbf)) != HFG_OK ||
+        (st = upload(&ctx->d_mol_off, ctx->mol_off)) != HFG_OK ||
+        (st = upload(&ctx->d_mol_active, all_active)) != HFG_OK)
+      return st;
+  }
   *out = ctx.release();
+  return HFG_OK;
+}
+
+extern "C" {
+
+hfg_status hfg_ctx_create(const hfg_shells *sh, const hfg_opts *opts, hfg_ctx **out) {
+  return create_context(sh, nullptr, 1, nullptr, opts, out);
+}
+
+hfg_status hfg_batch_create(const hfg_shells *mols, int32_t nmol, const hfg_opts *opts, hfg_ctx **out) {
+  using namespace hfg;
+  if (!out) return fail(HFG_INVALID_ARG, "out is null");
+  *out = nullptr;
+  if (!mols || nmol <= 0) return fail(HFG_INVALID_ARG, "no molecules");
+  hfg_opts o;
+  if (opts) o = *opts;
+  else hfg_default_opts(&o);
+  if (o.density_screening || o.incremental || o.mixed_cutoff > 0)
+    return fail(HFG_INVALID_ARG, "batched contexts run the plain FP64 form");
+  // one shell list: molecule after molecule, primitives concatenated
+  std::vector<double> center, expo, coef;
+  std::vector<int32_t> L, nprim, poff, aoff;
+  std::vector<int> shell_mol, nbf(nmol);
+  for (int m = 0; m < nmol; ++m) {
+    const hfg_shells &s = mols[m];
+    if (s.nshells <= 0 || !s.center || !s.L || !s.nprim || !s.prim_offset || !s.ao_offset || !s.exponent ||
+        !s.coefficient || s.nbf <= 0)
+      return fail(HFG_INVALID_ARG, "incomplete hfg_shells of molecule " + std::to_string(m));
+    nbf[m] = s.nbf;
+    for (int x = 0; x < s.nshells; ++x) {
+      if (s.nprim[x] <= 0 || s.prim_offset[x] < 0) return fail(HFG_INVALID_ARG, "shell without primitives");
+      center.insert(center.end(), s.center + 3 * x, s.center + 3 * x + 3);
+      L.push_back(s.L[x]);
+      nprim.push_back(s.nprim[x]);
+      poff.push_back((int32_t)expo.size());
+      aoff.push_back(s.ao_offset[x]);
+      expo.insert(expo.end(), s.exponent + s.prim_offset[x], s.exponent + s.prim_offset[x] + s.nprim[x]);
+      coef.insert(coef.end(), s.coefficient + s.prim_offset[x], s.coefficient + s.prim_offset[x] + s.nprim[x]);
+      shell_mol.push_back(m);
+    }
+  }
+  const hfg_shells all{(int32_t)L.size(), center.data(), L.data(), nprim.data(), poff.data(), aoff.data(),
+                       expo.data(), coef.data(), 0};
+  return create_context(&all, shell_mol.data(), nmol, nbf.data(), &o, out);
+}
+
+int32_t hfg_batch_size(const hfg_ctx *c) { return c && c->batch ? c->nmol : 0; }
+
+hfg_status hfg_batch_layout(const hfg_ctx *c, int32_t *nbf, int64_t *offset, int64_t *total) {
+  if (!c || !c->batch) return hfg::fail(HFG_INVALID_ARG, "not a batched context");
+  for (int m = 0; m < c->nmol; ++m) {
+    if (nbf) nbf[m] = c->mol_nbf[m];
+    if (offset) offset[m] = c->mol_off[m];
+  }
+  if (total) *total = c->batch_elems;
   return HFG_OK;
 }
 
@@ -847,6 +1056,28 @@ hfg_status hfg_fock_uhf_device(hfg_ctx *c, const double *dPa, const double *dPb,
   HFG_CUDA(cudaSetDevice(c->device));
   cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
   hfg_status st = direct_build(c, true, dPa, dPb, dGa, dGb, s);
+  if (st != HFG_OK) return st;
+  return finish_timing(c);
+}
+
+hfg_status hfg_fock_rhf_batch_device(hfg_ctx *c, const double *dP, double *dG, const uint8_t *active,
+                                     void *stream) {
+  if (!c || !dP || !dG) return fail(HFG_INVALID_ARG, "null argument");
+  if (!c->batch) return fail(HFG_INVALID_ARG, "not a batched context");
+  HFG_CUDA(cudaSetDevice(c->device));
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  hfg_status st = batch_build(c, false, dP, nullptr, dG, nullptr, active, s);
+  if (st != HFG_OK) return st;
+  return finish_timing(c);
+}
+
+hfg_status hfg_fock_uhf_batch_device(hfg_ctx *c, const double *dPa, const double *dPb, double *dGa, double *dGb,
+                                     const uint8_t *active, void *stream) {
+  if (!c || !dPa || !dPb || !dGa || !dGb) return fail(HFG_INVALID_ARG, "null argument");
+  if (!c->batch) return fail(HFG_INVALID_ARG, "not a batched context");
+  HFG_CUDA(cudaSetDevice(c->device));
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  hfg_status st = batch_build(c, true, dPa, dPb, dGa, dGb, active, s);
   if (st != HFG_OK) return st;
   return finish_timing(c);
 }
@@ -1060,6 +1291,7 @@ static hfg_status noalloc_scratch(int device, double **out) {
 extern "C" hfg_status hfg_fock_rhf_noalloc(hfg_ctx *c, const double *dP, double *dG, void *stream) {
   using namespace hfg;
   if (!c || !dP || !dG) return fail(HFG_INVALID_ARG, "null argument");
+  if (c->batch) return fail(HFG_INVALID_ARG, "batched context: use hfg_fock_rhf_batch_device");
   if (c->nbf > kNoAllocMaxNbf)
     return fail(HFG_INVALID_ARG, "hfg_fock_rhf_noalloc: " + std::to_string(c->nbf) +
                                      " basis functions exceed its fixed scratch of " +

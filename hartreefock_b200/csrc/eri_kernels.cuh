@@ -305,10 +305,17 @@ __global__ void __launch_bounds__(32 * fused_warps(LA, LB, LC, LD), fused_min_bl
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const int n = v.nbf;
   for (int t = blockIdx.x * kW + warp; t < cl.ntasks; t += gridDim.x * kW) {
     const Task task = launch_task(cl, t);
     const int bp = cl.bra_list[task.bra_pos];
+    // the task's molecule (batched contexts): its matrices and size
+    const MolView mv = task_molecule(v, bp);
+    if (mv.skip) continue;  // warp-uniform: the warp shares the bra pair
+    const int n = mv.n;
+    const double *Da = cl.Da + mv.base, *Db = cl.Db ? cl.Db + mv.base : nullptr;
+    const double *Dt = cl.Dt ? cl.Dt + mv.base : nullptr;
+    double *Jm = cl.J ? cl.J + mv.base : nullptr, *Kam = cl.Ka ? cl.Ka + mv.base : nullptr;
+    double *Kbm = cl.Kb ? cl.Kb + mv.base : nullptr;
     const int kpos = task.ket_start + lane;
     bool active = kpos < task.ket_end;
     const int kp = active ? cl.ket_list[kpos] : bp;
@@ -364,7 +371,7 @@ __global__ void __launch_bounds__(32 * fused_warps(LA, LB, LC, LD), fused_min_bl
       // degeneracy of the unique quartet among its 8 permutations
       const double s = (bdiag ? 0.5 : 1.0) * (kdiag ? 0.5 : 1.0) * (same ? 0.5 : 1.0);
       constexpr bool kUhf = MODE == kJkUhf;
-      const double *DJ = kUhf ? cl.Dt : cl.Da;
+      const double *DJ = kUhf ? Dt : Da;
       double jab[NA * NB], jcd[NC * ND];
       double kac[NA * NC], kad[NA * ND], kbc[NB * NC], kbd[NB * ND];
       double kac2[kUhf ? NA * NC : 1], kad2[kUhf ? NA * ND : 1], kbc2[kUhf ? NB * NC : 1], kbd2[kUhf ? NB * ND : 1];
@@ -403,49 +410,49 @@ __global__ void __launch_bounds__(32 * fused_warps(LA, LB, LC, LD), fused_min_bl
                 const double val = s * out[((a * NB + b) * NC + c) * ND + d];
                 jab[a * NB + b] += 2.0 * val * __ldg(&DJ[K * n + L]);
                 jcd[c * ND + d] += 2.0 * val * __ldg(&DJ[I * n + J]);
-                kac[a * NC + c] += val * __ldg(&cl.Da[J * n + L]);
-                kad[a * ND + d] += val * __ldg(&cl.Da[J * n + K]);
-                kbc[b * NC + c] += val * __ldg(&cl.Da[I * n + L]);
-                kbd[b * ND + d] += val * __ldg(&cl.Da[I * n + K]);
+                kac[a * NC + c] += val * __ldg(&Da[J * n + L]);
+                kad[a * ND + d] += val * __ldg(&Da[J * n + K]);
+                kbc[b * NC + c] += val * __ldg(&Da[I * n + L]);
+                kbd[b * ND + d] += val * __ldg(&Da[I * n + K]);
                 if constexpr (kUhf) {
-                  kac2[a * NC + c] += val * __ldg(&cl.Db[J * n + L]);
-                  kad2[a * ND + d] += val * __ldg(&cl.Db[J * n + K]);
-                  kbc2[b * NC + c] += val * __ldg(&cl.Db[I * n + L]);
-                  kbd2[b * ND + d] += val * __ldg(&cl.Db[I * n + K]);
+                  kac2[a * NC + c] += val * __ldg(&Db[J * n + L]);
+                  kad2[a * ND + d] += val * __ldg(&Db[J * n + K]);
+                  kbc2[b * NC + c] += val * __ldg(&Db[I * n + L]);
+                  kbd2[b * ND + d] += val * __ldg(&Db[I * n + K]);
                 }
               }
 #pragma unroll U
         for (int c = 0; c < NC; ++c)
 #pragma unroll U
-          for (int d = 0; d < ND; ++d) atomicAdd(&cl.J[(aoc + c) * n + aod + d], jcd[c * ND + d]);
+          for (int d = 0; d < ND; ++d) atomicAdd(&Jm[(aoc + c) * n + aod + d], jcd[c * ND + d]);
 #pragma unroll U
         for (int a = 0; a < NA; ++a) {
 #pragma unroll U
-          for (int c = 0; c < NC; ++c) atomicAdd(&cl.Ka[(aoa + a) * n + aoc + c], kac[a * NC + c]);
+          for (int c = 0; c < NC; ++c) atomicAdd(&Kam[(aoa + a) * n + aoc + c], kac[a * NC + c]);
 #pragma unroll U
-          for (int d = 0; d < ND; ++d) atomicAdd(&cl.Ka[(aoa + a) * n + aod + d], kad[a * ND + d]);
+          for (int d = 0; d < ND; ++d) atomicAdd(&Kam[(aoa + a) * n + aod + d], kad[a * ND + d]);
         }
 #pragma unroll U
         for (int b = 0; b < NB; ++b) {
 #pragma unroll U
-          for (int c = 0; c < NC; ++c) atomicAdd(&cl.Ka[(aob + b) * n + aoc + c], kbc[b * NC + c]);
+          for (int c = 0; c < NC; ++c) atomicAdd(&Kam[(aob + b) * n + aoc + c], kbc[b * NC + c]);
 #pragma unroll U
-          for (int d = 0; d < ND; ++d) atomicAdd(&cl.Ka[(aob + b) * n + aod + d], kbd[b * ND + d]);
+          for (int d = 0; d < ND; ++d) atomicAdd(&Kam[(aob + b) * n + aod + d], kbd[b * ND + d]);
         }
         if constexpr (kUhf) {
 #pragma unroll U
           for (int a = 0; a < NA; ++a) {
 #pragma unroll U
-            for (int c = 0; c < NC; ++c) atomicAdd(&cl.Kb[(aoa + a) * n + aoc + c], kac2[a * NC + c]);
+            for (int c = 0; c < NC; ++c) atomicAdd(&Kbm[(aoa + a) * n + aoc + c], kac2[a * NC + c]);
 #pragma unroll U
-            for (int d = 0; d < ND; ++d) atomicAdd(&cl.Kb[(aoa + a) * n + aod + d], kad2[a * ND + d]);
+            for (int d = 0; d < ND; ++d) atomicAdd(&Kbm[(aoa + a) * n + aod + d], kad2[a * ND + d]);
           }
 #pragma unroll U
           for (int b = 0; b < NB; ++b) {
 #pragma unroll U
-            for (int c = 0; c < NC; ++c) atomicAdd(&cl.Kb[(aob + b) * n + aoc + c], kbc2[b * NC + c]);
+            for (int c = 0; c < NC; ++c) atomicAdd(&Kbm[(aob + b) * n + aoc + c], kbc2[b * NC + c]);
 #pragma unroll U
-            for (int d = 0; d < ND; ++d) atomicAdd(&cl.Kb[(aob + b) * n + aod + d], kbd2[b * ND + d]);
+            for (int d = 0; d < ND; ++d) atomicAdd(&Kbm[(aob + b) * n + aod + d], kbd2[b * ND + d]);
           }
         }
       }
@@ -461,7 +468,7 @@ __global__ void __launch_bounds__(32 * fused_warps(LA, LB, LC, LD), fused_min_bl
 #pragma unroll U
         for (int a = 0; a < NA; ++a)
 #pragma unroll U
-          for (int b = 0; b < NB; ++b) atomicAdd(&cl.J[(aoa + a) * n + aob + b], jab[a * NB + b]);
+          for (int b = 0; b < NB; ++b) atomicAdd(&Jm[(aoa + a) * n + aob + b], jab[a * NB + b]);
       }
     }
   }

@@ -115,14 +115,20 @@ __global__ void __launch_bounds__(kThreads) eri_hrr_digest_kernel(const EngineVi
     active = active && density_bound(v, bp, kp) >= cl.dens_threshold;
     if (!__any_sync(0xffffffffu, active)) return;
   }
-  const int n = v.nbf;
+  const MolView mv = task_molecule(v, bp);
+  if (mv.skip) return;  // block-uniform: one task per block
+  const int n = mv.n;
+  const double *Da = cl.Da + mv.base, *Db = cl.Db ? cl.Db + mv.base : nullptr;
+  const double *Dt = cl.Dt ? cl.Dt + mv.base : nullptr;
+  double *Jm = cl.J ? cl.J + mv.base : nullptr, *Kam = cl.Ka ? cl.Ka + mv.base : nullptr;
+  double *Kbm = cl.Kb ? cl.Kb + mv.base : nullptr;
   const double X0 = v.pair_AB[3 * bp], X1 = v.pair_AB[3 * bp + 1], X2 = v.pair_AB[3 * bp + 2];
   const double Y0 = v.pair_AB[3 * kp], Y1 = v.pair_AB[3 * kp + 1], Y2 = v.pair_AB[3 * kp + 2];
   const int aoa = v.pair_ao_a[bp], aob = v.pair_ao_b[bp], aoc = v.pair_ao_a[kp], aod = v.pair_ao_b[kp];
   const bool bdiag = v.pair_sa[bp] == v.pair_sb[bp], kdiag = v.pair_sa[kp] == v.pair_sb[kp];
   const bool same = bp == kp;
   const double s = (bdiag ? 0.5 : 1.0) * (kdiag ? 0.5 : 1.0) * (same ? 0.5 : 1.0);
-  const double *DJ = kUhf ? cl.Dt : cl.Da;
+  const double *DJ = kUhf ? Dt : Da;
 
   double jcd[kJk ? NCD : 1];
 #pragma unroll
@@ -207,40 +213,40 @@ __global__ void __launch_bounds__(kThreads) eri_hrr_digest_kernel(const EngineVi
             const double val = s * out[c * ND + d];
             jab += 2.0 * val * __ldg(&DJ[K * n + L]);
             jcd[c * ND + d] += dij * out[c * ND + d];
-            kac[c] += val * __ldg(&cl.Da[J * n + L]);
-            kad[d] += val * __ldg(&cl.Da[J * n + K]);
-            kbc[c] += val * __ldg(&cl.Da[I * n + L]);
-            kbd[d] += val * __ldg(&cl.Da[I * n + K]);
+            kac[c] += val * __ldg(&Da[J * n + L]);
+            kad[d] += val * __ldg(&Da[J * n + K]);
+            kbc[c] += val * __ldg(&Da[I * n + L]);
+            kbd[d] += val * __ldg(&Da[I * n + K]);
             if constexpr (kUhf) {
-              kac2[c] += val * __ldg(&cl.Db[J * n + L]);
-              kad2[d] += val * __ldg(&cl.Db[J * n + K]);
-              kbc2[c] += val * __ldg(&cl.Db[I * n + L]);
-              kbd2[d] += val * __ldg(&cl.Db[I * n + K]);
+              kac2[c] += val * __ldg(&Db[J * n + L]);
+              kad2[d] += val * __ldg(&Db[J * n + K]);
+              kbc2[c] += val * __ldg(&Db[I * n + L]);
+              kbd2[d] += val * __ldg(&Db[I * n + K]);
             }
           }
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-          atomicAdd(&cl.Ka[I * n + aoc + c], kac[c]);
-          atomicAdd(&cl.Ka[J * n + aoc + c], kbc[c]);
+          atomicAdd(&Kam[I * n + aoc + c], kac[c]);
+          atomicAdd(&Kam[J * n + aoc + c], kbc[c]);
           if constexpr (kUhf) {
-            atomicAdd(&cl.Kb[I * n + aoc + c], kac2[c]);
-            atomicAdd(&cl.Kb[J * n + aoc + c], kbc2[c]);
+            atomicAdd(&Kbm[I * n + aoc + c], kac2[c]);
+            atomicAdd(&Kbm[J * n + aoc + c], kbc2[c]);
           }
         }
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
-          atomicAdd(&cl.Ka[I * n + aod + d], kad[d]);
-          atomicAdd(&cl.Ka[J * n + aod + d], kbd[d]);
+          atomicAdd(&Kam[I * n + aod + d], kad[d]);
+          atomicAdd(&Kam[J * n + aod + d], kbd[d]);
           if constexpr (kUhf) {
-            atomicAdd(&cl.Kb[I * n + aod + d], kad2[d]);
-            atomicAdd(&cl.Kb[J * n + aod + d], kbd2[d]);
+            atomicAdd(&Kbm[I * n + aod + d], kad2[d]);
+            atomicAdd(&Kbm[J * n + aod + d], kbd2[d]);
           }
         }
       }
       // the warp's 32 quartets share the bra pair and this (a b) row
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) jab += __shfl_xor_sync(0xffffffffu, jab, o);
-      if (lane == 0) atomicAdd(&cl.J[I * n + J], jab);
+      if (lane == 0) atomicAdd(&Jm[I * n + J], jab);
     }
   }
 
@@ -255,7 +261,7 @@ __global__ void __launch_bounds__(kThreads) eri_hrr_digest_kernel(const EngineVi
 #pragma unroll
         for (int w = 0; w < kWarpsPerBlock; ++w) t += jcd_sh[(w * NCD + x) * 32 + lane];
         const int c = x / ND, d = x - c * ND;
-        atomicAdd(&cl.J[(aoc + c) * n + aod + d], t);
+        atomicAdd(&Jm[(aoc + c) * n + aod + d], t);
       }
     }
   }

@@ -89,7 +89,25 @@ struct EngineView {
   const double *boys_table;   // [kBoysGrid][kBoysOrders] F_m(T_i)
   int nbf;
   int reference_convention;   // 1: reproduce the reference's (dd|dd) ET rows
+  // batched contexts (many molecules, one launch per class); null otherwise
+  const int *pair_mol;             // molecule of each shell pair
+  const int *mol_nbf;              // basis functions per molecule
+  const long long *mol_off;        // offset of each molecule's n x n matrices
+  const unsigned char *mol_active; // 0: skip the molecule in this build
 };
+
+// The molecule a task belongs to (its bra pair's): its size, the offset of
+// its matrices in the batch buffers, and whether this build skips it.
+struct MolView {
+  int n;
+  long long base;
+  bool skip;
+};
+__device__ __forceinline__ MolView task_molecule(const EngineView &v, int bp) {
+  if (!v.pair_mol) return MolView{v.nbf, 0, false};
+  const int m = v.pair_mol[bp];
+  return MolView{v.mol_nbf[m], v.mol_off[m], v.mol_active != nullptr && v.mol_active[m] == 0};
+}
 
 // One unit of work: a bra pair position in the class's pair list and a
 // range of at most 32 ket positions (kets of one primitive-count bucket).

@@ -26,7 +26,8 @@ EXPORTED = ["hfg_default_opts", "hfg_last_error", "hfg_device_count", "hfg_ctx_c
             "hfg_fock_rhf", "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz",
             "hfg_ctx_stats", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak",
             "hfg_fock_rhf_noalloc", "hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental",
-            "hfg_set_shard"]
+            "hfg_set_shard", "hfg_batch_create", "hfg_batch_size", "hfg_batch_layout", "hfg_fock_rhf_batch_device",
+            "hfg_fock_uhf_batch_device"]
 
 
 class HfgError(RuntimeError):
@@ -96,6 +97,14 @@ def library(path: str = LIB_PATH):
     L.hfg_schwarz.argtypes = [vp, dp, i64]
     L.hfg_ctx_stats.argtypes = [vp, ctypes.POINTER(hfg_stats)]
     L.hfg_fock_rhf_noalloc.argtypes = [vp, dp, dp, vp]
+    L.hfg_batch_create.argtypes = [ctypes.POINTER(hfg_shells), i32, ctypes.POINTER(hfg_opts), ctypes.POINTER(vp)]
+    L.hfg_batch_size.argtypes = [vp]
+    L.hfg_batch_size.restype = i32
+    L.hfg_batch_layout.argtypes = [vp, vp, vp, ctypes.POINTER(i64)]
+    L.hfg_fock_rhf_batch_device.argtypes = [vp, dp, dp, vp, vp]
+    L.hfg_fock_uhf_batch_device.argtypes = [vp, dp, dp, dp, dp, vp, vp]
+    for name in ("hfg_batch_create", "hfg_batch_layout", "hfg_fock_rhf_batch_device", "hfg_fock_uhf_batch_device"):
+        getattr(L, name).restype = ctypes.c_int
     L.hfg_fock_rhf_noalloc.restype = ctypes.c_int
     L.hfg_set_profiling.argtypes = [vp, i32]
     L.hfg_class_profile.argtypes = [vp, ctypes.POINTER(hfg_class_time), i32, ctypes.POINTER(i32)]
@@ -255,6 +264,80 @@ class Engine:
         n = ctypes.c_int32()
         _check(library().hfg_class_profile(self._h, arr, 64, ctypes.byref(n)))
         return [{k: getattr(arr[i], k) for k, _ in hfg_class_time._fields_} for i in range(n.value)]
+
+    def stats(self) -> dict:
+        s = hfg_stats()
+        _check(library().hfg_ctx_stats(self._h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in hfg_stats._fields_ if k != "reserved"}
+
+
+class BatchEngine:
+    """Many independent molecules in one context (hfg_batch_create): every
+    direct build is one launch per quartet class over all molecules' tasks.
+    Matrices are flat float64 CUDA tensors in the batch layout (molecule m's
+    nbf[m] x nbf[m] block at offset[m])."""
+
+    def __init__(self, molecules, schwarz_threshold: float = 1e-12, eri_convention: int = ERI_REFERENCE,
+                 device: int = 0):
+        """molecules: sequence of (Z, xyz_bohr, basis)."""
+        self.tables = [shell_table(Z, xyz, basis) for Z, xyz, basis in molecules]
+        self._keep = []
+        arr = (hfg_shells * len(self.tables))()
+        for i, t in enumerate(self.tables):
+            keep = [np.ascontiguousarray(x) for x in (t.center.ravel(), t.L, t.nprim, t.prim_offset, t.ao_offset,
+                                                      t.exponent, t.coefficient)]
+            self._keep.append(keep)
+            arr[i] = hfg_shells(len(t.L), *[_ptr(x) for x in keep], t.nbf)
+        o = default_opts()
+        o.schwarz_threshold = schwarz_threshold
+        o.eri_convention = eri_convention
+        o.device = device
+        h = ctypes.c_void_p()
+        _check(library().hfg_batch_create(arr, len(self.tables), ctypes.byref(o), ctypes.byref(h)))
+        self._h = h
+        self.nmol = len(self.tables)
+        self.nbf = np.zeros(self.nmol, dtype=np.int32)
+        self.offset = np.zeros(self.nmol, dtype=np.int64)
+        total = ctypes.c_int64()
+        _check(library().hfg_batch_layout(self._h, _ptr(self.nbf), _ptr(self.offset), ctypes.byref(total)))
+        self.total = total.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().hfg_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _active(self, active):
+        if active is None:
+            return None, None
+        a = np.ascontiguousarray(np.asarray(active, dtype=np.uint8))
+        assert a.size == self.nmol
+        return a, _ptr(a)
+
+    def fock_rhf(self, P, G, active=None):
+        """G blocks of the active molecules from the P blocks (flat CUDA
+        float64 tensors of `total` elements), on torch's current stream."""
+        import torch
+        keep, ap = self._active(active)
+        _check(library().hfg_fock_rhf_batch_device(self._h, ctypes.c_void_p(P.data_ptr()),
+                                                   ctypes.c_void_p(G.data_ptr()), ap,
+                                                   ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        return G
+
+    def fock_uhf(self, Pa, Pb, Ga, Gb, active=None):
+        import torch
+        keep, ap = self._active(active)
+        _check(library().hfg_fock_uhf_batch_device(self._h, ctypes.c_void_p(Pa.data_ptr()),
+                                                   ctypes.c_void_p(Pb.data_ptr()), ctypes.c_void_p(Ga.data_ptr()),
+                                                   ctypes.c_void_p(Gb.data_ptr()), ap,
+                                                   ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        return Ga, Gb
 
     def stats(self) -> dict:
         s = hfg_stats()

@@ -171,6 +171,24 @@ hfg_status hfg_set_incremental(hfg_ctx *ctx, int32_t on);
  * hfg_fock_rhf_noalloc are not sharded.  Default (0, 1). */
 hfg_status hfg_set_shard(hfg_ctx *ctx, int32_t rank, int32_t count);
 
+/* Batched contexts (many independent molecules; no reference counterpart:
+ * the reference runs one molecule per algorithm object).  hfg_batch_create
+ * takes one hfg_shells per molecule (AO offsets local to the molecule) and
+ * builds shell pairs and quartets within each molecule only; every direct
+ * build then runs one launch per quartet class over the tasks of all
+ * molecules.  Matrices of the batch live in flat device buffers, molecule m's
+ * nbf[m] x nbf[m] row-major block at offset[m] (hfg_batch_layout; `total`
+ * doubles in all).  `active` (host, one byte per molecule, or NULL = all)
+ * selects the molecules a build serves; the G blocks of the others are left
+ * untouched.  Plain FP64 form only; sharding applies.  The single-molecule
+ * entry points reject batched contexts. */
+hfg_status hfg_batch_create(const hfg_shells *mols, int32_t nmol, const hfg_opts *opts, hfg_ctx **out);
+int32_t hfg_batch_size(const hfg_ctx *ctx);
+hfg_status hfg_batch_layout(const hfg_ctx *ctx, int32_t *nbf, int64_t *offset, int64_t *total);
+hfg_status hfg_fock_rhf_batch_device(hfg_ctx *ctx, const double *dP, double *dG, const uint8_t *active, void *stream);
+hfg_status hfg_fock_uhf_batch_device(hfg_ctx *ctx, const double *dPa, const double *dPb, double *dGa, double *dGb,
+                                     const uint8_t *active, void *stream);
+
 /* Allocation-free variant of hfg_fock_rhf_device, for callers that must not
  * allocate device memory while they run: a serving loop under a fixed HBM
  * budget, code that cannot afford the implicit synchronisation of

@@ -1,0 +1,83 @@
+"""Batched contexts and the batched SCF: one launch per quartet class over
+many molecules of uneven size gives every molecule the G (and the converged
+energy) it gets alone."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_golden
+from hartreefock_b200 import batch
+from hartreefock_b200 import engine as E
+from hartreefock_b200 import molecules, scf
+
+pytestmark = pytest.mark.gpu
+
+
+def _mix():
+    g = load_golden("h2o_sto3g")
+    out = [dict(Z=list(g["Z"]), xyz=g["xyz"], basis="sto-3g")]
+    for k, basis in ((1, "6-31g*"), (2, "6-31g"), (3, "sto-3g")):
+        Z, xyz = molecules.water_cluster(k, seed=k)
+        out.append(dict(Z=list(Z), xyz=xyz, basis=basis))
+    for nc, basis in ((1, "sto-3g"), (3, "6-31g")):
+        Z, xyz = molecules.alkane(nc)
+        out.append(dict(Z=list(Z), xyz=xyz, basis=basis))
+    return out
+
+
+def _density(n, seed):
+    rng = np.random.default_rng(seed)
+    Q, _ = np.linalg.qr(rng.normal(size=(n, max(1, n // 4))))
+    return 2.0 * Q @ Q.T
+
+
+def test_batched_fock_equals_single_molecule_builds():
+    mols = _mix()
+    be = E.BatchEngine([(m["Z"], m["xyz"], m["basis"]) for m in mols])
+    flatP = np.zeros(be.total)
+    want = []
+    for i, m in enumerate(mols):
+        n = int(be.nbf[i])
+        P = _density(n, i)
+        flatP[be.offset[i]: be.offset[i] + n * n] = P.ravel()
+        want.append(E.Engine(m["Z"], m["xyz"], m["basis"]).fock_rhf(P))
+    dP = torch.from_numpy(flatP).cuda()
+    dG = torch.full_like(dP, 7.0)
+    active = np.ones(len(mols), dtype=np.uint8)
+    active[2] = 0
+    be.fock_rhf(dP, dG, active=active)
+    G = dG.cpu().numpy()
+    for i, w in enumerate(want):
+        n = int(be.nbf[i])
+        got = G[be.offset[i]: be.offset[i] + n * n].reshape(n, n)
+        if i == 2:
+            assert np.all(got == 7.0)  # inactive: left untouched
+        else:
+            assert np.abs(got - w).max() < 1e-11 * max(1.0, np.abs(w).max()), i
+
+
+def test_batched_scf_matches_single_molecule_scf():
+    mols = _mix()
+    kw = dict(alpha=0.75, init_guess=0.75)
+    bs = batch.BatchSCF(mols, **kw)
+    energies = bs.run()
+    assert bs.converged.all()
+    for i, m in enumerate(mols):
+        ref = scf.run_scf(m["Z"], m["xyz"], m["basis"], post_diis=0, **kw)
+        assert abs(energies[i] - ref["energy"]) < 1e-8, (i, energies[i], ref["energy"])
+
+
+def test_batched_uhf_scf_matches_single_molecule_scf():
+    mols = []
+    for basis in ("sto-3g", "6-31g"):
+        Z, xyz = molecules.hydroxyl()
+        mols.append(dict(Z=list(Z), xyz=xyz, basis=basis))
+        Z, xyz = molecules.methyl_planar()
+        mols.append(dict(Z=list(Z), xyz=xyz, basis=basis))
+    kw = dict(alpha=0.5, init_guess=0.0)
+    bs = batch.BatchSCF(mols, unrestricted=True, max_iter=1000, **kw)
+    energies = bs.run()
+    assert bs.converged.all()
+    for i, m in enumerate(mols):
+        ref = scf.run_scf(m["Z"], m["xyz"], m["basis"], unrestricted=True, post_diis=0, **kw)
+        assert abs(energies[i] - ref["energy"]) < 1e-6, (i, energies[i], ref["energy"])
