@@ -13,6 +13,8 @@ occupied.  All FP64.
 """
 from __future__ import annotations
 
+import time
+
 import numpy as np
 import torch
 
@@ -81,6 +83,11 @@ class BatchSCF:
         self.V = 0.5 * (V + V.transpose(1, 2)) * mask2
         self.mask2 = mask2
         self.shift = torch.diag_embed((~valid).double() * PAD_SHIFT)
+        # eigensolver buckets: molecules grouped by nbf rounded up to 8, so
+        # each batched solve runs at its own size instead of the largest
+        size = np.minimum(((self.nbf + 7) // 8) * 8, n)
+        self.buckets = [(int(b), np.nonzero(size == b)[0]) for b in np.unique(size)]
+        self.seconds = {"fock": 0.0, "diis": 0.0, "eigh": 0.0, "total": 0.0}
 
     # ---- flat <-> padded
     def to_flat(self, X):
@@ -102,6 +109,23 @@ class BatchSCF:
             F = h.clone()
         return F
 
+    def _eigh(self, Ft, active_np):
+        """Batched eigensolve of the active molecules, bucket by bucket
+        (hfg_eigh_batched); levels of padded rows and of inactive molecules
+        stay at PAD_SHIFT with unit vectors."""
+        M, n = self.M, self.nmax
+        w = torch.full((M, n), PAD_SHIFT, dtype=torch.float64, device=self.dev)
+        U = torch.eye(n, dtype=torch.float64, device=self.dev).expand(M, n, n).clone()
+        for b, idx in self.buckets:
+            sel = idx[active_np[idx] != 0]
+            if len(sel) == 0:
+                continue
+            t = torch.from_numpy(sel).to(self.dev)
+            wb, Ub = E.eigh_batched(Ft[t, :b, :b].contiguous())
+            w[t, :b] = wb
+            U[t, :b, :b] = Ub
+        return w, U
+
     def _occ_mask(self, spin):
         return (torch.arange(self.nmax, device=self.dev)[None, :] <
                 torch.from_numpy(self.nocc[spin]).to(self.dev)[:, None]).double()
@@ -118,8 +142,16 @@ class BatchSCF:
         iters = torch.zeros(M, dtype=torch.int64, device=dev)
         flatG = [torch.zeros(self.eng.total, dtype=torch.float64, device=dev) for _ in range(nspin)]
         builds = 0
+        sync = torch.cuda.synchronize if self.dev.type == "cuda" else (lambda: None)
+
+        def tick():
+            sync()
+            return time.perf_counter()
+
+        t_start = tick()
         for it in range(self.max_iter):
             act = active.clone()
+            active_np = act.cpu().numpy().astype(np.uint8)
             if it == 0:
                 F0 = self._guess_fock()
                 F = [F0.clone() for _ in range(nspin)]
@@ -127,18 +159,20 @@ class BatchSCF:
                     F[0][:, 0, 1] += 0.1
                     F[0][:, 1, 0] = F[0][:, 0, 1]
             else:
+                t0 = tick()
                 flatP = [self.to_flat(p) for p in P]
-                active_np = act.cpu().numpy().astype(np.uint8)
                 if self.uhf:
                     self.eng.fock_uhf(flatP[0], flatP[1], flatG[0], flatG[1], active=active_np)
                 else:
                     self.eng.fock_rhf(flatP[0], flatG[0], active=active_np)
                 builds += 1
                 F = [self.h + self.to_pad(g) for g in flatG]
+                self.seconds["fock"] += tick() - t0
             if not self.uhf:
                 F = [0.5 * (f + f.transpose(1, 2)) for f in F]
             used = torch.zeros(M, dtype=torch.bool, device=dev)
             err_est = torch.zeros(M, dtype=torch.float64, device=dev)
+            t0 = tick()
             if self.use_diis and it > 0:
                 for s in range(nspin):
                     err = self.S @ P[s] @ F[s] - F[s] @ P[s] @ self.S
@@ -151,10 +185,14 @@ class BatchSCF:
                         F[s], est = _diis_extrapolate(diisF[s], diisE[s])
                         err_est = err_est + est
                         used[:] = True
+            t1 = tick()
+            self.seconds["diis"] += t1 - t0
             Pn, eps = [], []
             for s in range(nspin):
                 Ft = self.V @ F[s] @ self.V + self.shift
-                w, Cp = torch.linalg.eigh(Ft)
+                w, Cp = self._eigh(Ft, active_np)
+                self.seconds["eigh"] += tick() - t1
+                t1 = tick()
                 C = self.V @ Cp
                 occ = self._occ_mask(s)
                 factor = 1.0 if self.uhf else 2.0
@@ -179,6 +217,7 @@ class BatchSCF:
             active = act & ~conv
             if not bool(active.any()):
                 break
+        self.seconds["total"] = tick() - t_start
         self.iterations = iters.cpu().numpy()
         self.converged = (~active).cpu().numpy()
         self.builds = builds
@@ -198,9 +237,10 @@ def _diis_extrapolate(Fs, Es):
     Bb[:, :m, :m] = B
     Bb[:, m, :m] = 1
     Bb[:, :m, m] = 1
-    rhs = torch.zeros(M, m + 1, 1, dtype=B.dtype, device=B.device)
-    rhs[:, m, 0] = 1
-    c = torch.linalg.lstsq(Bb, rhs).solution[:, :m, 0] if Bb.device.type == "cpu" else torch.linalg.solve(Bb, rhs)[:, :m, 0]
+    # the (m+1)^2 systems are tiny and turn rank-deficient near convergence:
+    # solved on the host by the SCF's own column-pivoted QR (DIIS.h:72),
+    # which also decides the reference's extrapolation there
+    c = torch.from_numpy(scf.pulay_solve(Bb.cpu().numpy())[:, :m]).to(B.device)
     F = torch.einsum("ai,aikl->akl", c, torch.stack(Fs, 1))
     est = torch.sqrt(torch.diagonal(B, dim1=1, dim2=2)[:, -2:].sum(1))
     return F, est

@@ -24,6 +24,9 @@ static hfg_status fail(hfg_status st, const std::string &msg) {
   return st;
 }
 
+// for entry points defined in other translation units (hfg_eigh_batched)
+hfg_status fail_external(hfg_status st, const std::string &msg) { return fail(st, msg); }
+
 #define HFG_CUDA(call)                                                                        \
   do {                                                                                        \
     cudaError_t err__ = (call);                                                               \

@@ -1166,6 +1166,19 @@ extern "C" {
 
 const char *hfd_last_error(void) { return g_driver_error.c_str(); }
 
+hfg_status hfd_pulay_solve(const double *B, int32_t m1, int32_t batch, double *c) {
+  if (!B || !c || m1 < 2 || batch < 0) return HFG_INVALID_ARG;
+  const size_t mm = (size_t)m1 * m1;
+  std::vector<double> rhs(m1, 0.0);
+  rhs[m1 - 1] = 1.0;
+  for (int b = 0; b < batch; ++b) {
+    const std::vector<double> x =
+        hfgpu::detail::pulay_solve(std::vector<double>(B + b * mm, B + (b + 1) * mm), m1, rhs);
+    std::copy(x.begin(), x.end(), c + (size_t)b * m1);
+  }
+  return HFG_OK;
+}
+
 void hfd_default_scf_opts(hfd_scf_opts *o) {
   if (!o) return;
   std::memset(o, 0, sizeof *o);

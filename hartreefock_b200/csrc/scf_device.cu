@@ -18,6 +18,7 @@
 #include <string>
 #include <vector>
 
+#include "../../include/hfgpu.h"
 #include "scf_device.h"
 
 namespace hfgpu {
@@ -281,3 +282,90 @@ void DeviceScf::CopyOut(int spin, double *P, double *C) {
 
 }  // namespace detail
 }  // namespace hfgpu
+
+// ---------------------------------------------------------------------------
+// hfg_eigh_batched (include/hfgpu.h): eigen-decomposition of a stack of small
+// symmetric matrices in one cuSOLVER batched Jacobi call, for the batched
+// SCF's F' = V F V step.  Handle and workspace are kept per host thread and
+// grown on demand.
+namespace {
+struct BatchedEigh {
+  cusolverDnHandle_t handle = nullptr;
+  cusolverDnParams_t params = nullptr;
+  int device = -1;
+  void *dwork = nullptr;
+  size_t dbytes = 0;
+  std::vector<char> hwork;
+  int *info = nullptr;
+  int64_t info_cap = 0;
+  ~BatchedEigh() {
+    if (dwork) cudaFree(dwork);
+    if (info) cudaFree(info);
+    if (params) cusolverDnDestroyParams(params);
+    if (handle) cusolverDnDestroy(handle);
+  }
+};
+thread_local BatchedEigh g_eigh;
+}  // namespace
+
+namespace hfg {
+hfg_status fail_external(hfg_status st, const std::string &msg);
+}
+
+extern "C" hfg_status hfg_eigh_batched(const double *dA, double *dV, double *dW, int32_t n, int32_t batch,
+                                       void *stream) {
+  using hfgpu::detail::ck;
+  if (!dA || !dV || !dW || n < 1 || batch < 1) return hfg::fail_external(HFG_INVALID_ARG, "hfg_eigh_batched: arguments");
+  try {
+    BatchedEigh &e = g_eigh;
+    int dev = 0;
+    ck(cudaGetDevice(&dev), "cudaGetDevice");
+    if (e.handle && e.device != dev) {
+      cusolverDnDestroyParams(e.params);
+      cusolverDnDestroy(e.handle);
+      if (e.dwork) cudaFree(e.dwork);
+      if (e.info) cudaFree(e.info);
+      e.handle = nullptr;
+      e.params = nullptr;
+      e.dwork = nullptr;
+      e.info = nullptr;
+      e.dbytes = 0;
+      e.info_cap = 0;
+    }
+    if (!e.handle) {
+      ck(cusolverDnCreate(&e.handle), "cusolverDnCreate");
+      ck(cusolverDnCreateParams(&e.params), "cusolverDnCreateParams");
+      e.device = dev;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    ck(cusolverDnSetStream(e.handle, s), "cusolverDnSetStream");
+    const size_t bytes = (size_t)n * n * batch * sizeof(double);
+    if (dV != dA) ck(cudaMemcpyAsync(dV, dA, bytes, cudaMemcpyDeviceToDevice, s), "copy A");
+    size_t dneed = 0, hneed = 0;
+    ck(cusolverDnXsyevBatched_bufferSize(e.handle, e.params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n,
+                                         CUDA_R_64F, dV, n, CUDA_R_64F, dW, CUDA_R_64F, &dneed, &hneed, batch),
+       "cusolverDnXsyevBatched_bufferSize");
+    if (dneed > e.dbytes) {
+      ck(cudaStreamSynchronize(s), "sync");
+      if (e.dwork) cudaFree(e.dwork);
+      e.dwork = nullptr;
+      ck(cudaMalloc(&e.dwork, dneed), "cudaMalloc eigh workspace");
+      e.dbytes = dneed;
+    }
+    if (hneed > e.hwork.size()) e.hwork.resize(hneed);
+    if (batch > e.info_cap) {
+      ck(cudaStreamSynchronize(s), "sync");
+      if (e.info) cudaFree(e.info);
+      e.info = nullptr;
+      ck(cudaMalloc(&e.info, sizeof(int) * batch), "cudaMalloc eigh info");
+      e.info_cap = batch;
+    }
+    ck(cusolverDnXsyevBatched(e.handle, e.params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, CUDA_R_64F, dV,
+                              n, CUDA_R_64F, dW, CUDA_R_64F, e.dwork, e.dbytes,
+                              e.hwork.empty() ? nullptr : e.hwork.data(), hneed, e.info, batch),
+       "cusolverDnXsyevBatched");
+    return HFG_OK;
+  } catch (const std::exception &ex) {
+    return hfg::fail_external(HFG_DEVICE_ERROR, ex.what());
+  }
+}

@@ -27,7 +27,7 @@ EXPORTED = ["hfg_default_opts", "hfg_last_error", "hfg_device_count", "hfg_ctx_c
             "hfg_ctx_stats", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak",
             "hfg_fock_rhf_noalloc", "hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental",
             "hfg_set_shard", "hfg_batch_create", "hfg_batch_size", "hfg_batch_layout", "hfg_fock_rhf_batch_device",
-            "hfg_fock_uhf_batch_device"]
+            "hfg_fock_uhf_batch_device", "hfg_eigh_batched"]
 
 
 class HfgError(RuntimeError):
@@ -113,6 +113,8 @@ def library(path: str = LIB_PATH):
     L.hfg_set_mixed_cutoff.argtypes = [vp, ctypes.c_double]
     L.hfg_set_incremental.argtypes = [vp, i32]
     L.hfg_set_shard.argtypes = [vp, i32, i32]
+    L.hfg_eigh_batched.argtypes = [dp, dp, dp, i32, i32, vp]
+    L.hfg_eigh_batched.restype = ctypes.c_int
     for name in ("hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental", "hfg_set_shard", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak", "hfg_ctx_create", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet", "hfg_fock_rhf",
                  "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz", "hfg_ctx_stats"):
         getattr(L, name).restype = ctypes.c_int
@@ -133,6 +135,24 @@ def measure_fp64_peak(device: int = 0) -> float:
     v = ctypes.c_double()
     _check(library().hfg_measure_fp64_peak(device, ctypes.byref(v)))
     return v.value
+
+
+def eigh_batched(A):
+    """Eigenvalues (ascending) and eigenvectors of a stack of symmetric
+    matrices, a contiguous float64 CUDA tensor [batch, n, n], by one batched
+    cuSOLVER call (hfg_eigh_batched) on torch's current stream.  Returns
+    (w [batch, n], U [batch, n, n]) with A = U diag(w) U^T, as
+    torch.linalg.eigh does."""
+    import torch
+    assert A.is_cuda and A.dtype == torch.float64 and A.dim() == 3 and A.shape[1] == A.shape[2]
+    A = A.contiguous()
+    b, n, _ = A.shape
+    X = torch.empty_like(A)
+    w = torch.empty(b, n, dtype=torch.float64, device=A.device)
+    _check(library().hfg_eigh_batched(ctypes.c_void_p(A.data_ptr()), ctypes.c_void_p(X.data_ptr()),
+                                      ctypes.c_void_p(w.data_ptr()), n, b,
+                                      ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    return w, X.transpose(1, 2)
 
 
 def default_opts() -> hfg_opts:

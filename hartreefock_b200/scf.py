@@ -36,7 +36,7 @@ class hfd_scf_result(ctypes.Structure):
                 ("seconds_init", ctypes.c_double)]
 
 
-DRIVER_SYMBOLS = ["hfd_default_scf_opts", "hfd_last_error", "hfd_scf", "hfd_one_electron"]
+DRIVER_SYMBOLS = ["hfd_default_scf_opts", "hfd_last_error", "hfd_scf", "hfd_one_electron", "hfd_pulay_solve"]
 
 
 def _lib():
@@ -53,6 +53,8 @@ def _lib():
                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                        ctypes.POINTER(ctypes.c_int32)]
         L.hfd_one_electron.restype = ctypes.c_int
+        L.hfd_pulay_solve.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]
+        L.hfd_pulay_solve.restype = ctypes.c_int
         L._hfd_ready = True
     return L
 
@@ -122,3 +124,16 @@ def one_electron(Z, xyz, basis: str):
         raise E.HfgError(st, L.hfd_last_error().decode())
     k = n.value
     return S[:k * k].reshape(k, k).copy(), h[:k * k].reshape(k, k).copy()
+
+
+def pulay_solve(B: np.ndarray) -> np.ndarray:
+    """Solutions c of B c = (0, ..., 0, 1) for a stack of bordered Pulay
+    matrices [batch, m+1, m+1] (hfd_pulay_solve: the SCF's own QR)."""
+    L = _lib()
+    B = np.ascontiguousarray(B, dtype=np.float64)
+    b, m1, _ = B.shape
+    c = np.empty((b, m1))
+    st = L.hfd_pulay_solve(B.ctypes.data_as(ctypes.c_void_p), m1, b, c.ctypes.data_as(ctypes.c_void_p))
+    if st != 0:
+        raise E.HfgError(st, "hfd_pulay_solve")
+    return c

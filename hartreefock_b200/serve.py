@@ -1,0 +1,261 @@
+"""Request loop for RHF/UHF jobs: continuous admission against an HBM budget.
+
+Jobs arrive at any time (Server.submit).  Each job is one SCF run through
+the driver (hfd_scf: RestrictedHartreeFock / UnrestrictedHartreeFock Init +
+Calculate over the direct GPU Fock builds), so its engine context (shell
+pairs, Schwarz and screening tables, quartet task lists) and its density,
+Fock matrix and DIIS history stay resident in HBM for the life of the job,
+on the job's own CUDA stream.  A fixed number of slots (worker threads; the
+driver call releases the GIL) run jobs at the same time, so the kernels of
+different jobs overlap on the device.  Jobs are admitted in arrival order as
+soon as a slot is free and the job's estimated device footprint fits in what
+is left of the budget; a job larger than the whole budget is refused with
+HFG_OOM_BUDGET.  Latency = completion time - submit time.
+
+The reference runs one algorithm object per std::thread with no shared
+state (HartreeFockDoc.cpp:372-405); a slot here is that thread, with the
+device as the shared resource the budget guards.
+
+draw_jobs() and poisson_stream() make and replay the synthetic request
+stream: 80% RHF water clusters / alkanes with sizes log-uniform over a
+function-count range, 20% UHF doublets (OH, planar CH3), bases drawn
+uniformly from 6-31G, 6-31G*, 6-31+G** (Cartesian).
+"""
+from __future__ import annotations
+
+import collections
+import math
+import threading
+import time
+
+import numpy as np
+
+from . import molecules
+from .basis_io import shell_table
+
+HFG_OOM_BUDGET = 3
+SERVE_BASES = ("6-31g", "6-31g*", "6-31+g**")
+
+
+def footprint_bytes(Z, xyz, basis: str, unrestricted: bool = False) -> int:
+    """Estimated device bytes of one job: quartet task lists (12 B per task
+    of up to 32 ket pairs over the triangle of shell pairs), primitive-pair
+    tables (96 B FP64 + 48 B FP32 per primitive pair), and the SCF's n x n
+    FP64 matrices (h, S, V, F, P, new P, C, G, work, 2 x 6 DIIS entries, the
+    incremental history; about 32 per spin), plus a fixed 16 MiB for the
+    Boys table, counters and library handles."""
+    t = shell_table(Z, xyz, basis)
+    ns = len(t.L)
+    pairs = ns * (ns + 1) // 2
+    prim_pairs = int(np.sum(np.triu(np.outer(t.nprim, t.nprim))))
+    tasks = pairs * (pairs + 1) // 2 // 32 + pairs
+    spins = 2 if unrestricted else 1
+    return int(12 * tasks + 144 * prim_pairs + 8 * t.nbf * t.nbf * 32 * spins + (16 << 20))
+
+
+class Job:
+    """One request; wait() blocks until it has finished."""
+
+    def __init__(self, jid, Z, xyz, basis, unrestricted, kwargs):
+        self.id, self.Z, self.xyz, self.basis = jid, list(Z), np.asarray(xyz, dtype=np.float64), basis
+        self.unrestricted, self.kwargs = unrestricted, dict(kwargs)
+        self.bytes = footprint_bytes(self.Z, self.xyz, basis, unrestricted)
+        self.t_submit = self.t_start = self.t_end = None
+        self.result, self.error = None, None
+        self._done = threading.Event()
+
+    def wait(self, timeout=None):
+        if not self._done.wait(timeout):
+            raise TimeoutError(f"job {self.id} still running")
+        if self.error is not None:
+            raise self.error
+        return self.result
+
+    @property
+    def latency(self) -> float:
+        return self.t_end - self.t_submit
+
+    @property
+    def done(self) -> bool:
+        return self._done.is_set()
+
+
+def _driver_runner(job: Job):
+    from . import scf
+    return scf.run_scf(job.Z, job.xyz, job.basis, unrestricted=job.unrestricted, want_density=False, **job.kwargs)
+
+
+class Server:
+    """slots: jobs on the device at once.  hbm_budget: bytes the admitted
+    jobs' footprints may add up to.  mixed: precision form of the Fock
+    builds (FP32 below mixed_cutoff, incremental, FP64 finish) for every
+    job; otherwise the plain FP64 form.  scf_kwargs go to every job's SCF
+    (scf.run_scf keywords); post_diis defaults to 0 here, the reference's
+    convergence test alone.  runner(job) -> result replaces the driver call
+    (host-side tests)."""
+
+    def __init__(self, slots: int = 8, hbm_budget: int = 32 << 30, mixed: bool = True, mixed_cutoff: float = 1e-4,
+                 scf_kwargs=None, runner=None):
+        if slots < 1 or hbm_budget <= 0:
+            raise ValueError("slots >= 1 and a positive budget are required")
+        self.slots, self.budget = slots, int(hbm_budget)
+        self.defaults = dict(post_diis=0)
+        if mixed:
+            self.defaults["mixed_cutoff"] = mixed_cutoff
+        self.defaults.update(scf_kwargs or {})
+        self.runner = runner or _driver_runner
+        self._cv = threading.Condition()
+        self._queue = collections.deque()
+        self._in_use = 0
+        self._running = 0
+        self._next_id = 0
+        self._closing = False
+        self.peak_bytes = 0
+        self.peak_running = 0
+        self.finished = []
+        self._workers = [threading.Thread(target=self._work, name=f"hfg-slot-{i}", daemon=True) for i in range(slots)]
+        for w in self._workers:
+            w.start()
+
+    def submit(self, Z, xyz, basis: str, unrestricted: bool = False, **kwargs) -> Job:
+        kw = dict(self.defaults)
+        kw.update(kwargs)
+        with self._cv:
+            if self._closing:
+                raise RuntimeError("server is closed")
+            job = Job(self._next_id, Z, xyz, basis, unrestricted, kw)
+            self._next_id += 1
+            job.t_submit = time.perf_counter()
+            if job.bytes > self.budget:
+                from .engine import HfgError
+                job.error = HfgError(HFG_OOM_BUDGET, f"job needs ~{job.bytes} B, budget {self.budget} B")
+                job.t_start = job.t_end = job.t_submit
+                job._done.set()
+                return job
+            self._queue.append(job)
+            self._cv.notify_all()
+        return job
+
+    def _admit(self):
+        """Head of the queue if it fits (caller holds the lock)."""
+        if self._queue and self._in_use + self._queue[0].bytes <= self.budget:
+            job = self._queue.popleft()
+            self._in_use += job.bytes
+            self._running += 1
+            self.peak_bytes = max(self.peak_bytes, self._in_use)
+            self.peak_running = max(self.peak_running, self._running)
+            return job
+        return None
+
+    def _work(self):
+        while True:
+            with self._cv:
+                job = self._admit()
+                while job is None:
+                    if self._closing and not self._queue:
+                        return
+                    self._cv.wait()
+                    job = self._admit()
+            job.t_start = time.perf_counter()
+            try:
+                job.result = self.runner(job)
+            except Exception as e:  # reported through Job.wait
+                job.error = e
+            job.t_end = time.perf_counter()
+            with self._cv:
+                self._in_use -= job.bytes
+                self._running -= 1
+                self.finished.append(job)
+                self._cv.notify_all()
+            job._done.set()
+
+    def drain(self, timeout=None):
+        """Wait until every submitted job has finished."""
+        deadline = None if timeout is None else time.monotonic() + timeout
+        with self._cv:
+            while self._queue or self._running:
+                left = None if deadline is None else deadline - time.monotonic()
+                if left is not None and left <= 0:
+                    raise TimeoutError("jobs still queued or running")
+                self._cv.wait(left)
+
+    def close(self):
+        with self._cv:
+            self._closing = True
+            self._cv.notify_all()
+        for w in self._workers:
+            w.join()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+# ---------------------------------------------------------------------------
+# synthetic request stream
+
+def _functions_per_atom(basis: str) -> dict:
+    return {z: shell_table([z], np.zeros((1, 3)), basis).nbf for z in (1, 6, 8)}
+
+
+def _rhf_molecule(target: float, basis: str, rng, fpa):
+    """Water cluster or alkane whose function count is nearest the target."""
+    water = fpa[8] + 2 * fpa[1]
+    if rng.random() < 0.5:
+        k = max(1, int(round(target / water)))
+        Z, xyz = molecules.water_cluster(k, seed=int(rng.integers(0, 1 << 30)))
+    else:
+        per_c, base = fpa[6] + 2 * fpa[1], 2 * fpa[1]
+        n = max(1, int(round((target - base) / per_c)))
+        Z, xyz = molecules.alkane(n)
+    return list(Z), xyz
+
+
+def draw_jobs(count: int, seed: int = 0, nbf_range=(5, 600), uhf_fraction: float = 0.2, bases=SERVE_BASES):
+    """[(Z, xyz, basis, unrestricted)]: RHF sizes log-uniform over nbf_range
+    (realised as the nearest water cluster or alkane), UHF OH / planar CH3."""
+    rng = np.random.default_rng(seed)
+    fpa = {b: _functions_per_atom(b) for b in bases}
+    lo, hi = math.log(nbf_range[0]), math.log(nbf_range[1])
+    out = []
+    for _ in range(count):
+        basis = bases[int(rng.integers(0, len(bases)))]
+        if rng.random() < uhf_fraction:
+            Z, xyz = molecules.hydroxyl() if rng.random() < 0.5 else molecules.methyl_planar()
+            out.append((list(Z), xyz, basis, True))
+        else:
+            Z, xyz = _rhf_molecule(math.exp(rng.uniform(lo, hi)), basis, rng, fpa[basis])
+            out.append((Z, xyz, basis, False))
+    return out
+
+
+UHF_KW = dict(alpha=0.5, init_guess=0.0)
+RHF_KW = dict(alpha=0.75, init_guess=0.75)
+
+
+def poisson_stream(server: Server, jobs, rate: float, seed: int = 0, timeout=None):
+    """Submit `jobs` with exponential inter-arrival times of mean 1/rate
+    seconds (rate in jobs/s; rate <= 0 submits all at once), wait for all,
+    and return (job objects, summary dict)."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, size=len(jobs)) if rate > 0 else np.zeros(len(jobs))
+    handles = []
+    t0 = time.perf_counter()
+    t_next = t0
+    for (Z, xyz, basis, uhf), gap in zip(jobs, gaps):
+        t_next += gap
+        delay = t_next - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        handles.append(server.submit(Z, xyz, basis, unrestricted=uhf, **(UHF_KW if uhf else RHF_KW)))
+    for h in handles:
+        h._done.wait(timeout)
+    t_end = max(h.t_end for h in handles)
+    lat = np.array([h.latency for h in handles if h.error is None]) * 1e3
+    summary = {"offered_rate": rate, "jobs": len(handles), "failed": sum(h.error is not None for h in handles),
+               "jobs_per_s": len(handles) / (t_end - t0), "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
+               "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
+               "peak_running": server.peak_running, "peak_bytes": server.peak_bytes}
+    return handles, summary

@@ -189,6 +189,14 @@ hfg_status hfg_fock_rhf_batch_device(hfg_ctx *ctx, const double *dP, double *dG,
 hfg_status hfg_fock_uhf_batch_device(hfg_ctx *ctx, const double *dPa, const double *dPb, double *dGa, double *dGb,
                                      const uint8_t *active, void *stream);
 
+/* Eigen-decomposition of `batch` symmetric n x n matrices (device, FP64,
+ * contiguous) in one batched cuSOLVER call on `stream`: dW receives batch x n
+ * ascending eigenvalues, dV batch x n x n eigenvectors with eigenvector k of
+ * matrix b in row k of block b (dV may equal dA).  The batched SCF's
+ * counterpart of the per-molecule Eigen::SelfAdjointEigenSolver step
+ * (RestrictedHartreeFock.cpp:121-124).  Workspace is kept per host thread. */
+hfg_status hfg_eigh_batched(const double *dA, double *dV, double *dW, int32_t n, int32_t batch, void *stream);
+
 /* Allocation-free variant of hfg_fock_rhf_device, for callers that must not
  * allocate device memory while they run: a serving loop under a fixed HBM
  * budget, code that cannot afford the implicit synchronisation of

@@ -58,6 +58,11 @@ typedef struct {
 void hfd_default_scf_opts(hfd_scf_opts *o);
 /* Text of the calling thread's last hfd_* failure. */
 const char *hfd_last_error(void);
+/* The Pulay (DIIS) system of DIIS.h:72 for `batch` molecules: B holds batch
+ * row-major m1 x m1 bordered matrices (error inner products, then the row
+ * and column of ones), c receives batch x m1 solutions of B c = (0,..,0,1)
+ * by the same column-pivoted Householder QR the SCF uses. */
+hfg_status hfd_pulay_solve(const double *B, int32_t m1, int32_t batch, double *c);
 /* atoms: Z[natoms], xyz[3*natoms] in bohr.  density (optional) receives
  * nbf*nbf (RHF) or 2*nbf*nbf (UHF: alpha then beta) doubles; pass its
  * capacity in `density_count`. */

@@ -1,0 +1,25 @@
+"""Serving on the device: jobs that run concurrently in the request loop
+(kernels of different jobs overlapping on their own streams) give the same
+converged energies as the same jobs run alone, within 1e-6 Eh for the
+precision form and 1e-9 Eh for the plain FP64 form."""
+import pytest
+
+from hartreefock_b200 import scf, serve
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("mixed,tol", [(True, 1e-6), (False, 1e-9)])
+def test_results_same_alone_and_in_the_mix(mixed, tol):
+    jobs = serve.draw_jobs(10, seed=11, nbf_range=(5, 80))
+    with serve.Server(slots=4, hbm_budget=8 << 30, mixed=mixed) as s:
+        handles, summ = serve.poisson_stream(s, jobs, rate=0.0)
+    assert summ["failed"] == 0 and summ["peak_running"] > 1
+    for h, (Z, xyz, basis, uhf) in zip(handles, jobs):
+        r = h.wait()
+        assert r["converged"], (h.id, basis, uhf)
+        kw = dict(serve.UHF_KW if uhf else serve.RHF_KW, post_diis=0)
+        if mixed:
+            kw["mixed_cutoff"] = 1e-4
+        alone = scf.run_scf(Z, xyz, basis, unrestricted=uhf, want_density=False, **kw)
+        assert abs(r["energy"] - alone["energy"]) <= tol, (h.id, basis, uhf, r["energy"], alone["energy"])
