@@ -176,6 +176,92 @@ def scf_comparison(waters: int):
     }
 
 
+def serving(count: int, slots: int = 8, seed: int = 5):
+    """The request loop (hartreefock_b200.serve) on a seeded Poisson stream of
+    `count` RHF/UHF jobs, precision form and plain FP64 builds: saturation
+    (every job submitted at once) and an offered rate of half of it."""
+    from hartreefock_b200 import serve
+    from hartreefock_b200.basis_io import shell_table
+    jobs = serve.draw_jobs(count, seed=seed)
+    out = {"workload": f"{count} jobs, seed {seed}: 80% RHF water clusters / C1-C10 alkanes, sizes log-uniform "
+                       "over 5-600 functions; 20% UHF OH / planar CH3; bases 6-31G, 6-31G*, 6-31+G** (Cartesian)",
+           "nbf": sorted(shell_table(Z, x, b).nbf for Z, x, b, u in jobs), "slots": slots,
+           "hbm_budget_gib": 40, "eri_convention": "exact"}
+    energies, converged = {}, {}
+    for name, mixed in (("mixed", True), ("fp64", False)):
+        runs = {}
+        with serve.Server(slots=slots, hbm_budget=40 << 30, mixed=mixed) as s:
+            hs, sat = serve.poisson_stream(s, jobs, rate=0.0, seed=1)
+        energies[name] = [h.result["energy"] if h.error is None else None for h in hs]
+        converged[name] = [h.error is None and h.result["converged"] for h in hs]
+        sat["not_converged"] = sum(1 for h in hs if h.error is not None or not h.result["converged"])
+        runs["saturation"] = sat
+        rate = 0.5 * sat["jobs_per_s"]
+        with serve.Server(slots=slots, hbm_budget=40 << 30, mixed=mixed) as s:
+            hs, half = serve.poisson_stream(s, jobs, rate=rate, seed=1)
+        runs["half_load"] = half
+        out[name] = runs
+    both = [i for i in range(len(jobs)) if converged["mixed"][i] and converged["fp64"][i]]
+    d = [abs(energies["mixed"][i] - energies["fp64"][i]) for i in both]
+    out["max_abs_dE_mixed_vs_fp64"] = max(d) if d else None
+    out["dE_over"] = f"{len(both)} jobs converged in both forms (1000-iteration cap)"
+    return out
+
+
+def batch_molecules(count: int, seed: int = 0):
+    """The batched-molecule mix: (H2O)_k k=1..6, staggered alkanes C1-C10,
+    UHF OH / planar CH3, bases STO-3G / 6-31G drawn per molecule from a seed."""
+    from hartreefock_b200 import molecules
+    rng = np.random.default_rng(seed)
+    kinds = [("w", k) for k in range(1, 7)] + [("a", n) for n in range(1, 11)] + [("oh", 0), ("ch3", 0)]
+    rhf, uhf = [], []
+    for i in range(count):
+        kind, k = kinds[int(rng.integers(0, len(kinds)))]
+        basis = ("sto-3g", "6-31g")[int(rng.integers(0, 2))]
+        if kind == "w":
+            Z, xyz = molecules.water_cluster(k, seed=int(rng.integers(0, 1 << 30)))
+        elif kind == "a":
+            Z, xyz = molecules.alkane(k)
+        else:
+            Z, xyz = molecules.hydroxyl() if kind == "oh" else molecules.methyl_planar()
+        (uhf if kind in ("oh", "ch3") else rhf).append(dict(Z=list(Z), xyz=xyz, basis=basis))
+    return rhf, uhf
+
+
+def batching(count: int, check: int = 8):
+    """BatchSCF over the batched-molecule mix (one Fock launch per quartet
+    class over every molecule per iteration); molecules/s, and |dE| against
+    single-molecule FP64 runs of `check` of them."""
+    import torch
+    from hartreefock_b200 import batch, scf
+    rhf, uhf = batch_molecules(count)
+    out = {"workload": f"{count} molecules: (H2O)_1-6, alkanes C1-C10, UHF OH / CH3; STO-3G / 6-31G", "runs": {}}
+    total_wall = 0.0
+    for name, mols, un, kw in (("rhf", rhf, False, dict(alpha=0.75, init_guess=0.75)),
+                               ("uhf", uhf, True, dict(alpha=0.5, init_guess=0.0))):
+        if not mols:
+            continue
+        t0 = time.perf_counter()
+        bs = batch.BatchSCF(mols, unrestricted=un, max_iter=1000, **kw)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        e = bs.run()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        total_wall += t2 - t0
+        errs = []
+        for i in list(range(0, len(mols), max(1, len(mols) // check)))[:check]:
+            m = mols[i]
+            r = scf.run_scf(m["Z"], m["xyz"], m["basis"], unrestricted=un, post_diis=0, want_density=False, **kw)
+            errs.append(abs(r["energy"] - e[i]))
+        out["runs"][name] = {"molecules": len(mols), "setup_s": t1 - t0, "scf_s": t2 - t1,
+                             "seconds": {k: round(v, 4) for k, v in bs.seconds.items()}, "fock_launch_rounds": bs.builds,
+                             "max_iterations": int(bs.iterations.max()), "converged": int(bs.converged.sum()),
+                             "nbf_max": bs.nmax, "max_abs_dE_vs_single_fp64": max(errs) if errs else None}
+    out["molecules_per_s"] = count / total_wall if total_wall else None
+    return out
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -215,6 +301,8 @@ def main():
     ap.add_argument("--waters", type=int, default=16,
                     help="cluster size; the benchmark workload is 16 (smaller values size profiler captures)")
     ap.add_argument("--scf-waters", type=int, default=SCF_WATERS, help="cluster of the SCF comparison (0: skip)")
+    ap.add_argument("--serve-jobs", type=int, default=24, help="jobs of the serving stream (0: skip)")
+    ap.add_argument("--batch-mols", type=int, default=0, help="molecules of the batched SCF (0: skip)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     WATERS = args.waters
@@ -354,6 +442,10 @@ def main():
     }
     if rank == 0 and world == 1 and args.scf_waters > 0:
         line["scf"] = scf_comparison(args.scf_waters)
+    if rank == 0 and world == 1 and args.serve_jobs > 0:
+        line["serving"] = serving(args.serve_jobs)
+    if rank == 0 and world == 1 and args.batch_mols > 0:
+        line["batching"] = batching(args.batch_mols)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = 1
         cb = cpu_baseline(args.ref_sample, threads)

@@ -83,10 +83,11 @@ class BatchSCF:
         self.V = 0.5 * (V + V.transpose(1, 2)) * mask2
         self.mask2 = mask2
         self.shift = torch.diag_embed((~valid).double() * PAD_SHIFT)
-        # eigensolver buckets: molecules grouped by nbf rounded up to 8, so
-        # each batched solve runs at its own size instead of the largest
-        size = np.minimum(((self.nbf + 7) // 8) * 8, n)
-        self.buckets = [(int(b), np.nonzero(size == b)[0]) for b in np.unique(size)]
+        # eigensolver buckets: molecules grouped by their exact nbf, so each
+        # batched solve runs at the molecule's own size with no padded level
+        # in it (a large padded level would set the solver's tolerance
+        # relative to itself and cost the real levels digits)
+        self.buckets = [(int(b), np.nonzero(self.nbf == b)[0]) for b in np.unique(self.nbf)]
         self.seconds = {"fock": 0.0, "diis": 0.0, "eigh": 0.0, "total": 0.0}
 
     # ---- flat <-> padded

@@ -1207,8 +1207,9 @@ hfg_status hfd_scf(const char *basis_path, int32_t natoms, const int32_t *Z, con
     mol.betaElectrons = (unsigned)opts->beta_electrons;
     mol.Init();
     std::unique_ptr<HartreeFock::HartreeFockAlgorithm> algo;
-    if (opts->unrestricted) algo.reset(new HartreeFock::UnrestrictedHartreeFock());
-    else algo.reset(new HartreeFock::RestrictedHartreeFock());
+    const int iters = opts->max_iterations > 0 ? opts->max_iterations : 3000;
+    if (opts->unrestricted) algo.reset(new HartreeFock::UnrestrictedHartreeFock(iters));
+    else algo.reset(new HartreeFock::RestrictedHartreeFock(iters));
     algo->alpha = opts->alpha;
     algo->initGuess = opts->init_guess;
     algo->UseDIIS = opts->use_diis != 0;

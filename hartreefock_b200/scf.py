@@ -23,7 +23,7 @@ class hfd_scf_opts(ctypes.Structure):
                 ("mixed_switch_diis", ctypes.c_double),
                 ("fp64_final_iterations", ctypes.c_int32), ("fp64_final_converge", ctypes.c_int32),
                 ("incremental", ctypes.c_int32), ("trace", ctypes.c_int32),
-                ("stop_at_precision_test", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("stop_at_precision_test", ctypes.c_int32), ("max_iterations", ctypes.c_int32)]
 
 
 class hfd_scf_result(ctypes.Structure):
@@ -64,7 +64,7 @@ def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75,
             want_density=True, mixed_cutoff=0.0, mixed_switch_energy=1e-7, mixed_switch_density=1e-7,
             mixed_switch_diis=1e-6,
             fp64_final_iterations=2, fp64_final_converge=False, incremental=False, trace=False,
-            stop_at_precision_test=False):
+            stop_at_precision_test=False, max_iterations=0):
     """RestrictedHartreeFock / UnrestrictedHartreeFock Init + Calculate.
 
     mixed_cutoff > 0 selects the precision form of the Fock builds (FP32
@@ -83,6 +83,7 @@ def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75,
     o.mixed_switch_diis = mixed_switch_diis
     o.trace = int(trace)
     o.stop_at_precision_test = int(stop_at_precision_test)
+    o.max_iterations = int(max_iterations)
     z = np.ascontiguousarray(Z, dtype=np.int32)
     x = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
     nbf_guess = 40 * len(z) + 64

@@ -16,10 +16,18 @@ The reference runs one algorithm object per std::thread with no shared
 state (HartreeFockDoc.cpp:372-405); a slot here is that thread, with the
 device as the shared resource the budget guards.
 
+Jobs use the exact electron-transfer recursion (HFG_ERI_EXACT) by
+default: the reference's (dd|dd) transfer (GaussianTwoElectrons.cpp:162)
+drops terms that matter when d shells on neighbouring atoms overlap, and
+propane in 6-31G* then has no physical solution (its SCF wanders below
+-1100 Eh instead of converging near -118.25 Eh).  The parity tests keep the
+reference convention; a caller can pass eri_convention to Server.
+
 draw_jobs() and poisson_stream() make and replay the synthetic request
-stream: 80% RHF water clusters / alkanes with sizes log-uniform over a
-function-count range, 20% UHF doublets (OH, planar CH3), bases drawn
-uniformly from 6-31G, 6-31G*, 6-31+G** (Cartesian).
+stream: 80% RHF water clusters / alkanes (C1-C10, larger sizes as water
+clusters) with sizes log-uniform over a function-count range, 20% UHF
+doublets (OH, planar CH3), bases drawn uniformly from 6-31G, 6-31G*,
+6-31+G** (Cartesian).
 """
 from __future__ import annotations
 
@@ -30,6 +38,7 @@ import time
 
 import numpy as np
 
+from . import engine as E
 from . import molecules
 from .basis_io import shell_table
 
@@ -89,9 +98,12 @@ class Server:
     """slots: jobs on the device at once.  hbm_budget: bytes the admitted
     jobs' footprints may add up to.  mixed: precision form of the Fock
     builds (FP32 below mixed_cutoff, incremental, FP64 finish) for every
-    job; otherwise the plain FP64 form.  scf_kwargs go to every job's SCF
-    (scf.run_scf keywords); post_diis defaults to 0 here, the reference's
-    convergence test alone.  runner(job) -> result replaces the driver call
+    job; otherwise plain FP64 builds.  Both stop on the precision form's
+    rule (|dE| < 1e-7, rms dD < 1e-7, DIIS error < 1e-6, then two full FP64
+    iterations), so the two differ only in their kernels.  scf_kwargs go to every job's SCF
+    (scf.run_scf keywords); the defaults here are post_diis 0 (the
+    reference's convergence test alone), at most 1000 iterations and the
+    exact ERI convention.  runner(job) -> result replaces the driver call
     (host-side tests)."""
 
     def __init__(self, slots: int = 8, hbm_budget: int = 32 << 30, mixed: bool = True, mixed_cutoff: float = 1e-4,
@@ -99,9 +111,11 @@ class Server:
         if slots < 1 or hbm_budget <= 0:
             raise ValueError("slots >= 1 and a positive budget are required")
         self.slots, self.budget = slots, int(hbm_budget)
-        self.defaults = dict(post_diis=0)
+        self.defaults = dict(post_diis=0, max_iterations=1000, eri_convention=E.ERI_EXACT)
         if mixed:
             self.defaults["mixed_cutoff"] = mixed_cutoff
+        else:
+            self.defaults["stop_at_precision_test"] = True
         self.defaults.update(scf_kwargs or {})
         self.runner = runner or _driver_runner
         self._cv = threading.Condition()
@@ -201,13 +215,14 @@ def _functions_per_atom(basis: str) -> dict:
 
 
 def _rhf_molecule(target: float, basis: str, rng, fpa):
-    """Water cluster or alkane whose function count is nearest the target."""
+    """Water cluster or alkane (C1-C10) whose function count is nearest the
+    target; targets beyond decane are water clusters."""
     water = fpa[8] + 2 * fpa[1]
-    if rng.random() < 0.5:
+    per_c, base = fpa[6] + 2 * fpa[1], 2 * fpa[1]
+    if rng.random() < 0.5 or target > 10 * per_c + base:
         k = max(1, int(round(target / water)))
         Z, xyz = molecules.water_cluster(k, seed=int(rng.integers(0, 1 << 30)))
     else:
-        per_c, base = fpa[6] + 2 * fpa[1], 2 * fpa[1]
         n = max(1, int(round((target - base) / per_c)))
         Z, xyz = molecules.alkane(n)
     return list(Z), xyz
@@ -231,8 +246,10 @@ def draw_jobs(count: int, seed: int = 0, nbf_range=(5, 600), uhf_fraction: float
     return out
 
 
-UHF_KW = dict(alpha=0.5, init_guess=0.0)
-RHF_KW = dict(alpha=0.75, init_guess=0.75)
+# SCF settings of the stream (HartreeFockAlgorithm::alpha / initGuess): the
+# pair under which most jobs of the mix converge within the iteration cap
+UHF_KW = dict(alpha=0.75, init_guess=0.75)
+RHF_KW = dict(alpha=0.5, init_guess=0.0)
 
 
 def poisson_stream(server: Server, jobs, rate: float, seed: int = 0, timeout=None):

@@ -35,7 +35,8 @@ typedef struct {
   int32_t incremental;       /* FP64 incremental builds (implied by mixed_cutoff > 0) */
   int32_t trace;             /* 1: one line per SCF step on stderr */
   int32_t stop_at_precision_test; /* plain builds, precision form's stopping rule */
-  int32_t reserved;
+  int32_t max_iterations;    /* the algorithm's iteration cap; 0 = 3000, the
+                                reference's default (RestrictedHartreeFock.h:31) */
 } hfd_scf_opts;
 
 typedef struct {
