@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <cstdlib>
 #include <mutex>
 #include <numeric>
 #include <set>
@@ -24,8 +25,11 @@ static hfg_status fail(hfg_status st, const std::string &msg) {
   return st;
 }
 
-// for entry points defined in other translation units (hfg_eigh_batched)
+// for entry points defined in other translation units (hfg_eigh_batched,
+// hfg_one_electron)
 hfg_status fail_external(hfg_status st, const std::string &msg) { return fail(st, msg); }
+static const std::vector<double> &boys_table_host();
+const std::vector<double> &boys_table_for_external() { return boys_table_host(); }
 
 #define HFG_CUDA(call)                                                                        \
   do {                                                                                        \
@@ -120,6 +124,7 @@ struct hfg_ctx {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int num_sms = 148;
+  int blocks_per_sm = 4;  // grid cap of the fused class kernels, in blocks per SM
   // device tables
   PrimPair *d_prim = nullptr;
   PrimPairF *d_primf = nullptr;
@@ -324,7 +329,7 @@ static int grid_for(const hfg_ctx *c, int ntasks, int cls) {
   const ClassEntry &e = kClasses[cls];
   const int w = fused_warps(e.la, e.lb, e.lc, e.ld);
   const int blocks = (ntasks + w - 1) / w;
-  return std::max(1, std::min(blocks, c->num_sms * 16));
+  return std::max(1, std::min(blocks, c->num_sms * c->blocks_per_sm));
 }
 
 // A class launch over all tasks, or with `sharded` over this context's
@@ -752,6 +757,9 @@ static hfg_status create_context(const hfg_shells *sh, const int *shell_mol, int
   ctx->device = ctx->opts.device;
   HFG_CUDA(cudaSetDevice(ctx->device));
   HFG_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  // tuning: HFG_BLOCKS_PER_SM overrides the grid cap (every block stages the
+  // class's Boys table once, so fewer, longer-lived blocks stage it less)
+  if (const char *e = std::getenv("HFG_BLOCKS_PER_SM")) ctx->blocks_per_sm = std::max(1, std::atoi(e));
   ctx->batch = shell_mol != nullptr;
   ctx->nmol = ctx->batch ? nmol : 1;
   ctx->nbf = ctx->batch ? 0 : sh->nbf;

@@ -49,39 +49,6 @@ int letter_l(char c) {
 
 inline int ncart(int L) { return (L + 1) * (L + 2) / 2; }
 
-double dfact(int n) {
-  double r = 1;
-  for (; n > 1; n -= 2) r *= n;
-  return r;
-}
-
-// Cartesian components in the reference's canonical order (xx, xy, xz, yy, yz, zz)
-void components(int L, std::vector<std::array<int, 3>> &out) {
-  out.clear();
-  for (int i = L; i >= 0; --i)
-    for (int j = L - i; j >= 0; --j) out.push_back({i, j, L - i - j});
-}
-
-// Boys function F_0..F_M(T): series below 30 (positive terms, downward
-// recursion), F_0 = sqrt(pi/T)/2 erf(sqrt T) and upward recursion above.
-void boys_host(int M, double T, double *F) {
-  if (T < 30.0) {
-    double term = 1.0 / (2 * M + 1), sum = 0;
-    for (int k = 0; k < 400; ++k) {
-      sum += term;
-      term *= 2.0 * T / (2 * M + 2 * k + 3);
-      if (term < sum * 1e-17) break;
-    }
-    const double e = std::exp(-T);
-    F[M] = e * sum;
-    for (int m = M - 1; m >= 0; --m) F[m] = (2 * T * F[m + 1] + e) / (2 * m + 1);
-  } else {
-    const double e = std::exp(-T);
-    F[0] = 0.5 * std::sqrt(M_PI / T) * std::erf(std::sqrt(T));
-    for (int m = 0; m < M; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) / (2 * T);
-  }
-}
-
 std::string trim(const std::string &s) {
   size_t a = s.find_first_not_of(" \t\r\n"), b = s.find_last_not_of(" \t\r\n");
   return a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
@@ -400,165 +367,6 @@ bool Systems::Molecule::LoadXYZ(const std::string &fileName, const Chemistry::Ba
 }
 
 // ===========================================================================
-// one-electron integrals (Obara-Saika), per contracted shell pair
-// ===========================================================================
-namespace {
-
-struct ShellView {
-  double c[3];
-  int L, nprim;
-  const double *e, *k;
-  int ao;
-};
-
-// primitive normalisation without the component part: (2a/pi)^(3/4) (4a)^(L/2)
-inline double radial_norm(double a, int L) { return std::pow(2 * a / M_PI, 0.75) * std::pow(4 * a, L / 2.0); }
-inline double comp_norm(const std::array<int, 3> &c) {
-  return 1.0 / std::sqrt(dfact(2 * c[0] - 1) * dfact(2 * c[1] - 1) * dfact(2 * c[2] - 1));
-}
-
-// S, T and V blocks of one shell pair (row-major into the full matrices)
-void shell_pair_one_electron(const ShellView &A, const ShellView &B, const std::vector<double> &nuc_xyz,
-                             const std::vector<int> &nuc_z, int n, double *S, double *T, double *V) {
-  std::vector<std::array<int, 3>> ca, cb;
-  components(A.L, ca);
-  components(B.L, cb);
-  const int na = (int)ca.size(), nb = (int)cb.size();
-  std::vector<double> s(na * nb, 0.0), t(na * nb, 0.0), v(na * nb, 0.0);
-  double AB[3];
-  double ab2 = 0;
-  for (int d = 0; d < 3; ++d) {
-    AB[d] = A.c[d] - B.c[d];
-    ab2 += AB[d] * AB[d];
-  }
-  const int LT = A.L + B.L;
-  // horizontal transfer (a|b+1_d) = (a+1_d|b) + AB_d (a|b): each (x|y) is a
-  // fixed combination of (e|0) with e on A, the same for every primitive
-  // pair and nucleus
-  struct Term {
-    int l, m, nn;
-    double c;
-  };
-  std::vector<std::vector<Term>> hrr(na * nb);
-  for (int x = 0; x < na; ++x)
-    for (int y = 0; y < nb; ++y) {
-      std::vector<std::pair<std::array<int, 3>, double>> terms{{ca[x], 1.0}};
-      std::array<int, 3> rem = cb[y];
-      for (int d = 0; d < 3; ++d)
-        while (rem[d] > 0) {
-          std::vector<std::pair<std::array<int, 3>, double>> nt;
-          for (auto &tm : terms) {
-            auto up = tm.first;
-            up[d] += 1;
-            nt.push_back({up, tm.second});
-            nt.push_back({tm.first, tm.second * AB[d]});
-          }
-          terms.swap(nt);
-          --rem[d];
-        }
-      for (auto &tm : terms) hrr[x * nb + y].push_back(Term{tm.first[0], tm.first[1], tm.first[2], tm.second});
-    }
-  for (int i = 0; i < A.nprim; ++i)
-    for (int j = 0; j < B.nprim; ++j) {
-      const double a = A.e[i], b = B.e[j], z = a + b, iz = 1.0 / z;
-      const double K = std::exp(-a * b * iz * ab2);
-      const double cc = A.k[i] * radial_norm(a, A.L) * B.k[j] * radial_norm(b, B.L);
-      double P[3], PA[3], PB[3];
-      for (int d = 0; d < 3; ++d) {
-        P[d] = (a * A.c[d] + b * B.c[d]) * iz;
-        PA[d] = P[d] - A.c[d];
-        PB[d] = P[d] - B.c[d];
-      }
-      // 1D overlaps O[d][i][j], i <= LA, j <= LB+2 (OS recursion)
-      double O[3][5][7] = {};
-      for (int d = 0; d < 3; ++d) {
-        O[d][0][0] = std::sqrt(M_PI * iz);
-        for (int jj = 0; jj <= B.L + 2; ++jj)
-          for (int ii = 0; ii <= A.L; ++ii) {
-            if (ii == 0 && jj == 0) continue;
-            double val;
-            if (ii > 0) {
-              val = PA[d] * O[d][ii - 1][jj];
-              if (ii > 1) val += (ii - 1) * 0.5 * iz * O[d][ii - 2][jj];
-              if (jj > 0) val += jj * 0.5 * iz * O[d][ii - 1][jj - 1];
-            } else {
-              val = PB[d] * O[d][0][jj - 1];
-              if (jj > 1) val += (jj - 1) * 0.5 * iz * O[d][0][jj - 2];
-            }
-            O[d][ii][jj] = val;
-          }
-      }
-      // nuclear attraction: (a|0)^(m) by the OS vertical recursion on A,
-      // then the horizontal transfer to B, per nucleus
-      for (int x = 0; x < na; ++x)
-        for (int y = 0; y < nb; ++y) {
-          const auto &p = ca[x], &q = cb[y];
-          double sxyz = 1, kin = 0;
-          double o[3], d2[3];
-          for (int d = 0; d < 3; ++d) {
-            o[d] = O[d][p[d]][q[d]];
-            // <i| d^2/dx^2 |j> = j(j-1) S_{i,j-2} - 2b(2j+1) S_{i,j} + 4b^2 S_{i,j+2}
-            const int jj = q[d];
-            d2[d] = (jj > 1 ? jj * (jj - 1) * O[d][p[d]][jj - 2] : 0.0) - 2 * b * (2 * jj + 1) * O[d][p[d]][jj] +
-                    4 * b * b * O[d][p[d]][jj + 2];
-            sxyz *= o[d];
-          }
-          kin = -0.5 * (d2[0] * o[1] * o[2] + o[0] * d2[1] * o[2] + o[0] * o[1] * d2[2]);
-          s[x * nb + y] += cc * K * sxyz;
-          t[x * nb + y] += cc * K * kin;
-        }
-      // nuclear part
-      for (size_t c = 0; c < nuc_z.size(); ++c) {
-        const double *C = &nuc_xyz[3 * c];
-        double PC[3], pc2 = 0;
-        for (int d = 0; d < 3; ++d) {
-          PC[d] = P[d] - C[d];
-          pc2 += PC[d] * PC[d];
-        }
-        double F[9];
-        boys_host(LT, z * pc2, F);
-        // W[l][m][n][mm] for l+m+n <= LT, via the vertical recursion
-        double W[5][5][5][5] = {};
-        for (int mm = 0; mm <= LT; ++mm) W[0][0][0][mm] = 2 * M_PI * iz * K * F[mm];
-        for (int L = 1; L <= LT; ++L)
-          for (int l = L; l >= 0; --l)
-            for (int m = L - l; m >= 0; --m) {
-              const int nn = L - l - m;
-              int e[3] = {l, m, nn};
-              const int d = l > 0 ? 0 : (m > 0 ? 1 : 2);
-              int e1[3] = {l, m, nn};
-              e1[d] -= 1;
-              for (int mm = 0; mm + L <= LT; ++mm) {
-                double val = PA[d] * W[e1[0]][e1[1]][e1[2]][mm] - PC[d] * W[e1[0]][e1[1]][e1[2]][mm + 1];
-                if (e1[d] > 0) {
-                  int e2[3] = {e1[0], e1[1], e1[2]};
-                  e2[d] -= 1;
-                  val += e1[d] * 0.5 * iz * (W[e2[0]][e2[1]][e2[2]][mm] - W[e2[0]][e2[1]][e2[2]][mm + 1]);
-                }
-                W[e[0]][e[1]][e[2]][mm] = val;
-              }
-            }
-        // horizontal transfer to B, on m = 0
-        for (int x = 0; x < na * nb; ++x) {
-          double val = 0;
-          for (const Term &tm : hrr[x]) val += tm.c * W[tm.l][tm.m][tm.nn][0];
-          v[x] -= nuc_z[c] * cc * val;
-        }
-      }
-    }
-  for (int x = 0; x < na; ++x)
-    for (int y = 0; y < nb; ++y) {
-      const double f = comp_norm(ca[x]) * comp_norm(cb[y]);
-      const size_t I = A.ao + x, J = B.ao + y;
-      S[I * n + J] = S[J * n + I] = f * s[x * nb + y];
-      T[I * n + J] = T[J * n + I] = f * t[x * nb + y];
-      V[I * n + J] = V[J * n + I] = f * v[x * nb + y];
-    }
-}
-
-}  // namespace
-
-// ===========================================================================
 // IntegralsRepository
 // ===========================================================================
 namespace GaussianIntegrals {
@@ -608,35 +416,24 @@ double IntegralsRepository::getElectronElectronDirect(int i, int j, int k, int l
   return v;
 }
 
-// QuantumMatrix.cpp:34-155 (overlap, kinetic, nuclear attraction), shell
-// pair by shell pair on the host's threads
+// QuantumMatrix.cpp:34-155 (overlap, kinetic, nuclear attraction): all
+// shell pairs on the device (hfg_one_electron)
 void IntegralsRepository::OneElectron(hfgpu::Matrix &S, hfgpu::Matrix &T, hfgpu::Matrix &V) const {
   const auto &t = molecule_->shellTable();
-  const int n = t.nbf, ns = (int)t.L.size();
+  const int n = t.nbf;
   S.resize(n, n);
   T.resize(n, n);
   V.resize(n, n);
-  std::vector<ShellView> sv(ns);
-  for (int s = 0; s < ns; ++s)
-    sv[s] = ShellView{{t.center[3 * s], t.center[3 * s + 1], t.center[3 * s + 2]}, t.L[s], t.nprim[s],
-                      &t.exponent[t.prim_offset[s]], &t.coefficient[t.prim_offset[s]], t.ao_offset[s]};
   std::vector<double> nxyz;
-  std::vector<int> nz;
+  std::vector<int32_t> nz;
   for (const auto &a : molecule_->atoms) {
     nxyz.insert(nxyz.end(), {a.position.X, a.position.Y, a.position.Z});
-    nz.push_back((int)a.Z);
+    nz.push_back((int32_t)a.Z);
   }
-  std::vector<std::pair<int, int>> pairs;
-  for (int a = 0; a < ns; ++a)
-    for (int b = 0; b <= a; ++b) pairs.push_back({a, b});
-  const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-  std::vector<std::thread> pool;
-  for (unsigned w = 0; w < nt; ++w)
-    pool.emplace_back([&, w]() {
-      for (size_t p = w; p < pairs.size(); p += nt)
-        shell_pair_one_electron(sv[pairs[p].first], sv[pairs[p].second], nxyz, nz, n, S.data(), T.data(), V.data());
-    });
-  for (auto &th : pool) th.join();
+  const hfg_shells sh = t.view();
+  if (hfg_one_electron(&sh, nxyz.data(), nz.data(), (int32_t)nz.size(), options.device, S.data(), T.data(),
+                       V.data()) != HFG_OK)
+    throw std::runtime_error(std::string("hfg_one_electron: ") + hfg_last_error());
 }
 
 }  // namespace GaussianIntegrals

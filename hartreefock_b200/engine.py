@@ -27,7 +27,7 @@ EXPORTED = ["hfg_default_opts", "hfg_last_error", "hfg_device_count", "hfg_ctx_c
             "hfg_ctx_stats", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak",
             "hfg_fock_rhf_noalloc", "hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental",
             "hfg_set_shard", "hfg_batch_create", "hfg_batch_size", "hfg_batch_layout", "hfg_fock_rhf_batch_device",
-            "hfg_fock_uhf_batch_device", "hfg_eigh_batched"]
+            "hfg_fock_uhf_batch_device", "hfg_eigh_batched", "hfg_one_electron"]
 
 
 class HfgError(RuntimeError):
@@ -115,6 +115,8 @@ def library(path: str = LIB_PATH):
     L.hfg_set_shard.argtypes = [vp, i32, i32]
     L.hfg_eigh_batched.argtypes = [dp, dp, dp, i32, i32, vp]
     L.hfg_eigh_batched.restype = ctypes.c_int
+    L.hfg_one_electron.argtypes = [ctypes.POINTER(hfg_shells), dp, dp, i32, i32, dp, dp, dp]
+    L.hfg_one_electron.restype = ctypes.c_int
     for name in ("hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental", "hfg_set_shard", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak", "hfg_ctx_create", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet", "hfg_fock_rhf",
                  "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz", "hfg_ctx_stats"):
         getattr(L, name).restype = ctypes.c_int
@@ -135,6 +137,20 @@ def measure_fp64_peak(device: int = 0) -> float:
     v = ctypes.c_double()
     _check(library().hfg_measure_fp64_peak(device, ctypes.byref(v)))
     return v.value
+
+
+def one_electron(Z, xyz, basis: str, device: int = 0):
+    """(S, T, V) of a molecule from the device one-electron kernels
+    (hfg_one_electron), row-major nbf x nbf float64 arrays."""
+    t = shell_table(Z, xyz, basis)
+    keep = [np.ascontiguousarray(x) for x in (t.center.ravel(), t.L, t.nprim, t.prim_offset, t.ao_offset,
+                                              t.exponent, t.coefficient)]
+    sh = hfg_shells(len(t.L), *[_ptr(x) for x in keep], t.nbf)
+    x = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
+    z = np.ascontiguousarray(Z, dtype=np.int32)
+    out = [np.zeros((t.nbf, t.nbf)) for _ in range(3)]
+    _check(library().hfg_one_electron(ctypes.byref(sh), _ptr(x), _ptr(z), len(z), device, *[_ptr(o) for o in out]))
+    return tuple(out)
 
 
 def eigh_batched(A):

@@ -189,6 +189,15 @@ hfg_status hfg_fock_rhf_batch_device(hfg_ctx *ctx, const double *dP, double *dG,
 hfg_status hfg_fock_uhf_batch_device(hfg_ctx *ctx, const double *dPa, const double *dPb, double *dGa, double *dGb,
                                      const uint8_t *active, void *stream);
 
+/* One-electron matrices on `device`: overlap S, kinetic energy T and
+ * nuclear attraction V (h = T + V), each row-major nbf x nbf in host memory,
+ * for the shells `shells` and the nuclei (xyz[3*natoms] bohr, charges Z).
+ * Replaces IntegralsRepository's one-electron part and QuantumMatrix
+ * (IntegralsRepository.cpp:34-321, QuantumMatrix.cpp:34-155).  Needs no
+ * context; allocates and frees its own device buffers. */
+hfg_status hfg_one_electron(const hfg_shells *shells, const double *xyz, const int32_t *Z, int32_t natoms,
+                            int32_t device, double *S, double *T, double *V);
+
 /* Eigen-decomposition of `batch` symmetric n x n matrices (device, FP64,
  * contiguous) in one batched cuSOLVER call on `stream`: dW receives batch x n
  * ascending eigenvalues, dV batch x n x n eigenvectors with eigenvector k of
