@@ -88,6 +88,10 @@ class BatchSCF:
         # in it (a large padded level would set the solver's tolerance
         # relative to itself and cost the real levels digits)
         self.buckets = [(int(b), np.nonzero(self.nbf == b)[0]) for b in np.unique(self.nbf)]
+        # open shells: which orbital of a degenerate level gets the unpaired
+        # electron depends on the solver's basis for that level, so UHF uses
+        # the single-molecule SCF's per-matrix solver (same states as alone)
+        self.eigh_method = 1 if unrestricted else 0
         self.seconds = {"fock": 0.0, "diis": 0.0, "eigh": 0.0, "total": 0.0}
 
     # ---- flat <-> padded
@@ -122,7 +126,7 @@ class BatchSCF:
             if len(sel) == 0:
                 continue
             t = torch.from_numpy(sel).to(self.dev)
-            wb, Ub = E.eigh_batched(Ft[t, :b, :b].contiguous())
+            wb, Ub = E.eigh_batched(Ft[t, :b, :b].contiguous(), method=self.eigh_method)
             w[t, :b] = wb
             U[t, :b, :b] = Ub
         return w, U

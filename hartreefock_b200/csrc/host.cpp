@@ -836,6 +836,14 @@ double RestrictedHartreeFock::Step(int iter) {
   return std::sqrt(change2);
 }
 
+double RestrictedHartreeFock::CalculateMp2Energy() {
+  const int n = numberOfOrbitals;
+  if (!inited || (int)C.rows() != n || (int)eigenvals.size() != n || nrOccupiedLevels >= (unsigned)n) return mp2Energy = 0;
+  check_engine(hfg_mp2_rhf(integralsRepository.engine(), C.data(), eigenvals.data(), (int32_t)nrOccupiedLevels, &mp2Energy),
+               "hfg_mp2_rhf");
+  return mp2Energy;
+}
+
 void UnrestrictedHartreeFock::Init(Systems::Molecule *molecule) {
   HartreeFockAlgorithm::Init(molecule);
   DensityMatrixPlus = Matrix::Zero(h.rows(), h.cols());
@@ -1041,6 +1049,8 @@ hfg_status hfd_scf(const char *basis_path, int32_t natoms, const int32_t *Z, con
     result->seconds_diis = algo->secondsDiis;
     result->seconds_total = algo->secondsTotal;
     result->seconds_init = algo->secondsInit;
+    if (opts->mp2 && !opts->unrestricted)
+      result->mp2_energy = static_cast<HartreeFock::RestrictedHartreeFock *>(algo.get())->CalculateMp2Energy();
     const int64_t nn = (int64_t)result->nbf * result->nbf;
     if (density) {
       if (opts->unrestricted) {

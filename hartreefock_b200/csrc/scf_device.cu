@@ -313,9 +313,10 @@ hfg_status fail_external(hfg_status st, const std::string &msg);
 }
 
 extern "C" hfg_status hfg_eigh_batched(const double *dA, double *dV, double *dW, int32_t n, int32_t batch,
-                                       void *stream) {
+                                       int32_t method, void *stream) {
   using hfgpu::detail::ck;
-  if (!dA || !dV || !dW || n < 1 || batch < 1) return hfg::fail_external(HFG_INVALID_ARG, "hfg_eigh_batched: arguments");
+  if (!dA || !dV || !dW || n < 1 || batch < 1 || method < 0 || method > 1)
+    return hfg::fail_external(HFG_INVALID_ARG, "hfg_eigh_batched: arguments");
   try {
     BatchedEigh &e = g_eigh;
     int dev = 0;
@@ -341,6 +342,33 @@ extern "C" hfg_status hfg_eigh_batched(const double *dA, double *dV, double *dW,
     ck(cusolverDnSetStream(e.handle, s), "cusolverDnSetStream");
     const size_t bytes = (size_t)n * n * batch * sizeof(double);
     if (dV != dA) ck(cudaMemcpyAsync(dV, dA, bytes, cudaMemcpyDeviceToDevice, s), "copy A");
+    if (method == 1) {
+      // one divide-and-conquer solve per matrix, the single-molecule SCF's solver
+      int lwork = 0;
+      ck(cusolverDnDsyevd_bufferSize(e.handle, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, dV, n, dW, &lwork),
+         "cusolverDnDsyevd_bufferSize");
+      const size_t need = (size_t)lwork * sizeof(double);
+      if (need > e.dbytes) {
+        ck(cudaStreamSynchronize(s), "sync");
+        if (e.dwork) cudaFree(e.dwork);
+        e.dwork = nullptr;
+        ck(cudaMalloc(&e.dwork, need), "cudaMalloc eigh workspace");
+        e.dbytes = need;
+      }
+      if (batch > e.info_cap) {
+        ck(cudaStreamSynchronize(s), "sync");
+        if (e.info) cudaFree(e.info);
+        e.info = nullptr;
+        ck(cudaMalloc(&e.info, sizeof(int) * batch), "cudaMalloc eigh info");
+        e.info_cap = batch;
+      }
+      const size_t nn = (size_t)n * n;
+      for (int b = 0; b < batch; ++b)
+        ck(cusolverDnDsyevd(e.handle, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, dV + b * nn, n,
+                            dW + (size_t)b * n, static_cast<double *>(e.dwork), lwork, e.info + b),
+           "cusolverDnDsyevd");
+      return HFG_OK;
+    }
     size_t dneed = 0, hneed = 0;
     ck(cusolverDnXsyevBatched_bufferSize(e.handle, e.params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n,
                                          CUDA_R_64F, dV, n, CUDA_R_64F, dW, CUDA_R_64F, &dneed, &hneed, batch),

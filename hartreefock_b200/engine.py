@@ -27,7 +27,8 @@ EXPORTED = ["hfg_default_opts", "hfg_last_error", "hfg_device_count", "hfg_ctx_c
             "hfg_ctx_stats", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak",
             "hfg_fock_rhf_noalloc", "hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental",
             "hfg_set_shard", "hfg_batch_create", "hfg_batch_size", "hfg_batch_layout", "hfg_fock_rhf_batch_device",
-            "hfg_fock_uhf_batch_device", "hfg_eigh_batched", "hfg_one_electron"]
+            "hfg_fock_uhf_batch_device", "hfg_eigh_batched", "hfg_one_electron",
+            "hfg_mo_eri_ovov", "hfg_mp2_rhf"]
 
 
 class HfgError(RuntimeError):
@@ -113,10 +114,14 @@ def library(path: str = LIB_PATH):
     L.hfg_set_mixed_cutoff.argtypes = [vp, ctypes.c_double]
     L.hfg_set_incremental.argtypes = [vp, i32]
     L.hfg_set_shard.argtypes = [vp, i32, i32]
-    L.hfg_eigh_batched.argtypes = [dp, dp, dp, i32, i32, vp]
+    L.hfg_eigh_batched.argtypes = [dp, dp, dp, i32, i32, i32, vp]
     L.hfg_eigh_batched.restype = ctypes.c_int
     L.hfg_one_electron.argtypes = [ctypes.POINTER(hfg_shells), dp, dp, i32, i32, dp, dp, dp]
     L.hfg_one_electron.restype = ctypes.c_int
+    L.hfg_mo_eri_ovov.argtypes = [vp, dp, i32, i32, i32, i32, dp, vp]
+    L.hfg_mo_eri_ovov.restype = ctypes.c_int
+    L.hfg_mp2_rhf.argtypes = [vp, dp, dp, i32, ctypes.POINTER(ctypes.c_double)]
+    L.hfg_mp2_rhf.restype = ctypes.c_int
     for name in ("hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental", "hfg_set_shard", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak", "hfg_ctx_create", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet", "hfg_fock_rhf",
                  "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz", "hfg_ctx_stats"):
         getattr(L, name).restype = ctypes.c_int
@@ -153,7 +158,7 @@ def one_electron(Z, xyz, basis: str, device: int = 0):
     return tuple(out)
 
 
-def eigh_batched(A):
+def eigh_batched(A, method: int = 0):
     """Eigenvalues (ascending) and eigenvectors of a stack of symmetric
     matrices, a contiguous float64 CUDA tensor [batch, n, n], by one batched
     cuSOLVER call (hfg_eigh_batched) on torch's current stream.  Returns
@@ -166,7 +171,7 @@ def eigh_batched(A):
     X = torch.empty_like(A)
     w = torch.empty(b, n, dtype=torch.float64, device=A.device)
     _check(library().hfg_eigh_batched(ctypes.c_void_p(A.data_ptr()), ctypes.c_void_p(X.data_ptr()),
-                                      ctypes.c_void_p(w.data_ptr()), n, b,
+                                      ctypes.c_void_p(w.data_ptr()), n, b, method,
                                       ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
     return w, X.transpose(1, 2)
 
@@ -271,6 +276,25 @@ class Engine:
         _check(library().hfg_fock_uhf_device(self._h, ctypes.c_void_p(Pa_ptr), ctypes.c_void_p(Pb_ptr),
                                              ctypes.c_void_p(Ga_ptr), ctypes.c_void_p(Gb_ptr),
                                              ctypes.c_void_p(stream)))
+
+    def mp2_rhf(self, C: np.ndarray, eps: np.ndarray, nocc: int) -> float:
+        """RHF MP2 correlation energy (hfg_mp2_rhf) from MO coefficients C
+        (nbf x nbf, AO rows, MO columns) and orbital energies."""
+        C = np.ascontiguousarray(C, dtype=np.float64)
+        eps = np.ascontiguousarray(eps, dtype=np.float64)
+        out = ctypes.c_double()
+        _check(library().hfg_mp2_rhf(self._h, _ptr(C), _ptr(eps), nocc, ctypes.byref(out)))
+        return out.value
+
+    def mo_eri_ovov_tensor(self, C, i0: int, ni: int, a0: int, na: int):
+        """(ia|jb) block as a torch CUDA tensor [ni*na, ni*na] (hfg_mo_eri_ovov)."""
+        import torch
+        C = C.contiguous()
+        X = torch.empty(ni * na, ni * na, dtype=torch.float64, device=C.device)
+        _check(library().hfg_mo_eri_ovov(self._h, ctypes.c_void_p(C.data_ptr()), i0, ni, a0, na,
+                                          ctypes.c_void_p(X.data_ptr()),
+                                          ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        return X
 
     def fock_reset(self):
         """Drop the incremental history: the next build starts from the full density."""

@@ -23,7 +23,8 @@ class hfd_scf_opts(ctypes.Structure):
                 ("mixed_switch_diis", ctypes.c_double),
                 ("fp64_final_iterations", ctypes.c_int32), ("fp64_final_converge", ctypes.c_int32),
                 ("incremental", ctypes.c_int32), ("trace", ctypes.c_int32),
-                ("stop_at_precision_test", ctypes.c_int32), ("max_iterations", ctypes.c_int32)]
+                ("stop_at_precision_test", ctypes.c_int32), ("max_iterations", ctypes.c_int32),
+                ("mp2", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class hfd_scf_result(ctypes.Structure):
@@ -33,7 +34,7 @@ class hfd_scf_result(ctypes.Structure):
                 ("fp64_quartets", ctypes.c_int64), ("mixed_steps", ctypes.c_int32), ("reserved", ctypes.c_int32),
                 ("seconds_fock", ctypes.c_double), ("seconds_eigen", ctypes.c_double),
                 ("seconds_diis", ctypes.c_double), ("seconds_total", ctypes.c_double),
-                ("seconds_init", ctypes.c_double)]
+                ("seconds_init", ctypes.c_double), ("mp2_energy", ctypes.c_double)]
 
 
 DRIVER_SYMBOLS = ["hfd_default_scf_opts", "hfd_last_error", "hfd_scf", "hfd_one_electron", "hfd_pulay_solve"]
@@ -64,7 +65,7 @@ def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75,
             want_density=True, mixed_cutoff=0.0, mixed_switch_energy=1e-7, mixed_switch_density=1e-7,
             mixed_switch_diis=1e-6,
             fp64_final_iterations=2, fp64_final_converge=False, incremental=False, trace=False,
-            stop_at_precision_test=False, max_iterations=0):
+            stop_at_precision_test=False, max_iterations=0, mp2=False):
     """RestrictedHartreeFock / UnrestrictedHartreeFock Init + Calculate.
 
     mixed_cutoff > 0 selects the precision form of the Fock builds (FP32
@@ -84,6 +85,7 @@ def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75,
     o.trace = int(trace)
     o.stop_at_precision_test = int(stop_at_precision_test)
     o.max_iterations = int(max_iterations)
+    o.mp2 = int(mp2)
     z = np.ascontiguousarray(Z, dtype=np.int32)
     x = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
     nbf_guess = 40 * len(z) + 64
@@ -99,7 +101,7 @@ def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75,
            "nbf": r.nbf, "fock_builds": r.fock_builds, "fock_ms_total": r.fock_ms_total,
            "fp32_quartets": r.fp32_quartets, "fp64_quartets": r.fp64_quartets, "mixed_steps": r.mixed_steps,
            "seconds_fock": r.seconds_fock, "seconds_eigen": r.seconds_eigen, "seconds_diis": r.seconds_diis,
-           "seconds_total": r.seconds_total, "seconds_init": r.seconds_init}
+           "seconds_total": r.seconds_total, "seconds_init": r.seconds_init, "mp2_energy": r.mp2_energy}
     if dens is not None:
         n = r.nbf
         if unrestricted:

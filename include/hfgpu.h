@@ -198,13 +198,34 @@ hfg_status hfg_fock_uhf_batch_device(hfg_ctx *ctx, const double *dPa, const doub
 hfg_status hfg_one_electron(const hfg_shells *shells, const double *xyz, const int32_t *Z, int32_t natoms,
                             int32_t device, double *S, double *T, double *V);
 
+/* AO -> MO transform for the post-HF consumers (no allocation-free form):
+ * dX receives the (ia|jb) block, i in [i0, i0+ni), a in [a0, a0+na), as a
+ * row-major (ni*na) x (ni*na) matrix with row i*na + a, from the MO
+ * coefficients dC (device, row-major nbf x nbf: AO rows, MO columns, the
+ * reference's C).  Replaces MolecularOrbitalsIntegralsRepository::
+ * getElectronElectron (IntegralsRepository.h:190-291) for that block.  Uses
+ * the context's stored-mode table (its screening and ERI convention),
+ * unpacked on the device: needs about 9/8 nbf^4 doubles free, else
+ * HFG_OOM_BUDGET.  Single-molecule contexts only. */
+hfg_status hfg_mo_eri_ovov(hfg_ctx *ctx, const double *dC, int32_t i0, int32_t ni, int32_t a0, int32_t na, double *dX,
+                           void *stream);
+/* RHF MP2 correlation energy from host C (row-major nbf x nbf) and orbital
+ * energies eps[nbf], the lowest nocc orbitals occupied:
+ * sum (ia|jb)[2(ia|jb) - (ib|ja)] / (e_i + e_j - e_a - e_b).  Replaces
+ * RestrictedHartreeFock::CalculateMp2Energy (RestrictedHartreeFock.cpp:251-288). */
+hfg_status hfg_mp2_rhf(hfg_ctx *ctx, const double *C, const double *eps, int32_t nocc, double *e_mp2);
+
 /* Eigen-decomposition of `batch` symmetric n x n matrices (device, FP64,
- * contiguous) in one batched cuSOLVER call on `stream`: dW receives batch x n
- * ascending eigenvalues, dV batch x n x n eigenvectors with eigenvector k of
- * matrix b in row k of block b (dV may equal dA).  The batched SCF's
+ * contiguous) on `stream`: dW receives batch x n ascending eigenvalues, dV
+ * batch x n x n eigenvectors with eigenvector k of matrix b in row k of block
+ * b (dV may equal dA).  method 0: one batched cuSOLVER call (Jacobi);
+ * method 1: one divide-and-conquer solve (dsyevd) per matrix, the solver of
+ * the single-molecule SCF -- within a degenerate level the two return
+ * different bases, which decides the occupied orbitals of open shells.  The batched SCF's
  * counterpart of the per-molecule Eigen::SelfAdjointEigenSolver step
  * (RestrictedHartreeFock.cpp:121-124).  Workspace is kept per host thread. */
-hfg_status hfg_eigh_batched(const double *dA, double *dV, double *dW, int32_t n, int32_t batch, void *stream);
+hfg_status hfg_eigh_batched(const double *dA, double *dV, double *dW, int32_t n, int32_t batch, int32_t method,
+                            void *stream);
 
 /* Allocation-free variant of hfg_fock_rhf_device, for callers that must not
  * allocate device memory while they run: a serving loop under a fixed HBM

@@ -37,6 +37,8 @@ typedef struct {
   int32_t stop_at_precision_test; /* plain builds, precision form's stopping rule */
   int32_t max_iterations;    /* the algorithm's iteration cap; 0 = 3000, the
                                 reference's default (RestrictedHartreeFock.h:31) */
+  int32_t mp2;               /* 1: RHF MP2 energy after the SCF (result.mp2_energy) */
+  int32_t reserved;
 } hfd_scf_opts;
 
 typedef struct {
@@ -54,6 +56,7 @@ typedef struct {
   /* wall-clock split of the SCF (seconds) */
   double seconds_fock, seconds_eigen, seconds_diis, seconds_total;
   double seconds_init;       /* Init: one-electron matrices, engine context, S^-1/2 */
+  double mp2_energy;         /* RestrictedHartreeFock::CalculateMp2Energy when opts.mp2 */
 } hfd_scf_result;
 
 void hfd_default_scf_opts(hfd_scf_opts *o);

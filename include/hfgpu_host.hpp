@@ -247,6 +247,8 @@ class HartreeFockAlgorithm {
   double Calculate();
   virtual double Step(int iter) = 0;
   double GetTotalEnergy() const { return totalEnergy; }
+  double GetMP2Energy() const { return mp2Energy; }  // HartreeFockAlgorithm.h:89-92
+  double mp2Energy = 0;
 
  protected:
   double totalEnergy;
@@ -294,6 +296,9 @@ class RestrictedHartreeFock : public HartreeFockAlgorithm {
   explicit RestrictedHartreeFock(int iterations = 3000) : HartreeFockAlgorithm(iterations) {}
   void Init(Systems::Molecule *molecule) override;
   double Step(int iter) override;
+  // RestrictedHartreeFock.cpp:251-288, after Calculate(): the (ia|jb)
+  // block by one device AO->MO transform (hfg_mp2_rhf)
+  double CalculateMp2Energy();
 
  protected:
   void SyncToDevice() override;

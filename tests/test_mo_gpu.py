@@ -1,0 +1,69 @@
+"""AO -> MO transform (hfg_mo_eri_ovov) and the RHF MP2 energy (hfg_mp2_rhf,
+RestrictedHartreeFock::CalculateMp2Energy) against a numpy restatement of
+RestrictedHartreeFock.cpp:251-288 over the oracle's packed ERI table."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from conftest import load_golden
+from hartreefock_b200 import engine as E
+from hartreefock_b200 import scf
+from hartreefock_b200.basis_io import basis_path
+
+pytestmark = pytest.mark.gpu
+
+
+def full_eri(packed, n):
+    idx = np.arange(n)
+    ij = np.where(idx[:, None] >= idx[None, :], idx[:, None] * (idx[:, None] + 1) // 2 + idx[None, :],
+                  idx[None, :] * (idx[None, :] + 1) // 2 + idx[:, None])
+    a, b = ij[:, :, None, None], ij[None, None, :, :]
+    return packed[np.where(a >= b, a * (a + 1) // 2 + b, b * (b + 1) // 2 + a)]
+
+
+def mp2_numpy(eri, C, eps, nocc):
+    Co, Cv = C[:, :nocc], C[:, nocc:]
+    ovov = np.einsum("mnls,mi,na,lj,sb->iajb", eri, Co, Cv, Co, Cv, optimize=True)
+    eo, ev = eps[:nocc], eps[nocc:]
+    d = eo[:, None, None, None] - ev[None, :, None, None] + eo[None, None, :, None] - ev[None, None, None, :]
+    return float(np.sum(ovov * (2 * ovov - ovov.transpose(0, 3, 2, 1)) / d)), ovov
+
+
+def _setup(name="h2o_631gs"):
+    g = load_golden(name)
+    Z, xyz, basis = list(g["Z"]), g["xyz"], str(g["basis"])
+    eng = E.Engine(Z, xyz, basis, schwarz_threshold=0.0)
+    mol = O.Molecule(Z, xyz, basis_path(basis))
+    return eng, full_eri(O.eri_packed(mol), mol.nbf), mol
+
+
+def test_mo_block_and_mp2_on_random_orbitals():
+    eng, eri, mol = _setup()
+    n, nocc = mol.nbf, 5
+    rng = np.random.default_rng(4)
+    C, _ = np.linalg.qr(rng.normal(size=(n, n)))
+    eps = np.concatenate([np.sort(rng.uniform(-20, -0.3, nocc)), np.sort(rng.uniform(0.2, 5, n - nocc))])
+    want, ovov = mp2_numpy(eri, C, eps, nocc)
+    got = eng.mp2_rhf(C, eps, nocc)
+    assert abs(got - want) <= 1e-11 * max(1.0, abs(want))
+    X = eng.mo_eri_ovov_tensor(torch.from_numpy(C).cuda(), 0, nocc, nocc, n - nocc).cpu().numpy()
+    assert np.abs(X - ovov.reshape(nocc * (n - nocc), -1)).max() < 1e-11
+    # twice in a row: no state carried between calls
+    assert eng.mp2_rhf(C, eps, nocc) == pytest.approx(got, abs=1e-13)
+
+
+def test_scf_mp2_matches_canonical_orbitals_of_the_converged_density():
+    g = load_golden("h2o_sto3g")
+    Z, xyz = list(g["Z"]), g["xyz"]
+    r = scf.run_scf(Z, xyz, "sto-3g", alpha=0.5, init_guess=0.0, schwarz_threshold=0.0, mp2=True)
+    mol = O.Molecule(Z, xyz, basis_path("sto-3g"))
+    n, packed = mol.nbf, O.eri_packed(mol)
+    S, T, V = O.one_electron(mol)
+    F = T + V + O.g_rhf(n, packed, r["density"])
+    s, U = np.linalg.eigh(S)
+    X = U @ np.diag(s ** -0.5) @ U.T
+    eps, Cp = np.linalg.eigh(X @ F @ X)
+    want, _ = mp2_numpy(full_eri(packed, n), X @ Cp, eps, 5)
+    assert want < 0
+    assert abs(r["mp2_energy"] - want) < 1e-8, (r["mp2_energy"], want)
