@@ -303,6 +303,7 @@ def main():
     ap.add_argument("--scf-waters", type=int, default=SCF_WATERS, help="cluster of the SCF comparison (0: skip)")
     ap.add_argument("--serve-jobs", type=int, default=24, help="jobs of the serving stream (0: skip)")
     ap.add_argument("--batch-mols", type=int, default=0, help="molecules of the batched SCF (0: skip)")
+    ap.add_argument("--no-autotune", action="store_true", help="fixed grid (4 blocks per SM) for every class")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     WATERS = args.waters
@@ -337,6 +338,8 @@ def main():
     torch.cuda.synchronize()
     stats_full = eng.stats()
     G_full = dG.clone()
+    # grid per class from the autotuner (timed on this density, before warm-up)
+    grids = eng.autotune(dP) if not args.no_autotune else {}
     # N > 1: every rank builds its shard of each class's tasks, one NCCL
     # all-reduce of G per build (hartreefock_b200/shards.py)
     sf = None
@@ -427,6 +430,7 @@ def main():
                    "schwarz_threshold": THRESHOLD, "shell_quartets": stats_full["shell_quartets"],
                    "function_quartets": stats_full["function_quartets"],
                    "l2": "flushed (256 MB write) between steps",
+                   "grid_blocks_per_sm": grids or "fixed 4",
                    "parallelism": f"task shards x{world}, one NCCL all-reduce of G per build" if world > 1
                    else "single GPU"},
         "e2e": {"value": e2e, "unit": "quartets/s", "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": n * n * 8},

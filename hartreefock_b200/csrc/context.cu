@@ -125,6 +125,7 @@ struct hfg_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int num_sms = 148;
   int blocks_per_sm = 4;  // grid cap of the fused class kernels, in blocks per SM
+  int tuned_bps[kNumClasses] = {};  // per class, from hfg_autotune (0 = blocks_per_sm)
   // device tables
   PrimPair *d_prim = nullptr;
   PrimPairF *d_primf = nullptr;
@@ -329,7 +330,8 @@ static int grid_for(const hfg_ctx *c, int ntasks, int cls) {
   const ClassEntry &e = kClasses[cls];
   const int w = fused_warps(e.la, e.lb, e.lc, e.ld);
   const int blocks = (ntasks + w - 1) / w;
-  return std::max(1, std::min(blocks, c->num_sms * c->blocks_per_sm));
+  const int bps = c->tuned_bps[cls] > 0 ? c->tuned_bps[cls] : c->blocks_per_sm;
+  return std::max(1, std::min(blocks, c->num_sms * bps));
 }
 
 // A class launch over all tasks, or with `sharded` over this context's
@@ -1240,6 +1242,64 @@ hfg_status hfg_set_mixed_cutoff(hfg_ctx *c, double cutoff) {
   if (!c) return hfg::fail(HFG_INVALID_ARG, "null context");
   if (!(cutoff >= 0) || !(cutoff < 1e300)) return hfg::fail(HFG_INVALID_ARG, "mixed cutoff must be finite and >= 0");
   c->mixed_cutoff = cutoff;
+  return HFG_OK;
+}
+
+// Grid autotuner: for every fused class with tasks, time the class's J/K
+// kernel at 1, 2, 4, 8 and 16 blocks per SM on the caller's density (one
+// warm-up and two timed launches each, CUDA events on the build stream) and
+// keep the fastest for the context's later builds.  Split classes keep
+// their fixed chunked launch.  The J/K scratch it writes is cleared by the
+// next build.
+hfg_status hfg_autotune(hfg_ctx *c, const double *dP, int32_t *chosen, int32_t cap, int32_t *count, void *stream) {
+  if (!c || !dP) return hfg::fail(HFG_INVALID_ARG, "null context or density");
+  using namespace hfg;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  const size_t tot = c->batch ? (size_t)c->batch_elems : (size_t)c->nbf * c->nbf;
+  hfg_status st;
+  if ((st = ensure(&c->d_J, tot)) != HFG_OK || (st = ensure(&c->d_Ka, tot)) != HFG_OK) return st;
+  if (c->batch) {
+    const std::vector<unsigned char> all(c->nmol, 1);
+    HFG_CUDA(cudaMemcpyAsync(c->d_mol_active, all.data(), c->nmol, cudaMemcpyHostToDevice, s));
+  }
+  const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
+  const int cand[] = {1, 2, 4, 8, 16};
+  int written = 0;
+  for (auto &q : c->qclasses) {
+    if (kSplit[q.cls] || q.tasks.empty()) continue;
+    ClassLaunch cl = base_launch(c, q, true);
+    if (cl.ntasks == 0) continue;
+    cl.Da = dP;
+    cl.Dt = dP;
+    cl.J = c->d_J;
+    cl.Ka = c->d_Ka;
+    float best = 1e30f;
+    int best_bps = c->blocks_per_sm;
+    for (int b : cand) {
+      c->tuned_bps[q.cls] = b;
+      const int grid = grid_for(c, cl.ntasks, q.cls);
+      kClasses[q.cls].launch(c->view(), cl, kJkRhf, ref, 0, grid, s);
+      HFG_CUDA(cudaEventRecord(c->ev0, s));
+      for (int r = 0; r < 2; ++r) kClasses[q.cls].launch(c->view(), cl, kJkRhf, ref, 0, grid, s);
+      HFG_CUDA(cudaEventRecord(c->ev1, s));
+      HFG_CUDA(cudaEventSynchronize(c->ev1));
+      HFG_CUDA(cudaGetLastError());
+      float ms = 0;
+      HFG_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+      if (ms < best) {
+        best = ms;
+        best_bps = b;
+      }
+    }
+    c->tuned_bps[q.cls] = best_bps;
+    if (chosen && written + 5 <= cap) {
+      const ClassEntry &e = kClasses[q.cls];
+      const int rec[5] = {e.la, e.lb, e.lc, e.ld, best_bps};
+      std::copy(rec, rec + 5, chosen + written);
+      written += 5;
+    }
+  }
+  if (count) *count = written / 5;
   return HFG_OK;
 }
 

@@ -28,7 +28,7 @@ EXPORTED = ["hfg_default_opts", "hfg_last_error", "hfg_device_count", "hfg_ctx_c
             "hfg_fock_rhf_noalloc", "hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental",
             "hfg_set_shard", "hfg_batch_create", "hfg_batch_size", "hfg_batch_layout", "hfg_fock_rhf_batch_device",
             "hfg_fock_uhf_batch_device", "hfg_eigh_batched", "hfg_one_electron",
-            "hfg_mo_eri_ovov", "hfg_mp2_rhf"]
+            "hfg_mo_eri_ovov", "hfg_mp2_rhf", "hfg_autotune"]
 
 
 class HfgError(RuntimeError):
@@ -122,6 +122,8 @@ def library(path: str = LIB_PATH):
     L.hfg_mo_eri_ovov.restype = ctypes.c_int
     L.hfg_mp2_rhf.argtypes = [vp, dp, dp, i32, ctypes.POINTER(ctypes.c_double)]
     L.hfg_mp2_rhf.restype = ctypes.c_int
+    L.hfg_autotune.argtypes = [vp, dp, vp, i32, ctypes.POINTER(i32), vp]
+    L.hfg_autotune.restype = ctypes.c_int
     for name in ("hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental", "hfg_set_shard", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak", "hfg_ctx_create", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet", "hfg_fock_rhf",
                  "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz", "hfg_ctx_stats"):
         getattr(L, name).restype = ctypes.c_int
@@ -156,6 +158,17 @@ def one_electron(Z, xyz, basis: str, device: int = 0):
     out = [np.zeros((t.nbf, t.nbf)) for _ in range(3)]
     _check(library().hfg_one_electron(ctypes.byref(sh), _ptr(x), _ptr(z), len(z), device, *[_ptr(o) for o in out]))
     return tuple(out)
+
+
+def _autotune(handle, P) -> dict:
+    import torch
+    dP = torch.as_tensor(np.asarray(P) if not isinstance(P, torch.Tensor) else P, dtype=torch.float64)
+    dP = dP.cuda().contiguous()
+    rec = np.zeros(5 * 32, dtype=np.int32)
+    n = ctypes.c_int32()
+    _check(library().hfg_autotune(handle, ctypes.c_void_p(dP.data_ptr()), _ptr(rec), len(rec), ctypes.byref(n),
+                                  ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    return {f"({r[0]}{r[1]}|{r[2]}{r[3]})": int(r[4]) for r in rec[:5 * n.value].reshape(-1, 5)}
 
 
 def eigh_batched(A, method: int = 0):
@@ -276,6 +289,11 @@ class Engine:
         _check(library().hfg_fock_uhf_device(self._h, ctypes.c_void_p(Pa_ptr), ctypes.c_void_p(Pb_ptr),
                                              ctypes.c_void_p(Ga_ptr), ctypes.c_void_p(Gb_ptr),
                                              ctypes.c_void_p(stream)))
+
+    def autotune(self, P) -> dict:
+        """Pick each fused class's grid (blocks per SM) by timing it on the
+        density P (numpy or torch CUDA tensor); returns {class: blocks/SM}."""
+        return _autotune(self._h, P)
 
     def mp2_rhf(self, C: np.ndarray, eps: np.ndarray, nocc: int) -> float:
         """RHF MP2 correlation energy (hfg_mp2_rhf) from MO coefficients C
@@ -398,6 +416,10 @@ class BatchEngine:
                                                    ctypes.c_void_p(Gb.data_ptr()), ap,
                                                    ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
         return Ga, Gb
+
+    def autotune(self, P) -> dict:
+        """Grid autotuner over the batch (P: flat density, batch layout)."""
+        return _autotune(self._h, P)
 
     def stats(self) -> dict:
         s = hfg_stats()

@@ -249,6 +249,14 @@ hfg_status hfg_schwarz(hfg_ctx *ctx, double *host_out, int64_t count);
 
 hfg_status hfg_ctx_stats(const hfg_ctx *ctx, hfg_stats *out);
 
+/* Grid autotuner (no reference counterpart): times every fused quartet
+ * class's J/K kernel at 1, 2, 4, 8 and 16 blocks per SM on the density dP
+ * (device; a flat batch buffer for batched contexts) and keeps the fastest
+ * grid per class for this context's later builds.  `chosen` (optional)
+ * receives up to cap/5 records (La, Lb, Lc, Ld, blocks per SM); *count the
+ * records written.  Costs about 15 launches per class. */
+hfg_status hfg_autotune(hfg_ctx *ctx, const double *dP, int32_t *chosen, int32_t cap, int32_t *count, void *stream);
+
 /* Per-class timing of the builds (no reference counterpart: instrumentation
  * for the roofline accounting).  With profiling on, every class launch of a
  * build is bracketed by CUDA events on the build's stream. */
