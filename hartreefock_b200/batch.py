@@ -6,10 +6,12 @@ per quartet class over all molecules' tasks) and the reference's SCF step
 all molecules at once in torch on the device: F = h + G, DIIS (keep 6, start
 at 5; DIIS.h:9-96), F' = V F V, batched eigensolve, new density, energy,
 mixing, the reference's convergence test per molecule.  Molecules that have
-converged drop out of the following builds (the engine's `active` mask).
-Matrices are padded to the largest molecule: a padded block carries a large
-diagonal shift in F', so its levels sort above every real one and are never
-occupied.  All FP64.
+converged drop out of the following builds (the engine's `active` mask), and
+once half of the working set has converged the torch state shrinks to the
+molecules still iterating (re-padded to the largest of them), so the cost of
+a step follows the active count.  Matrices are padded to the largest molecule
+of the working set: a padded block carries a large diagonal shift in F', so
+its levels sort above every real one and are never occupied.  All FP64.
 """
 from __future__ import annotations
 
@@ -42,15 +44,6 @@ class BatchSCF:
         self.nbf = self.eng.nbf.astype(np.int64)
         self.nmax = int(self.nbf.max())
         n = self.nmax
-        # flat (engine layout) <-> padded [M, n, n] index maps
-        rows, flat = [], []
-        for m in range(M):
-            k = int(self.nbf[m])
-            i, j = np.meshgrid(np.arange(k), np.arange(k), indexing="ij")
-            rows.append(m * n * n + i.ravel() * n + j.ravel())
-            flat.append(self.eng.offset[m] + i.ravel() * k + j.ravel())
-        self.pad_idx = torch.from_numpy(np.concatenate(rows)).to(self.dev)
-        self.flat_idx = torch.from_numpy(np.concatenate(flat)).to(self.dev)
         # one-electron matrices, S^-1/2, occupations, nuclear repulsion
         h = np.zeros((M, n, n))
         S = np.zeros((M, n, n))
@@ -83,45 +76,45 @@ class BatchSCF:
         self.V = 0.5 * (V + V.transpose(1, 2)) * mask2
         self.mask2 = mask2
         self.shift = torch.diag_embed((~valid).double() * PAD_SHIFT)
-        # eigensolver buckets: molecules grouped by their exact nbf, so each
-        # batched solve runs at the molecule's own size with no padded level
-        # in it (a large padded level would set the solver's tolerance
-        # relative to itself and cost the real levels digits)
-        self.buckets = [(int(b), np.nonzero(self.nbf == b)[0]) for b in np.unique(self.nbf)]
         # open shells: which orbital of a degenerate level gets the unpaired
         # electron depends on the solver's basis for that level, so UHF uses
         # the single-molecule SCF's per-matrix solver (same states as alone)
         self.eigh_method = 1 if unrestricted else 0
         self.seconds = {"fock": 0.0, "diis": 0.0, "eigh": 0.0, "total": 0.0}
 
-    # ---- flat <-> padded
-    def to_flat(self, X):
-        out = torch.zeros(self.eng.total, dtype=torch.float64, device=self.dev)
-        out[self.flat_idx] = X.reshape(-1)[self.pad_idx]
-        return out
+    # ---- the working set: molecules still iterating, padded to their largest
+    def _maps(self, W, n):
+        """flat (engine layout) <-> padded [len(W), n, n] index maps and the
+        eigensolver buckets of the working set W: molecules grouped by their
+        exact nbf, so each batched solve runs at the molecule's own size with
+        no padded level in it (a large padded level would set the solver's
+        tolerance relative to itself and cost the real levels digits)."""
+        rows, flat = [], []
+        for r, m in enumerate(W):
+            k = int(self.nbf[m])
+            i, j = np.meshgrid(np.arange(k), np.arange(k), indexing="ij")
+            rows.append(r * n * n + i.ravel() * n + j.ravel())
+            flat.append(self.eng.offset[m] + i.ravel() * k + j.ravel())
+        pad_idx = torch.from_numpy(np.concatenate(rows)).to(self.dev)
+        flat_idx = torch.from_numpy(np.concatenate(flat)).to(self.dev)
+        nb = self.nbf[W]
+        buckets = [(int(b), np.nonzero(nb == b)[0]) for b in np.unique(nb)]
+        return pad_idx, flat_idx, buckets
 
-    def to_pad(self, flat):
-        out = torch.zeros(self.M * self.nmax * self.nmax, dtype=torch.float64, device=self.dev)
-        out[self.pad_idx] = flat[self.flat_idx]
-        return out.reshape(self.M, self.nmax, self.nmax)
-
-    def _guess_fock(self):
-        h = self.h
+    def _guess_fock(self, h, S):
         if self.init_guess > 0:
             d = torch.diagonal(h, dim1=1, dim2=2)
-            F = self.init_guess * self.S * (d[:, :, None] + d[:, None, :]) * 0.5
-        else:
-            F = h.clone()
-        return F
+            return self.init_guess * S * (d[:, :, None] + d[:, None, :]) * 0.5
+        return h.clone()
 
-    def _eigh(self, Ft, active_np):
+    def _eigh(self, Ft, active_np, buckets):
         """Batched eigensolve of the active molecules, bucket by bucket
         (hfg_eigh_batched); levels of padded rows and of inactive molecules
         stay at PAD_SHIFT with unit vectors."""
-        M, n = self.M, self.nmax
-        w = torch.full((M, n), PAD_SHIFT, dtype=torch.float64, device=self.dev)
-        U = torch.eye(n, dtype=torch.float64, device=self.dev).expand(M, n, n).clone()
-        for b, idx in self.buckets:
+        Mw, n = Ft.shape[0], Ft.shape[1]
+        w = torch.full((Mw, n), PAD_SHIFT, dtype=torch.float64, device=self.dev)
+        U = torch.eye(n, dtype=torch.float64, device=self.dev).expand(Mw, n, n).clone()
+        for b, idx in buckets:
             sel = idx[active_np[idx] != 0]
             if len(sel) == 0:
                 continue
@@ -131,20 +124,26 @@ class BatchSCF:
             U[t, :b, :b] = Ub
         return w, U
 
-    def _occ_mask(self, spin):
-        return (torch.arange(self.nmax, device=self.dev)[None, :] <
-                torch.from_numpy(self.nocc[spin]).to(self.dev)[:, None]).double()
-
     def run(self):
-        M, n, dev = self.M, self.nmax, self.dev
+        M, dev = self.M, self.dev
         nspin = 2 if self.uhf else 1
+        # working set W (molecule ids) padded to n; it shrinks to the
+        # molecules still iterating once half of it has converged, so the
+        # per-step tensor work follows the active count
+        W, n = np.arange(M), self.nmax
+        h, S, V, shift = self.h, self.S, self.V, self.shift
+        nocc = self.nocc
+        enuc = torch.from_numpy(self.enuc).to(dev)
+        pad_idx, flat_idx, buckets = self._maps(W, n)
         P = [torch.zeros(M, n, n, dtype=torch.float64, device=dev) for _ in range(nspin)]
+        P_out = [torch.zeros(M, self.nmax, self.nmax, dtype=torch.float64, device=dev) for _ in range(nspin)]
         diisF = [[] for _ in range(nspin)]
         diisE = [[] for _ in range(nspin)]
         energy = torch.full((M,), float("inf"), dtype=torch.float64, device=dev)
+        iters = torch.zeros(M, dtype=torch.int64, device=dev)
+        converged = torch.zeros(M, dtype=torch.bool, device=dev)
         prev = torch.full((M,), float("inf"), dtype=torch.float64, device=dev)
         active = torch.ones(M, dtype=torch.bool, device=dev)
-        iters = torch.zeros(M, dtype=torch.int64, device=dev)
         flatG = [torch.zeros(self.eng.total, dtype=torch.float64, device=dev) for _ in range(nspin)]
         builds = 0
         sync = torch.cuda.synchronize if self.dev.type == "cuda" else (lambda: None)
@@ -153,34 +152,47 @@ class BatchSCF:
             sync()
             return time.perf_counter()
 
+        def to_flat(X):
+            out = torch.zeros(self.eng.total, dtype=torch.float64, device=dev)
+            out[flat_idx] = X.reshape(-1)[pad_idx]
+            return out
+
+        def to_pad(flat):
+            out = torch.zeros(len(W) * n * n, dtype=torch.float64, device=dev)
+            out[pad_idx] = flat[flat_idx]
+            return out.reshape(len(W), n, n)
+
         t_start = tick()
         for it in range(self.max_iter):
             act = active.clone()
             active_np = act.cpu().numpy().astype(np.uint8)
+            Wt = torch.from_numpy(W).to(dev)
             if it == 0:
-                F0 = self._guess_fock()
+                F0 = self._guess_fock(h, S)
                 F = [F0.clone() for _ in range(nspin)]
                 if self.uhf:  # UnrestrictedHartreeFock.cpp:214-219: asymmetry on the alpha guess
                     F[0][:, 0, 1] += 0.1
                     F[0][:, 1, 0] = F[0][:, 0, 1]
             else:
                 t0 = tick()
-                flatP = [self.to_flat(p) for p in P]
+                mask = np.zeros(M, dtype=np.uint8)
+                mask[W] = active_np
+                flatP = [to_flat(p) for p in P]
                 if self.uhf:
-                    self.eng.fock_uhf(flatP[0], flatP[1], flatG[0], flatG[1], active=active_np)
+                    self.eng.fock_uhf(flatP[0], flatP[1], flatG[0], flatG[1], active=mask)
                 else:
-                    self.eng.fock_rhf(flatP[0], flatG[0], active=active_np)
+                    self.eng.fock_rhf(flatP[0], flatG[0], active=mask)
                 builds += 1
-                F = [self.h + self.to_pad(g) for g in flatG]
+                F = [h + to_pad(g) for g in flatG]
                 self.seconds["fock"] += tick() - t0
             if not self.uhf:
                 F = [0.5 * (f + f.transpose(1, 2)) for f in F]
-            used = torch.zeros(M, dtype=torch.bool, device=dev)
-            err_est = torch.zeros(M, dtype=torch.float64, device=dev)
+            used = torch.zeros(len(W), dtype=torch.bool, device=dev)
+            err_est = torch.zeros(len(W), dtype=torch.float64, device=dev)
             t0 = tick()
             if self.use_diis and it > 0:
                 for s in range(nspin):
-                    err = self.S @ P[s] @ F[s] - F[s] @ P[s] @ self.S
+                    err = S @ P[s] @ F[s] - F[s] @ P[s] @ S
                     diisF[s].append(F[s].clone())
                     diisE[s].append(err)
                     if len(diisF[s]) > 6:
@@ -194,40 +206,62 @@ class BatchSCF:
             self.seconds["diis"] += t1 - t0
             Pn, eps = [], []
             for s in range(nspin):
-                Ft = self.V @ F[s] @ self.V + self.shift
-                w, Cp = self._eigh(Ft, active_np)
+                Ft = V @ F[s] @ V + shift
+                w, Cp = self._eigh(Ft, active_np, buckets)
                 self.seconds["eigh"] += tick() - t1
                 t1 = tick()
-                C = self.V @ Cp
-                occ = self._occ_mask(s)
+                C = V @ Cp
+                occ = (torch.arange(n, device=dev)[None, :] <
+                       torch.from_numpy(nocc[s][W]).to(dev)[:, None]).double()
                 factor = 1.0 if self.uhf else 2.0
                 Co = C * occ[:, None, :]
                 Pn.append(factor * Co @ Co.transpose(1, 2))
                 eps.append((w * occ).sum(1))
             if self.uhf:
-                e = 0.5 * (((Pn[0] + Pn[1]) * self.h).sum((1, 2)) + eps[0] + eps[1])
+                e = 0.5 * (((Pn[0] + Pn[1]) * h).sum((1, 2)) + eps[0] + eps[1])
             else:
-                e = 0.5 * (Pn[0] * self.h).sum((1, 2)) + eps[0]
-            e = e + torch.from_numpy(self.enuc).to(dev)
+                e = 0.5 * (Pn[0] * h).sum((1, 2)) + eps[0]
+            e = e + enuc[Wt]
             rms = torch.sqrt(sum(((pn - p) ** 2).sum((1, 2)) for pn, p in zip(Pn, P)))
             for s in range(nspin):
                 mix = torch.where(used[:, None, None], Pn[s], self.alpha * Pn[s] + (1 - self.alpha) * P[s])
                 P[s] = torch.where(act[:, None, None], mix, P[s])
-            energy = torch.where(act, e, energy)
-            dE = (prev - e).abs()
+            energy[Wt] = torch.where(act, e, energy[Wt])
+            dE = (prev[Wt] - e).abs()
             econv = E_CONV_DIIS if self.use_diis else E_CONV
             conv = (dE <= econv) & (rms < RMS_CONV) & (err_est < DIIS_CONV)
-            iters = torch.where(act, iters + 1, iters)
-            prev = torch.where(act, e, prev)
+            iters[Wt] = torch.where(act, iters[Wt] + 1, iters[Wt])
+            prev[Wt] = torch.where(act, e, prev[Wt])
+            converged[Wt] = converged[Wt] | (act & conv)
             active = act & ~conv
-            if not bool(active.any()):
+            n_active = int(active.sum())
+            if n_active == 0:
                 break
+            if n_active <= len(W) // 2:  # compact the working set
+                for s in range(nspin):
+                    P_out[s][Wt, :n, :n] = P[s]
+                keep = active.cpu().numpy().astype(bool)
+                kt = torch.from_numpy(np.nonzero(keep)[0]).to(dev)
+                W = W[keep]
+                n_new = int(self.nbf[W].max())
+                sl = (slice(None), slice(0, n_new), slice(0, n_new))
+                P = [p[kt][sl] for p in P]
+                diisF = [[x[kt][sl] for x in lst] for lst in diisF]
+                diisE = [[x[kt][sl] for x in lst] for lst in diisE]
+                Wt_new = torch.from_numpy(W).to(dev)
+                h, S, V, shift = (t[Wt_new][sl].contiguous() for t in (self.h, self.S, self.V, self.shift))
+                active = active[kt]
+                n = n_new
+                pad_idx, flat_idx, buckets = self._maps(W, n)
+        Wt = torch.from_numpy(W).to(dev)
+        for s in range(nspin):
+            P_out[s][Wt, :n, :n] = P[s]
         self.seconds["total"] = tick() - t_start
         self.iterations = iters.cpu().numpy()
-        self.converged = (~active).cpu().numpy()
+        self.converged = converged.cpu().numpy()
         self.builds = builds
         self.energies = energy.cpu().numpy()
-        self.densities = P
+        self.densities = P_out
         return self.energies
 
 

@@ -159,6 +159,11 @@ struct hfg_ctx {
   int *d_pair_mol = nullptr, *d_mol_nbf = nullptr;
   long long *d_mol_off = nullptr;
   unsigned char *d_mol_active = nullptr;
+  // batched builds with converged molecules: the active molecules' tasks of
+  // every class, compacted on the device, and their counts
+  Task *d_task_active = nullptr;
+  int *d_task_counts = nullptr;
+  std::vector<int> task_base;  // per quartet class, offset into d_task_active
   hfg_stats stats{};
   bool profiling = false;
   bool precision_form() const { return opts.density_screening || opts.incremental || mixed_cutoff > 0; }
@@ -202,7 +207,8 @@ struct hfg_ctx {
                     d_pair_AB,    d_pair_Q,        d_boys,       d_J,        d_Ka,         d_Kb,        d_P,
                     d_Pb,         d_Pt,            d_G,          d_Gb,       d_block,      d_scratch,   d_shell_ao,
                     d_shell_nf,   d_shell_dmax,    d_counters,   d_prev_P[0], d_prev_P[1], d_prev_G[0], d_prev_G[1],
-                    d_dP[0],      d_dP[1],         d_primf,      d_pair_mol, d_mol_nbf,    d_mol_off,   d_mol_active};
+                    d_dP[0],      d_dP[1],         d_primf,      d_pair_mol, d_mol_nbf,    d_mol_off,   d_mol_active,
+                    d_task_active, d_task_counts};
     for (void *b : bufs) cudaFree(b);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -604,6 +610,29 @@ __global__ void finalize_uhf_batch(const double *J, const double *Ka, const doub
   }
 }
 
+// Tasks of active molecules, in the class's order up to warp-sized groups:
+// each warp writes its kept tasks as one contiguous run (ballot + one
+// atomic per warp).
+__global__ void compact_active_tasks(const Task *__restrict__ tasks, int ntasks, const int *__restrict__ bra_list,
+                                     const int *__restrict__ pair_mol, const unsigned char *__restrict__ active,
+                                     Task *__restrict__ out, int *count) {
+  const int lane = threadIdx.x & 31;
+  for (int base = (blockIdx.x * blockDim.x + threadIdx.x) & ~31; base < ntasks; base += gridDim.x * blockDim.x) {
+    const int t = base + lane;
+    bool keep = false;
+    Task tk{};
+    if (t < ntasks) {
+      tk = tasks[t];
+      keep = active[pair_mol[bra_list[tk.bra_pos]]] != 0;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    int at = 0;
+    if (lane == 0 && m) at = atomicAdd(count, __popc(m));
+    at = __shfl_sync(0xffffffffu, at, 0);
+    if (keep) out[at + __popc(m & ((1u << lane) - 1))] = tk;
+  }
+}
+
 // Direct J/K build of a batched context: one launch per quartet class over
 // the tasks of all molecules (inactive molecules' tasks exit at once), then
 // G per active molecule.  `active`: host flags per molecule, or null = all.
@@ -623,11 +652,55 @@ static hfg_status batch_build(hfg_ctx *c, bool uhf, const double *dPa, const dou
     add_densities<<<std::max(1, std::min(1024, (int)((tot + 255) / 256))), 256, 0, s>>>(dPa, dPb, c->d_Pt, (int)tot);
     launches += 2;
   }
+  // with converged molecules, launch over the active molecules' tasks only
+  // (compacted on the device; one sync for the counts) instead of letting
+  // every warp read and skip the others'
+  bool compact = false;
+  std::vector<int> counts;
+  if (active && c->shard_count == 1) {
+    int nact = 0;
+    for (int m = 0; m < c->nmol; ++m) nact += active[m] != 0;
+    compact = nact < c->nmol;
+  }
+  if (compact) {
+    const size_t nq = c->qclasses.size();
+    if (!c->d_task_active) {
+      size_t total = 0;
+      c->task_base.assign(nq, 0);
+      for (size_t i = 0; i < nq; ++i) {
+        c->task_base[i] = (int)total;
+        total += c->qclasses[i].tasks.size();
+      }
+      HFG_CUDA(cudaMalloc((void **)&c->d_task_active, std::max<size_t>(1, total) * sizeof(Task)));
+      HFG_CUDA(cudaMalloc((void **)&c->d_task_counts, std::max<size_t>(1, nq) * sizeof(int)));
+    }
+    HFG_CUDA(cudaMemsetAsync(c->d_task_counts, 0, nq * sizeof(int), s));
+    for (size_t i = 0; i < nq; ++i) {
+      const QuartetClass &q = c->qclasses[i];
+      const int nt = (int)q.tasks.size();
+      if (nt == 0) continue;
+      const int grid = std::max(1, std::min(c->num_sms * 8, (nt + 255) / 256));
+      compact_active_tasks<<<grid, 256, 0, s>>>(q.d_tasks, nt, c->pclass[q.bra_pc].d_pairs, c->d_pair_mol,
+                                                c->d_mol_active, c->d_task_active + c->task_base[i],
+                                                c->d_task_counts + i);
+      ++launches;
+    }
+    counts.assign(nq, 0);
+    HFG_CUDA(cudaMemcpyAsync(counts.data(), c->d_task_counts, nq * sizeof(int), cudaMemcpyDeviceToHost, s));
+    HFG_CUDA(cudaStreamSynchronize(s));
+  }
   HFG_CUDA(cudaEventRecord(c->ev0, s));
   const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
   c->stats = hfg_stats{};
-  for (auto &q : c->qclasses) {
+  for (size_t qi = 0; qi < c->qclasses.size(); ++qi) {
+    auto &q = c->qclasses[qi];
     ClassLaunch cl = base_launch(c, q, true);
+    if (compact) {
+      cl.tasks = c->d_task_active + c->task_base[qi];
+      cl.task_offset = 0;
+      cl.task_stride = 1;
+      cl.ntasks = counts[qi];
+    }
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_a, s));
     cl.Da = dPa;
     cl.Db = dPb;
