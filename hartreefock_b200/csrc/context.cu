@@ -123,9 +123,31 @@ struct hfg_ctx {
   std::vector<QuartetClass> qclasses;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // class kernels of one build are independent (J/K by atomics): they run on
+  // the build stream and kAux more, forked and joined by events, so small
+  // molecules' classes overlap instead of queueing
+  static constexpr int kAux = 3;
+  cudaStream_t aux[kAux] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[kAux] = {};
   int num_sms = 148;
   int blocks_per_sm = 4;  // grid cap of the fused class kernels, in blocks per SM
   int tuned_bps[kNumClasses] = {};  // per class, from hfg_autotune (0 = blocks_per_sm)
+  // CUDA graph of the plain direct build (hfg_set_graphs): captured on the
+  // second build with the same buffers, stream and settings, replayed after
+  bool use_graphs = false;
+  unsigned config_version = 0;  // bumped by every setter that changes a build
+  struct GraphKey {
+    bool uhf = false;
+    const void *pa = nullptr, *pb = nullptr, *ga = nullptr, *gb = nullptr, *s = nullptr;
+    unsigned version = 0;
+    bool operator==(const GraphKey &o) const {
+      return uhf == o.uhf && pa == o.pa && pb == o.pb && ga == o.ga && gb == o.gb && s == o.s && version == o.version;
+    }
+  };
+  GraphKey graph_key, graph_seen;
+  bool graph_seen_valid = false;
+  cudaGraphExec_t graph_exec = nullptr;
+  hfg_stats graph_stats{};
   // device tables
   PrimPair *d_prim = nullptr;
   PrimPairF *d_primf = nullptr;
@@ -210,6 +232,12 @@ struct hfg_ctx {
                     d_dP[0],      d_dP[1],         d_primf,      d_pair_mol, d_mol_nbf,    d_mol_off,   d_mol_active,
                     d_task_active, d_task_counts};
     for (void *b : bufs) cudaFree(b);
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    for (int i = 0; i < kAux; ++i) {
+      if (aux[i]) cudaStreamDestroy(aux[i]);
+      if (ev_join[i]) cudaEventDestroy(ev_join[i]);
+    }
+    if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -446,6 +474,38 @@ static int ncomp_range(int lo, int hi) {
   return s;
 }
 
+// Fork / join of a build's class launches over the build stream and the
+// context's auxiliary streams.  Split classes share one scratch buffer, so
+// they all go to the first auxiliary stream, one after another; fused
+// classes take the build stream and the other auxiliary streams in turn.
+// Off (everything on the build stream) while per-class profiling is on.
+struct ClassStreams {
+  hfg_ctx *c;
+  cudaStream_t s;
+  bool on;
+  int next = 0;
+  hfg_status fork() {
+    if (!on) return HFG_OK;
+    HFG_CUDA(cudaEventRecord(c->ev_fork, s));
+    for (int i = 0; i < hfg_ctx::kAux; ++i) HFG_CUDA(cudaStreamWaitEvent(c->aux[i], c->ev_fork, 0));
+    return HFG_OK;
+  }
+  cudaStream_t pick(bool split) {
+    if (!on) return s;
+    if (split) return c->aux[0];
+    const int k = next++ % hfg_ctx::kAux;  // 0 = build stream, then aux[1..]
+    return k == 0 ? s : c->aux[k];
+  }
+  hfg_status join() {
+    if (!on) return HFG_OK;
+    for (int i = 0; i < hfg_ctx::kAux; ++i) {
+      HFG_CUDA(cudaEventRecord(c->ev_join[i], c->aux[i]));
+      HFG_CUDA(cudaStreamWaitEvent(s, c->ev_join[i], 0));
+    }
+    return HFG_OK;
+  }
+};
+
 // `prec`: 0 plain FP64, 1 density-screened FP64, 2 density-screened with
 // the per-task FP64/FP32 choice (the precision form).
 static hfg_status launch_class(hfg_ctx *c, const QuartetClass &q, const ClassLaunch &cl, int mode, bool ref,
@@ -486,8 +546,8 @@ static hfg_status launch_class(hfg_ctx *c, const QuartetClass &q, const ClassLau
 // full density; the precision form (see hfg_opts) first forms the density
 // difference (incremental), the shell-block maxima for the density
 // screening, and accumulates G onto the previous one.
-static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const double *dPb, double *dGa, double *dGb,
-                               cudaStream_t s) {
+static hfg_status direct_build_body(hfg_ctx *c, bool uhf, const double *dPa, const double *dPb, double *dGa,
+                                    double *dGb, cudaStream_t s, bool capturing) {
   if (c->batch) return fail(HFG_INVALID_ARG, "batched context: use hfg_fock_rhf/uhf_batch_device");
   const size_t nn = (size_t)c->nbf * c->nbf;
   const int n = c->nbf;
@@ -530,7 +590,9 @@ static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const do
     add_densities<<<256, 256, 0, s>>>(Da, Db, c->d_Pt, (int)nn);
     launches += 2;
   }
-  HFG_CUDA(cudaEventRecord(c->ev0, s));
+  if (!capturing) HFG_CUDA(cudaEventRecord(c->ev0, s));
+  ClassStreams cs{c, s, !c->profiling};
+  if ((st = cs.fork()) != HFG_OK) return st;
   const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
   const int prec = !precise ? 0 : c->mixed_cutoff > 0 ? 2 : 1;
   c->stats = hfg_stats{};
@@ -547,7 +609,7 @@ static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const do
     cl.mixed_cutoff = (float)c->mixed_cutoff;
     cl.counters = precise ? c->d_counters : nullptr;
     if (cl.ntasks > 0) {
-      st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, prec, s, &launches);
+      st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, prec, cs.pick(kSplit[q.cls] != nullptr), &launches);
       if (st != HFG_OK) return st;
     }
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_b, s));
@@ -559,7 +621,8 @@ static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const do
     c->stats.flops += share * q.flops;
   }
   HFG_CUDA(cudaGetLastError());
-  HFG_CUDA(cudaEventRecord(c->ev1, s));
+  if ((st = cs.join()) != HFG_OK) return st;
+  if (!capturing) HFG_CUDA(cudaEventRecord(c->ev1, s));
   const int fg = std::max(1, std::min(1024, (int)((nn + 255) / 256)));
   if (incremental) {
     if (uhf)
@@ -581,6 +644,54 @@ static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const do
   c->counted = precise;
   if (!precise) c->stats.fp64_shell_quartets = c->stats.shell_quartets;
   return HFG_OK;
+}
+
+// Direct build, through a CUDA graph where it can be: the plain form (no
+// profiling, a created stream) with graphs on.  The first build with given
+// buffers, stream and settings runs normally (and sizes every buffer); the
+// second is captured and instantiated; later ones replay the graph.  Any
+// change of buffers, stream or settings starts over.
+static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const double *dPb, double *dGa, double *dGb,
+                               cudaStream_t s) {
+  const bool graphable = c->use_graphs && !c->batch && !c->precision_form() && !c->profiling && s != nullptr &&
+                         s != cudaStreamLegacy && s != cudaStreamPerThread;
+  if (!graphable) return direct_build_body(c, uhf, dPa, dPb, dGa, dGb, s, false);
+  hfg_ctx::GraphKey key;
+  key.uhf = uhf;
+  key.pa = dPa;
+  key.pb = dPb;
+  key.ga = dGa;
+  key.gb = dGb;
+  key.s = s;
+  key.version = c->config_version;
+  if (!(c->graph_exec && c->graph_key == key) && c->graph_seen_valid && c->graph_seen == key) {
+    if (c->graph_exec) {
+      cudaGraphExecDestroy(c->graph_exec);
+      c->graph_exec = nullptr;
+    }
+    HFG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const hfg_status st = direct_build_body(c, uhf, dPa, dPb, dGa, dGb, s, true);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (st == HFG_OK && e == cudaSuccess && g) {
+      if (cudaGraphInstantiate(&c->graph_exec, g, 0) != cudaSuccess) c->graph_exec = nullptr;
+      c->graph_key = key;
+      c->graph_stats = c->stats;
+    }
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();  // a failed capture leaves nothing behind: build normally below
+    if (st != HFG_OK) return st;
+  }
+  if (c->graph_exec && c->graph_key == key) {
+    HFG_CUDA(cudaEventRecord(c->ev0, s));
+    HFG_CUDA(cudaGraphLaunch(c->graph_exec, s));
+    HFG_CUDA(cudaEventRecord(c->ev1, s));
+    c->stats = c->graph_stats;
+    return HFG_OK;
+  }
+  c->graph_seen = key;
+  c->graph_seen_valid = true;
+  return direct_build_body(c, uhf, dPa, dPb, dGa, dGb, s, false);
 }
 
 // Batched contexts: G of every active molecule, blockIdx.y = molecule.
@@ -690,6 +801,8 @@ static hfg_status batch_build(hfg_ctx *c, bool uhf, const double *dPa, const dou
     HFG_CUDA(cudaStreamSynchronize(s));
   }
   HFG_CUDA(cudaEventRecord(c->ev0, s));
+  ClassStreams cs{c, s, !c->profiling};
+  if ((st = cs.fork()) != HFG_OK) return st;
   const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
   c->stats = hfg_stats{};
   for (size_t qi = 0; qi < c->qclasses.size(); ++qi) {
@@ -709,7 +822,7 @@ static hfg_status batch_build(hfg_ctx *c, bool uhf, const double *dPa, const dou
     cl.Ka = c->d_Ka;
     cl.Kb = c->d_Kb;
     if (cl.ntasks > 0) {
-      st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, 0, s, &launches);
+      st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, 0, cs.pick(kSplit[q.cls] != nullptr), &launches);
       if (st != HFG_OK) return st;
     }
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_b, s));
@@ -719,6 +832,7 @@ static hfg_status batch_build(hfg_ctx *c, bool uhf, const double *dPa, const dou
     c->stats.flops += q.flops;
   }
   HFG_CUDA(cudaGetLastError());
+  if ((st = cs.join()) != HFG_OK) return st;
   HFG_CUDA(cudaEventRecord(c->ev1, s));
   int nmax = 0;
   for (int n : c->mol_nbf) nmax = std::max(nmax, n);
@@ -832,6 +946,7 @@ static hfg_status create_context(const hfg_shells *sh, const int *shell_mol, int
   ctx->device = ctx->opts.device;
   HFG_CUDA(cudaSetDevice(ctx->device));
   HFG_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  ctx->use_graphs = ctx->opts.cuda_graphs != 0;
   // tuning: HFG_BLOCKS_PER_SM overrides the grid cap (every block stages the
   // class's Boys table once, so fewer, longer-lived blocks stage it less)
   if (const char *e = std::getenv("HFG_BLOCKS_PER_SM")) ctx->blocks_per_sm = std::max(1, std::atoi(e));
@@ -980,6 +1095,11 @@ static hfg_status create_context(const hfg_shells *sh, const int *shell_mol, int
   HFG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   HFG_CUDA(cudaEventCreate(&ctx->ev0));
   HFG_CUDA(cudaEventCreate(&ctx->ev1));
+  HFG_CUDA(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+  for (int i = 0; i < hfg_ctx::kAux; ++i) {
+    HFG_CUDA(cudaStreamCreateWithFlags(&ctx->aux[i], cudaStreamNonBlocking));
+    HFG_CUDA(cudaEventCreateWithFlags(&ctx->ev_join[i], cudaEventDisableTiming));
+  }
 
   // ---- Schwarz bounds per pair class
   std::vector<std::vector<int>> by_class(kNumPairClasses);
@@ -1273,6 +1393,7 @@ hfg_status hfg_set_profiling(hfg_ctx *c, int32_t on) {
     if (!q.ev_b) HFG_CUDA(cudaEventCreate(&q.ev_b));
   }
   c->profiling = on != 0;
+  ++c->config_version;
   return HFG_OK;
 }
 
@@ -1308,6 +1429,7 @@ hfg_status hfg_ctx_stats(const hfg_ctx *c, hfg_stats *out) {
 hfg_status hfg_fock_reset(hfg_ctx *c) {
   if (!c) return hfg::fail(HFG_INVALID_ARG, "null context");
   c->inc_valid = false;
+  ++c->config_version;
   return HFG_OK;
 }
 
@@ -1315,6 +1437,7 @@ hfg_status hfg_set_mixed_cutoff(hfg_ctx *c, double cutoff) {
   if (!c) return hfg::fail(HFG_INVALID_ARG, "null context");
   if (!(cutoff >= 0) || !(cutoff < 1e300)) return hfg::fail(HFG_INVALID_ARG, "mixed cutoff must be finite and >= 0");
   c->mixed_cutoff = cutoff;
+  ++c->config_version;
   return HFG_OK;
 }
 
@@ -1373,6 +1496,14 @@ hfg_status hfg_autotune(hfg_ctx *c, const double *dP, int32_t *chosen, int32_t c
     }
   }
   if (count) *count = written / 5;
+  ++c->config_version;
+  return HFG_OK;
+}
+
+hfg_status hfg_set_graphs(hfg_ctx *c, int32_t on) {
+  if (!c) return hfg::fail(HFG_INVALID_ARG, "null context");
+  c->use_graphs = on != 0;
+  ++c->config_version;
   return HFG_OK;
 }
 
@@ -1381,6 +1512,7 @@ hfg_status hfg_set_shard(hfg_ctx *c, int32_t rank, int32_t count) {
   if (count < 1 || rank < 0 || rank >= count) return hfg::fail(HFG_INVALID_ARG, "shard rank outside [0, count)");
   c->shard_rank = rank;
   c->shard_count = count;
+  ++c->config_version;
   c->inc_valid = false;  // an incremental history belongs to one shard
   return HFG_OK;
 }
@@ -1389,6 +1521,7 @@ hfg_status hfg_set_incremental(hfg_ctx *c, int32_t on) {
   if (!c) return hfg::fail(HFG_INVALID_ARG, "null context");
   c->opts.incremental = on != 0;
   c->inc_valid = false;
+  ++c->config_version;
   return HFG_OK;
 }
 

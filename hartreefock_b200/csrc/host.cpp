@@ -464,6 +464,8 @@ void HartreeFockAlgorithm::Init(Systems::Molecule *molecule) {
     integralsRepository.options.density_screening = 1;
     integralsRepository.options.mixed_cutoff = std::max(0.0, mixedCutoff);
   }
+  // the SCF's builds reuse one density and one G buffer: replay them as a graph
+  integralsRepository.options.cuda_graphs = 1;
   integralsRepository.Reset(molecule);
   Matrix T, Vn;
   integralsRepository.OneElectron(overlap, T, Vn);

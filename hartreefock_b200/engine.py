@@ -28,7 +28,7 @@ EXPORTED = ["hfg_default_opts", "hfg_last_error", "hfg_device_count", "hfg_ctx_c
             "hfg_fock_rhf_noalloc", "hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental",
             "hfg_set_shard", "hfg_batch_create", "hfg_batch_size", "hfg_batch_layout", "hfg_fock_rhf_batch_device",
             "hfg_fock_uhf_batch_device", "hfg_eigh_batched", "hfg_one_electron",
-            "hfg_mo_eri_ovov", "hfg_mp2_rhf", "hfg_autotune"]
+            "hfg_mo_eri_ovov", "hfg_mp2_rhf", "hfg_autotune", "hfg_set_graphs"]
 
 
 class HfgError(RuntimeError):
@@ -47,7 +47,7 @@ class hfg_opts(ctypes.Structure):
     _fields_ = [("schwarz_threshold", ctypes.c_double), ("mixed_cutoff", ctypes.c_double),
                 ("eri_convention", ctypes.c_int32), ("device", ctypes.c_int32),
                 ("density_screening", ctypes.c_int32), ("incremental", ctypes.c_int32),
-                ("density_threshold", ctypes.c_double), ("reserved", ctypes.c_int32 * 2)]
+                ("density_threshold", ctypes.c_double), ("cuda_graphs", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class hfg_stats(ctypes.Structure):
@@ -124,6 +124,8 @@ def library(path: str = LIB_PATH):
     L.hfg_mp2_rhf.restype = ctypes.c_int
     L.hfg_autotune.argtypes = [vp, dp, vp, i32, ctypes.POINTER(i32), vp]
     L.hfg_autotune.restype = ctypes.c_int
+    L.hfg_set_graphs.argtypes = [vp, i32]
+    L.hfg_set_graphs.restype = ctypes.c_int
     for name in ("hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental", "hfg_set_shard", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak", "hfg_ctx_create", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet", "hfg_fock_rhf",
                  "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz", "hfg_ctx_stats"):
         getattr(L, name).restype = ctypes.c_int
@@ -289,6 +291,10 @@ class Engine:
         _check(library().hfg_fock_uhf_device(self._h, ctypes.c_void_p(Pa_ptr), ctypes.c_void_p(Pb_ptr),
                                              ctypes.c_void_p(Ga_ptr), ctypes.c_void_p(Gb_ptr),
                                              ctypes.c_void_p(stream)))
+
+    def set_graphs(self, on: bool = True):
+        """Replay the plain direct build as a CUDA graph (hfg_set_graphs)."""
+        _check(library().hfg_set_graphs(self._h, int(on)))
 
     def autotune(self, P) -> dict:
         """Pick each fused class's grid (blocks per SM) by timing it on the

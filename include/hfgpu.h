@@ -86,7 +86,9 @@ typedef struct {
   int32_t density_screening;/* 1: skip quartets below density_threshold */
   int32_t incremental;      /* 1: build from the density difference */
   double density_threshold; /* density screening cutoff; 0 = schwarz_threshold */
-  int32_t reserved[2];
+  int32_t cuda_graphs;      /* 1: plain-form direct builds replay a CUDA graph
+                               (hfg_set_graphs); default 0 */
+  int32_t reserved;
 } hfg_opts;
 
 typedef struct hfg_ctx hfg_ctx;
@@ -248,6 +250,14 @@ hfg_status hfg_fock_rhf_noalloc(hfg_ctx *ctx, const double *dP, double *dG, void
 hfg_status hfg_schwarz(hfg_ctx *ctx, double *host_out, int64_t count);
 
 hfg_status hfg_ctx_stats(const hfg_ctx *ctx, hfg_stats *out);
+
+/* CUDA graphs for the plain-form direct build (no reference counterpart):
+ * with `on`, the second hfg_fock_*_device / hfg_fock_* call with the same
+ * buffers, stream and settings is captured into a graph and later ones
+ * replay it (one launch instead of ~30).  Needs a created stream (not the
+ * legacy default stream; 0 selects the context's own).  Any setter
+ * (autotune, shard, precision settings, profiling) starts over. */
+hfg_status hfg_set_graphs(hfg_ctx *ctx, int32_t on);
 
 /* Grid autotuner (no reference counterpart): times every fused quartet
  * class's J/K kernel at 1, 2, 4, 8 and 16 blocks per SM on the density dP
