@@ -126,7 +126,7 @@ struct hfg_ctx {
   // class kernels of one build are independent (J/K by atomics): they run on
   // the build stream and kAux more, forked and joined by events, so small
   // molecules' classes overlap instead of queueing
-  static constexpr int kAux = 3;
+  static constexpr int kAux = 4;
   cudaStream_t aux[kAux] = {};
   cudaEvent_t ev_fork = nullptr, ev_join[kAux] = {};
   int num_sms = 148;
@@ -157,8 +157,10 @@ struct hfg_ctx {
   // work buffers
   double *d_J = nullptr, *d_Ka = nullptr, *d_Kb = nullptr, *d_P = nullptr, *d_Pb = nullptr, *d_Pt = nullptr;
   double *d_G = nullptr, *d_Gb = nullptr, *d_block = nullptr;
-  double *d_scratch = nullptr;  // split-path [e0|f0] blocks
-  size_t scratch_doubles = 0;
+  // split-path [e0|f0] blocks, one region per auxiliary stream (the split
+  // classes of a build run on those streams concurrently)
+  double *d_scratch[kAux] = {};
+  size_t scratch_doubles[kAux] = {};
   size_t scratch_budget_bytes = size_t(512) << 20;
   // precision form: density screening, FP32 cutoff, incremental history
   int nshells = 0;
@@ -227,7 +229,7 @@ struct hfg_ctx {
     for (auto &p : pclass) cudaFree(p.d_pairs);
     void *bufs[] = {d_prim,       d_pair_prim_off, d_pair_nprim, d_pair_sa,  d_pair_sb,    d_pair_ao_a, d_pair_ao_b,
                     d_pair_AB,    d_pair_Q,        d_boys,       d_J,        d_Ka,         d_Kb,        d_P,
-                    d_Pb,         d_Pt,            d_G,          d_Gb,       d_block,      d_scratch,   d_shell_ao,
+                    d_Pb,         d_Pt,            d_G,          d_Gb,       d_block,      d_scratch[0], d_shell_ao,
                     d_shell_nf,   d_shell_dmax,    d_counters,   d_prev_P[0], d_prev_P[1], d_prev_G[0], d_prev_G[1],
                     d_dP[0],      d_dP[1],         d_primf,      d_pair_mol, d_mol_nbf,    d_mol_off,   d_mol_active,
                     d_task_active, d_task_counts};
@@ -238,6 +240,7 @@ struct hfg_ctx {
       if (ev_join[i]) cudaEventDestroy(ev_join[i]);
     }
     if (ev_fork) cudaEventDestroy(ev_fork);
+    for (int i = 1; i < kAux; ++i) cudaFree(d_scratch[i]);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -475,15 +478,16 @@ static int ncomp_range(int lo, int hi) {
 }
 
 // Fork / join of a build's class launches over the build stream and the
-// context's auxiliary streams.  Split classes share one scratch buffer, so
-// they all go to the first auxiliary stream, one after another; fused
-// classes take the build stream and the other auxiliary streams in turn.
-// Off (everything on the build stream) while per-class profiling is on.
+// context's auxiliary streams.  Split classes take the auxiliary streams in
+// turn, each stream with its own scratch region; fused classes take the
+// build stream and the auxiliary streams in turn.  Off (everything on the
+// build stream, scratch region 0) while per-class profiling is on.
 struct ClassStreams {
   hfg_ctx *c;
   cudaStream_t s;
   bool on;
-  int next = 0;
+  int next = 0, next_split = 0;
+  int slot = 0;  // scratch region of the last split pick
   hfg_status fork() {
     if (!on) return HFG_OK;
     HFG_CUDA(cudaEventRecord(c->ev_fork, s));
@@ -491,10 +495,14 @@ struct ClassStreams {
     return HFG_OK;
   }
   cudaStream_t pick(bool split) {
+    slot = 0;
     if (!on) return s;
-    if (split) return c->aux[0];
-    const int k = next++ % hfg_ctx::kAux;  // 0 = build stream, then aux[1..]
-    return k == 0 ? s : c->aux[k];
+    if (split) {
+      slot = next_split++ % hfg_ctx::kAux;
+      return c->aux[slot];
+    }
+    const int k = next++ % (hfg_ctx::kAux + 1);  // 0 = build stream, then aux[0..]
+    return k == 0 ? s : c->aux[k - 1];
   }
   hfg_status join() {
     if (!on) return HFG_OK;
@@ -509,7 +517,7 @@ struct ClassStreams {
 // `prec`: 0 plain FP64, 1 density-screened FP64, 2 density-screened with
 // the per-task FP64/FP32 choice (the precision form).
 static hfg_status launch_class(hfg_ctx *c, const QuartetClass &q, const ClassLaunch &cl, int mode, bool ref,
-                               int prec, cudaStream_t s, int *launches) {
+                               int prec, cudaStream_t s, int *launches, int slot = 0) {
   const ClassEntry &e = kClasses[q.cls];
   if (!kSplit[q.cls]) {
     e.launch(c->view(), cl, mode, ref, prec, grid_for(c, cl.ntasks, q.cls), s);
@@ -519,23 +527,24 @@ static hfg_status launch_class(hfg_ctx *c, const QuartetClass &q, const ClassLau
   const size_t acc = (size_t)ncomp_range(e.la, e.la + e.lb) * ncomp_range(e.lc, e.lc + e.ld);
   const bool two = ref && e.la == 2 && e.lb == 2 && e.lc == 2 && e.ld == 2;
   const size_t per_task = 32 * acc * (two ? 2 : 1);
-  const int max_tasks = (int)std::max<size_t>(1, c->scratch_budget_bytes / (per_task * sizeof(double)));
+  const int max_tasks =
+      (int)std::max<size_t>(1, c->scratch_budget_bytes / hfg_ctx::kAux / (per_task * sizeof(double)));
   const int chunk_tasks = std::min(cl.ntasks, max_tasks);
   const size_t need = (size_t)chunk_tasks * per_task;
-  if (need > c->scratch_doubles) {
-    cudaFree(c->d_scratch);
-    c->d_scratch = nullptr;
-    c->scratch_doubles = 0;
-    HFG_CUDA(cudaMalloc((void **)&c->d_scratch, need * sizeof(double)));
-    c->scratch_doubles = need;
+  if (need > c->scratch_doubles[slot]) {
+    cudaFree(c->d_scratch[slot]);
+    c->d_scratch[slot] = nullptr;
+    c->scratch_doubles[slot] = 0;
+    HFG_CUDA(cudaMalloc((void **)&c->d_scratch[slot], need * sizeof(double)));
+    c->scratch_doubles[slot] = need;
   }
   for (int t0 = 0; t0 < cl.ntasks; t0 += chunk_tasks) {
     SplitChunk ch{};
     ch.ntasks = std::min(chunk_tasks, cl.ntasks - t0);
     ch.task0 = t0;
     ch.stride = (long long)ch.ntasks * 32;
-    ch.scr_fwd = c->d_scratch;
-    ch.scr_rev = c->d_scratch + acc * (size_t)ch.stride;
+    ch.scr_fwd = c->d_scratch[slot];
+    ch.scr_rev = c->d_scratch[slot] + acc * (size_t)ch.stride;
     kSplit[q.cls](c->view(), cl, ch, mode, ref, prec, s);
     *launches += 2;
   }
@@ -609,7 +618,8 @@ static hfg_status direct_build_body(hfg_ctx *c, bool uhf, const double *dPa, con
     cl.mixed_cutoff = (float)c->mixed_cutoff;
     cl.counters = precise ? c->d_counters : nullptr;
     if (cl.ntasks > 0) {
-      st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, prec, cs.pick(kSplit[q.cls] != nullptr), &launches);
+      const cudaStream_t cls_stream = cs.pick(kSplit[q.cls] != nullptr);
+      st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, prec, cls_stream, &launches, cs.slot);
       if (st != HFG_OK) return st;
     }
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_b, s));
@@ -822,7 +832,8 @@ static hfg_status batch_build(hfg_ctx *c, bool uhf, const double *dPa, const dou
     cl.Ka = c->d_Ka;
     cl.Kb = c->d_Kb;
     if (cl.ntasks > 0) {
-      st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, 0, cs.pick(kSplit[q.cls] != nullptr), &launches);
+      const cudaStream_t cls_stream = cs.pick(kSplit[q.cls] != nullptr);
+      st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, 0, cls_stream, &launches, cs.slot);
       if (st != HFG_OK) return st;
     }
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_b, s));
