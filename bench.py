@@ -137,7 +137,7 @@ def scf_comparison(waters: int):
     one-call driver (C++ host API: device-resident SCF over the engine)."""
     from hartreefock_b200 import molecules, scf
     Z, xyz = molecules.water_cluster(waters, seed=SEED)
-    kw = dict(alpha=0.75, init_guess=0.75, post_diis=0, schwarz_threshold=THRESHOLD)
+    kw = dict(alpha=0.75, init_guess=0.75, post_diis=0, schwarz_threshold=THRESHOLD, concurrent_classes=True)
     runs = {}
     for name, extra in (("fp64", {}), ("mixed", {"mixed_cutoff": 1e-4}),
                         ("fp64_same_criteria", {"stop_at_precision_test": True})):
@@ -304,6 +304,7 @@ def main():
     ap.add_argument("--serve-jobs", type=int, default=24, help="jobs of the serving stream (0: skip)")
     ap.add_argument("--batch-mols", type=int, default=0, help="molecules of the batched SCF (0: skip)")
     ap.add_argument("--no-autotune", action="store_true", help="fixed grid (4 blocks per SM) for every class")
+    ap.add_argument("--no-streams", action="store_true", help="every class kernel on the build stream")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     WATERS = args.waters
@@ -328,7 +329,7 @@ def main():
     n = eng.nbf
     P_host = synthetic_density(n)
     stream = torch.cuda.current_stream()
-    sptr = stream.cuda_stream
+    sptr = E._torch_stream()  # the builds run on torch's stream, between the timing events
     dP = torch.from_numpy(P_host).cuda()
     dG = torch.empty_like(dP)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
@@ -338,8 +339,10 @@ def main():
     torch.cuda.synchronize()
     stats_full = eng.stats()
     G_full = dG.clone()
-    # grid per class from the autotuner (timed on this density, before warm-up)
+    # grid per class from the autotuner (timed on this density, before warm-up),
+    # then the classes of every build over concurrent streams
     grids = eng.autotune(dP) if not args.no_autotune else {}
+    eng.set_streams(not args.no_streams)
     # N > 1: every rank builds its shard of each class's tasks, one NCCL
     # all-reduce of G per build (hartreefock_b200/shards.py)
     sf = None
@@ -431,6 +434,7 @@ def main():
                    "function_quartets": stats_full["function_quartets"],
                    "l2": "flushed (256 MB write) between steps",
                    "grid_blocks_per_sm": grids or "fixed 4",
+                   "class_streams": 1 if args.no_streams else 5,
                    "parallelism": f"task shards x{world}, one NCCL all-reduce of G per build" if world > 1
                    else "single GPU"},
         "e2e": {"value": e2e, "unit": "quartets/s", "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": n * n * 8},

@@ -104,6 +104,11 @@ static hfg_status upload(T **dst, const std::vector<T> &src) {
   if (src.empty()) return HFG_OK;
   HFG_CUDA(cudaMalloc((void **)dst, src.size() * sizeof(T)));
   HFG_CUDA(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  // a pageable-to-device cudaMemcpy returns once the data is staged; the DMA
+  // itself is queued on the legacy default stream, which the context's
+  // non-blocking streams do not wait for: let it land before any kernel of
+  // ours reads the table
+  HFG_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
   return HFG_OK;
 }
 
@@ -135,6 +140,8 @@ struct hfg_ctx {
   // CUDA graph of the plain direct build (hfg_set_graphs): captured on the
   // second build with the same buffers, stream and settings, replayed after
   bool use_graphs = false;
+  bool use_streams = false;  // class kernels over the auxiliary streams (hfg_set_streams)
+  cudaEvent_t ev_done = nullptr;  // end of the last build on its stream
   unsigned config_version = 0;  // bumped by every setter that changes a build
   struct GraphKey {
     bool uhf = false;
@@ -221,6 +228,12 @@ struct hfg_ctx {
   }
   ~hfg_ctx() {
     cudaSetDevice(device);
+    // the last build may still be queued (on the caller's stream and ours):
+    // let it finish before its buffers go
+    if (ev_done) cudaEventSynchronize(ev_done);
+    for (int i = 0; i < kAux; ++i)
+      if (aux[i]) cudaStreamSynchronize(aux[i]);
+    if (stream) cudaStreamSynchronize(stream);
     for (auto &q : qclasses) {
       cudaFree(q.d_tasks);
       if (q.ev_a) cudaEventDestroy(q.ev_a);
@@ -240,6 +253,7 @@ struct hfg_ctx {
       if (ev_join[i]) cudaEventDestroy(ev_join[i]);
     }
     if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_done) cudaEventDestroy(ev_done);
     for (int i = 1; i < kAux; ++i) cudaFree(d_scratch[i]);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -482,6 +496,10 @@ static int ncomp_range(int lo, int hi) {
 // turn, each stream with its own scratch region; fused classes take the
 // build stream and the auxiliary streams in turn.  Off (everything on the
 // build stream, scratch region 0) while per-class profiling is on.
+static void split_chunking(const hfg_ctx *c, int cls, int ntasks, bool ref, size_t *need, int *chunk_tasks);
+static int scratch_regions(const hfg_ctx *c);
+static hfg_status grow_scratch(hfg_ctx *c, int slot, size_t need);
+
 struct ClassStreams {
   hfg_ctx *c;
   cudaStream_t s;
@@ -504,6 +522,27 @@ struct ClassStreams {
     const int k = next++ % (hfg_ctx::kAux + 1);  // 0 = build stream, then aux[0..]
     return k == 0 ? s : c->aux[k - 1];
   }
+  // Sizes the scratch region of every split class before anything of the
+  // build is launched, following the order pick() will hand out regions in
+  // (`ntasks` per quartet class, in class order).
+  hfg_status presize(const std::vector<int> &ntasks, bool ref) {
+    std::vector<size_t> need(hfg_ctx::kAux, 0);
+    int k = 0;
+    for (size_t i = 0; i < c->qclasses.size(); ++i) {
+      const int cls = c->qclasses[i].cls;
+      if (!kSplit[cls] || ntasks[i] <= 0) continue;
+      size_t nd = 0;
+      int chunk = 1;
+      split_chunking(c, cls, ntasks[i], ref, &nd, &chunk);
+      const int slot_i = on ? k++ % hfg_ctx::kAux : 0;
+      need[slot_i] = std::max(need[slot_i], nd);
+    }
+    for (int i = 0; i < hfg_ctx::kAux; ++i) {
+      const hfg_status st = grow_scratch(c, i, need[i]);
+      if (st != HFG_OK) return st;
+    }
+    return HFG_OK;
+  }
   hfg_status join() {
     if (!on) return HFG_OK;
     for (int i = 0; i < hfg_ctx::kAux; ++i) {
@@ -516,6 +555,40 @@ struct ClassStreams {
 
 // `prec`: 0 plain FP64, 1 density-screened FP64, 2 density-screened with
 // the per-task FP64/FP32 choice (the precision form).
+// Scratch regions in use: one per auxiliary stream with concurrent classes,
+// else one.
+static int scratch_regions(const hfg_ctx *c) { return c->use_streams && !c->profiling ? hfg_ctx::kAux : 1; }
+
+// Scratch doubles and tasks per chunk of a split class launched over
+// `ntasks` tasks: chunks keep one region within its share of the scratch
+// budget.
+static void split_chunking(const hfg_ctx *c, int cls, int ntasks, bool ref, size_t *need, int *chunk_tasks) {
+  const ClassEntry &e = kClasses[cls];
+  const size_t acc = (size_t)ncomp_range(e.la, e.la + e.lb) * ncomp_range(e.lc, e.lc + e.ld);
+  const bool two = ref && e.la == 2 && e.lb == 2 && e.lc == 2 && e.ld == 2;
+  const size_t per_task = 32 * acc * (two ? 2 : 1);
+  const int max_tasks =
+      (int)std::max<size_t>(1, c->scratch_budget_bytes / scratch_regions(c) / (per_task * sizeof(double)));
+  *chunk_tasks = std::min(ntasks, max_tasks);
+  *need = (size_t)*chunk_tasks * per_task;
+}
+
+// Grows scratch region `slot` to `need` doubles.  The old region may still
+// be read by queued split kernels, so the device is drained before it is
+// freed (a build sizes its regions before it launches anything, so this
+// runs on the first builds only).
+static hfg_status grow_scratch(hfg_ctx *c, int slot, size_t need) {
+  if (need <= c->scratch_doubles[slot]) return HFG_OK;
+  HFG_CUDA(cudaDeviceSynchronize());
+  cudaFree(c->d_scratch[slot]);
+  c->d_scratch[slot] = nullptr;
+  c->scratch_doubles[slot] = 0;
+  HFG_CUDA(cudaMalloc((void **)&c->d_scratch[slot], need * sizeof(double)));
+  c->scratch_doubles[slot] = need;
+  ++c->config_version;  // a captured graph holds the old region
+  return HFG_OK;
+}
+
 static hfg_status launch_class(hfg_ctx *c, const QuartetClass &q, const ClassLaunch &cl, int mode, bool ref,
                                int prec, cudaStream_t s, int *launches, int slot = 0) {
   const ClassEntry &e = kClasses[q.cls];
@@ -525,19 +598,11 @@ static hfg_status launch_class(hfg_ctx *c, const QuartetClass &q, const ClassLau
     return HFG_OK;
   }
   const size_t acc = (size_t)ncomp_range(e.la, e.la + e.lb) * ncomp_range(e.lc, e.lc + e.ld);
-  const bool two = ref && e.la == 2 && e.lb == 2 && e.lc == 2 && e.ld == 2;
-  const size_t per_task = 32 * acc * (two ? 2 : 1);
-  const int max_tasks =
-      (int)std::max<size_t>(1, c->scratch_budget_bytes / hfg_ctx::kAux / (per_task * sizeof(double)));
-  const int chunk_tasks = std::min(cl.ntasks, max_tasks);
-  const size_t need = (size_t)chunk_tasks * per_task;
-  if (need > c->scratch_doubles[slot]) {
-    cudaFree(c->d_scratch[slot]);
-    c->d_scratch[slot] = nullptr;
-    c->scratch_doubles[slot] = 0;
-    HFG_CUDA(cudaMalloc((void **)&c->d_scratch[slot], need * sizeof(double)));
-    c->scratch_doubles[slot] = need;
-  }
+  size_t need = 0;
+  int chunk_tasks = 1;
+  split_chunking(c, q.cls, cl.ntasks, ref, &need, &chunk_tasks);
+  hfg_status st = grow_scratch(c, slot, need);
+  if (st != HFG_OK) return st;
   for (int t0 = 0; t0 < cl.ntasks; t0 += chunk_tasks) {
     SplitChunk ch{};
     ch.ntasks = std::min(chunk_tasks, cl.ntasks - t0);
@@ -599,10 +664,15 @@ static hfg_status direct_build_body(hfg_ctx *c, bool uhf, const double *dPa, con
     add_densities<<<256, 256, 0, s>>>(Da, Db, c->d_Pt, (int)nn);
     launches += 2;
   }
-  if (!capturing) HFG_CUDA(cudaEventRecord(c->ev0, s));
-  ClassStreams cs{c, s, !c->profiling};
-  if ((st = cs.fork()) != HFG_OK) return st;
   const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
+  ClassStreams cs{c, s, c->use_streams && !c->profiling};
+  {
+    std::vector<int> nt(c->qclasses.size());
+    for (size_t i = 0; i < nt.size(); ++i) nt[i] = base_launch(c, c->qclasses[i], true).ntasks;
+    if ((st = cs.presize(nt, ref)) != HFG_OK) return st;
+  }
+  if (!capturing) HFG_CUDA(cudaEventRecord(c->ev0, s));
+  if ((st = cs.fork()) != HFG_OK) return st;
   const int prec = !precise ? 0 : c->mixed_cutoff > 0 ? 2 : 1;
   c->stats = hfg_stats{};
   for (auto &q : c->qclasses) {
@@ -649,6 +719,7 @@ static hfg_status direct_build_body(hfg_ctx *c, bool uhf, const double *dPa, con
   }
   ++launches;
   HFG_CUDA(cudaGetLastError());
+  if (!capturing) HFG_CUDA(cudaEventRecord(c->ev_done, s));
   c->stats.kernel_launches = launches;
   c->stats.shell_pairs = c->npairs;
   c->counted = precise;
@@ -696,6 +767,7 @@ static hfg_status direct_build(hfg_ctx *c, bool uhf, const double *dPa, const do
     HFG_CUDA(cudaEventRecord(c->ev0, s));
     HFG_CUDA(cudaGraphLaunch(c->graph_exec, s));
     HFG_CUDA(cudaEventRecord(c->ev1, s));
+    HFG_CUDA(cudaEventRecord(c->ev_done, s));
     c->stats = c->graph_stats;
     return HFG_OK;
   }
@@ -810,10 +882,15 @@ static hfg_status batch_build(hfg_ctx *c, bool uhf, const double *dPa, const dou
     HFG_CUDA(cudaMemcpyAsync(counts.data(), c->d_task_counts, nq * sizeof(int), cudaMemcpyDeviceToHost, s));
     HFG_CUDA(cudaStreamSynchronize(s));
   }
-  HFG_CUDA(cudaEventRecord(c->ev0, s));
-  ClassStreams cs{c, s, !c->profiling};
-  if ((st = cs.fork()) != HFG_OK) return st;
   const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
+  ClassStreams cs{c, s, c->use_streams && !c->profiling};
+  {
+    std::vector<int> nt(c->qclasses.size());
+    for (size_t i = 0; i < nt.size(); ++i) nt[i] = compact ? counts[i] : base_launch(c, c->qclasses[i], true).ntasks;
+    if ((st = cs.presize(nt, ref)) != HFG_OK) return st;
+  }
+  HFG_CUDA(cudaEventRecord(c->ev0, s));
+  if ((st = cs.fork()) != HFG_OK) return st;
   c->stats = hfg_stats{};
   for (size_t qi = 0; qi < c->qclasses.size(); ++qi) {
     auto &q = c->qclasses[qi];
@@ -855,6 +932,7 @@ static hfg_status batch_build(hfg_ctx *c, bool uhf, const double *dPa, const dou
     finalize_rhf_batch<<<fg, 256, 0, s>>>(c->d_J, c->d_Ka, dGa, c->d_mol_nbf, c->d_mol_off, c->d_mol_active);
   ++launches;
   HFG_CUDA(cudaGetLastError());
+  HFG_CUDA(cudaEventRecord(c->ev_done, s));
   c->stats.kernel_launches = launches;
   c->stats.shell_pairs = c->npairs;
   c->stats.fp64_shell_quartets = c->stats.shell_quartets;
@@ -958,6 +1036,7 @@ static hfg_status create_context(const hfg_shells *sh, const int *shell_mol, int
   HFG_CUDA(cudaSetDevice(ctx->device));
   HFG_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device));
   ctx->use_graphs = ctx->opts.cuda_graphs != 0;
+  ctx->use_streams = ctx->opts.concurrent_classes != 0;
   // tuning: HFG_BLOCKS_PER_SM overrides the grid cap (every block stages the
   // class's Boys table once, so fewer, longer-lived blocks stage it less)
   if (const char *e = std::getenv("HFG_BLOCKS_PER_SM")) ctx->blocks_per_sm = std::max(1, std::atoi(e));
@@ -1107,6 +1186,7 @@ static hfg_status create_context(const hfg_shells *sh, const int *shell_mol, int
   HFG_CUDA(cudaEventCreate(&ctx->ev0));
   HFG_CUDA(cudaEventCreate(&ctx->ev1));
   HFG_CUDA(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+  HFG_CUDA(cudaEventCreateWithFlags(&ctx->ev_done, cudaEventDisableTiming));
   for (int i = 0; i < hfg_ctx::kAux; ++i) {
     HFG_CUDA(cudaStreamCreateWithFlags(&ctx->aux[i], cudaStreamNonBlocking));
     HFG_CUDA(cudaEventCreateWithFlags(&ctx->ev_join[i], cudaEventDisableTiming));
@@ -1507,6 +1587,13 @@ hfg_status hfg_autotune(hfg_ctx *c, const double *dP, int32_t *chosen, int32_t c
     }
   }
   if (count) *count = written / 5;
+  ++c->config_version;
+  return HFG_OK;
+}
+
+hfg_status hfg_set_streams(hfg_ctx *c, int32_t on) {
+  if (!c) return hfg::fail(HFG_INVALID_ARG, "null context");
+  c->use_streams = on != 0;
   ++c->config_version;
   return HFG_OK;
 }

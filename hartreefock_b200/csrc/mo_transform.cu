@@ -164,6 +164,7 @@ extern "C" hfg_status hfg_mp2_rhf(hfg_ctx *ctx, const double *C, const double *e
   if (e == cudaSuccess) e = buf.get(&dOut, 1);
   if (e == cudaSuccess) e = cudaMemcpy(dC, C, sizeof(double) * n * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dE, eps, sizeof(double) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);  // staged copies landed
   if (e == cudaSuccess) e = cudaMemset(dOut, 0, sizeof(double));
   if (e != cudaSuccess) return hfg::fail_external(HFG_OOM_BUDGET, std::string("hfg_mp2_rhf: ") + cudaGetErrorString(e));
   hfg_status st = transform(ctx, dC, 0, nocc, nocc, nv, dX, nullptr, buf);

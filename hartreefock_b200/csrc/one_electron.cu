@@ -171,11 +171,11 @@ __global__ void __launch_bounds__(32 * kOneWarps) one_electron_kernel(const OneS
 template <int LA, int LB>
 void launch_one(const OneShell *shells, const int2 *pairs, int npairs, const double *expo, const double *coef,
                 const double *nuc, int natoms, const double *boys, int n, double *S, double *T, double *V,
-                int num_sms) {
+                int num_sms, cudaStream_t st) {
   if (npairs == 0) return;
   const int blocks = std::min((npairs + kOneWarps - 1) / kOneWarps, num_sms * 4);
-  one_electron_kernel<LA, LB><<<blocks, 32 * kOneWarps>>>(shells, pairs, npairs, expo, coef, nuc, natoms, boys, n, S,
-                                                          T, V);
+  one_electron_kernel<LA, LB><<<blocks, 32 * kOneWarps, 0, st>>>(shells, pairs, npairs, expo, coef, nuc, natoms, boys,
+                                                                  n, S, T, V);
 }
 
 template <class T>
@@ -187,7 +187,10 @@ struct DeviceArray {
   cudaError_t upload(const std::vector<T> &v) {
     cudaError_t e = cudaMalloc(&p, std::max<size_t>(1, v.size()) * sizeof(T));
     if (e != cudaSuccess || v.empty()) return e;
-    return cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    e = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    // the staged copy's DMA runs on the legacy stream; the kernels below run
+    // on a stream of their own
+    return e == cudaSuccess ? cudaStreamSynchronize(cudaStreamLegacy) : e;
   }
 };
 
@@ -237,6 +240,15 @@ extern "C" hfg_status hfg_one_electron(const hfg_shells *sh, const double *nuc_x
   }
   cudaError_t e = cudaSetDevice(device);
   int num_sms = 148;
+  // a stream of this call's own: nothing here waits on, or is waited on by,
+  // the legacy default stream that other host threads share
+  struct OwnStream {
+    cudaStream_t s = nullptr;
+    ~OwnStream() {
+      if (s) cudaStreamDestroy(s);
+    }
+  } os;
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&os.s, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device);
   DeviceArray<OneShell> d_sh;
   DeviceArray<int2> d_pairs;
@@ -249,12 +261,12 @@ extern "C" hfg_status hfg_one_electron(const hfg_shells *sh, const double *nuc_x
   if (e == cudaSuccess) e = d_boys.upload(boys_table_for_external());
   const size_t nn = (size_t)n * n;
   if (e == cudaSuccess) e = cudaMalloc(&d_out.p, 3 * nn * sizeof(double));
-  if (e == cudaSuccess) e = cudaMemset(d_out.p, 0, 3 * nn * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_out.p, 0, 3 * nn * sizeof(double), os.s);
   if (e != cudaSuccess) return fail_external(HFG_OOM_BUDGET, std::string("hfg_one_electron: ") + cudaGetErrorString(e));
   double *dS = d_out.p, *dT = dS + nn, *dV = dT + nn;
 #define HFG_ONE(LA, LB)                                                                                              \
   launch_one<LA, LB>(d_sh.p, d_pairs.p + off[LA][LB], cnt[LA][LB], d_exp.p, d_coef.p, d_nuc.p, natoms, d_boys.p, n, \
-                     dS, dT, dV, num_sms)
+                     dS, dT, dV, num_sms, os.s)
   HFG_ONE(0, 0);
   HFG_ONE(1, 0);
   HFG_ONE(1, 1);
@@ -263,9 +275,10 @@ extern "C" hfg_status hfg_one_electron(const hfg_shells *sh, const double *nuc_x
   HFG_ONE(2, 2);
 #undef HFG_ONE
   e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpy(S, dS, nn * sizeof(double), cudaMemcpyDeviceToHost);
-  if (e == cudaSuccess) e = cudaMemcpy(T, dT, nn * sizeof(double), cudaMemcpyDeviceToHost);
-  if (e == cudaSuccess) e = cudaMemcpy(V, dV, nn * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(S, dS, nn * sizeof(double), cudaMemcpyDeviceToHost, os.s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(T, dT, nn * sizeof(double), cudaMemcpyDeviceToHost, os.s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(V, dV, nn * sizeof(double), cudaMemcpyDeviceToHost, os.s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(os.s);
   if (e != cudaSuccess) return fail_external(HFG_DEVICE_ERROR, std::string("hfg_one_electron: ") + cudaGetErrorString(e));
   return HFG_OK;
 }

@@ -28,7 +28,7 @@ EXPORTED = ["hfg_default_opts", "hfg_last_error", "hfg_device_count", "hfg_ctx_c
             "hfg_fock_rhf_noalloc", "hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental",
             "hfg_set_shard", "hfg_batch_create", "hfg_batch_size", "hfg_batch_layout", "hfg_fock_rhf_batch_device",
             "hfg_fock_uhf_batch_device", "hfg_eigh_batched", "hfg_one_electron",
-            "hfg_mo_eri_ovov", "hfg_mp2_rhf", "hfg_autotune", "hfg_set_graphs"]
+            "hfg_mo_eri_ovov", "hfg_mp2_rhf", "hfg_autotune", "hfg_set_graphs", "hfg_set_streams"]
 
 
 class HfgError(RuntimeError):
@@ -47,7 +47,7 @@ class hfg_opts(ctypes.Structure):
     _fields_ = [("schwarz_threshold", ctypes.c_double), ("mixed_cutoff", ctypes.c_double),
                 ("eri_convention", ctypes.c_int32), ("device", ctypes.c_int32),
                 ("density_screening", ctypes.c_int32), ("incremental", ctypes.c_int32),
-                ("density_threshold", ctypes.c_double), ("cuda_graphs", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("density_threshold", ctypes.c_double), ("cuda_graphs", ctypes.c_int32), ("concurrent_classes", ctypes.c_int32)]
 
 
 class hfg_stats(ctypes.Structure):
@@ -126,11 +126,22 @@ def library(path: str = LIB_PATH):
     L.hfg_autotune.restype = ctypes.c_int
     L.hfg_set_graphs.argtypes = [vp, i32]
     L.hfg_set_graphs.restype = ctypes.c_int
+    L.hfg_set_streams.argtypes = [vp, i32]
+    L.hfg_set_streams.restype = ctypes.c_int
     for name in ("hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental", "hfg_set_shard", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak", "hfg_ctx_create", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet", "hfg_fock_rhf",
                  "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz", "hfg_ctx_stats"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
+
+
+def _torch_stream() -> int:
+    """torch's current stream as a handle for the C ABI.  torch's default
+    stream is the legacy default stream, whose handle 0 the ABI reads as "the
+    context's own stream"; pass cudaStreamLegacy (1) instead, so that our
+    kernels stay ordered with torch's."""
+    import torch
+    return torch.cuda.current_stream().cuda_stream or 1
 
 
 def _check(st):
@@ -169,7 +180,7 @@ def _autotune(handle, P) -> dict:
     rec = np.zeros(5 * 32, dtype=np.int32)
     n = ctypes.c_int32()
     _check(library().hfg_autotune(handle, ctypes.c_void_p(dP.data_ptr()), _ptr(rec), len(rec), ctypes.byref(n),
-                                  ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+                                  ctypes.c_void_p(_torch_stream())))
     return {f"({r[0]}{r[1]}|{r[2]}{r[3]})": int(r[4]) for r in rec[:5 * n.value].reshape(-1, 5)}
 
 
@@ -187,7 +198,7 @@ def eigh_batched(A, method: int = 0):
     w = torch.empty(b, n, dtype=torch.float64, device=A.device)
     _check(library().hfg_eigh_batched(ctypes.c_void_p(A.data_ptr()), ctypes.c_void_p(X.data_ptr()),
                                       ctypes.c_void_p(w.data_ptr()), n, b, method,
-                                      ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+                                      ctypes.c_void_p(_torch_stream())))
     return w, X.transpose(1, 2)
 
 
@@ -273,14 +284,14 @@ class Engine:
         on torch's current stream."""
         import torch
         assert P.is_cuda and G.is_cuda and P.dtype == torch.float64 and P.is_contiguous() and G.is_contiguous()
-        self.fock_rhf_device(P.data_ptr(), G.data_ptr(), torch.cuda.current_stream().cuda_stream)
+        self.fock_rhf_device(P.data_ptr(), G.data_ptr(), _torch_stream())
 
     def fock_uhf_tensor(self, Pa, Pb, Ga, Gb):
         import torch
         for t in (Pa, Pb, Ga, Gb):
             assert t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()
         self.fock_uhf_device(Pa.data_ptr(), Pb.data_ptr(), Ga.data_ptr(), Gb.data_ptr(),
-                             torch.cuda.current_stream().cuda_stream)
+                             _torch_stream())
 
     def fock_rhf_noalloc(self, P_ptr: int, G_ptr: int, stream: int = 0):
         """Allocation-free direct RHF build (fixed 1024-function scratch)."""
@@ -291,6 +302,11 @@ class Engine:
         _check(library().hfg_fock_uhf_device(self._h, ctypes.c_void_p(Pa_ptr), ctypes.c_void_p(Pb_ptr),
                                              ctypes.c_void_p(Ga_ptr), ctypes.c_void_p(Gb_ptr),
                                              ctypes.c_void_p(stream)))
+
+    def set_streams(self, on: bool = True):
+        """Run a build's class kernels concurrently over the context's
+        auxiliary streams (hfg_set_streams)."""
+        _check(library().hfg_set_streams(self._h, int(on)))
 
     def set_graphs(self, on: bool = True):
         """Replay the plain direct build as a CUDA graph (hfg_set_graphs)."""
@@ -317,7 +333,7 @@ class Engine:
         X = torch.empty(ni * na, ni * na, dtype=torch.float64, device=C.device)
         _check(library().hfg_mo_eri_ovov(self._h, ctypes.c_void_p(C.data_ptr()), i0, ni, a0, na,
                                           ctypes.c_void_p(X.data_ptr()),
-                                          ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+                                          ctypes.c_void_p(_torch_stream())))
         return X
 
     def fock_reset(self):
@@ -411,7 +427,7 @@ class BatchEngine:
         keep, ap = self._active(active)
         _check(library().hfg_fock_rhf_batch_device(self._h, ctypes.c_void_p(P.data_ptr()),
                                                    ctypes.c_void_p(G.data_ptr()), ap,
-                                                   ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+                                                   ctypes.c_void_p(_torch_stream())))
         return G
 
     def fock_uhf(self, Pa, Pb, Ga, Gb, active=None):
@@ -420,7 +436,7 @@ class BatchEngine:
         _check(library().hfg_fock_uhf_batch_device(self._h, ctypes.c_void_p(Pa.data_ptr()),
                                                    ctypes.c_void_p(Pb.data_ptr()), ctypes.c_void_p(Ga.data_ptr()),
                                                    ctypes.c_void_p(Gb.data_ptr()), ap,
-                                                   ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+                                                   ctypes.c_void_p(_torch_stream())))
         return Ga, Gb
 
     def autotune(self, P) -> dict:

@@ -24,7 +24,7 @@ class hfd_scf_opts(ctypes.Structure):
                 ("fp64_final_iterations", ctypes.c_int32), ("fp64_final_converge", ctypes.c_int32),
                 ("incremental", ctypes.c_int32), ("trace", ctypes.c_int32),
                 ("stop_at_precision_test", ctypes.c_int32), ("max_iterations", ctypes.c_int32),
-                ("mp2", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("mp2", ctypes.c_int32), ("concurrent_classes", ctypes.c_int32)]
 
 
 class hfd_scf_result(ctypes.Structure):
@@ -65,7 +65,7 @@ def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75,
             want_density=True, mixed_cutoff=0.0, mixed_switch_energy=1e-7, mixed_switch_density=1e-7,
             mixed_switch_diis=1e-6,
             fp64_final_iterations=2, fp64_final_converge=False, incremental=False, trace=False,
-            stop_at_precision_test=False, max_iterations=0, mp2=False):
+            stop_at_precision_test=False, max_iterations=0, mp2=False, concurrent_classes=False):
     """RestrictedHartreeFock / UnrestrictedHartreeFock Init + Calculate.
 
     mixed_cutoff > 0 selects the precision form of the Fock builds (FP32
@@ -86,6 +86,7 @@ def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75,
     o.stop_at_precision_test = int(stop_at_precision_test)
     o.max_iterations = int(max_iterations)
     o.mp2 = int(mp2)
+    o.concurrent_classes = int(concurrent_classes)
     z = np.ascontiguousarray(Z, dtype=np.int32)
     x = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
     nbf_guess = 40 * len(z) + 64

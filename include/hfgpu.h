@@ -88,7 +88,9 @@ typedef struct {
   double density_threshold; /* density screening cutoff; 0 = schwarz_threshold */
   int32_t cuda_graphs;      /* 1: plain-form direct builds replay a CUDA graph
                                (hfg_set_graphs); default 0 */
-  int32_t reserved;
+  int32_t concurrent_classes; /* 1: a build's class kernels run concurrently
+                               on the build stream and four auxiliary streams
+                               (hfg_set_streams); default 0 */
 } hfg_opts;
 
 typedef struct hfg_ctx hfg_ctx;
@@ -258,6 +260,12 @@ hfg_status hfg_ctx_stats(const hfg_ctx *ctx, hfg_stats *out);
  * legacy default stream; 0 selects the context's own).  Any setter
  * (autotune, shard, precision settings, profiling) starts over. */
 hfg_status hfg_set_graphs(hfg_ctx *ctx, int32_t on);
+/* Concurrent class kernels (no reference counterpart): with `on`, the
+ * quartet classes of a direct or batched build are spread over the build
+ * stream and four auxiliary streams of the context (forked and joined by
+ * events; J/K accumulate by atomics, each split class stream has its own
+ * scratch region), so small molecules' class kernels overlap. */
+hfg_status hfg_set_streams(hfg_ctx *ctx, int32_t on);
 
 /* Grid autotuner (no reference counterpart): times every fused quartet
  * class's J/K kernel at 1, 2, 4, 8 and 16 blocks per SM on the density dP

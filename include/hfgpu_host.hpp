@@ -248,6 +248,11 @@ class HartreeFockAlgorithm {
   virtual double Step(int iter) = 0;
   double GetTotalEnergy() const { return totalEnergy; }
   double GetMP2Energy() const { return mp2Energy; }  // HartreeFockAlgorithm.h:89-92
+  // device execution of the Fock builds (no reference counterpart): CUDA-graph
+  // replay of plain builds, and a build's classes on concurrent streams.  For
+  // a process with one SCF at a time; off for host threads sharing a device.
+  bool cudaGraphs = false;
+  bool concurrentClasses = false;
   double mp2Energy = 0;
 
  protected:

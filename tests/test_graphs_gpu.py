@@ -1,13 +1,15 @@
-"""CUDA-graph replay of the plain direct build (hfg_set_graphs): the second
-build with the same buffers is captured, later ones replay it, and every
-result equals the build without graphs -- also when the density changes in
-place, when the buffers change and after a setter."""
+"""CUDA-graph replay of the plain direct build (hfg_set_graphs) and
+concurrent class streams (hfg_set_streams): the second build with the same
+buffers is captured, later ones replay it, and every result equals the
+single-stream build without graphs -- also when the density changes in
+place, when the buffers change and after a setter; SCF energies with both on
+equal those without."""
 import numpy as np
 import pytest
 import torch
 
 from hartreefock_b200 import engine as E
-from hartreefock_b200 import molecules
+from hartreefock_b200 import molecules, scf
 
 pytestmark = pytest.mark.gpu
 
@@ -23,6 +25,7 @@ def test_graph_replay_matches_plain_builds():
     plain = E.Engine(Z, xyz, "6-31g*")
     graph = E.Engine(Z, xyz, "6-31g*")
     graph.set_graphs(True)
+    graph.set_streams(True)
     n = plain.nbf
     dP = torch.zeros(n, n, dtype=torch.float64, device="cuda")
     dG = torch.zeros_like(dP)
@@ -57,6 +60,7 @@ def test_graph_replay_uhf():
     plain = E.Engine(Z, xyz, "6-31g*")
     graph = E.Engine(Z, xyz, "6-31g*")
     graph.set_graphs(True)
+    graph.set_streams(True)
     n = plain.nbf
     Pa, Pb = _density(n, 1) * 0.5, _density(n, 2) * 0.5
     t = [torch.from_numpy(x).cuda() for x in (Pa, Pb)]
@@ -68,3 +72,15 @@ def test_graph_replay_uhf():
     wa, wb = plain.fock_uhf(Pa, Pb)
     assert np.abs(Ga.cpu().numpy() - wa).max() < 1e-12 * max(1.0, np.abs(wa).max())
     assert np.abs(Gb.cpu().numpy() - wb).max() < 1e-12 * max(1.0, np.abs(wb).max())
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_scf_with_graphs_and_streams_matches(mixed):
+    Z, xyz = molecules.water_cluster(3, seed=2)
+    kw = dict(alpha=0.5, init_guess=0.0, post_diis=0, want_density=False)
+    if mixed:
+        kw["mixed_cutoff"] = 1e-4
+    a = scf.run_scf(Z, xyz, "6-31g*", **kw)
+    b = scf.run_scf(Z, xyz, "6-31g*", concurrent_classes=True, **kw)
+    assert a["converged"] and b["converged"]
+    assert abs(a["energy"] - b["energy"]) < (1e-6 if mixed else 1e-9)

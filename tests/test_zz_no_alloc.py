@@ -24,7 +24,7 @@ def test_noalloc_fock_matches_allocating_entry_point():
     A = rng.normal(size=(n, n)) * 0.1
     P = torch.from_numpy(A + A.T).cuda()
     G_ref = torch.empty_like(P)
-    stream = torch.cuda.current_stream().cuda_stream
+    stream = E._torch_stream()  # torch's stream: ordered with the fills and copies below
     eng.fock_rhf_device(P.data_ptr(), G_ref.data_ptr(), stream)
     torch.cuda.synchronize()
     want = G_ref.cpu().numpy()
