@@ -134,17 +134,21 @@ SCF_WATERS = 32
 
 def scf_comparison(waters: int):
     """Plain FP64 vs precision-form RHF of (H2O)_waters / 6-31G*, through the
-    one-call driver (C++ host API: device-resident SCF over the engine)."""
+    one-call driver (C++ host API: device-resident SCF over the engine).  Each
+    form runs twice and keeps its faster wall time (the first SCF of a form
+    also pays one-off costs: library handles, first allocations)."""
     from hartreefock_b200 import molecules, scf
     Z, xyz = molecules.water_cluster(waters, seed=SEED)
     kw = dict(alpha=0.75, init_guess=0.75, post_diis=0, schwarz_threshold=THRESHOLD, concurrent_classes=True)
     runs = {}
     for name, extra in (("fp64", {}), ("mixed", {"mixed_cutoff": 1e-4}),
                         ("fp64_same_criteria", {"stop_at_precision_test": True})):
-        t0 = time.perf_counter()
-        r = scf.run_scf(Z, xyz, BASIS, **kw, **extra)
-        wall = time.perf_counter() - t0
-        runs[name] = (wall, r)
+        for _ in range(2):
+            t0 = time.perf_counter()
+            r = scf.run_scf(Z, xyz, BASIS, **kw, **extra)
+            wall = time.perf_counter() - t0
+            if name not in runs or wall < runs[name][0]:
+                runs[name] = (wall, r)
     ref_wall, ref = runs["fp64"]
 
     def summary(name):
@@ -173,6 +177,9 @@ def scf_comparison(waters: int):
         "fp64_same_criteria": dict(summary("fp64_same_criteria"), criteria="plain FP64 builds, the mixed run's rule"),
         "speedup_wall": ref_wall / runs["mixed"][0],
         "speedup_wall_same_criteria": runs["fp64_same_criteria"][0] / runs["mixed"][0],
+        "speedup_init_plus_scf": (ref["seconds_init"] + ref["seconds_total"]) /
+                                 (runs["mixed"][1]["seconds_init"] + runs["mixed"][1]["seconds_total"]),
+        "timing": "wall of the faster of two runs per form; init_plus_scf excludes basis parsing and teardown",
     }
 
 
