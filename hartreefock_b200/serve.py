@@ -99,7 +99,7 @@ class Server:
     jobs' footprints may add up to.  mixed: precision form of the Fock
     builds (FP32 below mixed_cutoff, incremental, FP64 finish) for every
     job; otherwise plain FP64 builds.  Both stop on the precision form's
-    rule (|dE| < 1e-7, rms dD < 1e-7, DIIS error < 1e-6, then two full FP64
+    rule (|dE| < 1e-7, rms dD < 1e-7, DIIS error < 1e-7, then two full FP64
     iterations), so the two differ only in their kernels.  scf_kwargs go to every job's SCF
     (scf.run_scf keywords); the defaults here are post_diis 0 (the
     reference's convergence test alone), at most 1000 iterations and the
@@ -111,7 +111,10 @@ class Server:
         if slots < 1 or hbm_budget <= 0:
             raise ValueError("slots >= 1 and a positive budget are required")
         self.slots, self.budget = slots, int(hbm_budget)
-        self.defaults = dict(post_diis=0, max_iterations=1000, eri_convention=E.ERI_EXACT)
+        # the switch rule's DIIS error at 1e-7 (the SCF default is 1e-6): jobs of
+        # the stream with diffuse functions otherwise end up to ~1.3e-6 Eh apart
+        # between the two forms
+        self.defaults = dict(post_diis=0, max_iterations=1000, eri_convention=E.ERI_EXACT, mixed_switch_diis=1e-7)
         if mixed:
             self.defaults["mixed_cutoff"] = mixed_cutoff
         else:
