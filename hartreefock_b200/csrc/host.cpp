@@ -67,12 +67,16 @@ struct Gemm {
   cublasHandle_t h = nullptr;
   double *dA = nullptr, *dB = nullptr, *dC = nullptr;
   size_t capA = 0, capB = 0, capC = 0;
-  ~Gemm() {
+  void release() {
     if (h) cublasDestroy(h);
-    cudaFree(dA);
-    cudaFree(dB);
-    cudaFree(dC);
+    if (dA) cudaFree(dA);
+    if (dB) cudaFree(dB);
+    if (dC) cudaFree(dC);
+    h = nullptr;
+    dA = dB = dC = nullptr;
+    capA = capB = capC = 0;
   }
+  ~Gemm() { release(); }
 };
 Gemm &gemm_state() {
   static thread_local Gemm g;
@@ -147,13 +151,18 @@ struct Solver {
   int *info = nullptr;
   int cap = 0, lwork = 0;
   std::mutex mu;
-  ~Solver() {
+  void release() {
     if (h) cusolverDnDestroy(h);
-    cudaFree(dA);
-    cudaFree(dW);
-    cudaFree(work);
-    cudaFree(info);
+    if (dA) cudaFree(dA);
+    if (dW) cudaFree(dW);
+    if (work) cudaFree(work);
+    if (info) cudaFree(info);
+    h = nullptr;
+    dA = dW = work = nullptr;
+    info = nullptr;
+    cap = lwork = 0;
   }
+  ~Solver() { release(); }
 };
 Solver &solver() {
   static thread_local Solver s;
@@ -166,6 +175,15 @@ void check_solver(cusolverStatus_t e, const char *what) {
   if (e != CUSOLVER_STATUS_SUCCESS) throw std::runtime_error(std::string(what) + " failed");
 }
 }  // namespace
+
+// Frees this host thread's library handles and buffers while the thread (and
+// CUDA) are alive: a thread that exits otherwise frees them in its
+// thread-local destructors, which can run after the process has begun to
+// tear CUDA down.
+void release_thread_state() {
+  gemm_state().release();
+  solver().release();
+}
 
 void eigh(const Matrix &a, std::vector<double> &w, Matrix &v) {
   const int n = a.rows();
@@ -976,6 +994,11 @@ Systems::Molecule build_molecule(const char *basis_path, int32_t natoms, const i
 extern "C" {
 
 const char *hfd_last_error(void) { return g_driver_error.c_str(); }
+
+void hfd_release_thread(void) {
+  hfgpu::release_thread_state();
+  hfg_release_thread();
+}
 
 hfg_status hfd_pulay_solve(const double *B, int32_t m1, int32_t batch, double *c) {
   if (!B || !c || m1 < 2 || batch < 0) return HFG_INVALID_ARG;

@@ -298,12 +298,20 @@ struct BatchedEigh {
   std::vector<char> hwork;
   int *info = nullptr;
   int64_t info_cap = 0;
-  ~BatchedEigh() {
+  void release() {
     if (dwork) cudaFree(dwork);
     if (info) cudaFree(info);
     if (params) cusolverDnDestroyParams(params);
     if (handle) cusolverDnDestroy(handle);
+    dwork = nullptr;
+    info = nullptr;
+    params = nullptr;
+    handle = nullptr;
+    dbytes = 0;
+    info_cap = 0;
+    device = -1;
   }
+  ~BatchedEigh() { release(); }
 };
 thread_local BatchedEigh g_eigh;
 }  // namespace
@@ -397,3 +405,5 @@ extern "C" hfg_status hfg_eigh_batched(const double *dA, double *dV, double *dW,
     return hfg::fail_external(HFG_DEVICE_ERROR, ex.what());
   }
 }
+
+extern "C" void hfg_release_thread(void) { g_eigh.release(); }

@@ -28,7 +28,8 @@ EXPORTED = ["hfg_default_opts", "hfg_last_error", "hfg_device_count", "hfg_ctx_c
             "hfg_fock_rhf_noalloc", "hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental",
             "hfg_set_shard", "hfg_batch_create", "hfg_batch_size", "hfg_batch_layout", "hfg_fock_rhf_batch_device",
             "hfg_fock_uhf_batch_device", "hfg_eigh_batched", "hfg_one_electron",
-            "hfg_mo_eri_ovov", "hfg_mp2_rhf", "hfg_autotune", "hfg_set_graphs", "hfg_set_streams"]
+            "hfg_mo_eri_ovov", "hfg_mp2_rhf", "hfg_autotune", "hfg_set_graphs", "hfg_set_streams",
+            "hfg_release_thread"]
 
 
 class HfgError(RuntimeError):

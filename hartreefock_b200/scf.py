@@ -37,7 +37,8 @@ class hfd_scf_result(ctypes.Structure):
                 ("seconds_init", ctypes.c_double), ("mp2_energy", ctypes.c_double)]
 
 
-DRIVER_SYMBOLS = ["hfd_default_scf_opts", "hfd_last_error", "hfd_scf", "hfd_one_electron", "hfd_pulay_solve"]
+DRIVER_SYMBOLS = ["hfd_default_scf_opts", "hfd_last_error", "hfd_scf", "hfd_one_electron", "hfd_pulay_solve",
+                  "hfd_release_thread"]
 
 
 def _lib():
@@ -56,6 +57,8 @@ def _lib():
         L.hfd_one_electron.restype = ctypes.c_int
         L.hfd_pulay_solve.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]
         L.hfd_pulay_solve.restype = ctypes.c_int
+        L.hfd_release_thread.argtypes = []
+        L.hfd_release_thread.restype = None
         L._hfd_ready = True
     return L
 
@@ -141,3 +144,9 @@ def pulay_solve(B: np.ndarray) -> np.ndarray:
     if st != 0:
         raise E.HfgError(st, "hfd_pulay_solve")
     return c
+
+
+def release_thread():
+    """Free the calling thread's library handles (hfd_release_thread); worker
+    threads call it before they exit."""
+    _lib().hfd_release_thread()

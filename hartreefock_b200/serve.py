@@ -170,6 +170,9 @@ class Server:
                 job = self._admit()
                 while job is None:
                     if self._closing and not self._queue:
+                        if self.runner is _driver_runner:
+                            from . import scf
+                            scf.release_thread()  # this thread's handles, while CUDA is up
                         return
                     self._cv.wait()
                     job = self._admit()

@@ -219,6 +219,11 @@ hfg_status hfg_mo_eri_ovov(hfg_ctx *ctx, const double *dC, int32_t i0, int32_t n
  * RestrictedHartreeFock::CalculateMp2Energy (RestrictedHartreeFock.cpp:251-288). */
 hfg_status hfg_mp2_rhf(hfg_ctx *ctx, const double *C, const double *eps, int32_t nocc, double *e_mp2);
 
+/* Frees the calling host thread's library state (the batched eigensolver's
+ * handle and workspace).  For worker threads that exit while the process
+ * goes on: call it before the thread ends. */
+void hfg_release_thread(void);
+
 /* Eigen-decomposition of `batch` symmetric n x n matrices (device, FP64,
  * contiguous) on `stream`: dW receives batch x n ascending eigenvalues, dV
  * batch x n x n eigenvectors with eigenvector k of matrix b in row k of block

@@ -64,6 +64,11 @@ typedef struct {
 void hfd_default_scf_opts(hfd_scf_opts *o);
 /* Text of the calling thread's last hfd_* failure. */
 const char *hfd_last_error(void);
+/* Frees the calling host thread's handles and buffers (the SCF's host-side
+ * cuBLAS / cuSOLVER state and hfg_release_thread's).  A worker thread that
+ * ran hfd_scf calls it before it exits, so that nothing of it is freed by
+ * thread-exit destructors while the process tears CUDA down. */
+void hfd_release_thread(void);
 /* The Pulay (DIIS) system of DIIS.h:72 for `batch` molecules: B holds batch
  * row-major m1 x m1 bordered matrices (error inner products, then the row
  * and column of ones), c receives batch x m1 solutions of B c = (0,..,0,1)
