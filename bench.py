@@ -139,7 +139,7 @@ def scf_comparison(waters: int):
     also pays one-off costs: library handles, first allocations)."""
     from hartreefock_b200 import molecules, scf
     Z, xyz = molecules.water_cluster(waters, seed=SEED)
-    kw = dict(alpha=0.75, init_guess=0.75, post_diis=0, schwarz_threshold=THRESHOLD, concurrent_classes=True)
+    kw = dict(alpha=0.75, init_guess=0.75, post_diis=0, schwarz_threshold=THRESHOLD, concurrent_classes=2)
     runs = {}
     for name, extra in (("fp64", {}), ("mixed", {"mixed_cutoff": 1e-4}),
                         ("fp64_same_criteria", {"stop_at_precision_test": True})):

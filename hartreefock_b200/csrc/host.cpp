@@ -483,9 +483,8 @@ void HartreeFockAlgorithm::Init(Systems::Molecule *molecule) {
     integralsRepository.options.mixed_cutoff = std::max(0.0, mixedCutoff);
   }
   // the SCF's builds reuse one density and one G buffer: with cudaGraphs they
-  // replay as a graph; concurrentClasses spreads a build's classes over
-  // streams (both for one SCF per process: they are not for several host
-  // threads driving the device at once)
+  // replay as a graph (one host thread driving the device); concurrentClasses
+  // spreads a build's classes over streams
   integralsRepository.options.cuda_graphs = cudaGraphs ? 1 : 0;
   integralsRepository.options.concurrent_classes = concurrentClasses ? 1 : 0;
   integralsRepository.Reset(molecule);
@@ -1060,7 +1059,8 @@ hfg_status hfd_scf(const char *basis_path, int32_t natoms, const int32_t *Z, con
     algo->stopAtPrecisionTest = opts->stop_at_precision_test != 0;
     algo->incrementalFock = opts->incremental != 0;
     algo->traceIterations = opts->trace != 0;
-    algo->cudaGraphs = algo->concurrentClasses = opts->concurrent_classes != 0;
+    algo->concurrentClasses = opts->concurrent_classes >= 1;
+    algo->cudaGraphs = opts->concurrent_classes >= 2;
     algo->Init(&mol);
     const double e = algo->Calculate();
     std::memset(result, 0, sizeof *result);

@@ -89,7 +89,7 @@ def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75,
     o.stop_at_precision_test = int(stop_at_precision_test)
     o.max_iterations = int(max_iterations)
     o.mp2 = int(mp2)
-    o.concurrent_classes = int(concurrent_classes)
+    o.concurrent_classes = int(concurrent_classes)  # 0, 1 streams, 2 streams + graphs
     z = np.ascontiguousarray(Z, dtype=np.int32)
     x = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
     nbf_guess = 40 * len(z) + 64

@@ -102,19 +102,22 @@ class Server:
     rule (|dE| < 1e-7, rms dD < 1e-7, DIIS error < 1e-7, then two full FP64
     iterations), so the two differ only in their kernels.  scf_kwargs go to every job's SCF
     (scf.run_scf keywords); the defaults here are post_diis 0 (the
-    reference's convergence test alone), at most 1000 iterations and the
-    exact ERI convention.  runner(job) -> result replaces the driver call
+    reference's convergence test alone), at most 1000 iterations, the exact
+    ERI convention and each job's class kernels on concurrent streams (no
+    CUDA graphs: their capture does not mix with other threads' device-wide
+    synchronisation).  runner(job) -> result replaces the driver call
     (host-side tests)."""
 
     def __init__(self, slots: int = 8, hbm_budget: int = 32 << 30, mixed: bool = True, mixed_cutoff: float = 1e-4,
-                 scf_kwargs=None, runner=None):
+                 scf_kwargs=None, runner=None, concurrent_classes: bool = True):
         if slots < 1 or hbm_budget <= 0:
             raise ValueError("slots >= 1 and a positive budget are required")
         self.slots, self.budget = slots, int(hbm_budget)
         # the switch rule's DIIS error at 1e-7 (the SCF default is 1e-6): jobs of
         # the stream with diffuse functions otherwise end up to ~1.3e-6 Eh apart
         # between the two forms
-        self.defaults = dict(post_diis=0, max_iterations=1000, eri_convention=E.ERI_EXACT, mixed_switch_diis=1e-7)
+        self.defaults = dict(post_diis=0, max_iterations=1000, eri_convention=E.ERI_EXACT, mixed_switch_diis=1e-7,
+                             concurrent_classes=1 if concurrent_classes else 0)
         if mixed:
             self.defaults["mixed_cutoff"] = mixed_cutoff
         else:

@@ -38,9 +38,10 @@ typedef struct {
   int32_t max_iterations;    /* the algorithm's iteration cap; 0 = 3000, the
                                 reference's default (RestrictedHartreeFock.h:31) */
   int32_t mp2;               /* 1: RHF MP2 energy after the SCF (result.mp2_energy) */
-  int32_t concurrent_classes;/* 1: graphs and concurrent class streams for the builds
-                                (HartreeFockAlgorithm::cudaGraphs / concurrentClasses);
-                                for one SCF per process at a time */
+  int32_t concurrent_classes;/* 1: a build's classes on concurrent streams
+                                (HartreeFockAlgorithm::concurrentClasses); 2: also CUDA-graph
+                                replay of plain builds (cudaGraphs), for one host thread
+                                driving the device; 0: neither */
 } hfd_scf_opts;
 
 typedef struct {

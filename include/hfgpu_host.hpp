@@ -249,8 +249,9 @@ class HartreeFockAlgorithm {
   double GetTotalEnergy() const { return totalEnergy; }
   double GetMP2Energy() const { return mp2Energy; }  // HartreeFockAlgorithm.h:89-92
   // device execution of the Fock builds (no reference counterpart): CUDA-graph
-  // replay of plain builds, and a build's classes on concurrent streams.  For
-  // a process with one SCF at a time; off for host threads sharing a device.
+  // replay of plain builds (for one host thread driving the device: a capture
+  // does not mix with other threads' device-wide synchronisation), and a
+  // build's classes on concurrent streams.
   bool cudaGraphs = false;
   bool concurrentClasses = false;
   double mp2Energy = 0;

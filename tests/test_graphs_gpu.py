@@ -81,6 +81,6 @@ def test_scf_with_graphs_and_streams_matches(mixed):
     if mixed:
         kw["mixed_cutoff"] = 1e-4
     a = scf.run_scf(Z, xyz, "6-31g*", **kw)
-    b = scf.run_scf(Z, xyz, "6-31g*", concurrent_classes=True, **kw)
+    b = scf.run_scf(Z, xyz, "6-31g*", concurrent_classes=2, **kw)
     assert a["converged"] and b["converged"]
     assert abs(a["energy"] - b["energy"]) < (1e-6 if mixed else 1e-9)
