@@ -346,10 +346,10 @@ def main():
     torch.cuda.synchronize()
     stats_full = eng.stats()
     G_full = dG.clone()
-    # grid per class from the autotuner (timed on this density, before warm-up),
-    # then the classes of every build over concurrent streams
-    grids = eng.autotune(dP) if not args.no_autotune else {}
+    # the classes of every build over concurrent streams, then the grid from
+    # the autotuner (timed on this density, before warm-up)
     eng.set_streams(not args.no_streams)
+    grids = eng.autotune(dP) if not args.no_autotune else {}
     # N > 1: every rank builds its shard of each class's tasks, one NCCL
     # all-reduce of G per build (hartreefock_b200/shards.py)
     sf = None
@@ -440,7 +440,7 @@ def main():
                    "schwarz_threshold": THRESHOLD, "shell_quartets": stats_full["shell_quartets"],
                    "function_quartets": stats_full["function_quartets"],
                    "l2": "flushed (256 MB write) between steps",
-                   "grid_blocks_per_sm": grids or "fixed 4",
+                   "grid_blocks_per_sm": grids or ("fixed 4" if args.no_streams else "fixed 1"),
                    "class_streams": 1 if args.no_streams else 9,
                    "parallelism": f"task shards x{world}, one NCCL all-reduce of G per build" if world > 1
                    else "single GPU"},

@@ -135,7 +135,10 @@ struct hfg_ctx {
   cudaStream_t aux[kAux] = {};
   cudaEvent_t ev_fork = nullptr, ev_join[kAux] = {};
   int num_sms = 148;
-  int blocks_per_sm = 4;  // grid cap of the fused class kernels, in blocks per SM
+  // grid cap of the fused class kernels, in blocks per SM; 0 = automatic: 4
+  // with every class on the build stream, 1 with concurrent class streams
+  // (where other classes share the SMs)
+  int blocks_per_sm = 0;
   int tuned_bps[kNumClasses] = {};  // per class, from hfg_autotune (0 = blocks_per_sm)
   // CUDA graph of the plain direct build (hfg_set_graphs): captured on the
   // second build with the same buffers, stream and settings, replayed after
@@ -381,7 +384,8 @@ static int grid_for(const hfg_ctx *c, int ntasks, int cls) {
   const ClassEntry &e = kClasses[cls];
   const int w = fused_warps(e.la, e.lb, e.lc, e.ld);
   const int blocks = (ntasks + w - 1) / w;
-  const int bps = c->tuned_bps[cls] > 0 ? c->tuned_bps[cls] : c->blocks_per_sm;
+  const int def = c->blocks_per_sm > 0 ? c->blocks_per_sm : (c->use_streams && !c->profiling ? 1 : 4);
+  const int bps = c->tuned_bps[cls] > 0 ? c->tuned_bps[cls] : def;
   return std::max(1, std::min(blocks, c->num_sms * bps));
 }
 
@@ -1552,6 +1556,36 @@ hfg_status hfg_autotune(hfg_ctx *c, const double *dP, int32_t *chosen, int32_t c
   const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
   const int cand[] = {1, 2, 4, 8, 16};
   int written = 0;
+  if (c->use_streams && !c->batch && !c->precision_form()) {
+    // classes share the SMs: one cap for all, timed on whole builds
+    const size_t nn = (size_t)c->nbf * c->nbf;
+    if ((st = ensure(&c->d_G, nn)) != HFG_OK) return st;
+    float best = 1e30f;
+    int best_bps = 1;
+    for (int b : {1, 2, 4}) {
+      for (int k = 0; k < kNumClasses; ++k) c->tuned_bps[k] = b;
+      ++c->config_version;
+      float ms_sum = 0;
+      for (int r = 0; r < 3; ++r) {
+        if ((st = direct_build(c, false, dP, nullptr, c->d_G, nullptr, s)) != HFG_OK) return st;
+        if ((st = finish_timing(c)) != HFG_OK) return st;
+        if (r > 0) ms_sum += c->stats.last_build_ms;  // the first is a warm-up
+      }
+      if (ms_sum < best) {
+        best = ms_sum;
+        best_bps = b;
+      }
+    }
+    for (int k = 0; k < kNumClasses; ++k) c->tuned_bps[k] = best_bps;
+    if (chosen && cap >= 5) {
+      const int rec[5] = {-1, -1, -1, -1, best_bps};  // all classes
+      std::copy(rec, rec + 5, chosen);
+      written = 5;
+    }
+    if (count) *count = written / 5;
+    ++c->config_version;
+    return HFG_OK;
+  }
   for (auto &q : c->qclasses) {
     if (kSplit[q.cls] || q.tasks.empty()) continue;
     ClassLaunch cl = base_launch(c, q, true);
@@ -1561,7 +1595,7 @@ hfg_status hfg_autotune(hfg_ctx *c, const double *dP, int32_t *chosen, int32_t c
     cl.J = c->d_J;
     cl.Ka = c->d_Ka;
     float best = 1e30f;
-    int best_bps = c->blocks_per_sm;
+    int best_bps = 4;
     for (int b : cand) {
       c->tuned_bps[q.cls] = b;
       const int grid = grid_for(c, cl.ntasks, q.cls);

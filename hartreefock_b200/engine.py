@@ -182,7 +182,7 @@ def _autotune(handle, P) -> dict:
     n = ctypes.c_int32()
     _check(library().hfg_autotune(handle, ctypes.c_void_p(dP.data_ptr()), _ptr(rec), len(rec), ctypes.byref(n),
                                   ctypes.c_void_p(_torch_stream())))
-    return {f"({r[0]}{r[1]}|{r[2]}{r[3]})": int(r[4]) for r in rec[:5 * n.value].reshape(-1, 5)}
+    return {("all" if r[0] < 0 else f"({r[0]}{r[1]}|{r[2]}{r[3]})"): int(r[4]) for r in rec[:5 * n.value].reshape(-1, 5)}
 
 
 def eigh_batched(A, method: int = 0):

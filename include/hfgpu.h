@@ -277,7 +277,11 @@ hfg_status hfg_set_streams(hfg_ctx *ctx, int32_t on);
  * (device; a flat batch buffer for batched contexts) and keeps the fastest
  * grid per class for this context's later builds.  `chosen` (optional)
  * receives up to cap/5 records (La, Lb, Lc, Ld, blocks per SM); *count the
- * records written.  Costs about 15 launches per class. */
+ * records written.  Costs about 15 launches per class.  With concurrent
+ * class streams (hfg_set_streams) on a single-molecule plain-form context,
+ * the classes share the SMs, so one cap for all classes (1, 2 or 4 blocks
+ * per SM) is chosen from whole builds instead; its record is
+ * (-1, -1, -1, -1, blocks per SM). */
 hfg_status hfg_autotune(hfg_ctx *ctx, const double *dP, int32_t *chosen, int32_t cap, int32_t *count, void *stream);
 
 /* Per-class timing of the builds (no reference counterpart: instrumentation
