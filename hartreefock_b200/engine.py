@@ -440,6 +440,11 @@ class BatchEngine:
                                                    ctypes.c_void_p(_torch_stream())))
         return Ga, Gb
 
+    def set_streams(self, on: bool = True):
+        """Run a build's class kernels concurrently over the context's
+        auxiliary streams (hfg_set_streams)."""
+        _check(library().hfg_set_streams(self._h, int(on)))
+
     def autotune(self, P) -> dict:
         """Grid autotuner over the batch (P: flat density, batch layout)."""
         return _autotune(self._h, P)
