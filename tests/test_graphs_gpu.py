@@ -30,28 +30,31 @@ def test_graph_replay_matches_plain_builds():
     dP = torch.zeros(n, n, dtype=torch.float64, device="cuda")
     dG = torch.zeros_like(dP)
     torch.cuda.synchronize()  # the builds run on the context's own stream
-    for k in range(5):  # build 1 plain, 2 captured, 3-5 replayed; density changes in place each time
-        P = _density(n, k)
-        dP.copy_(torch.from_numpy(P))
+    # a created stream: the legacy default stream is not captured
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        for k in range(5):  # build 1 plain, 2 captured, 3-5 replayed; density changes in place each time
+            P = _density(n, k)
+            dP.copy_(torch.from_numpy(P))
+            torch.cuda.synchronize()
+            graph.fock_rhf_tensor(dP, dG)
+            torch.cuda.synchronize()
+            want = plain.fock_rhf(P)
+            got = dG.cpu().numpy()
+            assert np.abs(got - want).max() < 1e-12 * max(1.0, np.abs(want).max()), k
+        # new output buffer: built normally, then captured again
+        dG2 = torch.zeros_like(dP)
+        torch.cuda.synchronize()  # the builds run on the context's own stream
+        for _ in range(3):
+            graph.fock_rhf_tensor(dP, dG2)
         torch.cuda.synchronize()
-        graph.fock_rhf_tensor(dP, dG)
+        assert torch.allclose(dG2, dG, rtol=0, atol=1e-12 * float(dG.abs().max()))
+        # a setter invalidates the graph; the result stays the same
+        graph.autotune(dP)
+        for _ in range(3):
+            graph.fock_rhf_tensor(dP, dG2)
         torch.cuda.synchronize()
-        want = plain.fock_rhf(P)
-        got = dG.cpu().numpy()
-        assert np.abs(got - want).max() < 1e-12 * max(1.0, np.abs(want).max()), k
-    # new output buffer: built normally, then captured again
-    dG2 = torch.zeros_like(dP)
-    torch.cuda.synchronize()  # the builds run on the context's own stream
-    for _ in range(3):
-        graph.fock_rhf_tensor(dP, dG2)
-    torch.cuda.synchronize()
-    assert torch.allclose(dG2, dG, rtol=0, atol=1e-12 * float(dG.abs().max()))
-    # a setter invalidates the graph; the result stays the same
-    graph.autotune(dP)
-    for _ in range(3):
-        graph.fock_rhf_tensor(dP, dG2)
-    torch.cuda.synchronize()
-    assert torch.allclose(dG2, dG, rtol=0, atol=1e-12 * float(dG.abs().max()))
+        assert torch.allclose(dG2, dG, rtol=0, atol=1e-12 * float(dG.abs().max()))
     assert graph.stats()["shell_quartets"] == plain.stats()["shell_quartets"]
 
 
@@ -66,8 +69,10 @@ def test_graph_replay_uhf():
     t = [torch.from_numpy(x).cuda() for x in (Pa, Pb)]
     Ga, Gb = torch.zeros_like(t[0]), torch.zeros_like(t[0])
     torch.cuda.synchronize()
-    for _ in range(4):
-        graph.fock_uhf_tensor(t[0], t[1], Ga, Gb)
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        for _ in range(4):
+            graph.fock_uhf_tensor(t[0], t[1], Ga, Gb)
     torch.cuda.synchronize()
     wa, wb = plain.fock_uhf(Pa, Pb)
     assert np.abs(Ga.cpu().numpy() - wa).max() < 1e-12 * max(1.0, np.abs(wa).max())
