@@ -1,4 +1,4 @@
-// Split path for the large classes (more than 150 integrals per shell
+// Split path for the large classes (more than 100 integrals per shell
 // quartet): the fused kernel's per-thread state (the contracted [e0|f0]
 // block plus the full (ab|cd) block plus the J/K partials) does not fit the
 // register file there and spills heavily.  Here

@@ -550,11 +550,12 @@ def hrr_col_code(la, lb, lc, ld):
 
 
 def is_split_class(la, lb, lc, ld):
-    """Classes whose fused kernel spills most: more than 150 integrals per
-    shell quartet.  Below that ((dp|ds), (dd|ps) at 108) the fused kernel's
-    single digestion beats the split path's per-row atomics."""
+    """Classes whose fused kernel spills: more than 100 integrals per shell
+    quartet.  (dp|ds) and (dd|ps) (108) spill too (255 registers, local
+    memory traffic reaching DRAM in their fused kernel); split, (dp|ds) went
+    from ~0.9 to 0.65 ms per (H2O)16 build."""
     n = lambda L: (L + 1) * (L + 2) // 2
-    return n(la) * n(lb) * n(lc) * n(ld) > 150
+    return n(la) * n(lb) * n(lc) * n(ld) > 100
 
 
 def emit_split(out_dir):
