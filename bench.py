@@ -186,7 +186,8 @@ def scf_comparison(waters: int):
 def serving(count: int, slots: int = 8, seed: int = 5):
     """The request loop (hartreefock_b200.serve) on a seeded Poisson stream of
     `count` RHF/UHF jobs, precision form and plain FP64 builds: saturation
-    (every job submitted at once) and an offered rate of half of it."""
+    (every job submitted at once), then offered rates below it (0.25, 0.5 and
+    0.75 of saturation for the precision form, 0.5 for plain FP64)."""
     from hartreefock_b200 import serve
     from hartreefock_b200.basis_io import shell_table
     jobs = serve.draw_jobs(count, seed=seed)
@@ -203,10 +204,10 @@ def serving(count: int, slots: int = 8, seed: int = 5):
         converged[name] = [h.error is None and h.result["converged"] for h in hs]
         sat["not_converged"] = sum(1 for h in hs if h.error is not None or not h.result["converged"])
         runs["saturation"] = sat
-        rate = 0.5 * sat["jobs_per_s"]
-        with serve.Server(slots=slots, hbm_budget=40 << 30, mixed=mixed) as s:
-            hs, half = serve.poisson_stream(s, jobs, rate=rate, seed=1)
-        runs["half_load"] = half
+        for frac in ((0.25, 0.5, 0.75) if mixed else (0.5,)):
+            with serve.Server(slots=slots, hbm_budget=40 << 30, mixed=mixed) as s:
+                hs, part = serve.poisson_stream(s, jobs, rate=frac * sat["jobs_per_s"], seed=1)
+            runs["half_load" if frac == 0.5 else f"load_{frac:.2f}"] = part
         out[name] = runs
     both = [i for i in range(len(jobs)) if converged["mixed"][i] and converged["fp64"][i]]
     d = [abs(energies["mixed"][i] - energies["fp64"][i]) for i in both]
