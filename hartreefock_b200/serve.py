@@ -51,15 +51,18 @@ def footprint_bytes(Z, xyz, basis: str, unrestricted: bool = False) -> int:
     of up to 32 ket pairs over the triangle of shell pairs), primitive-pair
     tables (96 B FP64 + 48 B FP32 per primitive pair), and the SCF's n x n
     FP64 matrices (h, S, V, F, P, new P, C, G, work, 2 x 6 DIIS entries, the
-    incremental history; about 32 per spin), plus a fixed 16 MiB for the
-    Boys table, counters and library handles."""
+    incremental history; about 32 per spin), the split path's scratch for
+    shells with d functions (an upper bound: 32 quartets x 2 x 961 doubles
+    per task, at most the engine's 512 MiB budget), plus a fixed 16 MiB for
+    the Boys table, counters and library handles."""
     t = shell_table(Z, xyz, basis)
     ns = len(t.L)
     pairs = ns * (ns + 1) // 2
     prim_pairs = int(np.sum(np.triu(np.outer(t.nprim, t.nprim))))
     tasks = pairs * (pairs + 1) // 2 // 32 + pairs
     spins = 2 if unrestricted else 1
-    return int(12 * tasks + 144 * prim_pairs + 8 * t.nbf * t.nbf * 32 * spins + (16 << 20))
+    scratch = min(512 << 20, tasks * 32 * 2 * 961 * 8) if t.max_l >= 2 else 0
+    return int(12 * tasks + 144 * prim_pairs + 8 * t.nbf * t.nbf * 32 * spins + scratch + (16 << 20))
 
 
 class Job:
