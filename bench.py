@@ -442,7 +442,7 @@ def main():
                    "function_quartets": stats_full["function_quartets"],
                    "l2": "flushed (256 MB write) between steps",
                    "grid_blocks_per_sm": grids or ("fixed 4" if args.no_streams else "fixed 1"),
-                   "class_streams": 1 if args.no_streams else 9,
+                   "class_streams": 1 if args.no_streams else 13,
                    "parallelism": f"task shards x{world}, one NCCL all-reduce of G per build" if world > 1
                    else "single GPU"},
         "e2e": {"value": e2e, "unit": "quartets/s", "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": n * n * 8},

@@ -131,7 +131,7 @@ struct hfg_ctx {
   // class kernels of one build are independent (J/K by atomics): they run on
   // the build stream and kAux more, forked and joined by events, so small
   // molecules' classes overlap instead of queueing
-  static constexpr int kAux = 8;
+  static constexpr int kAux = 12;
   cudaStream_t aux[kAux] = {};
   cudaEvent_t ev_fork = nullptr, ev_join[kAux] = {};
   int num_sms = 148;

@@ -89,7 +89,7 @@ typedef struct {
   int32_t cuda_graphs;      /* 1: plain-form direct builds replay a CUDA graph
                                (hfg_set_graphs); default 0 */
   int32_t concurrent_classes; /* 1: a build's class kernels run concurrently
-                               on the build stream and eight auxiliary streams
+                               on the build stream and twelve auxiliary streams
                                (hfg_set_streams); default 0 */
 } hfg_opts;
 
@@ -267,7 +267,7 @@ hfg_status hfg_ctx_stats(const hfg_ctx *ctx, hfg_stats *out);
 hfg_status hfg_set_graphs(hfg_ctx *ctx, int32_t on);
 /* Concurrent class kernels (no reference counterpart): with `on`, the
  * quartet classes of a direct or batched build are spread over the build
- * stream and eight auxiliary streams of the context (forked and joined by
+ * stream and twelve auxiliary streams of the context (forked and joined by
  * events; J/K accumulate by atomics, each split class stream has its own
  * scratch region), so small molecules' class kernels overlap. */
 hfg_status hfg_set_streams(hfg_ctx *ctx, int32_t on);
