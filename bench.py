@@ -1,29 +1,39 @@
 """Benchmark: direct FP64 Fock build (ERI evaluation + J/K digestion) of a
-water cluster, (H2O)_16 / 6-31G* (304 Cartesian basis functions), seeded
-synthetic geometry.
+water cluster, (H2O)_32 / 6-31G* (608 Cartesian basis functions), seeded
+synthetic geometry -- the cluster of the precision-form target.
 
 A step is one two-electron Fock build G[P] over every Schwarz-significant
 shell quartet (threshold 1e-12).  The metric is ERI quartets/s: 8-fold
-unique contracted function quartets evaluated per second.
+unique contracted function quartets of the screened build per second.
 
-The same line carries "scf": complete RHF runs of (H2O)_32 / 6-31G* (608
-functions) through the C++ host API (the one-call driver, hfd_scf), once in
-the plain FP64 form (the reference's convergence thresholds) and once in the
-precision form (FP32 below a density-weighted bound of 1e-4, incremental
-builds from the density difference, two all-FP64 iterations at the end),
-with wall time, iterations, seconds per iteration, and the precision form's
-energy and density error against the FP64 run; plus the plain form stopped
-by the precision form's rule, for a comparison at equal criteria.
+The same line carries
+  "precision_form": the same cluster with the precision form (FP32 below a
+      bound of 1e-4, density screening, incremental builds): a first full
+      build and an incremental build, with their FP64+FP32 roofline;
+  "scf": complete RHF runs of (H2O)_32 through the C++ host API (hfd_scf),
+      plain FP64 vs the precision form, with energy and density errors;
+  "scf_vs_reference": the reference's own RHF (compiled headless) timed on
+      the host -- Init, Calculate, iterations -- beside the GPU SCF of the
+      same molecules;
+  "serving", "batching": the request loop and the batched SCF;
+  "cpu_baseline": the reference's own ERI path on one host thread, on a
+      uniform sample of the same build's quartets, as a time-to-solution rate.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 With N > 1 (torchrun, one rank per GPU, NCCL) the one build is sharded: each
-rank evaluates every N-th task of each quartet class and one all-reduce sums
-the partial G (hartreefock_b200/shards.py); scaling "strong" (the molecule
-is fixed), value = the whole build's quartets / the slowest rank's time.
-`--impl reference` times the reference's own CPU ERI path (oracle/_ref,
-compiled headless from the reference sources) on a bounded sample of the
-same workload with all host threads.
+rank evaluates its cost-balanced share of each quartet class's tasks and one
+all-reduce sums the partial G (hartreefock_b200/shards.py); scaling "strong"
+(the molecule is fixed), value = the whole build's quartets / the slowest
+rank's time.  `--impl reference` times the reference's own CPU ERI path
+(oracle/_ref, compiled headless from the reference sources) on a uniform
+sample of the same build's quartets with all host threads.
+
+Rates against the reference are time-to-solution rates: the reference
+evaluates every unique quartet (it does not screen), the engine only the
+Schwarz-significant ones, and both give the same G within the screening
+threshold; so the reference's rate is the engine's quartet count divided by
+the reference's time for its whole build (extrapolated from the sample).
 """
 from __future__ import annotations
 
@@ -41,7 +51,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WATERS = 16
+WATERS = 32
 BASIS = "6-31g*"
 SEED = 0
 THRESHOLD = 1e-12
@@ -114,18 +124,59 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
-def cpu_baseline(sample_per_thread: int, threads: int):
-    """The reference's own CPU ERI path (IntegralsRepository::getElectronElectron
-    over the build's loop order) on a sample of the same workload."""
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O  # test infrastructure: the reference built headless
-    from hartreefock_b200.basis_io import basis_path
-    Z, xyz = workload()
-    mol = O.Molecule(Z, xyz, basis_path(BASIS))
+    import oracle as O  # test infrastructure: the reference built headless, and the oracle
     if not os.path.exists(O.DRIVER_PATH):
         raise RuntimeError("oracle/_ref/ref_driver missing (build with make -C oracle ref)")
+    return O
+
+
+def reference_rate(sample_per_thread: int, threads: int, waters: int) -> dict:
+    """The reference's own CPU ERI path (IntegralsRepository::getElectronElectron,
+    one repository per thread) on quartets drawn uniformly from every 8-fold
+    unique quartet of the build, and the same rate as a time-to-solution rate
+    on the engine's unit: the Schwarz-significant quartets of the workload
+    (counted by the oracle with the engine's rule) over the time the
+    reference needs for its whole build."""
+    O = _oracle()
+    from hartreefock_b200 import molecules
+    from hartreefock_b200.basis_io import basis_path
+    Z, xyz = molecules.water_cluster(waters, seed=SEED)
+    mol = O.Molecule(Z, xyz, basis_path(BASIS))
     r = O.run_reference(mol, "bench", "/dev/null", extra=f"sample {sample_per_thread}\nthreads {threads}")
     out = json.loads(r["stdout"].strip().splitlines()[-1])
+    raw = out["quartets"] / out["seconds"]
+    cnt = O.screened_quartets(mol, THRESHOLD)
+    build_s = out["unique_quartets"] / raw
+    return {"raw_quartets_per_s": raw, "sampled_quartets": out["quartets"], "sample_seconds": out["seconds"],
+            "threads": threads, "unique_quartets": out["unique_quartets"], "screened_quartets": cnt["kept"],
+            "reference_build_s": build_s, "value": cnt["kept"] / build_s}
+
+
+def reference_scf(cases) -> list:
+    """The reference's own RestrictedHartreeFock (Init + Calculate, compiled
+    headless) on the host, one thread, beside the GPU SCF of the same
+    molecule through the C++ host API."""
+    O = _oracle()
+    from hartreefock_b200 import molecules, scf
+    from hartreefock_b200.basis_io import basis_path
+    out = []
+    for name, (Z, xyz), basis, alpha, guess in cases:
+        mol = O.Molecule(Z, xyz, basis_path(basis))
+        t0 = time.perf_counter()
+        r = O.run_reference(mol, "rhf", os.path.join(ROOT, "gpurun_out", "_ref_scf.bin") if os.path.isdir(
+            os.path.join(ROOT, "gpurun_out")) else "/tmp/_ref_scf.bin", alpha=alpha, init_guess=guess, post_diis=0)
+        wall = time.perf_counter() - t0
+        g = scf.run_scf(Z, xyz, basis, alpha=alpha, init_guess=guess, post_diis=0)
+        it = int(r["iterations"][0])
+        out.append({"molecule": name, "basis": basis, "nbf": mol.nbf, "alpha": alpha, "init_guess": guess,
+                    "reference": {"init_s": float(r["init_seconds"][0]), "scf_s": float(r["scf_seconds"][0]),
+                                  "iterations": it, "s_per_iter": float(r["scf_seconds"][0]) / max(1, it),
+                                  "wall_s": wall, "energy": float(r["energy"][0]), "cores": 1},
+                    "gpu": {"init_s": g["seconds_init"], "scf_s": g["seconds_total"], "iterations": g["iterations"],
+                            "s_per_iter": g["seconds_total"] / max(1, g["iterations"]), "energy": g["energy"]},
+                    "abs_dE": abs(g["energy"] - float(r["energy"][0]))})
     return out
 
 
@@ -274,27 +325,83 @@ def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    per_step = []
+    per_step, last = [], None
     for _ in range(args.warmup):
-        cpu_baseline(2000, threads)
+        reference_rate(500, threads, WATERS)
     for _ in range(args.steps):
-        out = cpu_baseline(args.ref_sample, threads)
-        per_step.append(out["quartets"] / out["seconds"])
+        last = reference_rate(args.ref_sample, threads, WATERS)
+        per_step.append(last["value"])
     value = float(np.mean(per_step))
     line = {
         "metric": METRIC, "value": value, "unit": "quartets/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * args.ref_sample * threads / value, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": 1e3 * last["screened_quartets"] / value, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"(H2O)_{WATERS} {BASIS} direct Fock build, seed {SEED}", "nbf": 19 * WATERS,
-                   "schwarz_threshold": THRESHOLD},
+        "config": {"workload": f"(H2O)_{WATERS} {BASIS} direct RHF Fock build, seed {SEED}", "nbf": 19 * WATERS,
+                   "schwarz_threshold": THRESHOLD, "function_quartets": last["screened_quartets"]},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "quartets/s", "cores": threads, "kind": "reference",
-                         "sample": f"{args.ref_sample} function quartets per thread through "
-                                   "IntegralsRepository::getElectronElectron, one repository per thread"},
+                         "sample": f"{args.ref_sample} quartets per thread drawn uniformly from all "
+                                   f"{last['unique_quartets']} unique quartets of the build, through "
+                                   "IntegralsRepository::getElectronElectron, one repository per thread; value = "
+                                   "the build's Schwarz-significant quartets / the reference's extrapolated time "
+                                   "for its whole (unscreened) build",
+                         "raw_quartets_per_s": float(np.mean([last["raw_quartets_per_s"]])),
+                         "reference_build_s": last["reference_build_s"]},
         "e2e": {"value": value, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def precision_form(Z, xyz, P_host, local, peak64, peak32, steps=5):
+    """The workload's first full build and an incremental build in the
+    precision form (FP32 below a density-weighted bound of 1e-4, density
+    screening at the Schwarz threshold, incremental from the density
+    difference), with their FP64 + FP32 roofline: the time the evaluated
+    quartets' flops need at the two measured peaks over the measured time
+    (flops split by the FP64 / FP32 quartet counts)."""
+    import torch
+    from hartreefock_b200 import engine as E
+    eng = E.Engine(Z, xyz, BASIS, schwarz_threshold=THRESHOLD, device=local, mixed_cutoff=1e-4,
+                   density_screening=True, incremental=True)
+    eng.set_streams(True)
+    sptr = E._torch_stream()
+    n = eng.nbf
+    rng = np.random.default_rng(7)
+    A = rng.normal(size=(n, n)) * 1e-4
+    P0 = torch.from_numpy(P_host).cuda()
+    P1 = torch.from_numpy(P_host + A + A.T).cuda()  # a mid-SCF-sized density change
+    G = torch.empty_like(P0)
+    out = {}
+    for name, seq in (("first_full_build", [P0]), ("incremental_build", [P0, P1])):
+        times, st = [], None
+        for _ in range(steps + 1):
+            eng.fock_reset()
+            for k, P in enumerate(seq):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                a.record()
+                eng.fock_rhf_device(P.data_ptr(), G.data_ptr(), sptr)
+                b.record()
+                torch.cuda.synchronize()
+                if k == len(seq) - 1:
+                    times.append(a.elapsed_time(b))
+                    st = eng.stats()
+        ms = float(np.median(times[1:]))
+        q64, q32 = st["fp64_shell_quartets"], st["fp32_shell_quartets"]
+        frac_eval = (q64 + q32) / max(1, st["shell_quartets"])
+        f64 = st["flops"] * q64 / max(1, st["shell_quartets"])
+        f32 = st["flops"] * q32 / max(1, st["shell_quartets"])
+        t_min = f64 / (peak64 * 1e12) + f32 / (peak32 * 1e12)
+        out[name] = {"ms": ms, "quartets_per_s": st["function_quartets"] * frac_eval / (ms / 1e3),
+                     "shell_quartets_fp64": q64, "shell_quartets_fp32": q32,
+                     "evaluated_fraction": frac_eval,
+                     "roofline": {"bound": "fp64+fp32", "achieved_fp64_tflops": f64 / (ms / 1e3) / 1e12,
+                                  "achieved_fp32_tflops": f32 / (ms / 1e3) / 1e12, "peak_fp64": peak64,
+                                  "peak_fp32": peak32, "frac": t_min / (ms / 1e3),
+                                  "note": "frac = (F64/peak64 + F32/peak32) / time; flops split by quartet counts"}}
+    eng.close()
+    return out
 
 
 def main():
@@ -306,11 +413,13 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--ref-sample", type=int, default=30000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--waters", type=int, default=16,
-                    help="cluster size; the benchmark workload is 16 (smaller values size profiler captures)")
+    ap.add_argument("--waters", type=int, default=WATERS,
+                    help="cluster size; the benchmark workload is 32 (smaller values size profiler captures)")
     ap.add_argument("--scf-waters", type=int, default=SCF_WATERS, help="cluster of the SCF comparison (0: skip)")
     ap.add_argument("--serve-jobs", type=int, default=24, help="jobs of the serving stream (0: skip)")
-    ap.add_argument("--batch-mols", type=int, default=0, help="molecules of the batched SCF (0: skip)")
+    ap.add_argument("--batch-mols", type=int, default=512, help="molecules of the batched SCF (0: skip)")
+    ap.add_argument("--no-reference-scf", action="store_true", help="skip the reference's SCF timing")
+    ap.add_argument("--no-precision", action="store_true", help="skip the precision-form builds")
     ap.add_argument("--no-autotune", action="store_true", help="fixed grid (4 blocks per SM) for every class")
     ap.add_argument("--no-streams", action="store_true", help="every class kernel on the build stream")
     args = ap.parse_args()
@@ -430,8 +539,10 @@ def main():
     eng.set_profiling(False)
     top = max(prof, key=lambda c: c["ms"])
     peak = E.measure_fp64_peak(local)
+    peak32 = E.measure_fp32_peak(local)
     # class flops are whole-class figures; a shard runs 1/world of them
     achieved = top["flops"] / world / (top["ms"] / 1e3) / 1e12
+    build_flops = stats_full["flops"]
 
     line = {
         "metric": METRIC, "value": value, "unit": "quartets/s", "n_gpus": world, "steps": args.steps,
@@ -447,33 +558,46 @@ def main():
                    else "single GPU"},
         "e2e": {"value": e2e, "unit": "quartets/s", "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": n * n * 8},
         "gpu_launches": stats["kernel_launches"] * args.steps,
-        "roofline": {"bound": "fp64", "kernel": f"eri_class_kernel<{top['la']},{top['lb']},{top['lc']},{top['ld']}> (J/K)",
+        "roofline": {"bound": "fp64", "kernel": f"({top['la']}{top['lb']}|{top['lc']}{top['ld']}) J/K class kernel",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "peak_source": "measured in-run: FP64 FMA microbenchmark (hfg_measure_fp64_peak)",
-                     # DRAM bytes of one launch of this kernel on this workload, from an ncu
-                     # capture (dram__bytes_read.sum + dram__bytes_write.sum): L2-resident
-                     "traffic": 5534720, "traffic_unit": "bytes per launch"},
-        "build_tflops": stats_full["flops"] / (total_ms / args.steps / 1e3) / 1e12,
+                     "traffic": None, "traffic_unit": "bytes per launch",
+                     "build": {"achieved": build_flops / world / (total_ms / args.steps / 1e3) / 1e12,
+                               "frac": build_flops / world / (total_ms / args.steps / 1e3) / 1e12 / peak},
+                     "fp32_peak": peak32},
         "classes": [{"class": f"({c['la']}{c['lb']}|{c['lc']}{c['ld']})", "ms": round(c["ms"], 4),
-                     "tflops": round(c["flops"] / max(c["ms"], 1e-9) / 1e9, 3)} for c in prof],
+                     "tflops": round(c["flops"] / max(c["ms"], 1e-9) / 1e9, 3), "tasks": c["tasks"],
+                     "lane_occupancy": round(c["lane_occupancy"], 3),
+                     "kernel": "warp per quartet" if c["warp_kernel"] else "thread per quartet"} for c in prof],
         "clocks": clocks.summary(),
     }
+    eng.close()
+    if rank == 0 and world == 1 and not args.no_precision:
+        line["precision_form"] = precision_form(Z, xyz, P_host, local, peak, peak32)
+        line["roofline"]["fp32"] = line["precision_form"]["first_full_build"]["roofline"]
     if rank == 0 and world == 1 and args.scf_waters > 0:
         line["scf"] = scf_comparison(args.scf_waters)
+    if rank == 0 and world == 1 and not args.no_reference_scf:
+        from hartreefock_b200 import molecules
+        line["scf_vs_reference"] = reference_scf([
+            ("H2O (README geometry)", molecules.H2O_README, "sto-3g", 0.5, 0.0),
+            ("(H2O)_2 seed 0", molecules.water_cluster(2, seed=0), "6-31g*", 0.75, 0.75)])
     if rank == 0 and world == 1 and args.serve_jobs > 0:
         line["serving"] = serving(args.serve_jobs)
     if rank == 0 and world == 1 and args.batch_mols > 0:
         line["batching"] = batching(args.batch_mols)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = 1
-        cb = cpu_baseline(args.ref_sample, threads)
-        line["cpu_baseline"] = {"value": cb["quartets"] / cb["seconds"], "unit": "quartets/s", "cores": threads,
-                                "kind": "reference",
-                                "sample": f"{cb['quartets']} function quartets of the same cluster through the "
-                                          "reference's IntegralsRepository::getElectronElectron, 1 thread"}
+        cb = reference_rate(args.ref_sample, 1, WATERS)
+        line["cpu_baseline"] = {"value": cb["value"], "unit": "quartets/s", "cores": 1, "kind": "reference",
+                                "sample": f"{cb['sampled_quartets']} quartets drawn uniformly from all "
+                                          f"{cb['unique_quartets']} unique quartets of the same cluster, through the "
+                                          "reference's IntegralsRepository::getElectronElectron, 1 thread; value = "
+                                          "the build's Schwarz-significant quartets / the reference's extrapolated "
+                                          "time for its whole (unscreened) build",
+                                "raw_quartets_per_s": cb["raw_quartets_per_s"],
+                                "reference_build_s": cb["reference_build_s"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    eng.close()
     if dist:
         dist.destroy_process_group()
     return 0

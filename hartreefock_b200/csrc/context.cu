@@ -15,6 +15,7 @@
 #include "../../include/hfgpu.h"
 #include "eri_dispatch.cuh"
 #include "eri_split_dispatch.cuh"
+#include "eri_warp_dispatch.cuh"
 
 namespace hfg {
 
@@ -94,6 +95,9 @@ struct QuartetClass {
   Task *d_tasks = nullptr;
   int64_t shell_quartets = 0, function_quartets = 0, prim_quartets = 0;
   double flops = 0;
+  // lane occupancy of the thread-per-quartet layout: primitive quartets the
+  // lanes evaluate over the lanes x the longest lane loop of each task
+  double lane_work = 0, warp_work = 0;
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;  // per-class timing (profiling on)
   float last_ms = 0;
 };
@@ -144,6 +148,7 @@ struct hfg_ctx {
   // second build with the same buffers, stream and settings, replayed after
   bool use_graphs = false;
   bool use_streams = false;  // class kernels over the auxiliary streams (hfg_set_streams)
+  bool use_warp = true;      // large classes on the warp-cooperative kernel (else the split path)
   cudaEvent_t ev_done = nullptr;  // end of the last build on its stream
   unsigned config_version = 0;  // bumped by every setter that changes a build
   struct GraphKey {
@@ -351,8 +356,14 @@ static void build_quartet_classes(hfg_ctx *c, double threshold) {
         int64_t end = lo;
         if (same) end = std::min<int64_t>(end, (int64_t)b + 1);
         if (end <= s0) continue;
-        for (int64_t st = s0; st < end; st += 32)
-          q.tasks.push_back(Task{(int)b, (int)st, (int)std::min<int64_t>(st + 32, end)});
+        for (int64_t st = s0; st < end; st += 32) {
+          const int64_t e1 = std::min<int64_t>(st + 32, end);
+          q.tasks.push_back(Task{(int)b, (int)st, (int)e1});
+          int64_t mx = 0;
+          for (int64_t k2 = st; k2 < e1; ++k2) mx = std::max<int64_t>(mx, c->pair_nprim[kets[k2]]);
+          q.lane_work += (double)bprim * (double)(kprim[e1] - kprim[st]);
+          q.warp_work += 32.0 * (double)bprim * (double)mx;
+        }
         q.shell_quartets += end - s0;
         if (same && end == (int64_t)b + 1) {
           // the diagonal quartet (bra == ket) counts its unique half
@@ -502,6 +513,8 @@ static int ncomp_range(int lo, int hi) {
 // build stream, scratch region 0) while per-class profiling is on.
 static void split_chunking(const hfg_ctx *c, int cls, int ntasks, bool ref, size_t *need, int *chunk_tasks);
 static int scratch_regions(const hfg_ctx *c);
+// the class runs the split (primitive + HRR/digest) kernels over scratch
+static bool uses_split(const hfg_ctx *c, int cls) { return kSplit[cls] && !(kWarp[cls] && c->use_warp); }
 static hfg_status grow_scratch(hfg_ctx *c, int slot, size_t need);
 
 struct ClassStreams {
@@ -534,7 +547,7 @@ struct ClassStreams {
     int k = 0;
     for (size_t i = 0; i < c->qclasses.size(); ++i) {
       const int cls = c->qclasses[i].cls;
-      if (!kSplit[cls] || ntasks[i] <= 0) continue;
+      if (!uses_split(c, cls) || ntasks[i] <= 0) continue;
       size_t nd = 0;
       int chunk = 1;
       split_chunking(c, cls, ntasks[i], ref, &nd, &chunk);
@@ -596,6 +609,11 @@ static hfg_status grow_scratch(hfg_ctx *c, int slot, size_t need) {
 static hfg_status launch_class(hfg_ctx *c, const QuartetClass &q, const ClassLaunch &cl, int mode, bool ref,
                                int prec, cudaStream_t s, int *launches, int slot = 0) {
   const ClassEntry &e = kClasses[q.cls];
+  if (kWarp[q.cls] && c->use_warp && mode != kBlock) {
+    kWarp[q.cls](c->view(), cl, mode, ref, prec, 0, s);
+    ++*launches;
+    return HFG_OK;
+  }
   if (!kSplit[q.cls]) {
     e.launch(c->view(), cl, mode, ref, prec, grid_for(c, cl.ntasks, q.cls), s);
     ++*launches;
@@ -692,7 +710,7 @@ static hfg_status direct_build_body(hfg_ctx *c, bool uhf, const double *dPa, con
     cl.mixed_cutoff = (float)c->mixed_cutoff;
     cl.counters = precise ? c->d_counters : nullptr;
     if (cl.ntasks > 0) {
-      const cudaStream_t cls_stream = cs.pick(kSplit[q.cls] != nullptr);
+      const cudaStream_t cls_stream = cs.pick(uses_split(c, q.cls));
       st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, prec, cls_stream, &launches, cs.slot);
       if (st != HFG_OK) return st;
     }
@@ -913,7 +931,7 @@ static hfg_status batch_build(hfg_ctx *c, bool uhf, const double *dPa, const dou
     cl.Ka = c->d_Ka;
     cl.Kb = c->d_Kb;
     if (cl.ntasks > 0) {
-      const cudaStream_t cls_stream = cs.pick(kSplit[q.cls] != nullptr);
+      const cudaStream_t cls_stream = cs.pick(uses_split(c, q.cls));
       st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, 0, cls_stream, &launches, cs.slot);
       if (st != HFG_OK) return st;
     }
@@ -1044,6 +1062,7 @@ static hfg_status create_context(const hfg_shells *sh, const int *shell_mol, int
   // tuning: HFG_BLOCKS_PER_SM overrides the grid cap (every block stages the
   // class's Boys table once, so fewer, longer-lived blocks stage it less)
   if (const char *e = std::getenv("HFG_BLOCKS_PER_SM")) ctx->blocks_per_sm = std::max(1, std::atoi(e));
+  if (const char *e = std::getenv("HFG_SPLIT_PATH")) ctx->use_warp = std::atoi(e) == 0;
   ctx->batch = shell_mol != nullptr;
   ctx->nmol = ctx->batch ? nmol : 1;
   ctx->nbf = ctx->batch ? 0 : sh->nbf;
@@ -1499,8 +1518,9 @@ hfg_status hfg_class_profile(const hfg_ctx *c, hfg_class_time *out, int32_t cap,
   for (const auto &q : c->qclasses) {
     if (n >= cap) break;
     const ClassEntry &e = kClasses[q.cls];
-    out[n] = hfg_class_time{e.la, e.lb, e.lc, e.ld, q.shell_quartets, q.function_quartets, q.prim_quartets,
-                            q.flops, (double)q.last_ms};
+    out[n] = hfg_class_time{e.la,    e.lb,    e.lc,         e.ld, q.shell_quartets, q.function_quartets, q.prim_quartets,
+                            q.flops, (double)q.last_ms, (int64_t)q.tasks.size(),
+                            q.warp_work > 0 ? q.lane_work / q.warp_work : 0.0, kWarp[q.cls] && c->use_warp ? 1 : 0, 0};
     ++n;
   }
   *count = n;
@@ -1587,7 +1607,7 @@ hfg_status hfg_autotune(hfg_ctx *c, const double *dP, int32_t *chosen, int32_t c
     return HFG_OK;
   }
   for (auto &q : c->qclasses) {
-    if (kSplit[q.cls] || q.tasks.empty()) continue;
+    if (kSplit[q.cls] || kWarp[q.cls] || q.tasks.empty()) continue;
     ClassLaunch cl = base_launch(c, q, true);
     if (cl.ntasks == 0) continue;
     cl.Da = dP;
@@ -1701,6 +1721,9 @@ extern "C" hfg_status hfg_fock_rhf_noalloc(hfg_ctx *c, const double *dP, double 
   using namespace hfg;
   if (!c || !dP || !dG) return fail(HFG_INVALID_ARG, "null argument");
   if (c->batch) return fail(HFG_INVALID_ARG, "batched context: use hfg_fock_rhf_batch_device");
+  if (c->precision_form())
+    return fail(HFG_INVALID_ARG, "hfg_fock_rhf_noalloc: the context has precision-form settings (density screening, "
+                                 "FP32 cutoff or incremental builds); this entry point does plain full FP64 builds only");
   if (c->nbf > kNoAllocMaxNbf)
     return fail(HFG_INVALID_ARG, "hfg_fock_rhf_noalloc: " + std::to_string(c->nbf) +
                                      " basis functions exceed its fixed scratch of " +
@@ -1723,7 +1746,9 @@ extern "C" hfg_status hfg_fock_rhf_noalloc(hfg_ctx *c, const double *dP, double 
     cl.Dt = dP;
     cl.J = J;
     cl.Ka = K;
-    kClasses[q.cls].launch(v, cl, kJkRhf, ref, 0, grid_for(c, cl.ntasks, q.cls), s);
+    // the large classes run warp-cooperatively: shared memory only, no scratch
+    if (kWarp[q.cls]) kWarp[q.cls](v, cl, kJkRhf, ref, 0, 0, s);
+    else kClasses[q.cls].launch(v, cl, kJkRhf, ref, 0, grid_for(c, cl.ntasks, q.cls), s);
   }
   const int fg = std::max(1, std::min(1024, (int)((nn + 255) / 256)));
   finalize_rhf<<<fg, 256, 0, s>>>(J, K, dG, n);

@@ -568,14 +568,14 @@ def emit_split(out_dir):
             continue
         tag = f"{la}{lb}{lc}{ld}"
         hdr.append(f"// ({la}{lb}|{lc}{ld}): bra row `ab` of the block, all ket (c d)")
-        hdr.append(f"template <class R> __device__ __forceinline__ void eri_hrr_row_{tag}(R* __restrict__ out, int ab,")
-        hdr.append("    const double* __restrict__ scr, long long stride, R X0, R X1, R X2, R Y0, R Y1, R Y2) {")
+        hdr.append(f"template <class R, class S> __device__ __forceinline__ void eri_hrr_row_{tag}(R* __restrict__ out, int ab,")
+        hdr.append("    const S* __restrict__ scr, long long stride, R X0, R X1, R X2, R Y0, R Y1, R Y2) {")
         hdr += ["  " + l for l in hrr_row_code(la, lb, lc, ld)]
         hdr.append("}")
         if (la, lb, lc, ld) == (2, 2, 2, 2):
             hdr.append(f"// ({la}{lb}|{lc}{ld}): ket column `ab` of a block stored with bra/ket exchanged")
-            hdr.append(f"template <class R> __device__ __forceinline__ void eri_hrr_col_{tag}(R* __restrict__ out, int ab,")
-            hdr.append("    const double* __restrict__ scr, long long stride, R X0, R X1, R X2, R Y0, R Y1, R Y2) {")
+            hdr.append(f"template <class R, class S> __device__ __forceinline__ void eri_hrr_col_{tag}(R* __restrict__ out, int ab,")
+            hdr.append("    const S* __restrict__ scr, long long stride, R X0, R X1, R X2, R Y0, R Y1, R Y2) {")
             hdr += ["  " + l for l in hrr_col_code(la, lb, lc, ld)]
             hdr.append("}")
         hdr.append("")
@@ -585,14 +585,14 @@ def emit_split(out_dir):
             continue
         tag = f"{la}{lb}{lc}{ld}"
         hdr.append(f"template <> struct EriRows<{la}, {lb}, {lc}, {ld}> {{")
-        hdr.append("  template <class R> static __device__ __forceinline__ void row(R* out, int ab, const double* scr,")
+        hdr.append("  template <class R, class S> static __device__ __forceinline__ void row(R* out, int ab, const S* scr,")
         hdr.append("      long long stride, R X0, R X1, R X2, R Y0, R Y1, R Y2) {")
-        hdr.append(f"    eri_hrr_row_{tag}<R>(out, ab, scr, stride, X0, X1, X2, Y0, Y1, Y2);")
+        hdr.append(f"    eri_hrr_row_{tag}<R, S>(out, ab, scr, stride, X0, X1, X2, Y0, Y1, Y2);")
         hdr.append("  }")
-        hdr.append("  template <class R> static __device__ __forceinline__ void col(R* out, int ab, const double* scr,")
+        hdr.append("  template <class R, class S> static __device__ __forceinline__ void col(R* out, int ab, const S* scr,")
         hdr.append("      long long stride, R X0, R X1, R X2, R Y0, R Y1, R Y2) {")
         if (la, lb, lc, ld) == (2, 2, 2, 2):
-            hdr.append(f"    eri_hrr_col_{tag}<R>(out, ab, scr, stride, X0, X1, X2, Y0, Y1, Y2);")
+            hdr.append(f"    eri_hrr_col_{tag}<R, S>(out, ab, scr, stride, X0, X1, X2, Y0, Y1, Y2);")
         hdr.append("  }")
         hdr.append("};")
     with open(os.path.join(out_dir, "eri_split_gen.cuh"), "w") as fh:
@@ -671,9 +671,243 @@ def emit_split(out_dir):
         fh.write("\n".join(lines))
 
 
+# ---------------------------------------------------------------------------
+# Warp-cooperative programs for the large classes.  One warp evaluates one
+# shell quartet: the per-primitive recursions (vertical recursion and
+# electron transfer, the same nodes, directions and reference-convention
+# pruning as ClassGen) become a list of operations ordered by dependency
+# depth; the warp's lanes run the operations of one depth level side by side
+# on intermediates held in shared memory, with a warp barrier between levels.
+# Every operation has the form
+#   out = c1 * w[a] + c2 * w[b] + c3 * w[c] + c4 * w[d]
+# with per-primitive coefficients selected by kind and Cartesian direction:
+#   vertical (kind 0):  PA_i, WP_i,    n1 * oo2z, -n1 * oo2z * roz
+#   transfer (kind 1):  delta_i, -zoe, n1 * oo2e,  n2 * oo2e
+# Absent operands read slot 0, which always holds zero.  Slots are assigned
+# by a liveness scan (a slot is reused from the level after its last read),
+# so the shared-memory footprint is the peak live set, not the node count.
+# ---------------------------------------------------------------------------
+class WarpProgram:
+    def __init__(self, la, lb, lc, ld, reference):
+        self.la, self.lb, self.lc, self.ld = la, lb, lc, ld
+        self.ltot = la + lb + lc + ld
+        self.reference = reference
+        self.nodes = []  # (kind, dir, operands(4 node ids or None), n1, n2); kind 'F' = Boys input
+        self.vmemo, self.tmemo = {}, {}
+        self.fnodes = []
+        for m in range(self.ltot + 1):
+            self.fnodes.append(self._node(("F", 0, (None,) * 4, 0, 0)))
+
+    def _node(self, spec):
+        self.nodes.append(spec)
+        return len(self.nodes) - 1
+
+    def vrr(self, e, m):
+        key = (e, m)
+        if key in self.vmemo:
+            return self.vmemo[key]
+        if tot(e) == 0:
+            nid = self.fnodes[m]
+        else:
+            i = direction(e)
+            e1 = add(e, i, -1)
+            a, b = self.vrr(e1, m), self.vrr(e1, m + 1)
+            c = d = None
+            n1 = 0
+            if e1[i] > 0:
+                e2 = add(e, i, -2)
+                c, d = self.vrr(e2, m), self.vrr(e2, m + 1)
+                n1 = e1[i]
+            nid = self._node((0, i, (a, b, c, d), n1, 0))
+        self.vmemo[key] = nid
+        return nid
+
+    def et(self, e, f):
+        key = (e, f)
+        if key in self.tmemo:
+            return self.tmemo[key]
+        if tot(f) == 0:
+            nid = self.vrr(e, 0)
+        elif self.reference and tot(e) < tot(f) - 1:
+            nid = None
+        else:
+            i = direction(f)
+            f1 = add(f, i, -1)
+            t1 = self.et(e, f1)
+            t2 = self.et(add(e, i, 1), f1)
+            t3 = self.et(add(e, i, -1), f1) if e[i] > 0 else None
+            t4 = self.et(e, add(f, i, -2)) if f1[i] > 0 else None
+            if t1 is None and t2 is None and t3 is None and t4 is None:
+                nid = None
+            else:
+                nid = self._node((1, i, (t1, t2, t3, t4), e[i] if t3 is not None else 0,
+                                  f1[i] if t4 is not None else 0))
+        self.tmemo[key] = nid
+        return nid
+
+    def build(self):
+        E = comps_range(self.la, self.la + self.lb)
+        Fc = comps_range(self.lc, self.lc + self.ld)
+        accn = [self.et(e, f) for e in E for f in Fc]
+        n = len(self.nodes)
+        level = [0] * n
+        for k, (kind, _, ops, _, _) in enumerate(self.nodes):
+            if kind != "F":
+                level[k] = 1 + max(level[o] for o in ops if o is not None)
+        nlev = max(level) if n else 0
+        last = [-1] * n
+        for k, (kind, _, ops, _, _) in enumerate(self.nodes):
+            for o in ops:
+                if o is not None:
+                    last[o] = max(last[o], level[k])
+        for o in accn:
+            if o is not None:
+                last[o] = nlev + 1  # read by the contraction after the last level
+        # slot 0: zero; F nodes first (written before level 1)
+        slot = [0] * n
+        free, nslots = [], 1
+        order = sorted(range(n), key=lambda k: (level[k], k))
+        by_level = {}
+        for k in order:
+            by_level.setdefault(level[k], []).append(k)
+        released = {}
+        for k in range(n):
+            if last[k] >= 0:
+                released.setdefault(last[k] + 1, []).append(k)
+        for L in range(nlev + 1):
+            for k in released.get(L, []):
+                free.append(slot[k])
+            free.sort(reverse=True)
+            for k in by_level.get(L, []):
+                if last[k] < 0 and self.nodes[k][0] != "F":
+                    raise RuntimeError("dead node")
+                if free:
+                    slot[k] = free.pop()
+                else:
+                    slot[k] = nslots
+                    nslots += 1
+        ops, bounds = [], [0]
+        for L in range(1, nlev + 1):
+            for k in by_level.get(L, []):
+                kind, i, operands, n1, n2 = self.nodes[k]
+                sl = [slot[o] if o is not None else 0 for o in operands]
+                ops.append((slot[k], i, kind, n1, n2, sl))
+            bounds.append(len(ops))
+        fslots = [slot[k] for k in self.fnodes]
+        acc = [slot[o] if o is not None else 0 for o in accn]
+        return dict(ops=ops, bounds=bounds, nslots=nslots, fslots=fslots, acc=acc, ne=len(E), nf=len(Fc))
+
+
+def warp_flops(prog):
+    """flops of one primitive quartet's recursions as the generated straight-line code counts them"""
+    return None
+
+
+def emit_warp(out_dir):
+    """eri_warp_gen.cuh: the level-ordered programs and traits of the large
+    classes (WarpProg<LA,LB,LC,LD,REF>), one launcher TU per large class and
+    the dispatch table kWarp[] (nullptr for the classes the per-thread kernel
+    serves)."""
+    pairs, quartets = canonical_classes()
+    hdr = ["// Generated by gen_eri.py -- do not edit.", "#pragma once", "", "#include <stdint.h>", "",
+           "namespace hfg {", "", "template <int LA, int LB, int LC, int LD, bool REF> struct WarpProg;"]
+    for (la, lb, lc, ld) in quartets:
+        if not is_split_class(la, lb, lc, ld):
+            continue
+        for ref in (False, True):
+            has_ref = (lc + ld) >= la + 2
+            pr = WarpProgram(la, lb, lc, ld, ref and has_ref).build()
+            tag = f"{la}{lb}{lc}{ld}" + ("r" if ref else "")
+            words = []
+            for (out, i, kind, n1, n2, sl) in pr["ops"]:
+                assert max(sl + [out]) < 65536 and n1 < 16 and n2 < 16
+                x = out | (i << 16) | (kind << 18) | (n1 << 20) | (n2 << 24)
+                words.append(f"{{{x}u, {sl[0] | (sl[1] << 16)}u, {sl[2] | (sl[3] << 16)}u, 0u}}")
+            hdr.append(f"// ({la}{lb}|{lc}{ld}) {'reference' if ref else 'exact'}: {len(pr['ops'])} operations in "
+                       f"{len(pr['bounds']) - 1} levels, {pr['nslots']} slots")
+            hdr.append(f"static __device__ const uint4 kWarpOps_{tag}[] = {{")
+            for k in range(0, len(words), 4):
+                hdr.append("    " + ", ".join(words[k:k + 4]) + ",")
+            hdr.append("};")
+            hdr.append(f"static __device__ const uint16_t kWarpAcc_{tag}[] = {{")
+            for k in range(0, len(pr["acc"]), 16):
+                hdr.append("    " + ", ".join(str(v) for v in pr["acc"][k:k + 16]) + ",")
+            hdr.append("};")
+            hdr.append(f"template <> struct WarpProg<{la}, {lb}, {lc}, {ld}, {'true' if ref else 'false'}> {{")
+            hdr.append(f"  static constexpr int kSlots = {pr['nslots']};")
+            hdr.append(f"  static constexpr int kOps = {len(pr['ops'])};")
+            hdr.append(f"  static constexpr int kLevels = {len(pr['bounds']) - 1};")
+            hdr.append(f"  static constexpr int kAcc = {pr['ne'] * pr['nf']};")
+            hdr.append("  static __device__ __forceinline__ const uint4 *ops() { return kWarpOps_%s; }" % tag)
+            hdr.append("  static __device__ __forceinline__ const uint16_t *acc() { return kWarpAcc_%s; }" % tag)
+            hdr.append("  static __device__ __forceinline__ int bound(int l) {")
+            hdr.append("    constexpr int b[] = {" + ", ".join(str(v) for v in pr["bounds"]) + "};")
+            hdr.append("    return b[l];")
+            hdr.append("  }")
+            hdr.append("  static __device__ __forceinline__ int fslot(int m) {")
+            hdr.append("    constexpr int f[] = {" + ", ".join(str(v) for v in pr["fslots"]) + "};")
+            hdr.append("    return f[m];")
+            hdr.append("  }")
+            hdr.append("};")
+    hdr += ["", "}  // namespace hfg", ""]
+    with open(os.path.join(out_dir, "eri_warp_gen.cuh"), "w") as fh:
+        fh.write("\n".join(hdr) + "\n")
+    modes = ("kStorePacked", "kJkRhf", "kJkUhf")
+    for (a, b, c, d) in quartets:
+        if not is_split_class(a, b, c, d):
+            continue
+        has_ref = (c + d) >= a + 2
+        tag = f"{a}{b}{c}{d}"
+        for scr in (False, True):
+            name = f"launch_warp_{tag}" + ("_scr" if scr else "")
+            lines = [f"// Generated by gen_eri.py: warp-cooperative launchers for the ({a}{b}|{c}{d}) class"
+                     + (" (density-screened J/K)." if scr else "."),
+                     '#include "eri_warp.cuh"', '#include "eri_warp_dispatch.cuh"', "", "namespace hfg {", "",
+                     f"void {name}(const EngineView &v, const ClassLaunch &cl, int mode, bool ref, int prec, int grid,",
+                     "             cudaStream_t s) {"]
+            if not scr:
+                lines += ["  if (prec != 0 && (mode == kJkRhf || mode == kJkUhf)) {",
+                          f"    launch_warp_{tag}_scr(v, cl, mode, ref, prec, grid, s);", "    return;", "  }"]
+            lines.append("  switch (mode) {")
+            for mode in (("kJkRhf", "kJkUhf") if scr else modes):
+                lines.append(f"    case {mode}:")
+                variants = [("kScreenMixed", "prec == 2"), ("kScreenFp64", None)] if scr else [("kScreenNone", None)]
+                for r in ((True, False) if has_ref else (False,)):
+                    cond = "ref" if (has_ref and r) else ("!ref" if has_ref else None)
+                    for sv, pc in variants:
+                        conds = " && ".join(x for x in (cond, pc) if x)
+                        call = f"launch_warp<{a}, {b}, {c}, {d}, {mode}, {'true' if r else 'false'}, {sv}>(v, cl, grid, s);"
+                        if conds:
+                            lines.append(f"      if ({conds}) {{ {call} break; }}")
+                        else:
+                            lines.append(f"      {call}")
+                lines.append("      break;")
+            lines += ["    default:", "      break;", "  }"]
+            lines += ["  (void)ref;", "  (void)prec;", "}", "", "}  // namespace hfg", ""]
+            with open(os.path.join(out_dir, f"eri_warp_{tag}" + ("_scr" if scr else "") + ".cu"), "w") as fh:
+                fh.write("\n".join(lines))
+    lines = ["// Generated by gen_eri.py: warp-cooperative launcher table.", "#pragma once",
+             '#include "hfg_internal.cuh"', "", "namespace hfg {", "",
+             "using WarpLauncher = void (*)(const EngineView &, const ClassLaunch &, int, bool, int, int, cudaStream_t);"]
+    for (a, b, c, d) in quartets:
+        if is_split_class(a, b, c, d):
+            for suf in ("", "_scr"):
+                lines.append(f"void launch_warp_{a}{b}{c}{d}{suf}(const EngineView &v, const ClassLaunch &cl, int mode, "
+                             "bool ref, int prec, int grid, cudaStream_t s);")
+    lines.append("")
+    lines.append("// warp-cooperative launcher per class (same order as kClasses), nullptr for per-thread classes")
+    lines.append("static const WarpLauncher kWarp[] = {")
+    for (a, b, c, d) in quartets:
+        lines.append(f"    {'launch_warp_%d%d%d%d' % (a, b, c, d) if is_split_class(a, b, c, d) else 'nullptr'},")
+    lines += ["};", "", "}  // namespace hfg", ""]
+    with open(os.path.join(out_dir, "eri_warp_dispatch.cuh"), "w") as fh:
+        fh.write("\n".join(lines))
+
+
 if __name__ == "__main__":
     here = os.path.dirname(os.path.abspath(__file__))
     out_dir = sys.argv[1] if len(sys.argv) > 1 else here
     main(os.path.join(out_dir, "eri_gen.cuh"))
     emit_launchers(out_dir)
     emit_split(out_dir)
+    emit_warp(out_dir)

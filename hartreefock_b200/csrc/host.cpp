@@ -22,6 +22,7 @@
 
 #include "../../include/hfgpu_driver.h"
 #include "../../include/hfgpu_host.hpp"
+#include "driver_internal.h"
 #include "scf_device.h"
 
 namespace {
@@ -356,14 +357,26 @@ hfg_shells Systems::Molecule::ShellTable::view() const {
   return s;
 }
 
+// Molecule::LoadXYZ (Molecule.cpp:143-199): count line, comment line, then
+// "symbol x y z" per atom with the coordinates as written; false on a short
+// file, an unknown symbol, an element the basis lacks, or a count line that
+// does not parse (the reference's catch-all).
 bool Systems::Molecule::LoadXYZ(const std::string &fileName, const Chemistry::Basis &basis) {
+  try {
+    return LoadXYZBody(fileName, basis);
+  } catch (...) {
+  }
+  return false;
+}
+
+bool Systems::Molecule::LoadXYZBody(const std::string &fileName, const Chemistry::Basis &basis) {
   std::ifstream f(fileName);
   if (!f) return false;
   std::string line;
   if (!std::getline(f, line)) return false;
-  const int n = std::stoi(line);
+  const unsigned n = (unsigned)std::stoi(line);
   if (!std::getline(f, line)) return false;
-  for (int i = 0; i < n; ++i) {
+  for (unsigned i = 0; i < n; ++i) {
     if (!std::getline(f, line)) return false;
     std::istringstream ls(line);
     std::string sym;
@@ -452,6 +465,49 @@ void IntegralsRepository::OneElectron(hfgpu::Matrix &S, hfgpu::Matrix &T, hfgpu:
   if (hfg_one_electron(&sh, nxyz.data(), nz.data(), (int32_t)nz.size(), options.device, S.data(), T.data(),
                        V.data()) != HFG_OK)
     throw std::runtime_error(std::string("hfg_one_electron: ") + hfg_last_error());
+}
+
+double MolecularOrbitalsIntegralsRepository::getElectronElectron(unsigned p, unsigned q, unsigned r, unsigned s,
+                                                                  const hfgpu::Matrix &C) {
+  if (mo_.empty()) {
+    hfg_ctx *ctx = repo_.engine();
+    n_ = hfg_ctx_nbf(ctx);
+    if (C.rows() != n_ || C.cols() != n_) throw std::invalid_argument("MO coefficients: nbf x nbf expected");
+    const size_t nn = (size_t)n_ * n_;
+    double *dC = nullptr, *dX = nullptr;
+    if (cudaMalloc(&dC, nn * sizeof(double)) != cudaSuccess || cudaMalloc(&dX, nn * nn * sizeof(double)) != cudaSuccess) {
+      cudaFree(dC);
+      throw std::runtime_error("MolecularOrbitalsIntegralsRepository: device allocation");
+    }
+    cudaMemcpy(dC, C.data(), nn * sizeof(double), cudaMemcpyHostToDevice);
+    const hfg_status st = hfg_mo_eri_full(ctx, dC, dX, nullptr);
+    mo_.resize(nn * nn);
+    if (st == HFG_OK) cudaMemcpy(mo_.data(), dX, nn * nn * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(dC);
+    cudaFree(dX);
+    if (st != HFG_OK) {
+      mo_.clear();
+      throw std::runtime_error(std::string("hfg_mo_eri_full: ") + hfg_last_error());
+    }
+  }
+  const size_t n = (size_t)n_;
+  return mo_[((size_t)p * n + q) * n * n + (size_t)r * n + s];
+}
+
+SpinOrbitalsElectronElectronIntegralsRepository::SpinOrbitalsElectronElectronIntegralsRepository(int numOrbitals)
+    : m_(2 * (size_t)numOrbitals), t_(m_ * m_ * m_ * m_, 0.0) {}
+
+SpinOrbitalsElectronElectronIntegralsRepository::SpinOrbitalsElectronElectronIntegralsRepository(
+    int numOrbitals, IntegralsRepository &repository, const hfgpu::Matrix &C)
+    : SpinOrbitalsElectronElectronIntegralsRepository(numOrbitals) {
+  Compute(repository, C);
+}
+
+void SpinOrbitalsElectronElectronIntegralsRepository::Compute(IntegralsRepository &repository, const hfgpu::Matrix &C) {
+  hfg_ctx *ctx = repository.engine();
+  if ((size_t)2 * hfg_ctx_nbf(ctx) != m_) throw std::invalid_argument("spin-orbital tensor: 2 nbf spin orbitals expected");
+  if (hfg_spin_orbital_eri(ctx, C.data(), t_.data(), (int64_t)t_.size()) != HFG_OK)
+    throw std::runtime_error(std::string("hfg_spin_orbital_eri: ") + hfg_last_error());
 }
 
 }  // namespace GaussianIntegrals
@@ -867,6 +923,19 @@ double RestrictedHartreeFock::CalculateMp2Energy() {
   return mp2Energy;
 }
 
+double UnrestrictedHartreeFock::CalculateMp2Energy() {
+  const int n = numberOfOrbitals;
+  if (!inited || (int)Cplus.rows() != n || (int)Cminus.rows() != n || (int)eigenvalsplus.size() != n ||
+      (int)eigenvalsminus.size() != n || nrOccupiedLevelsPlus >= (unsigned)n || nrOccupiedLevelsMinus < 1 ||
+      nrOccupiedLevelsMinus > nrOccupiedLevelsPlus)
+    return mp2Energy = 0;
+  check_engine(hfg_mp2_uhf(integralsRepository.engine(), Cplus.data(), eigenvalsplus.data(),
+                           (int32_t)nrOccupiedLevelsPlus, Cminus.data(), eigenvalsminus.data(),
+                           (int32_t)nrOccupiedLevelsMinus, &mp2Energy),
+               "hfg_mp2_uhf");
+  return mp2Energy;
+}
+
 void UnrestrictedHartreeFock::Init(Systems::Molecule *molecule) {
   HartreeFockAlgorithm::Init(molecule);
   DensityMatrixPlus = Matrix::Zero(h.rows(), h.cols());
@@ -990,6 +1059,114 @@ Systems::Molecule build_molecule(const char *basis_path, int32_t natoms, const i
 }
 }  // namespace
 
+namespace hfgpu {
+
+hfg_status run_scf(const char *basis_path, int32_t natoms, const int32_t *Z, const double *xyz,
+                   const hfd_scf_opts *opts, hfd_scf_result *result, double *density, int64_t density_count,
+                   const std::function<void(std::atomic_bool *)> &on_algorithm, std::string *error) {
+  if (!basis_path || natoms <= 0 || !Z || !xyz || !opts || !result) return HFG_INVALID_ARG;
+  try {
+    Systems::Molecule mol = build_molecule(basis_path, natoms, Z, xyz);
+    mol.alphaElectrons = (unsigned)opts->alpha_electrons;
+    mol.betaElectrons = (unsigned)opts->beta_electrons;
+    mol.Init();
+    std::unique_ptr<HartreeFock::HartreeFockAlgorithm> algo;
+    const int iters = opts->max_iterations > 0 ? opts->max_iterations : 3000;
+    if (opts->unrestricted) algo.reset(new HartreeFock::UnrestrictedHartreeFock(iters));
+    else algo.reset(new HartreeFock::RestrictedHartreeFock(iters));
+    algo->alpha = opts->alpha;
+    algo->initGuess = opts->init_guess;
+    algo->UseDIIS = opts->use_diis != 0;
+    algo->normalIterAfterDIIS = opts->post_diis;
+    algo->integralsRepository.options.eri_convention = opts->eri_convention;
+    algo->integralsRepository.options.schwarz_threshold = opts->schwarz_threshold;
+    algo->storedIntegralsBudget = 0;  // direct SCF: no stored table needed
+    algo->mixedCutoff = opts->mixed_cutoff;
+    algo->mixedSwitchEnergy = opts->mixed_switch_energy;
+    algo->fp64FinalIterations = opts->fp64_final_iterations;
+    algo->mixedSwitchDensity = opts->mixed_switch_density;
+    algo->mixedSwitchDiis = opts->mixed_switch_diis;
+    algo->fp64FinalConverge = opts->fp64_final_converge != 0;
+    algo->stopAtPrecisionTest = opts->stop_at_precision_test != 0;
+    algo->incrementalFock = opts->incremental != 0;
+    algo->traceIterations = opts->trace != 0;
+    algo->concurrentClasses = opts->concurrent_classes >= 1;
+    algo->cudaGraphs = opts->concurrent_classes >= 2;
+    // the hook sees the terminate flag for the algorithm's whole life
+    struct Publish {
+      const std::function<void(std::atomic_bool *)> &f;
+      Publish(const std::function<void(std::atomic_bool *)> &fn, std::atomic_bool *flag) : f(fn) {
+        if (f) f(flag);
+      }
+      ~Publish() {
+        if (f) f(nullptr);
+      }
+    } publish(on_algorithm, &algo->terminate);
+    algo->Init(&mol);
+    const double e = algo->Calculate();
+    std::memset(result, 0, sizeof *result);
+    result->energy = e;
+    result->homo = algo->HOMOEnergy;
+    result->converged = algo->converged ? 1 : 0;
+    result->iterations = algo->iterations;
+    result->nbf = algo->numberOfOrbitals;
+    result->fock_builds = algo->fockBuilds;
+    result->fock_ms_total = algo->fockMilliseconds;
+    result->fp32_quartets = algo->fp32Quartets;
+    result->fp64_quartets = algo->fp64Quartets;
+    result->mixed_steps = algo->mixedSteps;
+    result->seconds_fock = algo->secondsFock;
+    result->seconds_eigen = algo->secondsEigen;
+    result->seconds_diis = algo->secondsDiis;
+    result->seconds_total = algo->secondsTotal;
+    result->seconds_init = algo->secondsInit;
+    if (opts->mp2 && !opts->unrestricted)
+      result->mp2_energy = static_cast<HartreeFock::RestrictedHartreeFock *>(algo.get())->CalculateMp2Energy();
+    else if (opts->mp2)
+      result->mp2_energy = static_cast<HartreeFock::UnrestrictedHartreeFock *>(algo.get())->CalculateMp2Energy();
+    const int64_t nn = (int64_t)result->nbf * result->nbf;
+    if (density) {
+      if (opts->unrestricted) {
+        if (density_count < 2 * nn) return HFG_INVALID_ARG;
+        auto *u = static_cast<HartreeFock::UnrestrictedHartreeFock *>(algo.get());
+        std::memcpy(density, u->DensityMatrixPlus.data(), nn * sizeof(double));
+        std::memcpy(density + nn, u->DensityMatrixMinus.data(), nn * sizeof(double));
+      } else {
+        if (density_count < nn) return HFG_INVALID_ARG;
+        auto *r = static_cast<HartreeFock::RestrictedHartreeFock *>(algo.get());
+        std::memcpy(density, r->DensityMatrix.data(), nn * sizeof(double));
+      }
+    }
+    return HFG_OK;
+  } catch (const std::invalid_argument &ex) {
+    if (error) *error = ex.what();
+    return HFG_INVALID_ARG;
+  } catch (const std::exception &ex) {
+    if (error) *error = ex.what();
+    return HFG_DEVICE_ERROR;
+  }
+}
+
+
+
+int64_t job_footprint_bytes(const char *basis_path, int32_t natoms, const int32_t *Z, const double *xyz,
+                            bool unrestricted) {
+  Systems::Molecule mol = build_molecule(basis_path, natoms, Z, xyz);
+  mol.Init();
+  const auto &t = mol.shellTable();
+  const int64_t ns = (int64_t)t.L.size(), pairs = ns * (ns + 1) / 2;
+  int64_t prim_pairs = 0;
+  for (int64_t a = 0; a < ns; ++a)
+    for (int64_t b = 0; b <= a; ++b) prim_pairs += (int64_t)t.nprim[a] * t.nprim[b];
+  const int64_t tasks = pairs * (pairs + 1) / 2 / 32 + pairs;
+  const int64_t nn = (int64_t)t.nbf * t.nbf;
+  return 16 * tasks + 144 * prim_pairs + 8 * nn * 32 * (unrestricted ? 2 : 1) + (int64_t(16) << 20);
+}
+
+void release_driver_thread() { hfd_release_thread(); }
+
+}  // namespace hfgpu
+
 extern "C" {
 
 const char *hfd_last_error(void) { return g_driver_error.c_str(); }
@@ -1033,77 +1210,8 @@ void hfd_default_scf_opts(hfd_scf_opts *o) {
 
 hfg_status hfd_scf(const char *basis_path, int32_t natoms, const int32_t *Z, const double *xyz,
                    const hfd_scf_opts *opts, hfd_scf_result *result, double *density, int64_t density_count) {
-  if (!basis_path || natoms <= 0 || !Z || !xyz || !opts || !result) return HFG_INVALID_ARG;
-  try {
-    Systems::Molecule mol = build_molecule(basis_path, natoms, Z, xyz);
-    mol.alphaElectrons = (unsigned)opts->alpha_electrons;
-    mol.betaElectrons = (unsigned)opts->beta_electrons;
-    mol.Init();
-    std::unique_ptr<HartreeFock::HartreeFockAlgorithm> algo;
-    const int iters = opts->max_iterations > 0 ? opts->max_iterations : 3000;
-    if (opts->unrestricted) algo.reset(new HartreeFock::UnrestrictedHartreeFock(iters));
-    else algo.reset(new HartreeFock::RestrictedHartreeFock(iters));
-    algo->alpha = opts->alpha;
-    algo->initGuess = opts->init_guess;
-    algo->UseDIIS = opts->use_diis != 0;
-    algo->normalIterAfterDIIS = opts->post_diis;
-    algo->integralsRepository.options.eri_convention = opts->eri_convention;
-    algo->integralsRepository.options.schwarz_threshold = opts->schwarz_threshold;
-    algo->storedIntegralsBudget = 0;  // direct SCF: no stored table needed
-    algo->mixedCutoff = opts->mixed_cutoff;
-    algo->mixedSwitchEnergy = opts->mixed_switch_energy;
-    algo->fp64FinalIterations = opts->fp64_final_iterations;
-    algo->mixedSwitchDensity = opts->mixed_switch_density;
-    algo->mixedSwitchDiis = opts->mixed_switch_diis;
-    algo->fp64FinalConverge = opts->fp64_final_converge != 0;
-    algo->stopAtPrecisionTest = opts->stop_at_precision_test != 0;
-    algo->incrementalFock = opts->incremental != 0;
-    algo->traceIterations = opts->trace != 0;
-    algo->concurrentClasses = opts->concurrent_classes >= 1;
-    algo->cudaGraphs = opts->concurrent_classes >= 2;
-    algo->Init(&mol);
-    const double e = algo->Calculate();
-    std::memset(result, 0, sizeof *result);
-    result->energy = e;
-    result->homo = algo->HOMOEnergy;
-    result->converged = algo->converged ? 1 : 0;
-    result->iterations = algo->iterations;
-    result->nbf = algo->numberOfOrbitals;
-    result->fock_builds = algo->fockBuilds;
-    result->fock_ms_total = algo->fockMilliseconds;
-    result->fp32_quartets = algo->fp32Quartets;
-    result->fp64_quartets = algo->fp64Quartets;
-    result->mixed_steps = algo->mixedSteps;
-    result->seconds_fock = algo->secondsFock;
-    result->seconds_eigen = algo->secondsEigen;
-    result->seconds_diis = algo->secondsDiis;
-    result->seconds_total = algo->secondsTotal;
-    result->seconds_init = algo->secondsInit;
-    if (opts->mp2 && !opts->unrestricted)
-      result->mp2_energy = static_cast<HartreeFock::RestrictedHartreeFock *>(algo.get())->CalculateMp2Energy();
-    const int64_t nn = (int64_t)result->nbf * result->nbf;
-    if (density) {
-      if (opts->unrestricted) {
-        if (density_count < 2 * nn) return HFG_INVALID_ARG;
-        auto *u = static_cast<HartreeFock::UnrestrictedHartreeFock *>(algo.get());
-        std::memcpy(density, u->DensityMatrixPlus.data(), nn * sizeof(double));
-        std::memcpy(density + nn, u->DensityMatrixMinus.data(), nn * sizeof(double));
-      } else {
-        if (density_count < nn) return HFG_INVALID_ARG;
-        auto *r = static_cast<HartreeFock::RestrictedHartreeFock *>(algo.get());
-        std::memcpy(density, r->DensityMatrix.data(), nn * sizeof(double));
-      }
-    }
-    return HFG_OK;
-  } catch (const std::invalid_argument &ex) {
-    g_driver_error = ex.what();
-    return HFG_INVALID_ARG;
-  } catch (const std::exception &ex) {
-    g_driver_error = ex.what();
-    return HFG_DEVICE_ERROR;
-  }
+  return hfgpu::run_scf(basis_path, natoms, Z, xyz, opts, result, density, density_count, {}, &g_driver_error);
 }
-
 
 hfg_status hfd_one_electron(const char *basis_path, int32_t natoms, const int32_t *Z, const double *xyz, double *S,
                             double *h, int64_t capacity, int32_t *nbf) {
@@ -1120,6 +1228,34 @@ hfg_status hfd_one_electron(const char *basis_path, int32_t natoms, const int32_
     for (int x = 0; x < n * n; ++x) {
       if (S) S[x] = s.data()[x];
       if (h) h[x] = t.data()[x] + v.data()[x];
+    }
+    return HFG_OK;
+  } catch (const std::exception &ex) {
+    g_driver_error = ex.what();
+    return HFG_INVALID_ARG;
+  }
+}
+
+hfg_status hfd_load_xyz(const char *xyz_path, const char *basis_path, int32_t cap, int32_t *natoms, int32_t *Z,
+                        double *xyz, int32_t *nbf) {
+  if (!xyz_path || !basis_path || !natoms || !nbf) return HFG_INVALID_ARG;
+  try {
+    Chemistry::Basis basis;
+    basis.Load(basis_path);
+    Systems::Molecule mol;
+    if (!mol.LoadXYZ(xyz_path, basis)) {
+      g_driver_error = std::string("LoadXYZ failed for ") + xyz_path;
+      return HFG_INVALID_ARG;
+    }
+    *natoms = (int32_t)mol.atoms.size();
+    *nbf = (int32_t)mol.CountNumberOfContractedGaussians();
+    for (int32_t i = 0; i < *natoms && i < cap; ++i) {
+      if (Z) Z[i] = (int32_t)mol.atoms[i].Z;
+      if (xyz) {
+        xyz[3 * i] = mol.atoms[i].position.X;
+        xyz[3 * i + 1] = mol.atoms[i].position.Y;
+        xyz[3 * i + 2] = mol.atoms[i].position.Z;
+      }
     }
     return HFG_OK;
   } catch (const std::exception &ex) {

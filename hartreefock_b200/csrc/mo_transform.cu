@@ -1,8 +1,9 @@
-// AO -> MO transform of the two-electron integrals and the RHF MP2 energy,
+// AO -> MO transform of the two-electron integrals and the MP2 energies,
 // for the post-HF consumers of the integral tables:
 // MolecularOrbitalsIntegralsRepository::getElectronElectron
-// (IntegralsRepository.h:190-291) and RestrictedHartreeFock::CalculateMp2Energy
-// (RestrictedHartreeFock.cpp:251-288).
+// (IntegralsRepository.h:190-291), RestrictedHartreeFock::CalculateMp2Energy
+// (RestrictedHartreeFock.cpp:251-288) and
+// UnrestrictedHartreeFock::CalculateMp2Energy (UnrestrictedHartreeFock.cpp:295-375).
 //
 // The reference transforms one MO integral at a time (four nested
 // quarter-contractions, cached per index tuple).  Here the whole (ia|jb)
@@ -75,6 +76,30 @@ __global__ void mp2_energy(const double *__restrict__ X, const double *__restric
   if (threadIdx.x == 0) atomicAdd(out, part[0]);
 }
 
+// sum over the block of X^2 / (e_i + e_j - e_a - e_b), X[(i a),(j b)] with
+// row stride `ldx` (columns j*nb + b); the four index ranges read their
+// orbital energies from ei, ea, ej, eb
+__global__ void mp2_sum_sq(const double *__restrict__ X, long long ldx, int ni, int na, int nj, int nb,
+                           const double *__restrict__ ei, const double *__restrict__ ea, const double *__restrict__ ej,
+                           const double *__restrict__ eb, double *out) {
+  const long long rows = (long long)ni * na, cols = (long long)nj * nb, total = rows * cols;
+  double acc = 0;
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total; x += (long long)gridDim.x * blockDim.x) {
+    const long long r = x / cols, c = x - r * cols;
+    const int i = (int)(r / na), a = (int)(r - (long long)i * na), j = (int)(c / nb), b = (int)(c - (long long)j * nb);
+    const double v = X[r * ldx + c];
+    acc += v * v / (ei[i] + ej[j] - ea[a] - eb[b]);
+  }
+  __shared__ double part[256];
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) part[threadIdx.x] += part[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicAdd(out, part[0]);
+}
+
 int grid_for(long long total) { return (int)std::min<long long>(148LL * 32, (total + 255) / 256 + 1); }
 
 struct Buffers {
@@ -96,50 +121,88 @@ struct Blas {
   }
 };
 
+// The unpacked AO table M[(m n),(l s)] of the context (stored-mode build),
+// sized for `ov_max` columns of pair coefficients in the blocks that follow.
+struct MoTables {
+  int n = 0;
+  double *M = nullptr, *K1 = nullptr, *K2 = nullptr, *Y = nullptr;
+  long long cap = 0;  // columns of K1, K2, Y
+  Blas blas;
+};
+
+hfg_status prepare(hfg_ctx *ctx, long long ov_max, cudaStream_t s, Buffers &buf, MoTables &t, const char *who) {
+  const int n = hfg_ctx_nbf(ctx);
+  if (n <= 0) return hfg::fail_external(HFG_INVALID_ARG, std::string(who) + ": context without a single molecule");
+  const long long nn = (long long)n * n;
+  const int64_t count = hfg_packed_size(n);
+  size_t freeb = 0, totalb = 0;
+  cudaMemGetInfo(&freeb, &totalb);
+  const double need = 8.0 * ((double)count + (double)nn * nn + 3.0 * nn * ov_max);
+  if (need > 0.9 * (double)freeb)
+    return hfg::fail_external(HFG_OOM_BUDGET, std::string(who) + ": the unpacked AO table does not fit (" +
+                                                  std::to_string(need / 1e9) + " GB needed)");
+  double *packed = nullptr;
+  cudaError_t e = buf.get(&packed, (size_t)count);
+  if (e == cudaSuccess) e = buf.get(&t.M, (size_t)(nn * nn));
+  if (e == cudaSuccess) e = buf.get(&t.K1, (size_t)(nn * ov_max));
+  if (e == cudaSuccess) e = buf.get(&t.K2, (size_t)(nn * ov_max));
+  if (e == cudaSuccess) e = buf.get(&t.Y, (size_t)(nn * ov_max));
+  if (e != cudaSuccess) return hfg::fail_external(HFG_OOM_BUDGET, std::string(who) + ": " + cudaGetErrorString(e));
+  hfg_status st = hfg_eri_packed_device(ctx, packed, count, s);
+  if (st != HFG_OK) return st;
+  // stream 0 means the context's own stream for the packed build: finish it
+  // before the kernels below read the table
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return hfg::fail_external(HFG_DEVICE_ERROR, std::string(who) + ": " + cudaGetErrorString(e));
+  unpack_eri<<<grid_for(nn * nn), 256, 0, s>>>(packed, t.M, n);
+  if (cublasCreate(&t.blas.h) != CUBLAS_STATUS_SUCCESS || cublasSetStream(t.blas.h, s) != CUBLAS_STATUS_SUCCESS)
+    return hfg::fail_external(HFG_DEVICE_ERROR, std::string(who) + ": cuBLAS handle");
+  t.n = n;
+  t.cap = ov_max;
+  return HFG_OK;
+}
+
+// X[(i a),(j b)] = (i a | j b) with the bra pair's orbitals from C1 (i in
+// [i0, i0+ni), a in [a0, a0+na)) and the ket pair's from C2 (j in [j0, j0+nj),
+// b in [b0, b0+nb)); C1, C2 row-major n x n (AO rows, MO columns).
+hfg_status block(MoTables &t, const double *C1, int i0, int ni, int a0, int na, const double *C2, int j0, int nj,
+                 int b0, int nb, double *dX, cudaStream_t s, const char *who) {
+  const int n = t.n;
+  const long long nn = (long long)n * n, ov1 = (long long)ni * na, ov2 = (long long)nj * nb;
+  if (ov1 > t.cap || ov2 > t.cap) return hfg::fail_external(HFG_INVALID_ARG, std::string(who) + ": block size");
+  pair_coefficients<<<grid_for(nn * ov1), 256, 0, s>>>(C1, n, i0, ni, a0, na, t.K1);
+  pair_coefficients<<<grid_for(nn * ov2), 256, 0, s>>>(C2, n, j0, nj, b0, nb, t.K2);
+  const double one = 1.0, zero = 0.0;
+  // row-major Y = M K2  <=>  column-major Y^T = K2^T M^T
+  if (cublasDgemm(t.blas.h, CUBLAS_OP_N, CUBLAS_OP_N, (int)ov2, (int)nn, (int)nn, &one, t.K2, (int)ov2, t.M, (int)nn,
+                  &zero, t.Y, (int)ov2) != CUBLAS_STATUS_SUCCESS)
+    return hfg::fail_external(HFG_DEVICE_ERROR, std::string(who) + ": DGEMM M K");
+  // row-major X = K1^T Y  <=>  column-major X^T = Y^T K1
+  if (cublasDgemm(t.blas.h, CUBLAS_OP_N, CUBLAS_OP_T, (int)ov2, (int)ov1, (int)nn, &one, t.Y, (int)ov2, t.K1, (int)ov1,
+                  &zero, dX, (int)ov2) != CUBLAS_STATUS_SUCCESS)
+    return hfg::fail_external(HFG_DEVICE_ERROR, std::string(who) + ": DGEMM K^T Y");
+  return HFG_OK;
+}
+
+hfg_status finish(cudaStream_t s, const char *who) {
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return hfg::fail_external(HFG_DEVICE_ERROR, std::string(who) + ": " + cudaGetErrorString(e));
+  return HFG_OK;
+}
+
 hfg_status transform(hfg_ctx *ctx, const double *dC, int i0, int ni, int a0, int na, double *dX, cudaStream_t s,
                      Buffers &buf) {
   const int n = hfg_ctx_nbf(ctx);
   if (n <= 0) return hfg::fail_external(HFG_INVALID_ARG, "hfg_mo_eri_ovov: context without a single molecule");
   if (!dC || !dX || ni < 1 || na < 1 || i0 < 0 || a0 < 0 || i0 + ni > n || a0 + na > n)
     return hfg::fail_external(HFG_INVALID_ARG, "hfg_mo_eri_ovov: orbital ranges");
-  const long long nn = (long long)n * n, ov = (long long)ni * na;
-  const int64_t count = hfg_packed_size(n);
-  size_t freeb = 0, totalb = 0;
-  cudaMemGetInfo(&freeb, &totalb);
-  const double need = 8.0 * ((double)count + (double)nn * nn + 2.0 * nn * ov);
-  if (need > 0.9 * (double)freeb)
-    return hfg::fail_external(HFG_OOM_BUDGET, "hfg_mo_eri_ovov: the unpacked AO table does not fit (" +
-                                                  std::to_string(need / 1e9) + " GB needed)");
-  double *packed = nullptr, *M = nullptr, *K = nullptr, *Y = nullptr;
-  cudaError_t e = buf.get(&packed, (size_t)count);
-  if (e == cudaSuccess) e = buf.get(&M, (size_t)(nn * nn));
-  if (e == cudaSuccess) e = buf.get(&K, (size_t)(nn * ov));
-  if (e == cudaSuccess) e = buf.get(&Y, (size_t)(nn * ov));
-  if (e != cudaSuccess) return hfg::fail_external(HFG_OOM_BUDGET, std::string("hfg_mo_eri_ovov: ") + cudaGetErrorString(e));
-  hfg_status st = hfg_eri_packed_device(ctx, packed, count, s);
+  MoTables t;
+  hfg_status st = prepare(ctx, (long long)ni * na, s, buf, t, "hfg_mo_eri_ovov");
   if (st != HFG_OK) return st;
-  // stream 0 means the context's own stream for the packed build: finish it
-  // before the kernels below read the table
-  e = cudaDeviceSynchronize();
-  if (e != cudaSuccess) return hfg::fail_external(HFG_DEVICE_ERROR, std::string("hfg_mo_eri_ovov: ") + cudaGetErrorString(e));
-  unpack_eri<<<grid_for(nn * nn), 256, 0, s>>>(packed, M, n);
-  pair_coefficients<<<grid_for(nn * ov), 256, 0, s>>>(dC, n, i0, ni, a0, na, K);
-  Blas b;
-  if (cublasCreate(&b.h) != CUBLAS_STATUS_SUCCESS || cublasSetStream(b.h, s) != CUBLAS_STATUS_SUCCESS)
-    return hfg::fail_external(HFG_DEVICE_ERROR, "hfg_mo_eri_ovov: cuBLAS handle");
-  const double one = 1.0, zero = 0.0;
-  // row-major Y = M K  <=>  column-major Y^T = K^T M^T
-  if (cublasDgemm(b.h, CUBLAS_OP_N, CUBLAS_OP_N, (int)ov, (int)nn, (int)nn, &one, K, (int)ov, M, (int)nn, &zero, Y,
-                  (int)ov) != CUBLAS_STATUS_SUCCESS)
-    return hfg::fail_external(HFG_DEVICE_ERROR, "hfg_mo_eri_ovov: DGEMM M K");
-  // row-major X = K^T Y  <=>  column-major X^T = Y^T K
-  if (cublasDgemm(b.h, CUBLAS_OP_N, CUBLAS_OP_T, (int)ov, (int)ov, (int)nn, &one, Y, (int)ov, K, (int)ov, &zero, dX,
-                  (int)ov) != CUBLAS_STATUS_SUCCESS)
-    return hfg::fail_external(HFG_DEVICE_ERROR, "hfg_mo_eri_ovov: DGEMM K^T Y");
-  e = cudaStreamSynchronize(s);
-  if (e == cudaSuccess) e = cudaGetLastError();
-  if (e != cudaSuccess) return hfg::fail_external(HFG_DEVICE_ERROR, std::string("hfg_mo_eri_ovov: ") + cudaGetErrorString(e));
-  return HFG_OK;
+  st = block(t, dC, i0, ni, a0, na, dC, i0, ni, a0, na, dX, s, "hfg_mo_eri_ovov");
+  if (st != HFG_OK) return st;
+  return finish(s, "hfg_mo_eri_ovov");
 }
 
 }  // namespace
@@ -174,5 +237,133 @@ extern "C" hfg_status hfg_mp2_rhf(hfg_ctx *ctx, const double *C, const double *e
   e = cudaMemcpy(e_mp2, dOut, sizeof(double), cudaMemcpyDeviceToHost);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return hfg::fail_external(HFG_DEVICE_ERROR, std::string("hfg_mp2_rhf: ") + cudaGetErrorString(e));
+  return HFG_OK;
+}
+
+// UnrestrictedHartreeFock::CalculateMp2Energy (UnrestrictedHartreeFock.cpp:295-375):
+// 0.25 (S+ + S-), S = sum over occupied i, j and virtual a, b of one spin of
+// (ia|jb)^2 / (e_i + e_j - e_a - e_b).  The reference evaluates both sums
+// through one MolecularOrbitalsIntegralsRepository whose four caches are
+// keyed by orbital indices only (IntegralsRepository.h:190-291), so the
+// second sum reuses values the first one cached with the other spin's
+// coefficients.  With n+ >= n- occupied (occupied- within occupied+), the
+// quartet (i a | j b) of the second sum is therefore
+//   all C+                 when a and b are virtual in both spins,
+//   (i- a- | j+ b+)        when a is occupied+ only and b virtual+,
+//   all C-                 when b is occupied+ only,
+// with the second spin's orbital energies throughout; this reproduces it.
+extern "C" hfg_status hfg_mp2_uhf(hfg_ctx *ctx, const double *Cp, const double *ep, int32_t np, const double *Cm,
+                                  const double *em, int32_t nm, double *e_mp2) {
+  const char *who = "hfg_mp2_uhf";
+  if (!ctx || !Cp || !ep || !Cm || !em || !e_mp2) return hfg::fail_external(HFG_INVALID_ARG, "hfg_mp2_uhf: arguments");
+  const int n = hfg_ctx_nbf(ctx);
+  if (n <= 0 || np < 1 || nm < 1 || np >= n || nm > np)
+    return hfg::fail_external(HFG_INVALID_ARG, "hfg_mp2_uhf: occupied counts (need 1 <= n- <= n+ < nbf)");
+  const int vp = n - np, vm = n - nm, ns = np - nm;
+  Buffers buf;
+  double *dCp = nullptr, *dCm = nullptr, *dEp = nullptr, *dEm = nullptr, *dX = nullptr, *dOut = nullptr;
+  const long long ovmax = std::max<long long>((long long)np * vp, (long long)nm * vm);
+  cudaError_t e = buf.get(&dCp, (size_t)n * n);
+  if (e == cudaSuccess) e = buf.get(&dCm, (size_t)n * n);
+  if (e == cudaSuccess) e = buf.get(&dEp, (size_t)n);
+  if (e == cudaSuccess) e = buf.get(&dEm, (size_t)n);
+  if (e == cudaSuccess) e = buf.get(&dX, (size_t)(ovmax * ovmax));
+  if (e == cudaSuccess) e = buf.get(&dOut, 1);
+  if (e == cudaSuccess) e = cudaMemcpy(dCp, Cp, sizeof(double) * n * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dCm, Cm, sizeof(double) * n * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dEp, ep, sizeof(double) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dEm, em, sizeof(double) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);  // staged copies landed
+  if (e == cudaSuccess) e = cudaMemset(dOut, 0, sizeof(double));
+  if (e != cudaSuccess) return hfg::fail_external(HFG_OOM_BUDGET, std::string(who) + ": " + cudaGetErrorString(e));
+  cudaStream_t s = nullptr;
+  MoTables t;
+  hfg_status st = prepare(ctx, ovmax, s, buf, t, who);
+  if (st != HFG_OK) return st;
+  // S+: (ia|jb) with C+, i, j < n+, a, b >= n+
+  if ((st = block(t, dCp, 0, np, np, vp, dCp, 0, np, np, vp, dX, s, who)) != HFG_OK) return st;
+  const long long ovp = (long long)np * vp;
+  mp2_sum_sq<<<grid_for(ovp * ovp), 256, 0, s>>>(dX, ovp, np, vp, np, vp, dEp, dEp + np, dEp, dEp + np, dOut);
+  // S-, a and b virtual in both spins: the C+ block above, i, j < n-, with e-
+  mp2_sum_sq<<<grid_for((long long)nm * vp * nm * vp), 256, 0, s>>>(dX, ovp, nm, vp, nm, vp, dEm, dEm + np, dEm,
+                                                                   dEm + np, dOut);
+  if (ns > 0) {
+    // S-, a occupied+ only, b virtual+: (i- a- | j+ b+)
+    if ((st = block(t, dCm, 0, nm, nm, ns, dCp, 0, nm, np, vp, dX, s, who)) != HFG_OK) return st;
+    mp2_sum_sq<<<grid_for((long long)nm * ns * nm * vp), 256, 0, s>>>(dX, (long long)nm * vp, nm, ns, nm, vp, dEm,
+                                                                     dEm + nm, dEm, dEm + np, dOut);
+    // S-, b occupied+ only, any virtual- a: all C-
+    if ((st = block(t, dCm, 0, nm, nm, vm, dCm, 0, nm, nm, ns, dX, s, who)) != HFG_OK) return st;
+    mp2_sum_sq<<<grid_for((long long)nm * vm * nm * ns), 256, 0, s>>>(dX, (long long)nm * ns, nm, vm, nm, ns, dEm,
+                                                                     dEm + nm, dEm, dEm + nm, dOut);
+  }
+  if ((st = finish(s, who)) != HFG_OK) return st;
+  double sum = 0;
+  e = cudaMemcpy(&sum, dOut, sizeof(double), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return hfg::fail_external(HFG_DEVICE_ERROR, std::string(who) + ": " + cudaGetErrorString(e));
+  *e_mp2 = 0.25 * sum;
+  return HFG_OK;
+}
+
+namespace {
+
+// T[p][q][r][s] over 2n spin orbitals (spatial orbital p / 2, spin p % 2) from
+// X[(hp hq),(hr hs)] = (hp hq | hr hs):
+// T = (hp hr | hq hs) [p, r and q, s same spin] - (hp hs | hq hr) [p, s and q, r same spin]
+__global__ void spin_orbital_tensor(const double *__restrict__ X, int n, double *__restrict__ T) {
+  const long long m = 2LL * n, total = m * m * m * m, nn = (long long)n * n;
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total; x += (long long)gridDim.x * blockDim.x) {
+    const int s = (int)(x % m), r = (int)((x / m) % m), q = (int)((x / (m * m)) % m), p = (int)(x / (m * m * m));
+    const int hp = p >> 1, hq = q >> 1, hr = r >> 1, hs = s >> 1;
+    double v = 0.0;
+    if ((p & 1) == (r & 1) && (q & 1) == (s & 1)) v += X[((long long)hp * n + hr) * nn + (long long)hq * n + hs];
+    if ((p & 1) == (s & 1) && (q & 1) == (r & 1)) v -= X[((long long)hp * n + hs) * nn + (long long)hq * n + hr];
+    T[x] = v;
+  }
+}
+
+}  // namespace
+
+// The whole MO integral tensor (pq|rs), X[(p q),(r s)], p..s over every
+// orbital of dC (device, row-major nbf x nbf).
+extern "C" hfg_status hfg_mo_eri_full(hfg_ctx *ctx, const double *dC, double *dX, void *stream) {
+  const char *who = "hfg_mo_eri_full";
+  if (!ctx || !dC || !dX) return hfg::fail_external(HFG_INVALID_ARG, "hfg_mo_eri_full: arguments");
+  const int n = hfg_ctx_nbf(ctx);
+  if (n <= 0) return hfg::fail_external(HFG_INVALID_ARG, "hfg_mo_eri_full: context without a single molecule");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  Buffers buf;
+  MoTables t;
+  hfg_status st = prepare(ctx, (long long)n * n, s, buf, t, who);
+  if (st != HFG_OK) return st;
+  if ((st = block(t, dC, 0, n, 0, n, dC, 0, n, 0, n, dX, s, who)) != HFG_OK) return st;
+  return finish(s, who);
+}
+
+// SpinOrbitalsElectronElectronIntegralsRepository::Compute
+// (SpinOrbitalsElectronElectronIntegralsRepository.cpp:30-52) for host C
+// (row-major nbf x nbf): out receives the (2 nbf)^4 tensor, row-major
+// [p][q][r][s].
+extern "C" hfg_status hfg_spin_orbital_eri(hfg_ctx *ctx, const double *C, double *out, int64_t count) {
+  const char *who = "hfg_spin_orbital_eri";
+  if (!ctx || !C || !out) return hfg::fail_external(HFG_INVALID_ARG, "hfg_spin_orbital_eri: arguments");
+  const int n = hfg_ctx_nbf(ctx);
+  if (n <= 0) return hfg::fail_external(HFG_INVALID_ARG, "hfg_spin_orbital_eri: context without a single molecule");
+  const long long m = 2LL * n, total = m * m * m * m, nn = (long long)n * n;
+  if (count < total) return hfg::fail_external(HFG_INVALID_ARG, "hfg_spin_orbital_eri: output holds fewer than (2 nbf)^4");
+  Buffers buf;
+  double *dC = nullptr, *dX = nullptr, *dT = nullptr;
+  cudaError_t e = buf.get(&dC, (size_t)nn);
+  if (e == cudaSuccess) e = buf.get(&dX, (size_t)(nn * nn));
+  if (e == cudaSuccess) e = buf.get(&dT, (size_t)total);
+  if (e == cudaSuccess) e = cudaMemcpy(dC, C, sizeof(double) * nn, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
+  if (e != cudaSuccess) return hfg::fail_external(HFG_OOM_BUDGET, std::string(who) + ": " + cudaGetErrorString(e));
+  hfg_status st = hfg_mo_eri_full(ctx, dC, dX, nullptr);
+  if (st != HFG_OK) return st;
+  spin_orbital_tensor<<<grid_for(total), 256>>>(dX, n, dT);
+  e = cudaMemcpy(out, dT, sizeof(double) * total, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return hfg::fail_external(HFG_DEVICE_ERROR, std::string(who) + ": " + cudaGetErrorString(e));
   return HFG_OK;
 }

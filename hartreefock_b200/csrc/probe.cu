@@ -1,7 +1,7 @@
-// FP64 FMA issue-rate microbenchmark: the roofline denominator for the ERI
-// kernels, which run on the FP64 CUDA-core pipe.  Eight independent FMA
-// chains per thread keep the pipe full; the result is stored so the chains
-// are not eliminated.
+// FMA issue-rate microbenchmarks: the roofline denominators for the ERI
+// kernels, which run on the FP64 CUDA-core pipe (plain form) and partly on
+// the FP32 pipe (precision form).  Eight independent FMA chains per thread
+// keep the pipe full; the result is stored so the chains are not eliminated.
 #include <cuda_runtime.h>
 
 #include <string>
@@ -12,9 +12,10 @@ namespace {
 
 constexpr int kIters = 4096;
 
-__global__ void fma_chains(double *out, double a, double b) {
-  double x0 = threadIdx.x * 1e-9, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6,
-         x7 = x0 + 7;
+template <class T>
+__global__ void fma_chains(T *out, T a, T b) {
+  T x0 = T(threadIdx.x * 1e-9), x1 = x0 + T(1), x2 = x0 + T(2), x3 = x0 + T(3), x4 = x0 + T(4), x5 = x0 + T(5),
+    x6 = x0 + T(6), x7 = x0 + T(7);
 #pragma unroll 16
   for (int i = 0; i < kIters; ++i) {
     x0 = fma(x0, a, b);
@@ -29,24 +30,23 @@ __global__ void fma_chains(double *out, double a, double b) {
   out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
 }
 
-}  // namespace
-
-extern "C" hfg_status hfg_measure_fp64_peak(int32_t device, double *tflops) {
+template <class T>
+hfg_status measure_peak(int32_t device, double *tflops) {
   if (!tflops) return HFG_INVALID_ARG;
   if (cudaSetDevice(device) != cudaSuccess) return HFG_NO_DEVICE;
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   const int threads = 256, blocks = sms * 8;
-  double *out = nullptr;
-  if (cudaMalloc(&out, sizeof(double) * threads * blocks) != cudaSuccess) return HFG_OOM_BUDGET;
+  T *out = nullptr;
+  if (cudaMalloc(&out, sizeof(T) * threads * blocks) != cudaSuccess) return HFG_OOM_BUDGET;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  fma_chains<<<blocks, threads>>>(out, 0.999999, 1e-7);  // warm-up
+  fma_chains<T><<<blocks, threads>>>(out, T(0.999999), T(1e-7));  // warm-up
   float best = 1e30f;
   for (int r = 0; r < 5; ++r) {
     cudaEventRecord(e0);
-    fma_chains<<<blocks, threads>>>(out, 0.999999, 1e-7);
+    fma_chains<T><<<blocks, threads>>>(out, T(0.999999), T(1e-7));
     cudaEventRecord(e1);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -62,3 +62,9 @@ extern "C" hfg_status hfg_measure_fp64_peak(int32_t device, double *tflops) {
   *tflops = flops / (best * 1e-3) / 1e12;
   return HFG_OK;
 }
+
+}  // namespace
+
+extern "C" hfg_status hfg_measure_fp64_peak(int32_t device, double *tflops) { return measure_peak<double>(device, tflops); }
+
+extern "C" hfg_status hfg_measure_fp32_peak(int32_t device, double *tflops) { return measure_peak<float>(device, tflops); }

@@ -24,11 +24,11 @@ ERI_REFERENCE, ERI_EXACT = 0, 1
 EXPORTED = ["hfg_default_opts", "hfg_last_error", "hfg_device_count", "hfg_ctx_create", "hfg_ctx_destroy",
             "hfg_ctx_nbf", "hfg_packed_size", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet",
             "hfg_fock_rhf", "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz",
-            "hfg_ctx_stats", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak",
+            "hfg_ctx_stats", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak", "hfg_measure_fp32_peak",
             "hfg_fock_rhf_noalloc", "hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental",
             "hfg_set_shard", "hfg_batch_create", "hfg_batch_size", "hfg_batch_layout", "hfg_fock_rhf_batch_device",
             "hfg_fock_uhf_batch_device", "hfg_eigh_batched", "hfg_one_electron",
-            "hfg_mo_eri_ovov", "hfg_mp2_rhf", "hfg_autotune", "hfg_set_graphs", "hfg_set_streams",
+            "hfg_mo_eri_ovov", "hfg_mp2_rhf", "hfg_mp2_uhf", "hfg_mo_eri_full", "hfg_spin_orbital_eri", "hfg_autotune", "hfg_set_graphs", "hfg_set_streams",
             "hfg_release_thread"]
 
 
@@ -63,7 +63,9 @@ class hfg_stats(ctypes.Structure):
 class hfg_class_time(ctypes.Structure):
     _fields_ = [("la", ctypes.c_int32), ("lb", ctypes.c_int32), ("lc", ctypes.c_int32), ("ld", ctypes.c_int32),
                 ("shell_quartets", ctypes.c_int64), ("function_quartets", ctypes.c_int64),
-                ("primitive_quartets", ctypes.c_int64), ("flops", ctypes.c_double), ("ms", ctypes.c_double)]
+                ("primitive_quartets", ctypes.c_int64), ("flops", ctypes.c_double), ("ms", ctypes.c_double),
+                ("tasks", ctypes.c_int64), ("lane_occupancy", ctypes.c_double), ("warp_kernel", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 _lib = None
@@ -111,6 +113,7 @@ def library(path: str = LIB_PATH):
     L.hfg_set_profiling.argtypes = [vp, i32]
     L.hfg_class_profile.argtypes = [vp, ctypes.POINTER(hfg_class_time), i32, ctypes.POINTER(i32)]
     L.hfg_measure_fp64_peak.argtypes = [i32, ctypes.POINTER(ctypes.c_double)]
+    L.hfg_measure_fp32_peak.argtypes = [i32, ctypes.POINTER(ctypes.c_double)]
     L.hfg_fock_reset.argtypes = [vp]
     L.hfg_set_mixed_cutoff.argtypes = [vp, ctypes.c_double]
     L.hfg_set_incremental.argtypes = [vp, i32]
@@ -123,13 +126,17 @@ def library(path: str = LIB_PATH):
     L.hfg_mo_eri_ovov.restype = ctypes.c_int
     L.hfg_mp2_rhf.argtypes = [vp, dp, dp, i32, ctypes.POINTER(ctypes.c_double)]
     L.hfg_mp2_rhf.restype = ctypes.c_int
+    L.hfg_mp2_uhf.argtypes = [vp, dp, dp, i32, dp, dp, i32, ctypes.POINTER(ctypes.c_double)]
+    L.hfg_mp2_uhf.restype = ctypes.c_int
+    L.hfg_spin_orbital_eri.argtypes = [vp, dp, dp, ctypes.c_int64]
+    L.hfg_spin_orbital_eri.restype = ctypes.c_int
     L.hfg_autotune.argtypes = [vp, dp, vp, i32, ctypes.POINTER(i32), vp]
     L.hfg_autotune.restype = ctypes.c_int
     L.hfg_set_graphs.argtypes = [vp, i32]
     L.hfg_set_graphs.restype = ctypes.c_int
     L.hfg_set_streams.argtypes = [vp, i32]
     L.hfg_set_streams.restype = ctypes.c_int
-    for name in ("hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental", "hfg_set_shard", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak", "hfg_ctx_create", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet", "hfg_fock_rhf",
+    for name in ("hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental", "hfg_set_shard", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak", "hfg_measure_fp32_peak", "hfg_ctx_create", "hfg_eri_packed", "hfg_eri_packed_device", "hfg_eri_quartet", "hfg_fock_rhf",
                  "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz", "hfg_ctx_stats"):
         getattr(L, name).restype = ctypes.c_int
     _lib = L
@@ -157,6 +164,12 @@ def _ptr(a: np.ndarray):
 def measure_fp64_peak(device: int = 0) -> float:
     v = ctypes.c_double()
     _check(library().hfg_measure_fp64_peak(device, ctypes.byref(v)))
+    return v.value
+
+
+def measure_fp32_peak(device: int = 0) -> float:
+    v = ctypes.c_double()
+    _check(library().hfg_measure_fp32_peak(device, ctypes.byref(v)))
     return v.value
 
 
@@ -327,6 +340,23 @@ class Engine:
         _check(library().hfg_mp2_rhf(self._h, _ptr(C), _ptr(eps), nocc, ctypes.byref(out)))
         return out.value
 
+    def mp2_uhf(self, Cp, ep, nplus: int, Cm, em, nminus: int) -> float:
+        """UHF MP2 energy as the reference computes it (hfg_mp2_uhf)."""
+        out = ctypes.c_double()
+        arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (Cp, ep, Cm, em)]
+        _check(library().hfg_mp2_uhf(self._h, _ptr(arrs[0]), _ptr(arrs[1]), nplus, _ptr(arrs[2]), _ptr(arrs[3]),
+                                     nminus, ctypes.byref(out)))
+        return out.value
+
+    def spin_orbital_eri(self, C: np.ndarray) -> np.ndarray:
+        """The (2 nbf)^4 antisymmetrised spin-orbital tensor of MO coefficients C
+        (SpinOrbitalsElectronElectronIntegralsRepository::Compute)."""
+        m = 2 * self.nbf
+        out = np.empty((m, m, m, m), dtype=np.float64)
+        C = np.ascontiguousarray(C, dtype=np.float64)
+        _check(library().hfg_spin_orbital_eri(self._h, _ptr(C), _ptr(out), out.size))
+        return out
+
     def mo_eri_ovov_tensor(self, C, i0: int, ni: int, a0: int, na: int):
         """(ia|jb) block as a torch CUDA tensor [ni*na, ni*na] (hfg_mo_eri_ovov)."""
         import torch
@@ -364,7 +394,7 @@ class Engine:
         arr = (hfg_class_time * 64)()
         n = ctypes.c_int32()
         _check(library().hfg_class_profile(self._h, arr, 64, ctypes.byref(n)))
-        return [{k: getattr(arr[i], k) for k, _ in hfg_class_time._fields_} for i in range(n.value)]
+        return [{k: getattr(arr[i], k) for k, _ in hfg_class_time._fields_ if k != "reserved"} for i in range(n.value)]
 
     def stats(self) -> dict:
         s = hfg_stats()

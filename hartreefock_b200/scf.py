@@ -38,7 +38,7 @@ class hfd_scf_result(ctypes.Structure):
 
 
 DRIVER_SYMBOLS = ["hfd_default_scf_opts", "hfd_last_error", "hfd_scf", "hfd_one_electron", "hfd_pulay_solve",
-                  "hfd_release_thread"]
+                  "hfd_release_thread", "hfd_load_xyz"]
 
 
 def _lib():
@@ -55,6 +55,9 @@ def _lib():
                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
                                        ctypes.POINTER(ctypes.c_int32)]
         L.hfd_one_electron.restype = ctypes.c_int
+        L.hfd_load_xyz.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]
+        L.hfd_load_xyz.restype = ctypes.c_int
         L.hfd_pulay_solve.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]
         L.hfd_pulay_solve.restype = ctypes.c_int
         L.hfd_release_thread.argtypes = []
@@ -63,17 +66,13 @@ def _lib():
     return L
 
 
-def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75, use_diis=True, post_diis=500,
-            alpha_electrons=0, beta_electrons=0, eri_convention=E.ERI_REFERENCE, schwarz_threshold=1e-12,
-            want_density=True, mixed_cutoff=0.0, mixed_switch_energy=1e-7, mixed_switch_density=1e-7,
-            mixed_switch_diis=1e-6,
-            fp64_final_iterations=2, fp64_final_converge=False, incremental=False, trace=False,
-            stop_at_precision_test=False, max_iterations=0, mp2=False, concurrent_classes=False):
-    """RestrictedHartreeFock / UnrestrictedHartreeFock Init + Calculate.
-
-    mixed_cutoff > 0 selects the precision form of the Fock builds (FP32
-    below the cutoff, incremental from the density difference, all-FP64
-    final iterations); incremental=True alone gives FP64 incremental builds."""
+def scf_opts(unrestricted=False, alpha=0.75, init_guess=0.75, use_diis=True, post_diis=500,
+             alpha_electrons=0, beta_electrons=0, eri_convention=E.ERI_REFERENCE, schwarz_threshold=1e-12,
+             mixed_cutoff=0.0, mixed_switch_energy=1e-7, mixed_switch_density=1e-7, mixed_switch_diis=1e-6,
+             fp64_final_iterations=2, fp64_final_converge=False, incremental=False, trace=False,
+             stop_at_precision_test=False, max_iterations=0, mp2=False, concurrent_classes=False) -> hfd_scf_opts:
+    """hfd_scf_opts from keywords (the defaults of hfd_default_scf_opts where
+    not given)."""
     L = _lib()
     o = hfd_scf_opts()
     L.hfd_default_scf_opts(ctypes.byref(o))
@@ -90,6 +89,26 @@ def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75,
     o.max_iterations = int(max_iterations)
     o.mp2 = int(mp2)
     o.concurrent_classes = int(concurrent_classes)  # 0, 1 streams, 2 streams + graphs
+    return o
+
+
+def result_dict(r: hfd_scf_result) -> dict:
+    return {"energy": r.energy, "homo": r.homo, "converged": bool(r.converged), "iterations": r.iterations,
+            "nbf": r.nbf, "fock_builds": r.fock_builds, "fock_ms_total": r.fock_ms_total,
+            "fp32_quartets": r.fp32_quartets, "fp64_quartets": r.fp64_quartets, "mixed_steps": r.mixed_steps,
+            "seconds_fock": r.seconds_fock, "seconds_eigen": r.seconds_eigen, "seconds_diis": r.seconds_diis,
+            "seconds_total": r.seconds_total, "seconds_init": r.seconds_init, "mp2_energy": r.mp2_energy}
+
+
+def run_scf(Z, xyz, basis: str, unrestricted=False, want_density=True, **kw):
+    """RestrictedHartreeFock / UnrestrictedHartreeFock Init + Calculate
+    (scf_opts keywords).
+
+    mixed_cutoff > 0 selects the precision form of the Fock builds (FP32
+    below the cutoff, incremental from the density difference, all-FP64
+    final iterations); incremental=True alone gives FP64 incremental builds."""
+    L = _lib()
+    o = scf_opts(unrestricted=unrestricted, **kw)
     z = np.ascontiguousarray(Z, dtype=np.int32)
     x = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
     nbf_guess = 40 * len(z) + 64
@@ -101,11 +120,7 @@ def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75,
                    dens.ctypes.data_as(ctypes.c_void_p) if dens is not None else None, cap if dens is not None else 0)
     if st != 0:
         raise E.HfgError(st, L.hfd_last_error().decode())
-    out = {"energy": r.energy, "homo": r.homo, "converged": bool(r.converged), "iterations": r.iterations,
-           "nbf": r.nbf, "fock_builds": r.fock_builds, "fock_ms_total": r.fock_ms_total,
-           "fp32_quartets": r.fp32_quartets, "fp64_quartets": r.fp64_quartets, "mixed_steps": r.mixed_steps,
-           "seconds_fock": r.seconds_fock, "seconds_eigen": r.seconds_eigen, "seconds_diis": r.seconds_diis,
-           "seconds_total": r.seconds_total, "seconds_init": r.seconds_init, "mp2_energy": r.mp2_energy}
+    out = result_dict(r)
     if dens is not None:
         n = r.nbf
         if unrestricted:
@@ -114,6 +129,20 @@ def run_scf(Z, xyz, basis: str, unrestricted=False, alpha=0.75, init_guess=0.75,
         else:
             out["density"] = dens[:n * n].reshape(n, n).copy()
     return out
+
+
+def load_xyz(path: str, basis: str, cap: int = 4096):
+    """Systems::Molecule::LoadXYZ through the driver: (Z, xyz, nbf), or None
+    when LoadXYZ returns false."""
+    L = _lib()
+    z = np.zeros(cap, dtype=np.int32)
+    x = np.zeros(3 * cap)
+    n, nbf = ctypes.c_int32(), ctypes.c_int32()
+    st = L.hfd_load_xyz(path.encode(), basis_path(basis).encode(), cap, ctypes.byref(n),
+                        z.ctypes.data_as(ctypes.c_void_p), x.ctypes.data_as(ctypes.c_void_p), ctypes.byref(nbf))
+    if st != 0:
+        return None
+    return z[:n.value].tolist(), x[:3 * n.value].reshape(-1, 3), nbf.value
 
 
 def one_electron(Z, xyz, basis: str):

@@ -32,6 +32,7 @@ doublets (OH, planar CH3), bases drawn uniformly from 6-31G, 6-31G*,
 from __future__ import annotations
 
 import collections
+import ctypes
 import math
 import threading
 import time
@@ -40,29 +41,28 @@ import numpy as np
 
 from . import engine as E
 from . import molecules
-from .basis_io import shell_table
+from . import scf as _scf
+from .basis_io import basis_path, shell_table
 
 HFG_OOM_BUDGET = 3
 SERVE_BASES = ("6-31g", "6-31g*", "6-31+g**")
 
 
 def footprint_bytes(Z, xyz, basis: str, unrestricted: bool = False) -> int:
-    """Estimated device bytes of one job: quartet task lists (12 B per task
-    of up to 32 ket pairs over the triangle of shell pairs), primitive-pair
-    tables (96 B FP64 + 48 B FP32 per primitive pair), and the SCF's n x n
-    FP64 matrices (h, S, V, F, P, new P, C, G, work, 2 x 6 DIIS entries, the
-    incremental history; about 32 per spin), the split path's scratch for
-    shells with d functions (an upper bound: 32 quartets x 2 x 961 doubles
-    per task, at most the engine's 512 MiB budget), plus a fixed 16 MiB for
-    the Boys table, counters and library handles."""
+    """Estimated device bytes of one job, the estimate the native pool uses
+    too (job_footprint_bytes in hartreefock_b200/csrc/host.cpp): quartet task
+    lists (16 B per task of up to 32 ket pairs over the triangle of shell
+    pairs), primitive-pair tables (96 B FP64 + 48 B FP32 per primitive pair),
+    the SCF's n x n FP64 matrices (h, S, V, F, P, new P, C, G, work, 2 x 6
+    DIIS entries, the incremental history; about 32 per spin), plus a fixed
+    16 MiB for the Boys table, counters and library handles."""
     t = shell_table(Z, xyz, basis)
     ns = len(t.L)
     pairs = ns * (ns + 1) // 2
     prim_pairs = int(np.sum(np.triu(np.outer(t.nprim, t.nprim))))
     tasks = pairs * (pairs + 1) // 2 // 32 + pairs
     spins = 2 if unrestricted else 1
-    scratch = min(512 << 20, tasks * 32 * 2 * 961 * 8) if t.max_l >= 2 else 0
-    return int(12 * tasks + 144 * prim_pairs + 8 * t.nbf * t.nbf * 32 * spins + scratch + (16 << 20))
+    return int(16 * tasks + 144 * prim_pairs + 8 * t.nbf * t.nbf * 32 * spins + (16 << 20))
 
 
 class Job:
@@ -220,6 +220,159 @@ class Server:
 
 
 # ---------------------------------------------------------------------------
+# the native pool (C ABI hfg_pool_*, hartreefock_b200/csrc/pool.cpp)
+
+class hfg_job_spec(ctypes.Structure):
+    _fields_ = [("basis_path", ctypes.c_char_p), ("natoms", ctypes.c_int32), ("Z", ctypes.c_void_p),
+                ("xyz", ctypes.c_void_p), ("opts", _scf.hfd_scf_opts), ("timeout_s", ctypes.c_double)]
+
+
+class hfg_job_info(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int32), ("status", ctypes.c_int32), ("queue_s", ctypes.c_double),
+                ("run_s", ctypes.c_double), ("latency_s", ctypes.c_double), ("footprint_bytes", ctypes.c_int64),
+                ("result", _scf.hfd_scf_result)]
+
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED, JOB_TIMEOUT = range(6)
+POOL_SYMBOLS = ["hfg_pool_create", "hfg_job_submit", "hfg_job_poll", "hfg_job_wait", "hfg_job_cancel",
+                "hfg_pool_stats", "hfg_pool_last_error", "hfg_pool_destroy"]
+
+
+def _pool_lib():
+    L = E.library()
+    if not getattr(L, "_pool_ready", False):
+        vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+        L.hfg_pool_create.argtypes = [i32, i64, ctypes.POINTER(vp)]
+        L.hfg_job_submit.argtypes = [vp, ctypes.POINTER(hfg_job_spec), ctypes.POINTER(i64)]
+        L.hfg_job_poll.argtypes = [vp, i64, ctypes.POINTER(hfg_job_info)]
+        L.hfg_job_wait.argtypes = [vp, i64, ctypes.c_double, ctypes.POINTER(hfg_job_info)]
+        L.hfg_job_cancel.argtypes = [vp, i64]
+        L.hfg_pool_stats.argtypes = [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i64)]
+        L.hfg_pool_last_error.restype = ctypes.c_char_p
+        L.hfg_pool_destroy.argtypes = [vp]
+        L.hfg_pool_destroy.restype = None
+        for n in ("hfg_pool_create", "hfg_job_submit", "hfg_job_poll", "hfg_job_wait", "hfg_job_cancel",
+                  "hfg_pool_stats"):
+            getattr(L, n).restype = ctypes.c_int
+        L._pool_ready = True
+    return L
+
+
+class NativeJob:
+    """A job of the native pool: wait(), cancel(), state, result, latency."""
+
+    def __init__(self, server, jid, t_submit, keep):
+        self.server, self.id, self.t_submit, self._keep = server, jid, t_submit, keep
+        self.result, self.error, self.info = None, None, None
+        self.t_end = None
+        self._done = self  # poisson_stream waits on job._done.wait(timeout)
+
+    def _update(self, info):
+        self.info = info
+        if info.state >= JOB_DONE and self.t_end is None:
+            self.t_end = self.t_submit + info.latency_s
+            r = _scf.result_dict(info.result)
+            if info.state == JOB_DONE:
+                self.result = r
+            else:
+                self.result = r
+                self.error = E.HfgError(info.status, {JOB_FAILED: "failed", JOB_CANCELLED: "cancelled",
+                                                      JOB_TIMEOUT: "timed out"}[info.state])
+
+    def wait(self, timeout=None):
+        info = hfg_job_info()
+        st = _pool_lib().hfg_job_wait(self.server._h, self.id, float(timeout or 0), ctypes.byref(info))
+        self._update(info)
+        if st != 0 and info.state < JOB_DONE:
+            raise TimeoutError(f"job {self.id} still running")
+        if self.error is not None:
+            raise self.error
+        return self.result
+
+    def poll(self) -> int:
+        info = hfg_job_info()
+        _check_pool(_pool_lib().hfg_job_poll(self.server._h, self.id, ctypes.byref(info)))
+        self._update(info)
+        return info.state
+
+    def cancel(self):
+        _check_pool(_pool_lib().hfg_job_cancel(self.server._h, self.id))
+
+    @property
+    def latency(self) -> float:
+        return self.info.latency_s
+
+    @property
+    def done(self) -> bool:
+        return self.poll() >= JOB_DONE
+
+
+def _check_pool(st):
+    if st != 0:
+        raise E.HfgError(st, _pool_lib().hfg_pool_last_error().decode())
+
+
+class NativeServer:
+    """The request loop in native code (hfg_pool_*): the same slots, budget,
+    arrival-order admission and SCF defaults as Server, with the queue,
+    admission, cancellation and timeouts in C++ worker threads."""
+
+    def __init__(self, slots: int = 8, hbm_budget: int = 32 << 30, mixed: bool = True, mixed_cutoff: float = 1e-4,
+                 scf_kwargs=None, concurrent_classes: bool = True):
+        self.slots, self.budget = slots, int(hbm_budget)
+        self.defaults = dict(post_diis=0, max_iterations=1000, eri_convention=E.ERI_EXACT, mixed_switch_diis=1e-7,
+                             concurrent_classes=1 if concurrent_classes else 0)
+        if mixed:
+            self.defaults["mixed_cutoff"] = mixed_cutoff
+        else:
+            self.defaults["stop_at_precision_test"] = True
+        self.defaults.update(scf_kwargs or {})
+        h = ctypes.c_void_p()
+        _check_pool(_pool_lib().hfg_pool_create(slots, self.budget, ctypes.byref(h)))
+        self._h = h
+        self.peak_running, self.peak_bytes = 0, 0
+        self._stop = threading.Event()
+        self._sampler = threading.Thread(target=self._sample, daemon=True)
+        self._sampler.start()
+
+    def _sample(self):
+        r, q, b = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+        while not self._stop.wait(0.005):
+            if _pool_lib().hfg_pool_stats(self._h, ctypes.byref(r), ctypes.byref(q), ctypes.byref(b)) == 0:
+                self.peak_running = max(self.peak_running, r.value)
+                self.peak_bytes = max(self.peak_bytes, b.value)
+
+    def submit(self, Z, xyz, basis: str, unrestricted: bool = False, timeout_s: float = 0.0, **kwargs) -> NativeJob:
+        kw = dict(self.defaults)
+        kw.update(kwargs)
+        z = np.ascontiguousarray(Z, dtype=np.int32)
+        x = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
+        spec = hfg_job_spec()
+        path = basis_path(basis).encode()
+        spec.basis_path, spec.natoms = path, len(z)
+        spec.Z, spec.xyz = z.ctypes.data_as(ctypes.c_void_p), x.ctypes.data_as(ctypes.c_void_p)
+        spec.opts = _scf.scf_opts(unrestricted=unrestricted, **kw)
+        spec.timeout_s = float(timeout_s)
+        jid = ctypes.c_int64()
+        t = time.perf_counter()
+        _check_pool(_pool_lib().hfg_job_submit(self._h, ctypes.byref(spec), ctypes.byref(jid)))
+        return NativeJob(self, jid.value, t, (z, x, path))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._stop.set()
+            self._sampler.join()
+            _pool_lib().hfg_pool_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+# ---------------------------------------------------------------------------
 # synthetic request stream
 
 def _functions_per_atom(basis: str) -> dict:
@@ -280,7 +433,10 @@ def poisson_stream(server: Server, jobs, rate: float, seed: int = 0, timeout=Non
             time.sleep(delay)
         handles.append(server.submit(Z, xyz, basis, unrestricted=uhf, **(UHF_KW if uhf else RHF_KW)))
     for h in handles:
-        h._done.wait(timeout)
+        try:
+            h._done.wait(timeout)
+        except E.HfgError:
+            pass  # counted below through h.error
     t_end = max(h.t_end for h in handles)
     lat = np.array([h.latency for h in handles if h.error is None]) * 1e3
     summary = {"offered_rate": rate, "jobs": len(handles), "failed": sum(h.error is not None for h in handles),

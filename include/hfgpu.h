@@ -213,11 +213,36 @@ hfg_status hfg_one_electron(const hfg_shells *shells, const double *xyz, const i
  * HFG_OOM_BUDGET.  Single-molecule contexts only. */
 hfg_status hfg_mo_eri_ovov(hfg_ctx *ctx, const double *dC, int32_t i0, int32_t ni, int32_t a0, int32_t na, double *dX,
                            void *stream);
+/* The whole MO tensor (pq|rs) for every orbital of dC (device, row-major
+ * nbf x nbf), as dX[(p q),(r s)] (nbf^2 x nbf^2, row-major): the elements
+ * MolecularOrbitalsIntegralsRepository::getElectronElectron(p, q, r, s, C)
+ * returns (IntegralsRepository.h:190-291).  Needs about 11/8 nbf^4 doubles
+ * free.  Single-molecule contexts only. */
+hfg_status hfg_mo_eri_full(hfg_ctx *ctx, const double *dC, double *dX, void *stream);
+/* SpinOrbitalsElectronElectronIntegralsRepository::Compute
+ * (SpinOrbitalsElectronElectronIntegralsRepository.cpp:30-52) for host C
+ * (row-major nbf x nbf): out[((p m + q) m + r) m + s], m = 2 nbf, spin orbital
+ * p = spatial orbital p / 2 with spin p % 2, receives
+ *   (p/2 r/2 | q/2 s/2) [p, r and q, s of one spin] - (p/2 s/2 | q/2 r/2) [p, s and q, r of one spin],
+ * the antisymmetrised integrals of the CCSD and CIS consumers; `count` >= m^4. */
+hfg_status hfg_spin_orbital_eri(hfg_ctx *ctx, const double *C, double *out, int64_t count);
 /* RHF MP2 correlation energy from host C (row-major nbf x nbf) and orbital
  * energies eps[nbf], the lowest nocc orbitals occupied:
  * sum (ia|jb)[2(ia|jb) - (ib|ja)] / (e_i + e_j - e_a - e_b).  Replaces
  * RestrictedHartreeFock::CalculateMp2Energy (RestrictedHartreeFock.cpp:251-288). */
 hfg_status hfg_mp2_rhf(hfg_ctx *ctx, const double *C, const double *eps, int32_t nocc, double *e_mp2);
+/* UHF MP2 energy as UnrestrictedHartreeFock::CalculateMp2Energy computes it
+ * (UnrestrictedHartreeFock.cpp:295-375): 0.25 (S+ + S-), S = sum over the
+ * spin's occupied i, j and virtual a, b of (ia|jb)^2 / (e_i + e_j - e_a - e_b),
+ * from host C+ / C- (row-major nbf x nbf), orbital energies e+ / e- and the
+ * occupied counts n+ >= n- (lowest orbitals).  The reference evaluates both
+ * sums through one MolecularOrbitalsIntegralsRepository whose caches are
+ * keyed by orbital indices only (IntegralsRepository.h:190-291), so its S-
+ * reuses values cached with C+; this reproduces that: in S-, quartets with a
+ * and b virtual in both spins take C+, those with a occupied in + only take
+ * (i- a- | j+ b+), those with b occupied in + only take C-. */
+hfg_status hfg_mp2_uhf(hfg_ctx *ctx, const double *Cplus, const double *eplus, int32_t nplus, const double *Cminus,
+                       const double *eminus, int32_t nminus, double *e_mp2);
 
 /* Frees the calling host thread's library state (the batched eigensolver's
  * handle and workspace).  For worker threads that exit while the process
@@ -240,16 +265,23 @@ hfg_status hfg_eigh_batched(const double *dA, double *dV, double *dW, int32_t n,
  * allocate device memory while they run: a serving loop under a fixed HBM
  * budget, code that cannot afford the implicit synchronisation of
  * cudaMalloc/cudaFree, or a host without allocator access on that path.
- * No counterpart in the reference (its Fock build, RestrictedHartreeFock.cpp
- * :168-207, allocates freely).  The J/K accumulators live in a file-scope
- * device array of 2 x 1024 x 1024 doubles (16 MiB) that every GPU loading
- * the library keeps until exit; contexts above 1024 basis functions are
- * rejected with HFG_INVALID_ARG.  The context (created beforehand with
- * hfg_ctx_create, which does allocate) and the caller's device buffers dP, dG
- * are the only other memory used.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) and should come before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * (different streams or contexts at the same time) race on it. */
+ * No counterpart in the reference.  The J/K accumulators live in a
+ * file-scope device array of 2 x 1024 x 1024 doubles (16 MiB) that every GPU
+ * loading the library keeps until exit; contexts above 1024 basis functions
+ * are rejected with HFG_INVALID_ARG.  The large classes run on the
+ * warp-cooperative kernels (shared memory only), so no other scratch is
+ * used: the context (created beforehand with hfg_ctx_create, which does
+ * allocate) and the caller's device buffers dP, dG are the only other memory.
+ * The call always does a plain full FP64 build; a context with
+ * precision-form settings (density screening, an FP32 cutoff or incremental
+ * builds) is rejected with HFG_INVALID_ARG.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress) and should come
+ * before any stream capture; the CUDA driver also sizes its per-thread
+ * local-memory reservation on a kernel's first launch in the process, so a
+ * caller that must see no allocation inside the call makes one call (or one
+ * hfg_fock_rhf_device build) beforehand.  All calls share the array: calls
+ * that overlap on the GPU (different streams or contexts at the same time)
+ * race on it. */
 hfg_status hfg_fock_rhf_noalloc(hfg_ctx *ctx, const double *dP, double *dG, void *stream);
 
 /* Schwarz bounds sqrt(max (ij|ij)) per shell pair (a >= b), in pair order
@@ -294,6 +326,11 @@ typedef struct {
   int64_t primitive_quartets;
   double flops;             /* algorithmic flops of the class in one build */
   double ms;                /* device time of the class kernel, last build */
+  int64_t tasks;            /* tasks (one bra pair, <= 32 ket pairs) of the class */
+  double lane_occupancy;    /* primitive quartets the lanes evaluate / (32 x the longest
+                               lane loop) over the tasks, for a thread per quartet */
+  int32_t warp_kernel;      /* 1: one warp per quartet (the large classes) */
+  int32_t reserved;
 } hfg_class_time;
 hfg_status hfg_set_profiling(hfg_ctx *ctx, int32_t on);
 /* Writes up to `cap` entries (largest flops first); *count = entries written. */
@@ -303,6 +340,9 @@ hfg_status hfg_class_profile(const hfg_ctx *ctx, hfg_class_time *out, int32_t ca
  * microbenchmark on `device` (TFLOP/s, 2 flops per FMA).  Instrumentation
  * for the roofline denominator; no reference counterpart. */
 hfg_status hfg_measure_fp64_peak(int32_t device, double *tflops);
+/* The same for FP32 FMA (the precision form's FP32 quartets); no counterpart
+ * in the reference. */
+hfg_status hfg_measure_fp32_peak(int32_t device, double *tflops);
 
 #ifdef __cplusplus
 }

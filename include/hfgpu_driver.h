@@ -37,7 +37,7 @@ typedef struct {
   int32_t stop_at_precision_test; /* plain builds, precision form's stopping rule */
   int32_t max_iterations;    /* the algorithm's iteration cap; 0 = 3000, the
                                 reference's default (RestrictedHartreeFock.h:31) */
-  int32_t mp2;               /* 1: RHF MP2 energy after the SCF (result.mp2_energy) */
+  int32_t mp2;               /* 1: MP2 energy after the SCF (result.mp2_energy), RHF or UHF */
   int32_t concurrent_classes;/* 1: a build's classes on concurrent streams
                                 (HartreeFockAlgorithm::concurrentClasses); 2: also CUDA-graph
                                 replay of plain builds (cudaGraphs), for one host thread
@@ -59,7 +59,7 @@ typedef struct {
   /* wall-clock split of the SCF (seconds) */
   double seconds_fock, seconds_eigen, seconds_diis, seconds_total;
   double seconds_init;       /* Init: one-electron matrices, engine context, S^-1/2 */
-  double mp2_energy;         /* RestrictedHartreeFock::CalculateMp2Energy when opts.mp2 */
+  double mp2_energy;         /* Restricted/UnrestrictedHartreeFock::CalculateMp2Energy when opts.mp2 */
 } hfd_scf_result;
 
 void hfd_default_scf_opts(hfd_scf_opts *o);
@@ -80,10 +80,69 @@ hfg_status hfd_pulay_solve(const double *B, int32_t m1, int32_t batch, double *c
  * capacity in `density_count`. */
 hfg_status hfd_scf(const char *basis_path, int32_t natoms, const int32_t *Z, const double *xyz,
                    const hfd_scf_opts *opts, hfd_scf_result *result, double *density, int64_t density_count);
-/* Core Hamiltonian h = T + V and overlap S from the host one-electron code
- * (row-major nbf x nbf); *nbf is set. */
+/* Core Hamiltonian h = T + V and overlap S from the device one-electron
+ * kernels (hfg_one_electron), copied to the host row-major nbf x nbf; *nbf
+ * is set. */
 hfg_status hfd_one_electron(const char *basis_path, int32_t natoms, const int32_t *Z, const double *xyz, double *S,
                             double *h, int64_t capacity, int32_t *nbf);
+
+/* Systems::Molecule::LoadXYZ (Molecule.cpp:143-199) against the basis file:
+ * on success *natoms atoms with Z[i] and xyz[3 i ..] as written in the file
+ * (up to `cap` atoms) and *nbf Cartesian functions; HFG_INVALID_ARG when
+ * LoadXYZ returns false (short file, unknown symbol, element missing from
+ * the basis, unparsable count line).  Host only, no device work. */
+hfg_status hfd_load_xyz(const char *xyz_path, const char *basis_path, int32_t cap, int32_t *natoms, int32_t *Z,
+                        double *xyz, int32_t *nbf);
+
+/* ---------------------------------------------------------------------
+ * Serving pool: RHF/UHF jobs submitted at any time, run by `slots` worker
+ * threads whose SCFs share the device (each job's engine context, density,
+ * Fock matrix, DIIS history and screening tables stay in device memory for
+ * the life of the job), admitted in arrival order as soon as a slot is free
+ * and the job's estimated footprint fits in what is left of the budget.
+ * The reference's counterpart is its one-std::thread-per-job document
+ * (HartreeFockDoc.cpp:372-405) with HartreeFockAlgorithm::terminate
+ * (HartreeFockAlgorithm.h:57) as the stop: a cancelled or timed-out job
+ * stops between two SCF iterations.
+ * --------------------------------------------------------------------- */
+typedef struct hfg_pool hfg_pool;
+
+enum { HFG_JOB_QUEUED = 0, HFG_JOB_RUNNING = 1, HFG_JOB_DONE = 2, HFG_JOB_FAILED = 3, HFG_JOB_CANCELLED = 4,
+       HFG_JOB_TIMEOUT = 5 };
+
+typedef struct {
+  const char *basis_path;   /* copied at submission, as are Z and xyz */
+  int32_t natoms;
+  const int32_t *Z;
+  const double *xyz;        /* bohr, 3 per atom */
+  hfd_scf_opts opts;        /* the job's SCF (hfd_scf's options) */
+  double timeout_s;         /* > 0: bound on submission-to-end time */
+} hfg_job_spec;
+
+typedef struct {
+  int32_t state;            /* HFG_JOB_* */
+  hfg_status status;        /* HFG_OK, the SCF's error, HFG_CANCELLED or HFG_TIMEOUT */
+  double queue_s, run_s, latency_s;  /* submission to start, start to end, submission to end */
+  int64_t footprint_bytes;  /* the admission estimate */
+  hfd_scf_result result;    /* set once the job has ended (energy so far when stopped) */
+} hfg_job_info;
+
+/* slots >= 1 worker threads; hbm_budget_bytes bounds the admitted jobs' summed estimates. */
+hfg_status hfg_pool_create(int32_t slots, int64_t hbm_budget_bytes, hfg_pool **out);
+/* Queues a job; HFG_OOM_BUDGET when its estimate exceeds the whole budget. */
+hfg_status hfg_job_submit(hfg_pool *pool, const hfg_job_spec *spec, int64_t *job_id);
+/* Non-blocking state of a job. */
+hfg_status hfg_job_poll(hfg_pool *pool, int64_t job_id, hfg_job_info *info);
+/* Waits until the job has ended (timeout_s <= 0: no bound); HFG_TIMEOUT if it has not. */
+hfg_status hfg_job_wait(hfg_pool *pool, int64_t job_id, double timeout_s, hfg_job_info *info);
+/* A queued job leaves the queue; a running one stops between SCF iterations;
+ * both end as HFG_JOB_CANCELLED.  No effect on an ended job. */
+hfg_status hfg_job_cancel(hfg_pool *pool, int64_t job_id);
+/* Jobs running and queued now, and the budget they hold. */
+hfg_status hfg_pool_stats(hfg_pool *pool, int32_t *running, int32_t *queued, int64_t *used_bytes);
+const char *hfg_pool_last_error(void);
+/* Cancels queued and running jobs, waits for the workers, frees the pool. */
+void hfg_pool_destroy(hfg_pool *pool);
 
 #ifdef __cplusplus
 }

@@ -15,8 +15,9 @@
 // iterations run on the same GPU in FP64 (Fock assembly, DIIS,
 // orthogonalisation, cuSOLVER eigensolves, densities), with the public
 // fields (DensityMatrix, C, eigenvalues, energies) brought back to the host
-// at the end of Calculate() or of a Step() called on its own.  One-electron
-// matrices and S^-1/2 are formed on the host at Init.  Matrices are
+// at the end of Calculate() or of a Step() called on its own.  The
+// one-electron matrices (S, T, V) are computed on the device at Init
+// (hfg_one_electron) and S^-1/2 is formed there too.  Matrices are
 // row-major (hfgpu::Matrix) instead of Eigen::MatrixXd; element access
 // M(i, j) is the same.
 #pragma once
@@ -129,6 +130,7 @@ class Molecule {
   const ShellTable &shellTable() const { return table_; }
 
  private:
+  bool LoadXYZBody(const std::string &fileName, const Chemistry::Basis &basis);
   ShellTable table_;
 };
 
@@ -179,6 +181,43 @@ class IntegralsRepository {
   Systems::Molecule *molecule_ = nullptr;
   hfg_ctx *ctx_ = nullptr;
   std::vector<double> packed_;
+};
+
+// MO integrals for the post-HF consumers (IntegralsRepository.h:190-291).
+// getElectronElectron(p, q, r, s, C) = sum C(mu,p) C(nu,q) C(l,r) C(s',s)
+// (mu nu | l s'); the first call computes the whole tensor for its C on the
+// device (hfg_mo_eri_full) and later calls read it.  Like the reference,
+// whose caches are keyed by orbital indices only, later calls with another
+// C return the first C's values.
+class MolecularOrbitalsIntegralsRepository {
+ public:
+  explicit MolecularOrbitalsIntegralsRepository(IntegralsRepository &repository) : repo_(repository) {}
+  double getElectronElectron(unsigned p, unsigned q, unsigned r, unsigned s, const hfgpu::Matrix &C);
+
+ private:
+  IntegralsRepository &repo_;
+  int n_ = 0;
+  std::vector<double> mo_;
+};
+
+// Antisymmetrised spin-orbital integrals for CCSD / CIS
+// (SpinOrbitalsElectronElectronIntegralsRepository.cpp:10-52): spin orbital
+// p is spatial orbital p / 2 with spin p % 2, and
+// (p, q, r, s) = (p/2 r/2 | q/2 s/2)[same spins p r, q s] - (p/2 s/2 | q/2 r/2)[same spins p s, q r],
+// computed on the device (hfg_spin_orbital_eri).
+class SpinOrbitalsElectronElectronIntegralsRepository {
+ public:
+  explicit SpinOrbitalsElectronElectronIntegralsRepository(int numOrbitals);
+  SpinOrbitalsElectronElectronIntegralsRepository(int numOrbitals, IntegralsRepository &repository,
+                                                  const hfgpu::Matrix &C);
+  void Compute(IntegralsRepository &repository, const hfgpu::Matrix &C);
+  double operator()(unsigned p, unsigned q, unsigned r, unsigned s) const {
+    return t_[((static_cast<size_t>(p) * m_ + q) * m_ + r) * m_ + s];
+  }
+
+ private:
+  size_t m_ = 0;
+  std::vector<double> t_;
 };
 
 }  // namespace GaussianIntegrals
@@ -326,6 +365,8 @@ class UnrestrictedHartreeFock : public HartreeFockAlgorithm {
   explicit UnrestrictedHartreeFock(int iterations = 3000) : HartreeFockAlgorithm(iterations) {}
   void Init(Systems::Molecule *molecule) override;
   double Step(int iter) override;
+  // UnrestrictedHartreeFock.cpp:295-375, on the device (hfg_mp2_uhf)
+  double CalculateMp2Energy();
 
  protected:
   void SyncToDevice() override;

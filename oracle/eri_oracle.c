@@ -396,6 +396,15 @@ void orc_eri_packed(int n, const orc_function *f, const orc_primitive *p, int ma
     }
 }
 
+/* Diagonal quartets (ij|ij), i >= j, at index i(i+1)/2 + j: the Schwarz
+ * bounds of the function pairs.  OpenMP over i. */
+void orc_eri_diagonal(int n, const orc_function *f, const orc_primitive *p, int max_boys_m, int exact_et,
+                      double *out) {
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j <= i; ++j) out[two_index(i, j)] = orc_eri(f, p, i, j, i, j, max_boys_m, exact_et);
+}
+
 void orc_g_rhf(int n, const double *packed, const double *P, double *G) {
 #pragma omp parallel for
   for (int i = 0; i < n; ++i)
@@ -409,6 +418,28 @@ void orc_g_rhf(int n, const double *packed, const double *P, double *G) {
         }
       G[i * n + j] = g;
     }
+}
+
+/* Rows of RestrictedHartreeFock::InitFockMatrix's two-electron part
+ * (RestrictedHartreeFock.cpp:189-200) straight from the contracted accessor,
+ * no stored table, for molecules whose packed table does not fit:
+ * G_ij = sum_kl P_kl [(ij|kl) - 1/2 (il|kj)] for i in rows[0..nrows), all j.
+ * The J sum uses the symmetry of P (kl and lk together).  OpenMP over j. */
+void orc_g_rhf_rows(int n, const orc_function *f, const orc_primitive *p, int max_boys_m, int exact_et,
+                    const double *P, const int *rows, int nrows, double *out) {
+  for (int r = 0; r < nrows; ++r) {
+    const int i = rows[r];
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int j = 0; j < n; ++j) {
+      double coulomb = 0, exchange = 0;
+      for (int k = 0; k < n; ++k) {
+        for (int l = 0; l < k; ++l) coulomb += 2.0 * P[k * n + l] * orc_eri(f, p, i, j, k, l, max_boys_m, exact_et);
+        coulomb += P[k * n + k] * orc_eri(f, p, i, j, k, k, max_boys_m, exact_et);
+        for (int l = 0; l < n; ++l) exchange += P[k * n + l] * orc_eri(f, p, i, l, k, j, max_boys_m, exact_et);
+      }
+      out[(size_t)r * n + j] = coulomb - 0.5 * exchange;
+    }
+  }
 }
 
 void orc_g_uhf(int n, const double *packed, const double *Pa, const double *Pb, double *Ga, double *Gb) {

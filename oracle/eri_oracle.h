@@ -61,9 +61,17 @@ int64_t orc_packed_size(int n);
 void orc_eri_packed(int n, const orc_function *f, const orc_primitive *p, int max_boys_m, int exact_et,
                     double *out);
 
+/* (ij|ij) for every function pair i >= j, at index i(i+1)/2 + j. */
+void orc_eri_diagonal(int n, const orc_function *f, const orc_primitive *p, int max_boys_m, int exact_et,
+                      double *out);
+
 /* RestrictedHartreeFock::InitFockMatrix two-electron part
  * (RestrictedHartreeFock.cpp:189-200): G_ij = sum_kl P_kl[(ij|kl) - 1/2 (il|kj)]. */
 void orc_g_rhf(int n, const double *packed, const double *P, double *G);
+/* Selected rows of the same G, evaluated through orc_eri without a stored
+ * table (large molecules): out[r][j] = G_{rows[r], j}. */
+void orc_g_rhf_rows(int n, const orc_function *f, const orc_primitive *p, int max_boys_m, int exact_et,
+                    const double *P, const int *rows, int nrows, double *out);
 /* UnrestrictedHartreeFock::InitFockMatrices (UnrestrictedHartreeFock.cpp:225-238). */
 void orc_g_uhf(int n, const double *packed, const double *Pa, const double *Pb, double *Ga, double *Gb);
 

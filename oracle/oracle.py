@@ -206,6 +206,9 @@ def lib():
         L.orc_eri_packed.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, pd]
         L.orc_g_rhf.argtypes = [ctypes.c_int, pd, pd, pd]
         L.orc_g_uhf.argtypes = [ctypes.c_int, pd, pd, pd, pd, pd]
+        L.orc_eri_diagonal.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, pd]
+        L.orc_g_rhf_rows.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, pd,
+                                     ctypes.POINTER(ctypes.c_int), ctypes.c_int, pd]
         L.orc_one_electron.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, pd,
                                        ctypes.POINTER(ctypes.c_int), ctypes.c_int, pd, pd, pd]
         _lib = L
@@ -248,6 +251,64 @@ def g_rhf(n, packed, P):
     G = np.zeros((n, n))
     lib().orc_g_rhf(n, _p(packed), _p(np.ascontiguousarray(P)), _p(G))
     return G
+
+
+def screened_quartets(mol: Molecule, threshold: float) -> dict:
+    """Size of a direct Fock build under Schwarz screening: shells are the
+    functions of one (shell ID, L) (the s and p parts of an SP shell are two
+    shells), Q_ab = sqrt(max |(ij|ij)|) over the function pairs of the shell
+    pair (exact electron transfer), and a shell quartet {ab, cd} is kept when
+    Q_ab Q_cd >= threshold.  Returns the 8-fold unique function quartets kept
+    and in total."""
+    n = mol.nbf
+    diag = np.zeros(n * (n + 1) // 2)
+    lib().orc_eri_diagonal(n, ctypes.byref(mol.functions), ctypes.byref(mol.primitives), mol.max_boys_m, 1,
+                           _p(diag))
+    key = [(f.shell_id, f.l + f.m + f.n) for f in mol.functions]
+    shells = []
+    for i, k in enumerate(key):
+        if i == 0 or k != key[i - 1]:
+            shells.append([])
+        shells[-1].append(i)
+    Q, fcount = [], []
+    for a in range(len(shells)):
+        for b in range(a + 1):
+            m = 0.0
+            for i in shells[a]:
+                for j in shells[b]:
+                    m = max(m, abs(diag[two_index(i, j)]))
+            Q.append(np.sqrt(m))
+            na, nb = len(shells[a]), len(shells[b])
+            fcount.append(na * (na + 1) // 2 if a == b else na * nb)
+    Q, fcount = np.array(Q), np.array(fcount, dtype=np.float64)
+    order = np.argsort(-Q)
+    Q, fcount = Q[order], fcount[order]
+    prefix = np.concatenate([[0.0], np.cumsum(fcount)])
+    kept = 0.0
+    for p_ in range(len(Q)):
+        if Q[p_] <= 0:
+            break
+        # partners q < p_ (larger or equal bound) with Q_p Q_q >= threshold: all of them
+        # when Q_p^2 >= threshold, else a prefix of the sorted list
+        hi = int(np.searchsorted(-Q, -(threshold / Q[p_]), side="right"))
+        m = min(hi, p_)
+        kept += fcount[p_] * prefix[m]
+        if Q[p_] * Q[p_] >= threshold:
+            kept += fcount[p_] * (fcount[p_] + 1) / 2
+    npair = n * (n + 1) // 2
+    return {"kept": int(round(kept)), "total": npair * (npair + 1) // 2}
+
+
+def g_rhf_rows(mol: Molecule, P, rows, exact_et=False) -> np.ndarray:
+    """Rows of the RHF two-electron matrix G[P] straight from the contracted
+    ERIs (no stored table): out[r] = G[rows[r], :]."""
+    n = mol.nbf
+    rows = np.ascontiguousarray(rows, dtype=np.int32)
+    out = np.zeros((len(rows), n))
+    lib().orc_g_rhf_rows(n, ctypes.byref(mol.functions), ctypes.byref(mol.primitives), mol.max_boys_m,
+                         int(exact_et), _p(np.ascontiguousarray(P, dtype=np.float64)),
+                         rows.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(rows), _p(out))
+    return out
 
 
 def g_uhf(n, packed, Pa, Pb):

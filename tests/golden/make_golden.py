@@ -29,7 +29,7 @@ def fixtures():
     return {
         # README.md water, STO-3G, initGuess 0, alpha 0.5
         "h2o_sto3g": dict(Z=h2o_Z, xyz=h2o_xyz, basis="sto-3g", ref_basis="sto3g.txt", eri=True,
-                          scf=[("rhf", 0.5, 0.0), ("uhf", 0.5, 0.0)]),
+                          scf=[("rhf", 0.5, 0.0), ("uhf", 0.5, 0.0)], spinorb=True),
         # two oxygens: exercises every class up to (dd|dd), two-centre bras included
         "o2_631gs": dict(Z=[8, 8], xyz=np.array([[0.0, 0.0, 0.0], [0.3, -0.2, 2.3]]), basis="6-31g*",
                          ref_basis="6-31g_st_.1.nw", eri=True, scf=[]),
@@ -58,8 +58,15 @@ def main():
                 out["h"] = r["h"].reshape(mol.nbf, mol.nbf)
                 out["enuc"] = r["enuc"]
             for kind, alpha, guess in fx["scf"]:
-                r = O.run_reference(mol, kind, os.path.join(td, kind + ".bin"), alpha=alpha, init_guess=guess)
+                so = kind == "rhf" and fx.get("spinorb", False)
+                r = O.run_reference(mol, kind, os.path.join(td, kind + ".bin"), alpha=alpha, init_guess=guess,
+                                    extra="mp2 1" + ("\nspinorb 1" if so else ""))
+                if so:
+                    # SpinOrbitalsElectronElectronIntegralsRepository over the converged C
+                    out["rhf_C"] = r["C"].reshape(mol.nbf, mol.nbf)
+                    out["spin_orbital_eri"] = r["spin_orbital_eri"]
                 out[f"{kind}_energy"] = r["energy"]
+                out[f"{kind}_mp2"] = r["mp2"]
                 out[f"{kind}_alpha"] = np.array(alpha)
                 out[f"{kind}_initguess"] = np.array(guess)
                 if kind == "rhf":

@@ -11,10 +11,12 @@ import pytest
 from conftest import ROOT
 from hartreefock_b200 import engine as E
 from hartreefock_b200 import scf
+from hartreefock_b200 import serve
 
 STRUCTS = [("hfg_shells", E.hfg_shells), ("hfg_opts", E.hfg_opts), ("hfg_stats", E.hfg_stats),
            ("hfg_class_time", E.hfg_class_time), ("hfd_scf_opts", scf.hfd_scf_opts),
-           ("hfd_scf_result", scf.hfd_scf_result)]
+           ("hfd_scf_result", scf.hfd_scf_result), ("hfg_job_spec", serve.hfg_job_spec),
+           ("hfg_job_info", serve.hfg_job_info)]
 
 
 def _c_layout():

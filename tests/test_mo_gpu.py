@@ -67,3 +67,36 @@ def test_scf_mp2_matches_canonical_orbitals_of_the_converged_density():
     want, _ = mp2_numpy(full_eri(packed, n), X @ Cp, eps, 5)
     assert want < 0
     assert abs(r["mp2_energy"] - want) < 1e-8, (r["mp2_energy"], want)
+
+
+MP2_TOL = 1e-8  # Eh: MP2 energies of SCF runs that match the reference's energies within 1e-9
+
+
+@pytest.mark.parametrize("name,kind", [("h2o_sto3g", "rhf"), ("h2o_631gs", "rhf"), ("h2o2_631gs", "rhf"),
+                                       ("h2o_sto3g", "uhf"), ("oh_631g", "uhf")])
+def test_scf_mp2_matches_reference(name, kind):
+    """CalculateMp2Energy after the SCF, RHF (RestrictedHartreeFock.cpp:251-288)
+    and UHF (UnrestrictedHartreeFock.cpp:295-375, including its orbital-index
+    cache), against the values the reference itself printed."""
+    g = load_golden(name)
+    r = scf.run_scf(list(g["Z"]), g["xyz"], str(g["basis"]), unrestricted=(kind == "uhf"),
+                    alpha=float(g[f"{kind}_alpha"]), init_guess=float(g[f"{kind}_initguess"]),
+                    schwarz_threshold=0.0, mp2=True)
+    assert r["converged"]
+    want = float(g[f"{kind}_mp2"][0])
+    assert want < 0
+    assert abs(r["mp2_energy"] - want) < MP2_TOL, (r["mp2_energy"], want)
+
+
+def test_spin_orbital_tensor_matches_reference():
+    """SpinOrbitalsElectronElectronIntegralsRepository::Compute over the
+    reference's own converged C (README water, STO-3G), element by element."""
+    g = load_golden("h2o_sto3g")
+    eng = E.Engine(list(g["Z"]), g["xyz"], "sto-3g", schwarz_threshold=0.0)
+    T = eng.spin_orbital_eri(g["rhf_C"])
+    want = g["spin_orbital_eri"].reshape(T.shape)
+    assert np.abs(T - want).max() < 1e-12
+    # antisymmetry <pq||rs> = -<pq||sr> and the spin selection
+    assert np.abs(T + T.transpose(0, 1, 3, 2)).max() < 1e-12
+    assert np.abs(T[0, 1, 0, 1] - want[0, 1, 0, 1]) < 1e-12
+    eng.close()

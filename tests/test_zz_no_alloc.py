@@ -14,11 +14,16 @@ from conftest import load_golden
 pytestmark = pytest.mark.gpu
 
 
-def test_noalloc_fock_matches_allocating_entry_point():
+@pytest.mark.parametrize("name,convention", [("h2o2_631gs", "reference"), ("o2_631gs", "reference"),
+                                             ("o2_631gs", "exact")])
+def test_noalloc_fock_matches_allocating_entry_point(name, convention):
+    """Both ERI conventions, on molecules whose d shells reach every class up
+    to (dd|dd) (O2: two-centre d pairs)."""
     import torch
     from hartreefock_b200 import engine as E
-    g = load_golden("h2o2_631gs")
-    eng = E.Engine(list(g["Z"]), g["xyz"], str(g["basis"]), schwarz_threshold=1e-12)
+    g = load_golden(name)
+    conv = E.ERI_REFERENCE if convention == "reference" else E.ERI_EXACT
+    eng = E.Engine(list(g["Z"]), g["xyz"], str(g["basis"]), schwarz_threshold=1e-12, eri_convention=conv)
     n = eng.nbf
     rng = np.random.default_rng(7)
     A = rng.normal(size=(n, n)) * 0.1
@@ -46,5 +51,15 @@ def test_noalloc_rejects_contexts_above_its_scratch():
     eng = E.Engine(Z, xyz, "6-31g*", schwarz_threshold=1e-10)
     assert eng.nbf > 1024
     with pytest.raises(E.HfgError, match="exceed"):
+        eng.fock_rhf_noalloc(0x1000, 0x1000)
+    eng.close()
+
+
+def test_noalloc_rejects_precision_form_contexts():
+    from hartreefock_b200 import engine as E
+    g = load_golden("h2o_631gs")
+    eng = E.Engine(list(g["Z"]), g["xyz"], str(g["basis"]), schwarz_threshold=1e-12)
+    eng.set_mixed_cutoff(1e-4)
+    with pytest.raises(E.HfgError, match="precision-form"):
         eng.fock_rhf_noalloc(0x1000, 0x1000)
     eng.close()
