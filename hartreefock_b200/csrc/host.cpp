@@ -313,6 +313,13 @@ double Systems::Molecule::NuclearRepulsionEnergy() const {
   return e;
 }
 
+double Systems::Molecule::NuclearElectricFieldEnergy() const {
+  double e = 0;
+  for (const auto &a : atoms)
+    e -= double(a.Z) * (a.position.X * ElectricField.X + a.position.Y * ElectricField.Y + a.position.Z * ElectricField.Z);
+  return e;
+}
+
 void Systems::Molecule::Init() {
   ShellTable t;
   int ao = 0;
@@ -510,6 +517,17 @@ void SpinOrbitalsElectronElectronIntegralsRepository::Compute(IntegralsRepositor
     throw std::runtime_error(std::string("hfg_spin_orbital_eri: ") + hfg_last_error());
 }
 
+void IntegralsRepository::Moments(hfgpu::Matrix &Mx, hfgpu::Matrix &My, hfgpu::Matrix &Mz) const {
+  const auto &t = molecule_->shellTable();
+  const int n = t.nbf;
+  Mx.resize(n, n);
+  My.resize(n, n);
+  Mz.resize(n, n);
+  const hfg_shells sh = t.view();
+  if (hfg_moments(&sh, options.device, Mx.data(), My.data(), Mz.data()) != HFG_OK)
+    throw std::runtime_error(std::string("hfg_moments: ") + hfg_last_error());
+}
+
 }  // namespace GaussianIntegrals
 
 // ===========================================================================
@@ -546,8 +564,14 @@ void HartreeFockAlgorithm::Init(Systems::Molecule *molecule) {
   integralsRepository.Reset(molecule);
   Matrix T, Vn;
   integralsRepository.OneElectron(overlap, T, Vn);
+  integralsRepository.Moments(momentX, momentY, momentZ);
+  // h = T + V + E . moments (HartreeFockAlgorithm.cpp:38)
   h = T + Vn;
+  const hfgpu::Vector3D &E = molecule->ElectricField;
+  if (E.X != 0 || E.Y != 0 || E.Z != 0) h = h + E.X * momentX + E.Y * momentY + E.Z * momentZ;
+  molecule_ = molecule;
   nuclearRepulsionEnergy = molecule->NuclearRepulsionEnergy();
+  nuclearElectricFieldEnergy = molecule->NuclearElectricFieldEnergy();
   numberOfOrbitals = (int)molecule->shellTable().nbf;
   // the reference always stores the 8-fold table at Init
   // (HartreeFockAlgorithm.cpp:45); it is kept here when it fits the budget
@@ -569,6 +593,33 @@ void HartreeFockAlgorithm::Init(Systems::Molecule *molecule) {
   inited = true;
   secondsInit = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_init).count();
 }
+
+hfgpu::Vector3D HartreeFockAlgorithm::GetNuclearMoment() const {
+  hfgpu::Vector3D m;
+  if (!molecule_) return m;
+  for (const auto &a : molecule_->atoms) {
+    m.X += double(a.Z) * a.position.X;
+    m.Y += double(a.Z) * a.position.Y;
+    m.Z += double(a.Z) * a.position.Z;
+  }
+  return m;
+}
+
+namespace {
+hfgpu::Vector3D electronic_moment(hfgpu::Vector3D m, const Matrix &P, const Matrix *P2, const Matrix &Mx,
+                                  const Matrix &My, const Matrix &Mz) {
+  const int n = P.rows();
+  if (Mx.rows() != n) return m;
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      const double d = P(i, j) + (P2 ? (*P2)(i, j) : 0.0);
+      m.X -= d * Mx(i, j);
+      m.Y -= d * My(i, j);
+      m.Z -= d * Mz(i, j);
+    }
+  return m;
+}
+}  // namespace
 
 double HartreeFockAlgorithm::Calculate() {
   double curEnergy = 0, prevEnergy = std::numeric_limits<double>::infinity();
@@ -915,12 +966,20 @@ double RestrictedHartreeFock::Step(int iter) {
   return std::sqrt(change2);
 }
 
+hfgpu::Vector3D RestrictedHartreeFock::GetMoment() const {
+  return electronic_moment(GetNuclearMoment(), DensityMatrix, nullptr, momentX, momentY, momentZ);
+}
+
 double RestrictedHartreeFock::CalculateMp2Energy() {
   const int n = numberOfOrbitals;
   if (!inited || (int)C.rows() != n || (int)eigenvals.size() != n || nrOccupiedLevels >= (unsigned)n) return mp2Energy = 0;
   check_engine(hfg_mp2_rhf(integralsRepository.engine(), C.data(), eigenvals.data(), (int32_t)nrOccupiedLevels, &mp2Energy),
                "hfg_mp2_rhf");
   return mp2Energy;
+}
+
+hfgpu::Vector3D UnrestrictedHartreeFock::GetMoment() const {
+  return electronic_moment(GetNuclearMoment(), DensityMatrixPlus, &DensityMatrixMinus, momentX, momentY, momentZ);
 }
 
 double UnrestrictedHartreeFock::CalculateMp2Energy() {
@@ -1069,6 +1128,7 @@ hfg_status run_scf(const char *basis_path, int32_t natoms, const int32_t *Z, con
     Systems::Molecule mol = build_molecule(basis_path, natoms, Z, xyz);
     mol.alphaElectrons = (unsigned)opts->alpha_electrons;
     mol.betaElectrons = (unsigned)opts->beta_electrons;
+    mol.ElectricField = {opts->electric_field[0], opts->electric_field[1], opts->electric_field[2]};
     mol.Init();
     std::unique_ptr<HartreeFock::HartreeFockAlgorithm> algo;
     const int iters = opts->max_iterations > 0 ? opts->max_iterations : 3000;
@@ -1120,6 +1180,10 @@ hfg_status run_scf(const char *basis_path, int32_t natoms, const int32_t *Z, con
     result->seconds_diis = algo->secondsDiis;
     result->seconds_total = algo->secondsTotal;
     result->seconds_init = algo->secondsInit;
+    const hfgpu::Vector3D mu = algo->GetMoment();
+    result->dipole[0] = mu.X;
+    result->dipole[1] = mu.Y;
+    result->dipole[2] = mu.Z;
     if (opts->mp2 && !opts->unrestricted)
       result->mp2_energy = static_cast<HartreeFock::RestrictedHartreeFock *>(algo.get())->CalculateMp2Energy();
     else if (opts->mp2)

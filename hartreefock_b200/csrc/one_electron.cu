@@ -168,6 +168,86 @@ __global__ void __launch_bounds__(32 * kOneWarps) one_electron_kernel(const OneS
   }
 }
 
+// Dipole moment integrals about the origin (MomentMatrix::Calculate,
+// QuantumMatrix.cpp:61-98, through GaussianMoment::CalculateMoment,
+// GaussianMoment.cpp:44-90): per axis d, m(i,j) = s(i+1,j) + A_d s(i,j), so
+// that M_d = m_d(a_d, b_d) s(a_e, b_e) s(a_f, b_f) over the other two axes.
+// One warp per shell pair, lanes over primitive pairs, warp sums.
+template <int LA, int LB>
+__global__ void __launch_bounds__(32 * kOneWarps) moment_kernel(const OneShell *__restrict__ shells,
+                                                                 const int2 *__restrict__ pairs, int npairs,
+                                                                 const double *__restrict__ expo,
+                                                                 const double *__restrict__ coef, int n, double *Mx,
+                                                                 double *My, double *Mz) {
+  constexpr int NA = ncart(LA), NB = ncart(LB);
+  const int lane = threadIdx.x & 31;
+  for (int w = blockIdx.x * kOneWarps + (threadIdx.x >> 5); w < npairs; w += gridDim.x * kOneWarps) {
+    const OneShell A = shells[pairs[w].x], B = shells[pairs[w].y];
+    const double AB0 = A.c[0] - B.c[0], AB1 = A.c[1] - B.c[1], AB2 = A.c[2] - B.c[2];
+    const double ab2 = AB0 * AB0 + AB1 * AB1 + AB2 * AB2;
+    double acc[3][NA * NB];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int x = 0; x < NA * NB; ++x) acc[d][x] = 0.0;
+    const int npp = A.nprim * B.nprim;
+    for (int q = lane; q < npp; q += 32) {
+      const int i = q / B.nprim, j = q - i * B.nprim;
+      const double a = expo[A.prim_off + i], b = expo[B.prim_off + j], p = a + b, ip = 1.0 / p;
+      const double K = exp(-a * b * ip * ab2);
+      const double cc = coef[A.prim_off + i] * pow(2.0 * a / M_PI, 0.75) * pow(4.0 * a, 0.5 * LA) *
+                        coef[B.prim_off + j] * pow(2.0 * b / M_PI, 0.75) * pow(4.0 * b, 0.5 * LB) * K;
+      double s[3][LA + 2][LB + 1], m[3][LA + 1][LB + 1];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double P = (a * A.c[d] + b * B.c[d]) * ip;
+        const double PA = P - A.c[d], PB = P - B.c[d];
+        s[d][0][0] = sqrt(M_PI * ip);
+#pragma unroll
+        for (int x = 0; x < LA + 1; ++x) s[d][x + 1][0] = PA * s[d][x][0] + (x > 0 ? x * s[d][x - 1][0] : 0.0) * 0.5 * ip;
+#pragma unroll
+        for (int y = 0; y < LB; ++y)
+#pragma unroll
+          for (int x = 0; x <= LA + 1; ++x)
+            s[d][x][y + 1] = PB * s[d][x][y] +
+                             ((x > 0 ? x * s[d][x - 1][y] : 0.0) + (y > 0 ? y * s[d][x][y - 1] : 0.0)) * 0.5 * ip;
+#pragma unroll
+        for (int x = 0; x <= LA; ++x)
+#pragma unroll
+          for (int y = 0; y <= LB; ++y) m[d][x][y] = s[d][x + 1][y] + A.c[d] * s[d][x][y];
+      }
+#pragma unroll
+      for (int ca = 0; ca < NA; ++ca)
+#pragma unroll
+        for (int cb = 0; cb < NB; ++cb) {
+          const int x0 = cart_exp(LA, ca, 0), y0 = cart_exp(LB, cb, 0);
+          const int x1 = cart_exp(LA, ca, 1), y1 = cart_exp(LB, cb, 1);
+          const int x2 = cart_exp(LA, ca, 2), y2 = cart_exp(LB, cb, 2);
+          const double s0 = s[0][x0][y0], s1 = s[1][x1][y1], s2 = s[2][x2][y2];
+          acc[0][ca * NB + cb] += cc * m[0][x0][y0] * s1 * s2;
+          acc[1][ca * NB + cb] += cc * s0 * m[1][x1][y1] * s2;
+          acc[2][ca * NB + cb] += cc * s0 * s1 * m[2][x2][y2];
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int x = 0; x < NA * NB; ++x) acc[d][x] = warp_sum(acc[d][x]);
+    if (lane == 0) {
+      double *M[3] = {Mx, My, Mz};
+#pragma unroll
+      for (int ca = 0; ca < NA; ++ca)
+#pragma unroll
+        for (int cb = 0; cb < NB; ++cb) {
+          const double nn = comp_norm<LA>(ca) * comp_norm<LB>(cb);
+          const long long r = A.ao + ca, c = B.ao + cb;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) M[d][r * n + c] = M[d][c * n + r] = nn * acc[d][ca * NB + cb];
+        }
+    }
+  }
+}
+
 template <int LA, int LB>
 void launch_one(const OneShell *shells, const int2 *pairs, int npairs, const double *expo, const double *coef,
                 const double *nuc, int natoms, const double *boys, int n, double *S, double *T, double *V,
@@ -197,11 +277,33 @@ struct DeviceArray {
 }  // namespace
 }  // namespace hfg
 
+namespace hfg {
+namespace {
+// S, T, V (nuclei given) and / or the dipole moment matrices (Mx given)
+hfg_status one_electron_all(const hfg_shells *sh, const double *nuc_xyz, const int32_t *nuc_Z, int32_t natoms,
+                            int32_t device, double *S, double *T, double *V, double *Mx, double *My, double *Mz);
+}  // namespace
+}  // namespace hfg
+
 extern "C" hfg_status hfg_one_electron(const hfg_shells *sh, const double *nuc_xyz, const int32_t *nuc_Z,
                                        int32_t natoms, int32_t device, double *S, double *T, double *V) {
   using namespace hfg;
   if (!sh || sh->nshells < 1 || sh->nbf < 1 || !nuc_xyz || !nuc_Z || natoms < 1 || !S || !T || !V)
     return fail_external(HFG_INVALID_ARG, "hfg_one_electron: arguments");
+  return one_electron_all(sh, nuc_xyz, nuc_Z, natoms, device, S, T, V, nullptr, nullptr, nullptr);
+}
+
+extern "C" hfg_status hfg_moments(const hfg_shells *sh, int32_t device, double *Mx, double *My, double *Mz) {
+  using namespace hfg;
+  if (!sh || sh->nshells < 1 || sh->nbf < 1 || !Mx || !My || !Mz)
+    return fail_external(HFG_INVALID_ARG, "hfg_moments: arguments");
+  return one_electron_all(sh, nullptr, nullptr, 0, device, nullptr, nullptr, nullptr, Mx, My, Mz);
+}
+
+namespace hfg {
+namespace {
+hfg_status one_electron_all(const hfg_shells *sh, const double *nuc_xyz, const int32_t *nuc_Z, int32_t natoms,
+                            int32_t device, double *S, double *T, double *V, double *Mx, double *My, double *Mz) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail_external(HFG_NO_DEVICE, "no CUDA device");
   if (device < 0 || device >= ndev) return fail_external(HFG_INVALID_ARG, "device out of range");
@@ -233,7 +335,7 @@ extern "C" hfg_status hfg_one_electron(const hfg_shells *sh, const double *nuc_x
       cnt[la][lb] = (int)lists[la][lb].size();
       all.insert(all.end(), lists[la][lb].begin(), lists[la][lb].end());
     }
-  std::vector<double> nuc(4 * (size_t)natoms);
+  std::vector<double> nuc(4 * (size_t)std::max(natoms, 1));
   for (int c = 0; c < natoms; ++c) {
     for (int d = 0; d < 3; ++d) nuc[4 * c + d] = nuc_xyz[3 * c + d];
     nuc[4 * c + 3] = (double)nuc_Z[c];
@@ -260,25 +362,49 @@ extern "C" hfg_status hfg_one_electron(const hfg_shells *sh, const double *nuc_x
   if (e == cudaSuccess) e = d_nuc.upload(nuc);
   if (e == cudaSuccess) e = d_boys.upload(boys_table_for_external());
   const size_t nn = (size_t)n * n;
-  if (e == cudaSuccess) e = cudaMalloc(&d_out.p, 3 * nn * sizeof(double));
-  if (e == cudaSuccess) e = cudaMemsetAsync(d_out.p, 0, 3 * nn * sizeof(double), os.s);
+  if (e == cudaSuccess) e = cudaMalloc(&d_out.p, 6 * nn * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_out.p, 0, 6 * nn * sizeof(double), os.s);
   if (e != cudaSuccess) return fail_external(HFG_OOM_BUDGET, std::string("hfg_one_electron: ") + cudaGetErrorString(e));
-  double *dS = d_out.p, *dT = dS + nn, *dV = dT + nn;
+  double *dS = d_out.p, *dT = dS + nn, *dV = dT + nn, *dMx = dV + nn, *dMy = dMx + nn, *dMz = dMy + nn;
+  if (S) {
 #define HFG_ONE(LA, LB)                                                                                              \
   launch_one<LA, LB>(d_sh.p, d_pairs.p + off[LA][LB], cnt[LA][LB], d_exp.p, d_coef.p, d_nuc.p, natoms, d_boys.p, n, \
                      dS, dT, dV, num_sms, os.s)
-  HFG_ONE(0, 0);
-  HFG_ONE(1, 0);
-  HFG_ONE(1, 1);
-  HFG_ONE(2, 0);
-  HFG_ONE(2, 1);
-  HFG_ONE(2, 2);
+    HFG_ONE(0, 0);
+    HFG_ONE(1, 0);
+    HFG_ONE(1, 1);
+    HFG_ONE(2, 0);
+    HFG_ONE(2, 1);
+    HFG_ONE(2, 2);
 #undef HFG_ONE
+  }
+  if (Mx) {
+#define HFG_MOM(LA, LB)                                                                                           \
+  if (cnt[LA][LB])                                                                                                \
+    moment_kernel<LA, LB><<<std::min((cnt[LA][LB] + kOneWarps - 1) / kOneWarps, num_sms * 4), 32 * kOneWarps, 0, \
+                            os.s>>>(d_sh.p, d_pairs.p + off[LA][LB], cnt[LA][LB], d_exp.p, d_coef.p, n, dMx, dMy, dMz)
+    HFG_MOM(0, 0);
+    HFG_MOM(1, 0);
+    HFG_MOM(1, 1);
+    HFG_MOM(2, 0);
+    HFG_MOM(2, 1);
+    HFG_MOM(2, 2);
+#undef HFG_MOM
+  }
   e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpyAsync(S, dS, nn * sizeof(double), cudaMemcpyDeviceToHost, os.s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(T, dT, nn * sizeof(double), cudaMemcpyDeviceToHost, os.s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(V, dV, nn * sizeof(double), cudaMemcpyDeviceToHost, os.s);
+  if (S) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(S, dS, nn * sizeof(double), cudaMemcpyDeviceToHost, os.s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(T, dT, nn * sizeof(double), cudaMemcpyDeviceToHost, os.s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(V, dV, nn * sizeof(double), cudaMemcpyDeviceToHost, os.s);
+  }
+  if (Mx) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(Mx, dMx, nn * sizeof(double), cudaMemcpyDeviceToHost, os.s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(My, dMy, nn * sizeof(double), cudaMemcpyDeviceToHost, os.s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(Mz, dMz, nn * sizeof(double), cudaMemcpyDeviceToHost, os.s);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(os.s);
   if (e != cudaSuccess) return fail_external(HFG_DEVICE_ERROR, std::string("hfg_one_electron: ") + cudaGetErrorString(e));
   return HFG_OK;
 }
+}  // namespace
+}  // namespace hfg

@@ -24,7 +24,8 @@ class hfd_scf_opts(ctypes.Structure):
                 ("fp64_final_iterations", ctypes.c_int32), ("fp64_final_converge", ctypes.c_int32),
                 ("incremental", ctypes.c_int32), ("trace", ctypes.c_int32),
                 ("stop_at_precision_test", ctypes.c_int32), ("max_iterations", ctypes.c_int32),
-                ("mp2", ctypes.c_int32), ("concurrent_classes", ctypes.c_int32)]
+                ("mp2", ctypes.c_int32), ("concurrent_classes", ctypes.c_int32),
+                ("electric_field", ctypes.c_double * 3)]
 
 
 class hfd_scf_result(ctypes.Structure):
@@ -34,7 +35,7 @@ class hfd_scf_result(ctypes.Structure):
                 ("fp64_quartets", ctypes.c_int64), ("mixed_steps", ctypes.c_int32), ("reserved", ctypes.c_int32),
                 ("seconds_fock", ctypes.c_double), ("seconds_eigen", ctypes.c_double),
                 ("seconds_diis", ctypes.c_double), ("seconds_total", ctypes.c_double),
-                ("seconds_init", ctypes.c_double), ("mp2_energy", ctypes.c_double)]
+                ("seconds_init", ctypes.c_double), ("mp2_energy", ctypes.c_double), ("dipole", ctypes.c_double * 3)]
 
 
 DRIVER_SYMBOLS = ["hfd_default_scf_opts", "hfd_last_error", "hfd_scf", "hfd_one_electron", "hfd_pulay_solve",
@@ -70,7 +71,8 @@ def scf_opts(unrestricted=False, alpha=0.75, init_guess=0.75, use_diis=True, pos
              alpha_electrons=0, beta_electrons=0, eri_convention=E.ERI_REFERENCE, schwarz_threshold=1e-12,
              mixed_cutoff=0.0, mixed_switch_energy=1e-7, mixed_switch_density=1e-7, mixed_switch_diis=1e-6,
              fp64_final_iterations=2, fp64_final_converge=False, incremental=False, trace=False,
-             stop_at_precision_test=False, max_iterations=0, mp2=False, concurrent_classes=False) -> hfd_scf_opts:
+             stop_at_precision_test=False, max_iterations=0, mp2=False, concurrent_classes=False,
+             electric_field=(0.0, 0.0, 0.0)) -> hfd_scf_opts:
     """hfd_scf_opts from keywords (the defaults of hfd_default_scf_opts where
     not given)."""
     L = _lib()
@@ -89,6 +91,8 @@ def scf_opts(unrestricted=False, alpha=0.75, init_guess=0.75, use_diis=True, pos
     o.max_iterations = int(max_iterations)
     o.mp2 = int(mp2)
     o.concurrent_classes = int(concurrent_classes)  # 0, 1 streams, 2 streams + graphs
+    for d in range(3):
+        o.electric_field[d] = float(electric_field[d])
     return o
 
 
@@ -97,7 +101,8 @@ def result_dict(r: hfd_scf_result) -> dict:
             "nbf": r.nbf, "fock_builds": r.fock_builds, "fock_ms_total": r.fock_ms_total,
             "fp32_quartets": r.fp32_quartets, "fp64_quartets": r.fp64_quartets, "mixed_steps": r.mixed_steps,
             "seconds_fock": r.seconds_fock, "seconds_eigen": r.seconds_eigen, "seconds_diis": r.seconds_diis,
-            "seconds_total": r.seconds_total, "seconds_init": r.seconds_init, "mp2_energy": r.mp2_energy}
+            "seconds_total": r.seconds_total, "seconds_init": r.seconds_init, "mp2_energy": r.mp2_energy,
+            "dipole": [r.dipole[0], r.dipole[1], r.dipole[2]]}
 
 
 def run_scf(Z, xyz, basis: str, unrestricted=False, want_density=True, **kw):

@@ -202,6 +202,11 @@ hfg_status hfg_fock_uhf_batch_device(hfg_ctx *ctx, const double *dPa, const doub
 hfg_status hfg_one_electron(const hfg_shells *shells, const double *xyz, const int32_t *Z, int32_t natoms,
                             int32_t device, double *S, double *T, double *V);
 
+/* Dipole moment matrices about the origin, <a|x|b>, <a|y|b>, <a|z|b>
+ * (row-major nbf x nbf): MomentMatrix::Calculate (QuantumMatrix.cpp:61-98)
+ * through GaussianMoment (GaussianMoment.cpp:44-90), on the device. */
+hfg_status hfg_moments(const hfg_shells *shells, int32_t device, double *Mx, double *My, double *Mz);
+
 /* AO -> MO transform for the post-HF consumers (no allocation-free form):
  * dX receives the (ia|jb) block, i in [i0, i0+ni), a in [a0, a0+na), as a
  * row-major (ni*na) x (ni*na) matrix with row i*na + a, from the MO

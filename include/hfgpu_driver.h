@@ -42,6 +42,7 @@ typedef struct {
                                 (HartreeFockAlgorithm::concurrentClasses); 2: also CUDA-graph
                                 replay of plain builds (cudaGraphs), for one host thread
                                 driving the device; 0: neither */
+  double electric_field[3];  /* Molecule::ElectricField: h += E . dipole moments (HartreeFockAlgorithm.cpp:38) */
 } hfd_scf_opts;
 
 typedef struct {
@@ -60,6 +61,7 @@ typedef struct {
   double seconds_fock, seconds_eigen, seconds_diis, seconds_total;
   double seconds_init;       /* Init: one-electron matrices, engine context, S^-1/2 */
   double mp2_energy;         /* Restricted/UnrestrictedHartreeFock::CalculateMp2Energy when opts.mp2 */
+  double dipole[3];          /* GetMoment(): nuclear minus electronic dipole about the origin (au) */
 } hfd_scf_result;
 
 void hfd_default_scf_opts(hfd_scf_opts *o);

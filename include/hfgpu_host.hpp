@@ -110,12 +110,14 @@ class Molecule {
   std::vector<AtomWithShells> atoms;
   unsigned int alphaElectrons = 0;
   unsigned int betaElectrons = 0;
+  hfgpu::Vector3D ElectricField;  // Molecule.h:19; enters h as E . moments
 
   void Init();  // Molecule.cpp:127-140 (occupations)
   unsigned int CountNumberOfContractedGaussians() const;
   unsigned int ElectronsNumber() const;
   unsigned int GetMaxAngularMomentum() const;
   double NuclearRepulsionEnergy() const;
+  double NuclearElectricFieldEnergy() const;  // Molecule.cpp:86-95
   // Molecule::LoadXYZ (Molecule.cpp:143-199): count line, comment line,
   // then "<symbol> x y z" per atom (coordinates used as given, bohr)
   bool LoadXYZ(const std::string &fileName, const Chemistry::Basis &basis);
@@ -173,6 +175,8 @@ class IntegralsRepository {
   // One-electron matrices (QuantumMatrix.cpp:34-155): overlap, kinetic,
   // nuclear attraction; row-major nbf x nbf.
   void OneElectron(hfgpu::Matrix &S, hfgpu::Matrix &T, hfgpu::Matrix &V) const;
+  // Dipole moment matrices about the origin (MomentMatrix, QuantumMatrix.cpp:61-98)
+  void Moments(hfgpu::Matrix &Mx, hfgpu::Matrix &My, hfgpu::Matrix &Mz) const;
 
   hfg_ctx *engine();
   hfg_opts options;  // engine options, used at the next Reset/first use
@@ -286,7 +290,15 @@ class HartreeFockAlgorithm {
   double Calculate();
   virtual double Step(int iter) = 0;
   double GetTotalEnergy() const { return totalEnergy; }
+  double GetNuclearElectricFieldEnergy() const { return nuclearElectricFieldEnergy; }
   double GetMP2Energy() const { return mp2Energy; }  // HartreeFockAlgorithm.h:89-92
+  // sum_A Z_A R_A (HartreeFockAlgorithm.cpp:234-242)
+  hfgpu::Vector3D GetNuclearMoment() const;
+  // nuclear moment - sum_ij P_ij <i|r|j> (RestrictedHartreeFock.cpp:319-335,
+  // UnrestrictedHartreeFock.cpp:408-424)
+  virtual hfgpu::Vector3D GetMoment() const = 0;
+  // MomentMatrix: matrix, matrixY, matrixZ (HartreeFockAlgorithm.h)
+  hfgpu::Matrix momentX, momentY, momentZ;
   // device execution of the Fock builds (no reference counterpart): CUDA-graph
   // replay of plain builds (for one host thread driving the device: a capture
   // does not mix with other threads' device-wide synchronisation), and a
@@ -298,6 +310,8 @@ class HartreeFockAlgorithm {
  protected:
   double totalEnergy;
   double nuclearRepulsionEnergy = 0;
+  double nuclearElectricFieldEnergy = 0;
+  Systems::Molecule *molecule_ = nullptr;
   hfgpu::Matrix overlap;  // overlapMatrix.matrix
   hfgpu::Matrix V, Vt;    // S^-1/2
   int maxIterations;
@@ -344,6 +358,7 @@ class RestrictedHartreeFock : public HartreeFockAlgorithm {
   // RestrictedHartreeFock.cpp:251-288, after Calculate(): the (ia|jb)
   // block by one device AO->MO transform (hfg_mp2_rhf)
   double CalculateMp2Energy();
+  hfgpu::Vector3D GetMoment() const override;
 
  protected:
   void SyncToDevice() override;
@@ -367,6 +382,7 @@ class UnrestrictedHartreeFock : public HartreeFockAlgorithm {
   double Step(int iter) override;
   // UnrestrictedHartreeFock.cpp:295-375, on the device (hfg_mp2_uhf)
   double CalculateMp2Energy();
+  hfgpu::Vector3D GetMoment() const override;
 
  protected:
   void SyncToDevice() override;

@@ -11,6 +11,7 @@
 //                                atom with that Z, as Molecule::LoadXYZ does
 //                                (Molecule.cpp:143-199)
 //   electrons <alpha> <beta>     optional explicit occupations
+//   field <Ex> <Ey> <Ez>         Molecule::ElectricField (enters h, HartreeFockAlgorithm.cpp:38)
 //   alpha <a> | initguess <g> | diis <0|1> | postdiis <n>   algorithm fields
 //   xyz <file>                   Molecule::LoadXYZ(file, basis) instead of atom lines
 //                                (Molecule.cpp:143-199); mode xyz prints the result
@@ -107,6 +108,7 @@ int main() {
   int mp2 = 0;
   int spinorb = 0;
   unsigned alphaEl = 0, betaEl = 0;
+  double field[3] = {0, 0, 0};
   struct AtomSpec { unsigned Z; double x, y, z; };
   std::vector<AtomSpec> specs;
 
@@ -118,6 +120,7 @@ int main() {
     if (key == "basis") ls >> basisFile;
     else if (key == "atom") { AtomSpec a{}; ls >> a.Z >> a.x >> a.y >> a.z; specs.push_back(a); }
     else if (key == "electrons") ls >> alphaEl >> betaEl;
+    else if (key == "field") ls >> field[0] >> field[1] >> field[2];
     else if (key == "alpha") ls >> alpha;
     else if (key == "initguess") ls >> initGuess;
     else if (key == "diis") ls >> useDiis;
@@ -162,6 +165,7 @@ int main() {
   }
   molecule.alphaElectrons = alphaEl;
   molecule.betaElectrons = betaEl;
+  molecule.ElectricField = Vector3D<double>(field[0], field[1], field[2]);
   molecule.Init();
 
   if (mode == "eri") {
@@ -214,6 +218,10 @@ int main() {
     w.put("init_seconds", std::chrono::duration<double>(t1 - t0).count());
     w.put("scf_seconds", std::chrono::duration<double>(t2 - t1).count());
     w.put("iterations", static_cast<double>(crhf ? crhf->steps : cuhf->steps));
+    {
+      const Vector3D<double> mu = algo->GetMoment();
+      w.put("dipole", std::vector<double>{mu.X, mu.Y, mu.Z});
+    }
     if (mp2) w.put("mp2", algo->CalculateMp2Energy());
     if (spinorb && crhf) {
       const int n = crhf->numberOfOrbitals;

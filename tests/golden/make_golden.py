@@ -44,7 +44,37 @@ def fixtures():
     }
 
 
+# Test::InitWaterMolecule (Test.cpp:572-608): O, H1, H2 in bohr
+CRAWFORD_WATER = ([8, 1, 1], np.array([[0.0, -0.143225816552, 0.0], [1.638036840407, 1.136548822547, 0.0],
+                                       [-1.638036840407, 1.136548822547, 0.0]]))
+
+
+def dipole_fixture(td):
+    """Test::TestWaterDipoleMoment (Test.cpp:627-733): the Crawford water in
+    STO-3G, RHF without DIIS, alpha 0.5, initGuess 0.7; the analytic dipole
+    (GetMoment) and the SCF energies in fields of +-0.001 au along each axis."""
+    Z, xyz = CRAWFORD_WATER
+    mol = O.Molecule(Z, xyz, os.path.join(REF_DIR, "sto3g.txt"))
+    kw = dict(alpha=0.5, init_guess=0.7, use_diis=False)
+    r = O.run_reference(mol, "rhf", os.path.join(td, "d.bin"), **kw)
+    out = {"Z": np.array(Z), "xyz": xyz, "basis": np.array("sto-3g"), "alpha": np.array(0.5),
+           "initguess": np.array(0.7), "use_diis": np.array(0), "rhf_energy": r["energy"], "dipole": r["dipole"],
+           "enuc_test": np.array(8.002367061810450)}
+    fields = []
+    for axis in range(3):
+        for sign in (-1, 1):
+            f = [0.0, 0.0, 0.0]
+            f[axis] = sign * 1e-3
+            rf = O.run_reference(mol, "rhf", os.path.join(td, "f.bin"), extra="field %.17g %.17g %.17g" % tuple(f), **kw)
+            fields.append(f + [float(rf["energy"][0])])
+    out["field_energies"] = np.array(fields)  # rows: Ex, Ey, Ez, E
+    np.savez_compressed(os.path.join(HERE, "h2o_crawford_sto3g.npz"), **out)
+    print("h2o_crawford_sto3g", r["dipole"], np.linalg.norm(r["dipole"]))
+
+
 def main():
+    with tempfile.TemporaryDirectory() as td:
+        dipole_fixture(td)
     for name, fx in fixtures().items():
         out = {"Z": np.array(fx["Z"]), "xyz": np.asarray(fx["xyz"]), "basis": np.array(fx["basis"])}
         mol = O.Molecule(fx["Z"], fx["xyz"], os.path.join(REF_DIR, fx["ref_basis"]))
