@@ -64,6 +64,11 @@ def workload():
     return Z, xyz
 
 
+# the large classes with a split path (primitive kernel, then HRR/digest)
+SPLIT_CLASSES = {(2, 1, 1, 1), (2, 1, 2, 0), (2, 1, 2, 1), (2, 2, 1, 0), (2, 2, 1, 1), (2, 2, 2, 0), (2, 2, 2, 1),
+                 (2, 2, 2, 2)}
+
+
 def synthetic_density(n, seed=1):
     """A symmetric density of realistic magnitude: 2 C C^T of random
     orthonormal occupied vectors."""
@@ -301,7 +306,7 @@ def batching(count: int, check: int = 8):
         if not mols:
             continue
         t0 = time.perf_counter()
-        bs = batch.BatchSCF(mols, unrestricted=un, max_iter=1000, **kw)
+        bs = batch.BatchSCF(mols, unrestricted=un, max_iter=1000, graphs=True, **kw)
         torch.cuda.synchronize()
         t1 = time.perf_counter()
         e = bs.run()
@@ -316,7 +321,8 @@ def batching(count: int, check: int = 8):
         out["runs"][name] = {"molecules": len(mols), "setup_s": t1 - t0, "scf_s": t2 - t1,
                              "seconds": {k: round(v, 4) for k, v in bs.seconds.items()}, "fock_launch_rounds": bs.builds,
                              "max_iterations": int(bs.iterations.max()), "converged": int(bs.converged.sum()),
-                             "nbf_max": bs.nmax, "max_abs_dE_vs_single_fp64": max(errs) if errs else None}
+                             "nbf_max": bs.nmax, "max_abs_dE_vs_single_fp64": max(errs) if errs else None,
+                             "cuda_graph_captures": bs.graph_captures}
     out["molecules_per_s"] = count / total_wall if total_wall else None
     return out
 
@@ -458,6 +464,13 @@ def main():
     G_full = dG.clone()
     # the classes of every build over concurrent streams, then the grid from
     # the autotuner (timed on this density, before warm-up)
+    # task shapes (lanes per quartet for long contractions) from the task
+    # autotuner, then the classes of every build over concurrent streams
+    # and the grid from the grid autotuner (both timed on this density,
+    # before warm-up)
+    tasks = eng.autotune_tasks(dP) if not args.no_autotune else {}
+    # the large classes' kernel (warp-cooperative or split), timed both ways
+    paths = eng.autotune_paths(dP) if not args.no_autotune else {}
     eng.set_streams(not args.no_streams)
     grids = eng.autotune(dP) if not args.no_autotune else {}
     # N > 1: every rank builds its shard of each class's tasks, one NCCL
@@ -553,6 +566,8 @@ def main():
                    "function_quartets": stats_full["function_quartets"],
                    "l2": "flushed (256 MB write) between steps",
                    "grid_blocks_per_sm": grids or ("fixed 4" if args.no_streams else "fixed 1"),
+                   "large_class_kernels": paths or "default: warp for (22|22), split for the rest",
+                   "prim_quartets_per_lane_target": tasks or "fixed 96",
                    "class_streams": 1 if args.no_streams else 13,
                    "parallelism": f"task shards x{world}, one NCCL all-reduce of G per build" if world > 1
                    else "single GPU"},
@@ -568,7 +583,9 @@ def main():
         "classes": [{"class": f"({c['la']}{c['lb']}|{c['lc']}{c['ld']})", "ms": round(c["ms"], 4),
                      "tflops": round(c["flops"] / max(c["ms"], 1e-9) / 1e9, 3), "tasks": c["tasks"],
                      "lane_occupancy": round(c["lane_occupancy"], 3),
-                     "kernel": "warp per quartet" if c["warp_kernel"] else "thread per quartet"} for c in prof],
+                     "kernel": "warp per quartet" if c["warp_kernel"] else
+                     "split: thread per quartet, then HRR/digest" if (c["la"], c["lb"], c["lc"], c["ld"]) in SPLIT_CLASSES
+                     else "thread per quartet"} for c in prof],
         "clocks": clocks.summary(),
     }
     eng.close()

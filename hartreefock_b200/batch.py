@@ -34,10 +34,19 @@ class BatchSCF:
     it was a wash: 20.2 vs 21.7 molecules/s)."""
 
     def __init__(self, molecules, unrestricted=False, alpha=0.75, init_guess=0.75, max_iter=300,
-                 use_diis=True, schwarz_threshold=1e-12, device="cuda", concurrent_classes=False):
+                 use_diis=True, schwarz_threshold=1e-12, device="cuda", concurrent_classes=False, graphs=False,
+                 replay=8):
         self.mols = list(molecules)
         self.uhf = unrestricted
         self.alpha, self.init_guess, self.max_iter, self.use_diis = alpha, init_guess, max_iter, use_diis
+        # graphs: every SCF iteration after the DIIS history has filled is
+        # captured once per working set as a CUDA graph (asynchronous batched
+        # build on the device work queue, device DIIS solve, eigensolves,
+        # density, energy, mixing and the convergence test, all on the
+        # device) and replayed `replay` times between host checks of the
+        # active count; converged molecules are frozen by the device mask
+        self.graphs, self.replay = graphs, max(1, int(replay))
+        self.graph_captures = 0
         self.dev = torch.device(device)
         self.eng = E.BatchEngine([(m["Z"], m["xyz"], m["basis"]) for m in self.mols],
                                  schwarz_threshold=schwarz_threshold)
@@ -128,6 +137,14 @@ class BatchSCF:
         return w, U
 
     def run(self):
+        if self.graphs and self.dev.type == "cuda":
+            return self._run_graphs()
+        return self._run_eager()
+
+    def _run_eager(self, keep_state=False):
+        """The host-driven loop.  keep_state: no working-set compaction, and
+        the device state at the end (densities, DIIS history, previous
+        energies, the active mask) is returned for the captured loop."""
         M, dev = self.M, self.dev
         nspin = 2 if self.uhf else 1
         # working set W (molecule ids) padded to n; it shrinks to the
@@ -240,7 +257,7 @@ class BatchSCF:
             n_active = int(active.sum())
             if n_active == 0:
                 break
-            if n_active <= len(W) // 2:  # compact the working set
+            if n_active <= len(W) // 2 and not keep_state:  # compact the working set
                 for s in range(nspin):
                     P_out[s][Wt, :n, :n] = P[s]
                 keep = active.cpu().numpy().astype(bool)
@@ -265,7 +282,202 @@ class BatchSCF:
         self.builds = builds
         self.energies = energy.cpu().numpy()
         self.densities = P_out
+        if keep_state:
+            # six history slots, oldest first; missing ones are zero
+            # placeholders that the next append pushes out
+            hist = ([[torch.zeros_like(P[0]) for _ in range(6 - len(diisF[s]))] + list(diisF[s]) for s in range(nspin)],
+                    [[torch.zeros_like(P[0]) for _ in range(6 - len(diisE[s]))] + list(diisE[s]) for s in range(nspin)])
+            return {"P": P, "hist": hist, "prev": prev, "active": active.cpu().numpy().astype(bool),
+                    "iterations": it + 1}
         return self.energies
+
+    def _run_graphs(self):
+        """The captured loop: iterations 0-5 (the DIIS history fills) run in
+        the host-driven loop, then one iteration per working set is captured
+        and replayed; the working set shrinks to the molecules still
+        iterating (and is captured again) once half of it has converged."""
+        M, dev = self.M, self.dev
+        nspin = 2 if self.uhf else 1
+        t_start = time.perf_counter()
+        keep_hist = 6  # DIIS.h:9
+        econv = E_CONV_DIIS if self.use_diis else E_CONV
+        enuc_all = torch.from_numpy(self.enuc).to(dev)
+        nocc_all = [torch.from_numpy(self.nocc[s]).to(dev) for s in range(nspin)]
+        P_out = [torch.zeros(M, self.nmax, self.nmax, dtype=torch.float64, device=dev) for _ in range(nspin)]
+
+        eager = BatchSCF.__new__(BatchSCF)
+        eager.__dict__.update(self.__dict__)
+        eager.max_iter = min(self.max_iter, keep_hist)
+        state = eager._run_eager(keep_state=True)
+        energy = torch.from_numpy(eager.energies).to(dev)
+        iters = torch.from_numpy(eager.iterations).to(dev)
+        converged = torch.from_numpy(eager.converged).to(dev)
+        self.seconds = dict(eager.seconds)
+        builds = eager.builds
+        P, hist, prev, it = state["P"], state["hist"], state["prev"], state["iterations"]
+        for s in range(nspin):
+            P_out[s].copy_(eager.densities[s])
+        active = torch.from_numpy(state["active"]).to(dev)
+        W = np.nonzero(state["active"])[0]
+
+        def step(st, diis_on):
+            """One SCF iteration of the working set, device only."""
+            st.was_active.copy_(st.active)
+            st.mask.zero_()
+            st.mask[st.Wt] = st.active.to(torch.uint8)
+            for s in range(nspin):
+                st.flatP[s].zero_()
+                st.flatP[s][st.flat_idx] = st.P[s].reshape(-1)[st.pad_idx]
+            if self.uhf:
+                self.eng.fock_uhf_async(st.flatP[0], st.flatP[1], st.flatG[0], st.flatG[1], st.mask)
+            else:
+                self.eng.fock_rhf_async(st.flatP[0], st.flatG[0], st.mask)
+            Mw, n = len(st.W), st.n
+            F = []
+            for s in range(nspin):
+                g = torch.zeros(Mw * n * n, dtype=torch.float64, device=dev)
+                g[st.pad_idx] = st.flatG[s][st.flat_idx]
+                f = st.h + g.reshape(Mw, n, n)
+                if not self.uhf:
+                    f = 0.5 * (f + f.transpose(1, 2))
+                F.append(f)
+            err_est = torch.zeros(Mw, dtype=torch.float64, device=dev)
+            if diis_on:
+                for s in range(nspin):
+                    err = st.S @ st.P[s] @ F[s] - F[s] @ st.P[s] @ st.S
+                    # the history, oldest first: drop the oldest, append this one
+                    st.hist_F[s][:-1] = st.hist_F[s][1:].clone()
+                    st.hist_E[s][:-1] = st.hist_E[s][1:].clone()
+                    st.hist_F[s][-1] = F[s]
+                    st.hist_E[s][-1] = err
+                    Ee = st.hist_E[s].transpose(0, 1)  # [Mw, keep, n, n]
+                    B = torch.einsum("aikl,ajkl->aij", Ee, Ee)
+                    m = keep_hist
+                    Bb = torch.zeros(Mw, m + 1, m + 1, dtype=torch.float64, device=dev)
+                    Bb[:, :m, :m] = B
+                    Bb[:, m, :m] = 1
+                    Bb[:, :m, m] = 1
+                    c = E.pulay_solve_device(Bb)[:, :m]
+                    F[s] = torch.einsum("ai,iakl->akl", c, st.hist_F[s])
+                    err_est = err_est + torch.sqrt(torch.diagonal(B, dim1=1, dim2=2)[:, -2:].sum(1))
+            Pn, eps = [], []
+            for s in range(nspin):
+                st.Ft.copy_(st.V @ F[s] @ st.V + st.shift)
+                for b, idx in st.bucket_idx:
+                    wb, Ub = E.eigh_batched(st.Ft[idx, :b, :b].contiguous(), method=self.eigh_method)
+                    st.w[idx, :b] = wb
+                    st.U[idx, :b, :b] = Ub
+                C = st.V @ st.U
+                factor = 1.0 if self.uhf else 2.0
+                Co = C * st.occ[s][:, None, :]
+                Pn.append(factor * Co @ Co.transpose(1, 2))
+                eps.append((st.w * st.occ[s]).sum(1))
+            if self.uhf:
+                e = 0.5 * (((Pn[0] + Pn[1]) * st.h).sum((1, 2)) + eps[0] + eps[1])
+            else:
+                e = 0.5 * (Pn[0] * st.h).sum((1, 2)) + eps[0]
+            e = e + st.enuc
+            rms = torch.sqrt(sum(((pn - p) ** 2).sum((1, 2)) for pn, p in zip(Pn, st.P)))
+            act = st.was_active
+            for s in range(nspin):
+                mix = Pn[s] if diis_on else self.alpha * Pn[s] + (1 - self.alpha) * st.P[s]
+                st.P[s].copy_(torch.where(act[:, None, None], mix, st.P[s]))
+            st.e.copy_(torch.where(act, e, st.e))
+            dE = (st.prev - e).abs()
+            st.conv.copy_(act & (dE <= econv) & (rms < RMS_CONV) & (err_est < DIIS_CONV))
+            st.prev.copy_(torch.where(act, e, st.prev))
+            st.active.copy_(act & ~st.conv)
+            st.converged.copy_(st.converged | st.conv)
+            st.iters.copy_(st.iters + act.long())
+
+        while len(W) and it < self.max_iter:
+            n = int(self.nbf[W].max())
+            sl = (slice(None), slice(0, n), slice(0, n))
+            st = _GraphState()
+            st.W, st.n = W, n
+            st.Wt = torch.from_numpy(W).to(dev)
+            Mw = len(W)
+            st.h, st.S, st.V, st.shift = (t[st.Wt][sl].contiguous() for t in (self.h, self.S, self.V, self.shift))
+            st.pad_idx, st.flat_idx, buckets = self._maps(W, n)
+            st.bucket_idx = [(b, torch.from_numpy(idx).to(dev)) for b, idx in buckets]
+            st.P = [p[st.Wt][sl].contiguous() for p in P]
+            st.hist_F = [torch.stack([x[st.Wt][sl] for x in hist[0][s]], 0).contiguous() for s in range(nspin)]
+            st.hist_E = [torch.stack([x[st.Wt][sl] for x in hist[1][s]], 0).contiguous() for s in range(nspin)]
+            st.prev = prev[st.Wt].contiguous()
+            st.active = active[st.Wt].contiguous()
+            st.enuc = enuc_all[st.Wt].contiguous()
+            st.occ = [(torch.arange(n, device=dev)[None, :] < nocc_all[s][st.Wt][:, None]).double()
+                      for s in range(nspin)]
+            st.flatP = [torch.zeros(self.eng.total, dtype=torch.float64, device=dev) for _ in range(nspin)]
+            st.flatG = [torch.zeros(self.eng.total, dtype=torch.float64, device=dev) for _ in range(nspin)]
+            st.mask = torch.zeros(M, dtype=torch.uint8, device=dev)
+            st.e = energy[st.Wt].contiguous()
+            st.conv = torch.zeros(Mw, dtype=torch.bool, device=dev)
+            st.was_active = torch.zeros(Mw, dtype=torch.bool, device=dev)
+            st.converged = torch.zeros(Mw, dtype=torch.bool, device=dev)
+            st.iters = torch.zeros(Mw, dtype=torch.int64, device=dev)
+            st.Ft = torch.zeros(Mw, n, n, dtype=torch.float64, device=dev)
+            st.w = torch.full((Mw, n), PAD_SHIFT, dtype=torch.float64, device=dev)
+            st.U = torch.eye(n, dtype=torch.float64, device=dev).expand(Mw, n, n).clone()
+            step(st, self.use_diis)  # eager warm-up of this shape (allocations, workspaces)
+            it += 1
+            builds += 1
+            torch.cuda.synchronize()
+            g = torch.cuda.CUDAGraph()
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(side):
+                with torch.cuda.graph(g):
+                    step(st, self.use_diis)
+            torch.cuda.current_stream().wait_stream(side)
+            self.graph_captures += 1
+            while it < self.max_iter:
+                k = min(self.replay, self.max_iter - it)
+                for _ in range(k):
+                    g.replay()
+                it += k
+                builds += k
+                n_act = int(st.active.sum())
+                if n_act == 0 or n_act <= Mw // 2:
+                    break
+            # results of the working set, and the state of the molecules still
+            # iterating for the next (smaller) one
+            energy[st.Wt] = st.e
+            iters[st.Wt] += st.iters
+            converged[st.Wt] |= st.converged
+            for s in range(nspin):
+                P_out[s][st.Wt, :n, :n] = st.P[s]
+            act_now = st.active.cpu().numpy().astype(bool)
+            P = [torch.zeros(M, self.nmax, self.nmax, dtype=torch.float64, device=dev) for _ in range(nspin)]
+            hist = ([[torch.zeros(M, self.nmax, self.nmax, dtype=torch.float64, device=dev)
+                      for _ in range(keep_hist)] for _ in range(nspin)],
+                    [[torch.zeros(M, self.nmax, self.nmax, dtype=torch.float64, device=dev)
+                      for _ in range(keep_hist)] for _ in range(nspin)])
+            for s in range(nspin):
+                P[s][st.Wt, :n, :n] = st.P[s]
+                for j in range(keep_hist):
+                    hist[0][s][j][st.Wt, :n, :n] = st.hist_F[s][j]
+                    hist[1][s][j][st.Wt, :n, :n] = st.hist_E[s][j]
+            prev = torch.full((M,), float("inf"), dtype=torch.float64, device=dev)
+            prev[st.Wt] = st.prev
+            active = torch.zeros(M, dtype=torch.bool, device=dev)
+            active[st.Wt] = st.active
+            W = W[act_now]
+            del g
+        torch.cuda.synchronize()
+        self.seconds["total"] = time.perf_counter() - t_start
+        self.iterations = iters.cpu().numpy()
+        self.converged = converged.cpu().numpy()
+        self.builds = builds
+        self.energies = energy.cpu().numpy()
+        self.densities = P_out
+        return self.energies
+
+
+class _GraphState:
+    """Device state of one working set for the captured iteration: every
+    tensor a replay reads or writes keeps its storage for the life of the
+    graph."""
 
 
 def _diis_extrapolate(Fs, Es):

@@ -98,6 +98,8 @@ struct QuartetClass {
   // lane occupancy of the thread-per-quartet layout: primitive quartets the
   // lanes evaluate over the lanes x the longest lane loop of each task
   double lane_work = 0, warp_work = 0;
+  // estimated flops of tasks [0, t): shards take contiguous ranges of equal cost
+  std::vector<double> cost_prefix;
   cudaEvent_t ev_a = nullptr, ev_b = nullptr;  // per-class timing (profiling on)
   float last_ms = 0;
 };
@@ -144,11 +146,23 @@ struct hfg_ctx {
   // (where other classes share the SMs)
   int blocks_per_sm = 0;
   int tuned_bps[kNumClasses] = {};  // per class, from hfg_autotune (0 = blocks_per_sm)
+  // primitive quartets per lane that the task builder aims for when it
+  // spreads a quartet over a lane group (0: one lane per quartet); per class
+  // from hfg_autotune, else prim_target
+  int prim_target = 96;
+  int class_prim_target[kNumClasses] = {};
   // CUDA graph of the plain direct build (hfg_set_graphs): captured on the
   // second build with the same buffers, stream and settings, replayed after
   bool use_graphs = false;
   bool use_streams = false;  // class kernels over the auxiliary streams (hfg_set_streams)
-  bool use_warp = true;      // large classes on the warp-cooperative kernel (else the split path)
+  // large classes with both kernels: 1 = the warp-cooperative kernel, 0 =
+  // the split path (primitive kernel + HRR/digest over scratch); per class,
+  // from hfg_autotune_paths / hfg_set_class_path, else the default below
+  int8_t warp_class[kNumClasses] = {};
+  // direct builds: the fused and warp-cooperative class kernels take their
+  // tasks from a device work queue (one counter per class, one atomic per
+  // warp and task) instead of a grid-stride walk
+  bool use_queue = false;
   cudaEvent_t ev_done = nullptr;  // end of the last build on its stream
   unsigned config_version = 0;  // bumped by every setter that changes a build
   struct GraphKey {
@@ -202,6 +216,7 @@ struct hfg_ctx {
   // every class, compacted on the device, and their counts
   Task *d_task_active = nullptr;
   int *d_task_counts = nullptr;
+  int *d_queue = nullptr;  // per quartet class: the device work queue's counter
   std::vector<int> task_base;  // per quartet class, offset into d_task_active
   hfg_stats stats{};
   bool profiling = false;
@@ -253,7 +268,7 @@ struct hfg_ctx {
                     d_Pb,         d_Pt,            d_G,          d_Gb,       d_block,      d_scratch[0], d_shell_ao,
                     d_shell_nf,   d_shell_dmax,    d_counters,   d_prev_P[0], d_prev_P[1], d_prev_G[0], d_prev_G[1],
                     d_dP[0],      d_dP[1],         d_primf,      d_pair_mol, d_mol_nbf,    d_mol_off,   d_mol_active,
-                    d_task_active, d_task_counts};
+                    d_task_active, d_task_counts, d_queue};
     for (void *b : bufs) cudaFree(b);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     for (int i = 0; i < kAux; ++i) {
@@ -268,6 +283,10 @@ struct hfg_ctx {
     if (stream) cudaStreamDestroy(stream);
   }
 };
+
+// the large class runs on the warp-cooperative kernel (classes with only
+// that kernel always do)
+static bool class_on_warp(const hfg_ctx *c, int cls) { return kWarp[cls] && (c->warp_class[cls] || !kSplit[cls]); }
 
 namespace hfg {
 
@@ -336,6 +355,19 @@ static void build_quartet_classes(hfg_ctx *c, double threshold) {
     const double pf = prim_flops(ci, c->opts.eri_convention == HFG_ERI_REFERENCE);
     const double hf = hrr_flops(ci);
     const int ltot = ce.la + ce.lb + ce.lc + ce.ld;
+    // the longest ket contraction of each bucket segment
+    std::vector<int> segmax(KL.seg_start.size(), 0);
+    for (size_t g = 0; g + 1 < KL.seg_start.size(); ++g)
+      for (int64_t k2 = KL.seg_start[g]; k2 < KL.seg_start[g + 1]; ++k2)
+        segmax[g] = std::max(segmax[g], c->pair_nprim[kets[k2]]);
+    // fused thread-per-quartet classes: lanes per quartet so that a lane's
+    // share of a quartet's primitive quartets stays near the target (long
+    // contractions spread over 2..32 lanes, fewer kets per task); the large
+    // classes (split path: one lane per quartet; warp kernel: one warp per
+    // quartet) keep 32 kets per task
+    const bool grouped = !kSplit[ci] && !kWarp[ci];
+    const int target = c->class_prim_target[ci] > 0 ? c->class_prim_target[ci]
+                       : c->class_prim_target[ci] < 0 ? 0 : c->prim_target;
     for (size_t b = 0; b < bras.size(); ++b) {
       const double qb = c->pair_Q[bras[b]];
       if (!(qb > 0)) continue;
@@ -356,13 +388,29 @@ static void build_quartet_classes(hfg_ctx *c, double threshold) {
         int64_t end = lo;
         if (same) end = std::min<int64_t>(end, (int64_t)b + 1);
         if (end <= s0) continue;
-        for (int64_t st = s0; st < end; st += 32) {
-          const int64_t e1 = std::min<int64_t>(st + 32, end);
-          q.tasks.push_back(Task{(int)b, (int)st, (int)e1});
+        int per_task = 32;
+        if (grouped && target > 0) {
+          const double work = (double)bprim * segmax[mol * kBuckets + k];
+          int G = 1;
+          while (G < 32 && work / G > target) G <<= 1;
+          per_task = 32 / G;
+        }
+        for (int64_t st = s0; st < end; st += per_task) {
+          const int64_t e1 = std::min<int64_t>(st + per_task, end);
+          Task tk{(int)b, (int)st, (int)e1};
+          int m2 = 1;
+          while (m2 < e1 - st) m2 <<= 1;
+          if (grouped)
+            while ((32 >> tk.lg) > m2) ++tk.lg;  // 32 / 2^lg lane groups, at least the task's kets
+          q.tasks.push_back(tk);
           int64_t mx = 0;
           for (int64_t k2 = st; k2 < e1; ++k2) mx = std::max<int64_t>(mx, c->pair_nprim[kets[k2]]);
           q.lane_work += (double)bprim * (double)(kprim[e1] - kprim[st]);
-          q.warp_work += 32.0 * (double)bprim * (double)mx;
+          q.warp_work += 32.0 * std::ceil((double)bprim * (double)mx / (double)(1 << tk.lg));
+          if (q.cost_prefix.empty()) q.cost_prefix.push_back(0.0);
+          q.cost_prefix.push_back(q.cost_prefix.back() +
+                                  (double)bprim * (double)(kprim[e1] - kprim[st]) * (pf + boys_geom_flops(ltot)) +
+                                  (double)(e1 - st) * hf);
         }
         q.shell_quartets += end - s0;
         if (same && end == (int64_t)b + 1) {
@@ -400,21 +448,53 @@ static int grid_for(const hfg_ctx *c, int ntasks, int cls) {
   return std::max(1, std::min(blocks, c->num_sms * bps));
 }
 
+// Shard `rank` of `count` of tasks with running cost `prefix` (ntasks + 1
+// entries from 0): shard r begins at the first task whose prefix reaches
+// r / count of the total, so the shards tile the tasks in order.
+static void shard_range(const double *prefix, int64_t ntasks, int rank, int count, int64_t *first, int64_t *n) {
+  const double whole = prefix[ntasks];
+  auto bound = [&](int r) -> int64_t {
+    if (r <= 0) return 0;
+    if (r >= count) return ntasks;
+    const double target = whole * r / count;
+    return std::min<int64_t>(ntasks, std::lower_bound(prefix, prefix + ntasks + 1, target) - prefix);
+  };
+  const int64_t lo = bound(rank), hi = bound(rank + 1);
+  *first = lo;
+  *n = std::max<int64_t>(0, hi - lo);
+}
+
 // A class launch over all tasks, or with `sharded` over this context's
-// shard of them: every shard_count-th task from shard_rank (the tasks of a
-// class are in bucket, then Schwarz order, so the interleave spreads cheap
-// and expensive tasks evenly over the shards).
+// shard of them: a contiguous range of the class's tasks whose estimated
+// cost (primitive quartets x the class's recursion and Boys flops, plus its
+// horizontal recursions per quartet) is 1/shard_count of the class's, so
+// shards of uneven task mixes take equal work.
 static ClassLaunch base_launch(const hfg_ctx *c, const QuartetClass &q, bool sharded = false) {
   ClassLaunch cl{};
   cl.bra_list = c->pclass[q.bra_pc].d_pairs;
   cl.ket_list = c->pclass[q.ket_pc].d_pairs;
   cl.tasks = q.d_tasks;
   const int total = (int)q.tasks.size();
-  cl.task_offset = sharded ? c->shard_rank : 0;
-  cl.task_stride = sharded ? c->shard_count : 1;
-  cl.ntasks = total > cl.task_offset ? (total - cl.task_offset + cl.task_stride - 1) / cl.task_stride : 0;
+  cl.task_offset = 0;
+  cl.task_stride = 1;
+  cl.ntasks = total;
+  if (sharded && c->shard_count > 1 && (int)q.cost_prefix.size() == total + 1) {
+    int64_t first = 0, count = 0;
+    shard_range(q.cost_prefix.data(), total, c->shard_rank, c->shard_count, &first, &count);
+    cl.task_offset = (int)first;
+    cl.ntasks = (int)count;
+  }
   cl.same_class = q.bra_pc == q.ket_pc;
   return cl;
+}
+
+// the cost share of a launch in its class (shards report their part of the
+// class's quartet and flop counts)
+static double launch_share(const QuartetClass &q, const ClassLaunch &cl) {
+  if (q.tasks.empty()) return 0.0;
+  if ((int)q.cost_prefix.size() != (int)q.tasks.size() + 1 || q.cost_prefix.back() <= 0)
+    return (double)cl.ntasks / (double)q.tasks.size();
+  return (q.cost_prefix[cl.task_offset + cl.ntasks] - q.cost_prefix[cl.task_offset]) / q.cost_prefix.back();
 }
 
 __global__ void finalize_rhf(const double *J, const double *K, double *G, int n) {
@@ -514,7 +594,7 @@ static int ncomp_range(int lo, int hi) {
 static void split_chunking(const hfg_ctx *c, int cls, int ntasks, bool ref, size_t *need, int *chunk_tasks);
 static int scratch_regions(const hfg_ctx *c);
 // the class runs the split (primitive + HRR/digest) kernels over scratch
-static bool uses_split(const hfg_ctx *c, int cls) { return kSplit[cls] && !(kWarp[cls] && c->use_warp); }
+static bool uses_split(const hfg_ctx *c, int cls) { return kSplit[cls] && !class_on_warp(c, cls); }
 static hfg_status grow_scratch(hfg_ctx *c, int slot, size_t need);
 
 struct ClassStreams {
@@ -609,7 +689,7 @@ static hfg_status grow_scratch(hfg_ctx *c, int slot, size_t need) {
 static hfg_status launch_class(hfg_ctx *c, const QuartetClass &q, const ClassLaunch &cl, int mode, bool ref,
                                int prec, cudaStream_t s, int *launches, int slot = 0) {
   const ClassEntry &e = kClasses[q.cls];
-  if (kWarp[q.cls] && c->use_warp && mode != kBlock) {
+  if (class_on_warp(c, q.cls) && mode != kBlock) {
     kWarp[q.cls](c->view(), cl, mode, ref, prec, 0, s);
     ++*launches;
     return HFG_OK;
@@ -687,6 +767,12 @@ static hfg_status direct_build_body(hfg_ctx *c, bool uhf, const double *dPa, con
     launches += 2;
   }
   const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
+  const size_t nq = c->qclasses.size();
+  if (c->use_queue && nq > 0) {
+    if (!c->d_queue) HFG_CUDA(cudaMalloc((void **)&c->d_queue, nq * sizeof(int)));
+    HFG_CUDA(cudaMemsetAsync(c->d_queue, 0, nq * sizeof(int), s));
+    ++launches;
+  }
   ClassStreams cs{c, s, c->use_streams && !c->profiling};
   {
     std::vector<int> nt(c->qclasses.size());
@@ -697,9 +783,11 @@ static hfg_status direct_build_body(hfg_ctx *c, bool uhf, const double *dPa, con
   if ((st = cs.fork()) != HFG_OK) return st;
   const int prec = !precise ? 0 : c->mixed_cutoff > 0 ? 2 : 1;
   c->stats = hfg_stats{};
-  for (auto &q : c->qclasses) {
+  for (size_t qi = 0; qi < nq; ++qi) {
+    QuartetClass &q = c->qclasses[qi];
     ClassLaunch cl = base_launch(c, q, true);
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_a, s));
+    if (c->use_queue && !uses_split(c, q.cls)) cl.queue = c->d_queue + qi;
     cl.Da = Da;
     cl.Db = Db;
     cl.Dt = uhf ? c->d_Pt : Da;
@@ -715,8 +803,8 @@ static hfg_status direct_build_body(hfg_ctx *c, bool uhf, const double *dPa, con
       if (st != HFG_OK) return st;
     }
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_b, s));
-    // a shard's share of the class, in proportion to its tasks
-    const double share = q.tasks.empty() ? 0.0 : (double)cl.ntasks / (double)q.tasks.size();
+    // a shard's share of the class, in proportion to its estimated cost
+    const double share = launch_share(q, cl);
     c->stats.shell_quartets += (int64_t)(share * (double)q.shell_quartets + 0.5);
     c->stats.function_quartets += (int64_t)(share * (double)q.function_quartets + 0.5);
     c->stats.primitive_quartets += (int64_t)(share * (double)q.prim_quartets + 0.5);
@@ -962,6 +1050,104 @@ static hfg_status batch_build(hfg_ctx *c, bool uhf, const double *dPa, const dou
   return HFG_OK;
 }
 
+// Batched build with no host synchronisation (the batched SCF captures it in
+// a CUDA graph): the active mask is read from device memory, every class's
+// active tasks are compacted on the device and the class kernels take them
+// from a device work queue (count and counter in device memory, one fixed
+// grid per class), then G per active molecule.  Large classes must run the
+// warp-cooperative kernels (no scratch, no host-sized chunks).  Buffers are
+// allocated by the first call.
+static hfg_status batch_build_async(hfg_ctx *c, bool uhf, const double *dPa, const double *dPb, double *dGa,
+                                    double *dGb, const unsigned char *d_active, cudaStream_t s) {
+  const size_t tot = (size_t)c->batch_elems;
+  const size_t nq = c->qclasses.size();
+  hfg_status st;
+  for (size_t i = 0; i < nq; ++i)
+    if (uses_split(c, c->qclasses[i].cls))
+      return fail(HFG_INVALID_ARG, "asynchronous batched builds need the warp-cooperative large-class kernels");
+  if ((st = ensure(&c->d_J, tot)) != HFG_OK || (st = ensure(&c->d_Ka, tot)) != HFG_OK) return st;
+  if (uhf && ((st = ensure(&c->d_Kb, tot)) != HFG_OK || (st = ensure(&c->d_Pt, tot)) != HFG_OK)) return st;
+  if (!c->d_task_active) {
+    size_t total = 0;
+    c->task_base.assign(nq, 0);
+    for (size_t i = 0; i < nq; ++i) {
+      c->task_base[i] = (int)total;
+      total += c->qclasses[i].tasks.size();
+    }
+    HFG_CUDA(cudaMalloc((void **)&c->d_task_active, std::max<size_t>(1, total) * sizeof(Task)));
+    HFG_CUDA(cudaMalloc((void **)&c->d_task_counts, std::max<size_t>(1, nq) * sizeof(int)));
+  }
+  if (!c->d_queue) HFG_CUDA(cudaMalloc((void **)&c->d_queue, std::max<size_t>(1, nq) * sizeof(int)));
+  HFG_CUDA(cudaMemsetAsync(c->d_J, 0, tot * sizeof(double), s));
+  HFG_CUDA(cudaMemsetAsync(c->d_Ka, 0, tot * sizeof(double), s));
+  int launches = 2;
+  if (uhf) {
+    HFG_CUDA(cudaMemsetAsync(c->d_Kb, 0, tot * sizeof(double), s));
+    add_densities<<<std::max(1, std::min(1024, (int)((tot + 255) / 256))), 256, 0, s>>>(dPa, dPb, c->d_Pt, (int)tot);
+    launches += 2;
+  }
+  HFG_CUDA(cudaMemsetAsync(c->d_task_counts, 0, nq * sizeof(int), s));
+  HFG_CUDA(cudaMemsetAsync(c->d_queue, 0, nq * sizeof(int), s));
+  launches += 2;
+  for (size_t i = 0; i < nq; ++i) {
+    const QuartetClass &q = c->qclasses[i];
+    const int nt = (int)q.tasks.size();
+    if (nt == 0) continue;
+    const int grid = std::max(1, std::min(c->num_sms * 8, (nt + 255) / 256));
+    compact_active_tasks<<<grid, 256, 0, s>>>(q.d_tasks, nt, c->pclass[q.bra_pc].d_pairs, c->d_pair_mol, d_active,
+                                              c->d_task_active + c->task_base[i], c->d_task_counts + i);
+    ++launches;
+  }
+  EngineView v = c->view();
+  v.mol_active = d_active;
+  const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
+  ClassStreams cs{c, s, c->use_streams && !c->profiling};
+  if ((st = cs.fork()) != HFG_OK) return st;
+  c->stats = hfg_stats{};
+  for (size_t qi = 0; qi < nq; ++qi) {
+    auto &q = c->qclasses[qi];
+    if (q.tasks.empty()) continue;
+    ClassLaunch cl = base_launch(c, q, false);
+    cl.tasks = c->d_task_active + c->task_base[qi];
+    cl.task_offset = 0;
+    cl.task_stride = 1;
+    cl.ntasks = (int)q.tasks.size();  // bound: the grid sizes from it
+    cl.ntasks_dev = c->d_task_counts + qi;
+    cl.queue = c->d_queue + qi;
+    cl.Da = dPa;
+    cl.Db = dPb;
+    cl.Dt = uhf ? c->d_Pt : dPa;
+    cl.J = c->d_J;
+    cl.Ka = c->d_Ka;
+    cl.Kb = c->d_Kb;
+    const cudaStream_t cls_stream = cs.pick(false);
+    const int mode = uhf ? kJkUhf : kJkRhf;
+    if (kWarp[q.cls]) kWarp[q.cls](v, cl, mode, ref, 0, 0, cls_stream);
+    else kClasses[q.cls].launch(v, cl, mode, ref, 0, grid_for(c, cl.ntasks, q.cls), cls_stream);
+    ++launches;
+    c->stats.shell_quartets += q.shell_quartets;
+    c->stats.function_quartets += q.function_quartets;
+    c->stats.primitive_quartets += q.prim_quartets;
+    c->stats.flops += q.flops;
+  }
+  HFG_CUDA(cudaGetLastError());
+  if ((st = cs.join()) != HFG_OK) return st;
+  int nmax = 0;
+  for (int n : c->mol_nbf) nmax = std::max(nmax, n);
+  const dim3 fg(std::max(1, std::min(64, (nmax * nmax + 255) / 256)), c->nmol);
+  if (uhf)
+    finalize_uhf_batch<<<fg, 256, 0, s>>>(c->d_J, c->d_Ka, c->d_Kb, dGa, dGb, c->d_mol_nbf, c->d_mol_off, d_active);
+  else
+    finalize_rhf_batch<<<fg, 256, 0, s>>>(c->d_J, c->d_Ka, dGa, c->d_mol_nbf, c->d_mol_off, d_active);
+  ++launches;
+  HFG_CUDA(cudaGetLastError());
+  c->stats.kernel_launches = launches;
+  c->stats.shell_pairs = c->npairs;
+  c->stats.fp64_shell_quartets = c->stats.shell_quartets;
+  c->counted = false;
+  return HFG_OK;
+}
+
 static hfg_status finish_timing(hfg_ctx *c) {
   HFG_CUDA(cudaEventSynchronize(c->ev1));
   float ms = 0;
@@ -1062,7 +1248,21 @@ static hfg_status create_context(const hfg_shells *sh, const int *shell_mol, int
   // tuning: HFG_BLOCKS_PER_SM overrides the grid cap (every block stages the
   // class's Boys table once, so fewer, longer-lived blocks stage it less)
   if (const char *e = std::getenv("HFG_BLOCKS_PER_SM")) ctx->blocks_per_sm = std::max(1, std::atoi(e));
-  if (const char *e = std::getenv("HFG_SPLIT_PATH")) ctx->use_warp = std::atoi(e) == 0;
+  // tuning: HFG_PRIM_TARGET sets the lane-group target (0: one lane per quartet)
+  if (const char *e = std::getenv("HFG_PRIM_TARGET")) ctx->prim_target = std::max(0, std::atoi(e));
+  // default kernel per large class: the warp-cooperative kernel where one
+  // quartet's primitive work fills a warp -- (dd|dd), 1296 Cartesian
+  // components -- the split path for the rest; HFG_SPLIT_PATH=1 / HFG_WARP_PATH=1
+  // put every large class on one of them
+  for (int k = 0; k < kNumClasses; ++k) {
+    const ClassEntry &e = kClasses[k];
+    ctx->warp_class[k] = kWarp[k] && e.la + e.lb + e.lc + e.ld >= 8 ? 1 : 0;
+  }
+  if (const char *e = std::getenv("HFG_WORK_QUEUE")) ctx->use_queue = std::atoi(e) != 0;
+  if (const char *e = std::getenv("HFG_SPLIT_PATH"); e && std::atoi(e) != 0)
+    std::fill(std::begin(ctx->warp_class), std::end(ctx->warp_class), int8_t(0));
+  if (const char *e = std::getenv("HFG_WARP_PATH"); e && std::atoi(e) != 0)
+    std::fill(std::begin(ctx->warp_class), std::end(ctx->warp_class), int8_t(1));
   ctx->batch = shell_mol != nullptr;
   ctx->nmol = ctx->batch ? nmol : 1;
   ctx->nbf = ctx->batch ? 0 : sh->nbf;
@@ -1402,6 +1602,22 @@ hfg_status hfg_fock_uhf_batch_device(hfg_ctx *c, const double *dPa, const double
   return finish_timing(c);
 }
 
+hfg_status hfg_fock_rhf_batch_async(hfg_ctx *c, const double *dP, double *dG, const uint8_t *d_active,
+                                    void *stream) {
+  if (!c || !dP || !dG || !d_active) return fail(HFG_INVALID_ARG, "null argument");
+  if (!c->batch) return fail(HFG_INVALID_ARG, "not a batched context");
+  HFG_CUDA(cudaSetDevice(c->device));
+  return batch_build_async(c, false, dP, nullptr, dG, nullptr, d_active, stream ? (cudaStream_t)stream : c->stream);
+}
+
+hfg_status hfg_fock_uhf_batch_async(hfg_ctx *c, const double *dPa, const double *dPb, double *dGa, double *dGb,
+                                    const uint8_t *d_active, void *stream) {
+  if (!c || !dPa || !dPb || !dGa || !dGb || !d_active) return fail(HFG_INVALID_ARG, "null argument");
+  if (!c->batch) return fail(HFG_INVALID_ARG, "not a batched context");
+  HFG_CUDA(cudaSetDevice(c->device));
+  return batch_build_async(c, true, dPa, dPb, dGa, dGb, d_active, stream ? (cudaStream_t)stream : c->stream);
+}
+
 hfg_status hfg_fock_rhf(hfg_ctx *c, const double *P, double *G) {
   if (!c || !P || !G) return fail(HFG_INVALID_ARG, "null argument");
   HFG_CUDA(cudaSetDevice(c->device));
@@ -1520,7 +1736,7 @@ hfg_status hfg_class_profile(const hfg_ctx *c, hfg_class_time *out, int32_t cap,
     const ClassEntry &e = kClasses[q.cls];
     out[n] = hfg_class_time{e.la,    e.lb,    e.lc,         e.ld, q.shell_quartets, q.function_quartets, q.prim_quartets,
                             q.flops, (double)q.last_ms, (int64_t)q.tasks.size(),
-                            q.warp_work > 0 ? q.lane_work / q.warp_work : 0.0, kWarp[q.cls] && c->use_warp ? 1 : 0, 0};
+                            q.warp_work > 0 ? q.lane_work / q.warp_work : 0.0, class_on_warp(c, q.cls) ? 1 : 0, 0};
     ++n;
   }
   *count = n;
@@ -1645,6 +1861,172 @@ hfg_status hfg_autotune(hfg_ctx *c, const double *dP, int32_t *chosen, int32_t c
   return HFG_OK;
 }
 
+}  // extern "C"
+
+namespace hfg {
+// Rebuilds every class's task list (after a change of the lane-group
+// target): host lists, device copies, and the batched builds' compaction
+// buffers, which are sized from the lists.
+static hfg_status rebuild_tasks(hfg_ctx *c) {
+  HFG_CUDA(cudaDeviceSynchronize());  // queued builds may still read the old lists
+  for (auto &q : c->qclasses) {
+    cudaFree(q.d_tasks);
+    if (q.ev_a) cudaEventDestroy(q.ev_a);
+    if (q.ev_b) cudaEventDestroy(q.ev_b);
+  }
+  build_quartet_classes(c, c->opts.schwarz_threshold);
+  hfg_status st = upload_classes(c);
+  if (st != HFG_OK) return st;
+  if (c->profiling)
+    for (auto &q : c->qclasses) {
+      HFG_CUDA(cudaEventCreate(&q.ev_a));
+      HFG_CUDA(cudaEventCreate(&q.ev_b));
+    }
+  cudaFree(c->d_task_active);
+  cudaFree(c->d_task_counts);
+  cudaFree(c->d_queue);
+  c->d_task_active = nullptr;
+  c->d_task_counts = nullptr;
+  c->d_queue = nullptr;
+  c->task_base.clear();
+  ++c->config_version;
+  return HFG_OK;
+}
+}  // namespace hfg
+
+extern "C" {
+
+hfg_status hfg_set_prim_target(hfg_ctx *c, int32_t target) {
+  if (!c || target < 0) return hfg::fail(HFG_INVALID_ARG, "null context or negative target");
+  c->prim_target = target;
+  std::fill(std::begin(c->class_prim_target), std::end(c->class_prim_target), 0);
+  return hfg::rebuild_tasks(c);
+}
+
+// Task-shape autotuner: for every thread-per-quartet class, the primitive
+// quartets per lane that the task builder aims for when it spreads a quartet
+// over a lane group (0: one lane per quartet, then 48, 96, 192, 384),
+// each timed on the class's J/K kernel alone (one warm-up, two timed
+// launches, CUDA events) with the caller's density; the fastest is kept.
+hfg_status hfg_autotune_tasks(hfg_ctx *c, const double *dP, int32_t *chosen, int32_t cap, int32_t *count,
+                              void *stream) {
+  using namespace hfg;
+  if (!c || !dP) return fail(HFG_INVALID_ARG, "null context or density");
+  if (c->batch) return fail(HFG_INVALID_ARG, "hfg_autotune_tasks: single-molecule contexts");
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  const size_t nn = (size_t)c->nbf * c->nbf;
+  hfg_status st;
+  if ((st = ensure(&c->d_J, nn)) != HFG_OK || (st = ensure(&c->d_Ka, nn)) != HFG_OK) return st;
+  const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
+  const int cand[] = {0, 48, 96, 192, 384};
+  std::vector<float> best(kNumClasses, 1e30f);
+  std::vector<int> best_t(kNumClasses, c->prim_target);
+  for (int t : cand) {
+    c->prim_target = t;
+    std::fill(std::begin(c->class_prim_target), std::end(c->class_prim_target), 0);
+    if ((st = rebuild_tasks(c)) != HFG_OK) return st;
+    for (auto &q : c->qclasses) {
+      if (kWarp[q.cls] || kSplit[q.cls]) continue;  // one warp per quartet: no lane groups
+      ClassLaunch cl = base_launch(c, q, true);
+      if (cl.ntasks == 0) continue;
+      cl.Da = dP;
+      cl.Dt = dP;
+      cl.J = c->d_J;
+      cl.Ka = c->d_Ka;
+      const int grid = grid_for(c, cl.ntasks, q.cls);
+      kClasses[q.cls].launch(c->view(), cl, kJkRhf, ref, 0, grid, s);
+      HFG_CUDA(cudaEventRecord(c->ev0, s));
+      for (int r = 0; r < 2; ++r) kClasses[q.cls].launch(c->view(), cl, kJkRhf, ref, 0, grid, s);
+      HFG_CUDA(cudaEventRecord(c->ev1, s));
+      HFG_CUDA(cudaEventSynchronize(c->ev1));
+      HFG_CUDA(cudaGetLastError());
+      float ms = 0;
+      HFG_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+      if (ms < best[q.cls]) {
+        best[q.cls] = ms;
+        best_t[q.cls] = t;
+      }
+    }
+  }
+  c->prim_target = 96;
+  int written = 0;
+  for (int k = 0; k < kNumClasses; ++k) {
+    // class_prim_target: > 0 a target, -1 one lane per quartet, 0 the default
+    c->class_prim_target[k] = best[k] < 1e30f ? (best_t[k] > 0 ? best_t[k] : -1) : 0;
+    if (best[k] < 1e30f && chosen && written + 5 <= cap) {
+      const ClassEntry &e = kClasses[k];
+      const int rec[5] = {e.la, e.lb, e.lc, e.ld, best_t[k]};
+      std::copy(rec, rec + 5, chosen + written);
+      written += 5;
+    }
+  }
+  if (count) *count = written / 5;
+  return rebuild_tasks(c);
+}
+
+hfg_status hfg_set_class_path(hfg_ctx *c, int32_t la, int32_t lb, int32_t lc, int32_t ld, int32_t path) {
+  if (!c) return hfg::fail(HFG_INVALID_ARG, "null context");
+  for (int k = 0; k < kNumClasses; ++k) {
+    const ClassEntry &e = kClasses[k];
+    if (e.la != la || e.lb != lb || e.lc != lc || e.ld != ld) continue;
+    if (!kWarp[k] || !kSplit[k]) return hfg::fail(HFG_INVALID_ARG, "hfg_set_class_path: class without both kernels");
+    c->warp_class[k] = path != 0 ? 1 : 0;
+    ++c->config_version;
+    return HFG_OK;
+  }
+  return hfg::fail(HFG_INVALID_ARG, "hfg_set_class_path: no such canonical quartet class");
+}
+
+// Kernel autotuner for the classes with both kernels: each timed on the
+// class's J/K build alone (one warm-up, two timed launches, CUDA events)
+// with the caller's density, warp kernel against split path; the faster is
+// kept.
+hfg_status hfg_autotune_paths(hfg_ctx *c, const double *dP, int32_t *chosen, int32_t cap, int32_t *count,
+                              void *stream) {
+  using namespace hfg;
+  if (!c || !dP) return fail(HFG_INVALID_ARG, "null context or density");
+  if (c->batch) return fail(HFG_INVALID_ARG, "hfg_autotune_paths: single-molecule contexts");
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+  const size_t nn = (size_t)c->nbf * c->nbf;
+  hfg_status st;
+  if ((st = ensure(&c->d_J, nn)) != HFG_OK || (st = ensure(&c->d_Ka, nn)) != HFG_OK) return st;
+  const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
+  int written = 0;
+  for (auto &q : c->qclasses) {
+    if (!kWarp[q.cls] || !kSplit[q.cls] || q.tasks.empty()) continue;
+    ClassLaunch cl = base_launch(c, q, true);
+    if (cl.ntasks == 0) continue;
+    cl.Da = dP;
+    cl.Dt = dP;
+    cl.J = c->d_J;
+    cl.Ka = c->d_Ka;
+    float ms[2] = {0, 0};
+    for (int path = 0; path < 2; ++path) {
+      c->warp_class[q.cls] = (int8_t)path;
+      int launches = 0;
+      if ((st = launch_class(c, q, cl, kJkRhf, ref, 0, s, &launches)) != HFG_OK) return st;
+      HFG_CUDA(cudaEventRecord(c->ev0, s));
+      for (int r = 0; r < 2; ++r)
+        if ((st = launch_class(c, q, cl, kJkRhf, ref, 0, s, &launches)) != HFG_OK) return st;
+      HFG_CUDA(cudaEventRecord(c->ev1, s));
+      HFG_CUDA(cudaEventSynchronize(c->ev1));
+      HFG_CUDA(cudaGetLastError());
+      HFG_CUDA(cudaEventElapsedTime(&ms[path], c->ev0, c->ev1));
+    }
+    const int pick = ms[1] < ms[0] ? 1 : 0;
+    c->warp_class[q.cls] = (int8_t)pick;
+    if (chosen && written + 5 <= cap) {
+      const ClassEntry &e = kClasses[q.cls];
+      const int rec[5] = {e.la, e.lb, e.lc, e.ld, pick};
+      std::copy(rec, rec + 5, chosen + written);
+      written += 5;
+    }
+  }
+  if (count) *count = written / 5;
+  ++c->config_version;
+  return HFG_OK;
+}
+
 hfg_status hfg_set_streams(hfg_ctx *c, int32_t on) {
   if (!c) return hfg::fail(HFG_INVALID_ARG, "null context");
   c->use_streams = on != 0;
@@ -1666,6 +2048,22 @@ hfg_status hfg_set_shard(hfg_ctx *c, int32_t rank, int32_t count) {
   c->shard_count = count;
   ++c->config_version;
   c->inc_valid = false;  // an incremental history belongs to one shard
+  return HFG_OK;
+}
+
+hfg_status hfg_shard_range(const double *cost_prefix, int64_t ntasks, int32_t rank, int32_t count, int64_t *first,
+                           int64_t *ntasks_out) {
+  if (!cost_prefix || !first || !ntasks_out || ntasks < 0) return hfg::fail(HFG_INVALID_ARG, "hfg_shard_range: arguments");
+  if (count < 1 || rank < 0 || rank >= count) return hfg::fail(HFG_INVALID_ARG, "shard rank outside [0, count)");
+  shard_range(cost_prefix, ntasks, rank, count, first, ntasks_out);
+  return HFG_OK;
+}
+
+hfg_status hfg_copy_device(void *dst, const void *src, int64_t bytes, void *stream) {
+  if (!dst || !src || bytes < 0) return hfg::fail(HFG_INVALID_ARG, "hfg_copy_device: arguments");
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  HFG_CUDA(cudaMemcpyAsync(dst, src, (size_t)bytes, cudaMemcpyDeviceToDevice, s));
+  HFG_CUDA(cudaStreamSynchronize(s));
   return HFG_OK;
 }
 

@@ -123,9 +123,65 @@ __device__ __forceinline__ void boys_eval_f32(float *F, float T, float scale, co
 // accumulated into acc: the primitive loops.  R = double: FP64 throughout;
 // R = float: the FP32 primitive pairs and FP32 arithmetic (mixed
 // precision), with the Boys function's edges in FP64.
+// lg > 0: the 2^lg lanes of an aligned lane group share the quartet; lane gl
+// of the group takes the primitive quartets gl, gl + 2^lg, ... of the
+// (ket primitive, bra primitive) grid and the group sums its accumulators
+// with shuffles afterwards (warp-shuffle contraction), so every lane of the
+// group ends with the whole contracted block.  lg is warp-uniform.
+template <int LA, int LB, int LC, int LD, bool REF, class R>
+__device__ __forceinline__ void accumulate_primitives_grouped(const EngineView &v, const double *tab, int bp, int kp,
+                                                              int npk, R *acc, int lg) {
+  constexpr int LTOT = LA + LB + LC + LD;
+  using Cls = EriClass<LA, LB, LC, LD, REF>;
+  const int G = 1 << lg, gl = threadIdx.x & (G - 1);
+  const int offb = v.pair_prim_off[bp], npb = v.pair_nprim[bp];
+  const int offk = v.pair_prim_off[kp];
+  const int total = npk * npb;
+  int ik = npb > 0 ? gl / npb : 0, ib = npb > 0 ? gl - ik * npb : 0;
+  for (int w = gl; w < total; w += G) {
+    if constexpr (std::is_same<R, float>::value) {
+      const PrimPairF pk = v.primf[offk + ik], pb = v.primf[offb + ib];
+      const float rs = rsqrtf(pb.zeta + pk.zeta);
+      const float rho = pb.zeta * pk.zeta * (rs * rs);
+      const float PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;
+      const float T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+      float F[LTOT + 1];
+      boys_eval_f32<LTOT>(F, T, pb.K * pk.K * rs, tab);
+      const float roz = rho * pb.inv_zeta, ie = pk.inv_zeta;
+      Cls::template prim<float>(acc, F, pb.PAx, pb.PAy, pb.PAz, -roz * PQx, -roz * PQy, -roz * PQz,
+                                0.5f * pb.inv_zeta, roz, -(pb.bABx + pk.bABx) * ie, -(pb.bABy + pk.bABy) * ie,
+                                -(pb.bABz + pk.bABz) * ie, pb.zeta * ie, 0.5f * ie);
+    } else {
+      const PrimPair pk = v.prim[offk + ik], pb = v.prim[offb + ib];
+      const double rs = rsqrt(pb.zeta + pk.zeta);
+      const double rho = pb.zeta * pk.zeta * (rs * rs);
+      const double PQx = pb.Px - pk.Px, PQy = pb.Py - pk.Py, PQz = pb.Pz - pk.Pz;
+      const double T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+      double F[LTOT + 1];
+      boys_eval<LTOT, double>(F, T, pb.K * pk.K * rs, tab);
+      const double roz = rho * pb.inv_zeta, ie = pk.inv_zeta;
+      Cls::template prim<double>(acc, F, pb.PAx, pb.PAy, pb.PAz, -roz * PQx, -roz * PQy, -roz * PQz,
+                                 0.5 * pb.inv_zeta, roz, -(pb.bABx + pk.bABx) * ie, -(pb.bABy + pk.bABy) * ie,
+                                 -(pb.bABz + pk.bABz) * ie, pb.zeta * ie, 0.5 * ie);
+    }
+    ib += G;
+    while (ib >= npb) {
+      ib -= npb;
+      ++ik;
+    }
+  }
+  for (int o = 1; o < G; o <<= 1)
+#pragma unroll
+    for (int x = 0; x < Cls::kAcc; ++x) acc[x] += __shfl_xor_sync(0xffffffffu, acc[x], o);
+}
+
 template <int LA, int LB, int LC, int LD, bool REF, class R>
 __device__ __forceinline__ void accumulate_primitives(const EngineView &v, const double *tab, int bp, int kp, int npk,
-                                                      R *acc) {
+                                                      R *acc, int lg = 0) {
+  if (lg > 0) {
+    accumulate_primitives_grouped<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, npk, acc, lg);
+    return;
+  }
   constexpr int LTOT = LA + LB + LC + LD;
   using Cls = EriClass<LA, LB, LC, LD, REF>;
   const int offb = v.pair_prim_off[bp], npb = v.pair_nprim[bp];
@@ -181,13 +237,14 @@ __device__ __forceinline__ void accumulate_primitives(const EngineView &v, const
 // yields an all-zero block (inactive lanes).  R is the arithmetic type
 // (see accumulate_primitives).
 template <int LA, int LB, int LC, int LD, bool REF, class R = double>
-__device__ __forceinline__ void quartet_block(const EngineView &v, const double *tab, int bp, int kp, int npk, R *out) {
+__device__ __forceinline__ void quartet_block(const EngineView &v, const double *tab, int bp, int kp, int npk, R *out,
+                                              int lg = 0) {
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   using Cls = EriClass<LA, LB, LC, LD, REF>;
   R acc[Cls::kAcc];
 #pragma unroll
   for (int x = 0; x < Cls::kAcc; ++x) acc[x] = R(0);
-  accumulate_primitives<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, npk, acc);
+  accumulate_primitives<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, npk, acc, lg);
   Cls::template hrr<R>(out, acc, R(v.pair_AB[3 * bp]), R(v.pair_AB[3 * bp + 1]), R(v.pair_AB[3 * bp + 2]),
                        R(v.pair_AB[3 * kp]), R(v.pair_AB[3 * kp + 1]), R(v.pair_AB[3 * kp + 2]));
   constexpr int U = kUnrollBlock<NA * NB * NC * ND>;
@@ -222,7 +279,7 @@ __device__ __forceinline__ float density_bound(const EngineView &v, int bp, int 
 // the kept quartets per precision.
 template <int SCR>
 __device__ __forceinline__ bool screen_task(const EngineView &v, const ClassLaunch &cl, int bp, int kp, bool active,
-                                            bool *keep, bool *fp64) {
+                                            bool *keep, bool *fp64, bool leader = true) {
   const float bnd = active ? density_bound(v, bp, kp) : 0.0f;
   const bool k = active && bnd >= cl.dens_threshold;
   *keep = k;
@@ -236,7 +293,8 @@ __device__ __forceinline__ bool screen_task(const EngineView &v, const ClassLaun
     hi = m >= cl.mixed_cutoff;
   }
   *fp64 = hi;
-  if ((threadIdx.x & 31) == 0 && cl.counters) atomicAdd(&cl.counters[hi ? 0 : 1], (unsigned long long)__popc(kept));
+  const unsigned counted = __ballot_sync(0xffffffffu, k && leader);  // one lane per quartet
+  if ((threadIdx.x & 31) == 0 && cl.counters) atomicAdd(&cl.counters[hi ? 0 : 1], (unsigned long long)__popc(counted));
   return true;
 }
 
@@ -282,11 +340,11 @@ static __device__ __noinline__ void dddd_reference_values(const EngineView &v, c
 
 template <int LA, int LB, int LC, int LD, bool REF, class R>
 __device__ __forceinline__ void quartet_values(const EngineView &v, const double *tab, int bp, int kp, int npk,
-                                               R *out) {
+                                               R *out, int lg) {
   if constexpr (REF && LA == 2 && LB == 2 && LC == 2 && LD == 2) {
-    dddd_reference_values<R>(v, tab, bp, kp, npk, out);
+    dddd_reference_values<R>(v, tab, bp, kp, npk, out);  // single-quartet queries only: lg == 0
   } else {
-    quartet_block<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, npk, out);
+    quartet_block<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, npk, out, lg);
   }
 }
 
@@ -305,7 +363,8 @@ __global__ void __launch_bounds__(32 * fused_warps(LA, LB, LC, LD), fused_min_bl
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  for (int t = blockIdx.x * kW + warp; t < cl.ntasks; t += gridDim.x * kW) {
+  const int ntasks = launch_ntasks(cl);
+  for (int t = first_task(cl, blockIdx.x * kW + warp); t < ntasks; t = next_task(cl, t, gridDim.x * kW)) {
     const Task task = launch_task(cl, t);
     const int bp = cl.bra_list[task.bra_pos];
     // the task's molecule (batched contexts): its matrices and size
@@ -316,27 +375,32 @@ __global__ void __launch_bounds__(32 * fused_warps(LA, LB, LC, LD), fused_min_bl
     const double *Dt = cl.Dt ? cl.Dt + mv.base : nullptr;
     double *Jm = cl.J ? cl.J + mv.base : nullptr, *Kam = cl.Ka ? cl.Ka + mv.base : nullptr;
     double *Kbm = cl.Kb ? cl.Kb + mv.base : nullptr;
-    const int kpos = task.ket_start + lane;
+    // 2^lg lanes per quartet (lg warp-uniform): lane group `lane >> lg`
+    // takes that ket of the task, and only its first lane digests the result
+    const int lg = task.lg;
+    const int gl = lane & ((1 << lg) - 1);
+    const int kpos = task.ket_start + (lane >> lg);
     bool active = kpos < task.ket_end;
     const int kp = active ? cl.ket_list[kpos] : bp;
     bool fp64 = true;
     if constexpr (SCR != kScreenNone) {
       bool keep;
-      if (!screen_task<SCR>(v, cl, bp, kp, active, &keep, &fp64)) continue;  // warp-uniform
+      if (!screen_task<SCR>(v, cl, bp, kp, active, &keep, &fp64, gl == 0)) continue;  // warp-uniform
       active = keep;
     }
     const int npk = active ? v.pair_nprim[kp] : 0;
 
     double out[N];
     if (SCR != kScreenMixed || fp64) {
-      quartet_values<LA, LB, LC, LD, REF, double>(v, tab, bp, kp, npk, out);
+      quartet_values<LA, LB, LC, LD, REF, double>(v, tab, bp, kp, npk, out, lg);
     } else if constexpr (SCR == kScreenMixed) {
       // FP32 evaluation, FP64 from here on (digestion, accumulation)
       float o32[N];
-      quartet_values<LA, LB, LC, LD, REF, float>(v, tab, bp, kp, npk, o32);
+      quartet_values<LA, LB, LC, LD, REF, float>(v, tab, bp, kp, npk, o32, lg);
 #pragma unroll kUnrollBlock<N>
       for (int x = 0; x < N; ++x) out[x] = (double)o32[x];
     }
+    active = active && gl == 0;
     // blocks above 81 integrals live in local memory anyway: keep their
     // epilogue loops rolled (code size, compile time)
     constexpr int U = kUnrollBlock<NA * NB * NC * ND>;

@@ -127,7 +127,7 @@ __device__ __forceinline__ void warp_contract(const EngineView &v, int bp, int k
       const double roz = rho * pb.inv_zeta, ie = pk.inv_zeta;
       const R PA0 = R(pb.PAx), PA1 = R(pb.PAy), PA2 = R(pb.PAz);
       const R WP0 = R(-roz * PQx), WP1 = R(-roz * PQy), WP2 = R(-roz * PQz);
-      const R oo2z = R(0.5 * pb.inv_zeta), oo2z_roz = R(0.5 * pb.inv_zeta * roz);
+      const R oo2z = R(0.5 * pb.inv_zeta), mroz = R(-roz);
       const R DL0 = R(-(pb.bABx + pk.bABx) * ie), DL1 = R(-(pb.bABy + pk.bABy) * ie), DL2 = R(-(pb.bABz + pk.bABz) * ie);
       const R mzoe = R(-pb.zeta * ie), oo2e = R(0.5 * ie);
 #pragma unroll
@@ -147,11 +147,15 @@ __device__ __forceinline__ void warp_contract(const EngineView &v, int bp, int k
           const R pa = dir == 0 ? PA0 : dir == 1 ? PA1 : PA2;
           const R wp = dir == 0 ? WP0 : dir == 1 ? WP1 : WP2;
           const R dl = dir == 0 ? DL0 : dir == 1 ? DL1 : DL2;
+          // vertical: PA a + WP b + n1 oo2z (c - roz d)
+          // transfer: delta a - zoe b + oo2e (n1 c + n2 d)
+          // (the class kernels' association: the pair difference is formed
+          // before its prefactor, so near-cancelling terms keep their bits)
           const R c1 = et ? dl : pa;
           const R c2 = et ? mzoe : wp;
-          const R c3 = n1 * (et ? oo2e : oo2z);
-          const R c4 = et ? n2 * oo2e : -n1 * oo2z_roz;
-          w[x & 0xffff] = c1 * a + c2 * b + c3 * c + c4 * d;
+          const R c3 = et ? oo2e : n1 * oo2z;
+          const R t = (et ? n1 : R(1)) * c + (et ? n2 : mroz) * d;
+          w[x & 0xffff] = c1 * a + c2 * b + c3 * t;
         }
         __syncwarp();
       }
@@ -239,8 +243,10 @@ __global__ void __launch_bounds__(32 * WarpShape<LA, LB, LC, LD, REF>::kWarps)
   double *base = warp_smem + (size_t)warp * (S::kBytes / 8);
   double *o = base + S::kRDoubles;
   unsigned long long n64 = 0, n32 = 0;
-  const long long nunits = (long long)cl.ntasks * 32;
-  for (long long u = (long long)blockIdx.x * S::kWarps + warp; u < nunits; u += (long long)gridDim.x * S::kWarps) {
+  const long long nunits = (long long)launch_ntasks(cl) * 32;
+  const long long ustride = (long long)gridDim.x * S::kWarps;
+  for (long long u = cl.queue ? warp_fetch(cl.queue, 1) : (long long)blockIdx.x * S::kWarps + warp; u < nunits;
+       u = cl.queue ? warp_fetch(cl.queue, 1) : u + ustride) {
     const Task task = launch_task(cl, (int)(u >> 5));
     const int kpos = task.ket_start + (int)(u & 31);
     if (kpos >= task.ket_end) continue;  // warp-uniform

@@ -678,11 +678,10 @@ def emit_split(out_dir):
 # pruning as ClassGen) become a list of operations ordered by dependency
 # depth; the warp's lanes run the operations of one depth level side by side
 # on intermediates held in shared memory, with a warp barrier between levels.
-# Every operation has the form
-#   out = c1 * w[a] + c2 * w[b] + c3 * w[c] + c4 * w[d]
-# with per-primitive coefficients selected by kind and Cartesian direction:
-#   vertical (kind 0):  PA_i, WP_i,    n1 * oo2z, -n1 * oo2z * roz
-#   transfer (kind 1):  delta_i, -zoe, n1 * oo2e,  n2 * oo2e
+# Every operation has one of the two forms
+#   vertical (kind 0):  out = PA_i w[a] + WP_i w[b] + n1 oo2z (w[c] - roz w[d])
+#   transfer (kind 1):  out = delta_i w[a] - zoe w[b] + oo2e (n1 w[c] + n2 w[d])
+# with per-primitive coefficients selected by kind and Cartesian direction.
 # Absent operands read slot 0, which always holds zero.  Slots are assigned
 # by a liveness scan (a slot is reused from the level after its last read),
 # so the shared-memory footprint is the peak live set, not the node count.
@@ -852,48 +851,61 @@ def emit_warp(out_dir):
     hdr += ["", "}  // namespace hfg", ""]
     with open(os.path.join(out_dir, "eri_warp_gen.cuh"), "w") as fh:
         fh.write("\n".join(hdr) + "\n")
+    # one translation unit per (class, mode) and precision variant, so the
+    # large classes' instantiations compile in parallel; launch_warp_<tag>
+    # dispatches on the mode and the precision form
     modes = ("kStorePacked", "kJkRhf", "kJkUhf")
+    decls = []
     for (a, b, c, d) in quartets:
         if not is_split_class(a, b, c, d):
             continue
         has_ref = (c + d) >= a + 2
         tag = f"{a}{b}{c}{d}"
-        for scr in (False, True):
-            name = f"launch_warp_{tag}" + ("_scr" if scr else "")
-            lines = [f"// Generated by gen_eri.py: warp-cooperative launchers for the ({a}{b}|{c}{d}) class"
-                     + (" (density-screened J/K)." if scr else "."),
+        parts = [(m, False) for m in modes] + [(m, True) for m in ("kJkRhf", "kJkUhf")]
+        for mode, scr in parts:
+            fn = f"launch_warp_{tag}_{'s' if scr else 'm'}{modes.index(mode)}"
+            decls.append(f"void {fn}(const EngineView &v, const ClassLaunch &cl, bool ref, int prec, int grid, "
+                         "cudaStream_t s);")
+            lines = [f"// Generated by gen_eri.py: warp-cooperative ({a}{b}|{c}{d}) kernels, mode {mode}"
+                     + (", density-screened." if scr else "."),
                      '#include "eri_warp.cuh"', '#include "eri_warp_dispatch.cuh"', "", "namespace hfg {", "",
-                     f"void {name}(const EngineView &v, const ClassLaunch &cl, int mode, bool ref, int prec, int grid,",
-                     "             cudaStream_t s) {"]
-            if not scr:
-                lines += ["  if (prec != 0 && (mode == kJkRhf || mode == kJkUhf)) {",
-                          f"    launch_warp_{tag}_scr(v, cl, mode, ref, prec, grid, s);", "    return;", "  }"]
-            lines.append("  switch (mode) {")
-            for mode in (("kJkRhf", "kJkUhf") if scr else modes):
-                lines.append(f"    case {mode}:")
-                variants = [("kScreenMixed", "prec == 2"), ("kScreenFp64", None)] if scr else [("kScreenNone", None)]
-                for r in ((True, False) if has_ref else (False,)):
-                    cond = "ref" if (has_ref and r) else ("!ref" if has_ref else None)
-                    for sv, pc in variants:
-                        conds = " && ".join(x for x in (cond, pc) if x)
-                        call = f"launch_warp<{a}, {b}, {c}, {d}, {mode}, {'true' if r else 'false'}, {sv}>(v, cl, grid, s);"
-                        if conds:
-                            lines.append(f"      if ({conds}) {{ {call} break; }}")
-                        else:
-                            lines.append(f"      {call}")
-                lines.append("      break;")
-            lines += ["    default:", "      break;", "  }"]
+                     f"void {fn}(const EngineView &v, const ClassLaunch &cl, bool ref, int prec, int grid, "
+                     "cudaStream_t s) {"]
+            variants = [("kScreenMixed", "prec == 2"), ("kScreenFp64", None)] if scr else [("kScreenNone", None)]
+            for r in ((True, False) if has_ref else (False,)):
+                cond = "ref" if (has_ref and r) else ("!ref" if has_ref else None)
+                for sv, pc in variants:
+                    conds = " && ".join(x for x in (cond, pc) if x)
+                    call = f"launch_warp<{a}, {b}, {c}, {d}, {mode}, {'true' if r else 'false'}, {sv}>(v, cl, grid, s);"
+                    lines.append(f"  if ({conds}) {{ {call} return; }}" if conds else f"  {call}")
             lines += ["  (void)ref;", "  (void)prec;", "}", "", "}  // namespace hfg", ""]
-            with open(os.path.join(out_dir, f"eri_warp_{tag}" + ("_scr" if scr else "") + ".cu"), "w") as fh:
+            with open(os.path.join(out_dir, f"eri_warp_{tag}_{'s' if scr else 'm'}{modes.index(mode)}.cu"), "w") as fh:
                 fh.write("\n".join(lines))
+        lines = [f"// Generated by gen_eri.py: warp-cooperative launcher of the ({a}{b}|{c}{d}) class.",
+                 '#include "eri_warp_dispatch.cuh"', "", "namespace hfg {", "",
+                 f"void launch_warp_{tag}(const EngineView &v, const ClassLaunch &cl, int mode, bool ref, int prec, "
+                 "int grid, cudaStream_t s) {",
+                 "  const bool scr = prec != 0 && (mode == kJkRhf || mode == kJkUhf);",
+                 "  switch (mode) {"]
+        for k, mode in enumerate(modes):
+            lines.append(f"    case {mode}:")
+            if mode == "kStorePacked":
+                lines.append(f"      launch_warp_{tag}_m{k}(v, cl, ref, prec, grid, s);")
+            else:
+                lines.append(f"      if (scr) launch_warp_{tag}_s{k}(v, cl, ref, prec, grid, s);")
+                lines.append(f"      else launch_warp_{tag}_m{k}(v, cl, ref, prec, grid, s);")
+            lines.append("      break;")
+        lines += ["    default:", "      break;", "  }", "}", "", "}  // namespace hfg", ""]
+        with open(os.path.join(out_dir, f"eri_warp_{tag}.cu"), "w") as fh:
+            fh.write("\n".join(lines))
     lines = ["// Generated by gen_eri.py: warp-cooperative launcher table.", "#pragma once",
              '#include "hfg_internal.cuh"', "", "namespace hfg {", "",
              "using WarpLauncher = void (*)(const EngineView &, const ClassLaunch &, int, bool, int, int, cudaStream_t);"]
+    lines += decls
     for (a, b, c, d) in quartets:
         if is_split_class(a, b, c, d):
-            for suf in ("", "_scr"):
-                lines.append(f"void launch_warp_{a}{b}{c}{d}{suf}(const EngineView &v, const ClassLaunch &cl, int mode, "
-                             "bool ref, int prec, int grid, cudaStream_t s);")
+            lines.append(f"void launch_warp_{a}{b}{c}{d}(const EngineView &v, const ClassLaunch &cl, int mode, "
+                         "bool ref, int prec, int grid, cudaStream_t s);")
     lines.append("")
     lines.append("// warp-cooperative launcher per class (same order as kClasses), nullptr for per-thread classes")
     lines.append("static const WarpLauncher kWarp[] = {")

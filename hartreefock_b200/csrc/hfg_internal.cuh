@@ -111,10 +111,14 @@ __device__ __forceinline__ MolView task_molecule(const EngineView &v, int bp) {
 
 // One unit of work: a bra pair position in the class's pair list and a
 // range of at most 32 ket positions (kets of one primitive-count bucket).
-struct Task {
+// lg: the thread-per-quartet kernels give each quartet 2^lg lanes, which
+// split its primitive quartets and sum them with warp shuffles (tasks with
+// fewer kets than lanes, and long contractions); 0 = one lane per quartet.
+struct __align__(16) Task {
   int bra_pos;
   int ket_start;
   int ket_end;
+  int lg = 0;
 };
 
 struct ClassLaunch {
@@ -136,11 +140,35 @@ struct ClassLaunch {
   float dens_threshold;  // skip quartets whose density-weighted bound is below
   float mixed_cutoff;    // tasks whose largest bound is below run in FP32
   unsigned long long *counters;  // [0] FP64, [1] FP32 quartets evaluated
+  // device work queue (batched builds without host synchronisation): the
+  // task count lives in device memory (written by the compaction of the
+  // active molecules' tasks) and warps take the next task from an atomic
+  // counter that starts at 0; null = ntasks above, static grid-stride order
+  const int *ntasks_dev;
+  int *queue;
 };
 
 // task t of a launch (shards take every task_stride-th task of the class)
 __device__ __forceinline__ Task launch_task(const ClassLaunch &cl, int t) {
   return cl.tasks[cl.task_offset + (long long)t * cl.task_stride];
+}
+
+// Tasks of the launch: the device count when the queue is on.
+__device__ __forceinline__ int launch_ntasks(const ClassLaunch &cl) {
+  return cl.ntasks_dev ? *cl.ntasks_dev : cl.ntasks;
+}
+// A warp's first task and its next one after t: the grid-stride order
+// (start, start + stride, ...) or, with the queue, one atomic per warp.
+__device__ __forceinline__ int warp_fetch(int *queue, int step) {
+  int t = 0;
+  if ((threadIdx.x & 31) == 0) t = atomicAdd(queue, step);
+  return __shfl_sync(0xffffffffu, t, 0);
+}
+__device__ __forceinline__ int first_task(const ClassLaunch &cl, int start) {
+  return cl.queue ? warp_fetch(cl.queue, 1) : start;
+}
+__device__ __forceinline__ int next_task(const ClassLaunch &cl, int t, int stride) {
+  return cl.queue ? warp_fetch(cl.queue, 1) : t + stride;
 }
 
 // One chunk of a split-path class launch (see eri_split.cuh): scratch for

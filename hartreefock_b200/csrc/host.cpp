@@ -537,6 +537,11 @@ namespace HartreeFock {
 
 using hfgpu::Matrix;
 
+namespace {
+// throws std::runtime_error with the engine's message unless st is HFG_OK
+void check_engine(hfg_status st, const char *what);
+}  // namespace
+
 // Constants.h:6-10
 constexpr double kEnergyConvergenceDIIS = 1E-11;
 constexpr double kEnergyConvergence = 1E-13;
@@ -579,6 +584,10 @@ void HartreeFockAlgorithm::Init(Systems::Molecule *molecule) {
     integralsRepository.CalculateElectronElectronIntegrals();
   else
     integralsRepository.engine();
+  if (shardCount > 1) {
+    if (!allReduce) throw std::invalid_argument("sharded SCF without an all-reduce of G");
+    check_engine(hfg_set_shard(integralsRepository.engine(), shardRank, shardCount), "hfg_set_shard");
+  }
   // V = S^-1/2 = U s^-1/2 U^T, symmetrised (HartreeFockAlgorithm.cpp:48-59)
   std::vector<double> w;
   Matrix U;
@@ -940,6 +949,7 @@ double RestrictedHartreeFock::Step(int iter) {
     const auto t0 = std::chrono::steady_clock::now();
     check_engine(hfg_fock_rhf_device(integralsRepository.engine(), d.density(0), d.g_buffer(0), d.stream()),
                  "hfg_fock_rhf_device");
+    if (shardCount > 1) allReduce(d.g_buffer(0), (size_t)numberOfOrbitals * numberOfOrbitals, d.stream());
     AccountDevice(std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
     d.FockFromG(0, d.g_buffer(0), true);
   }
@@ -985,8 +995,7 @@ hfgpu::Vector3D UnrestrictedHartreeFock::GetMoment() const {
 double UnrestrictedHartreeFock::CalculateMp2Energy() {
   const int n = numberOfOrbitals;
   if (!inited || (int)Cplus.rows() != n || (int)Cminus.rows() != n || (int)eigenvalsplus.size() != n ||
-      (int)eigenvalsminus.size() != n || nrOccupiedLevelsPlus >= (unsigned)n || nrOccupiedLevelsMinus < 1 ||
-      nrOccupiedLevelsMinus > nrOccupiedLevelsPlus)
+      (int)eigenvalsminus.size() != n)
     return mp2Energy = 0;
   check_engine(hfg_mp2_uhf(integralsRepository.engine(), Cplus.data(), eigenvalsplus.data(),
                            (int32_t)nrOccupiedLevelsPlus, Cminus.data(), eigenvalsminus.data(),
@@ -1057,6 +1066,10 @@ double UnrestrictedHartreeFock::Step(int iter) {
     check_engine(hfg_fock_uhf_device(integralsRepository.engine(), d.density(0), d.density(1), d.g_buffer(0),
                                      d.g_buffer(1), d.stream()),
                  "hfg_fock_uhf_device");
+    if (shardCount > 1) {
+      allReduce(d.g_buffer(0), (size_t)numberOfOrbitals * numberOfOrbitals, d.stream());
+      allReduce(d.g_buffer(1), (size_t)numberOfOrbitals * numberOfOrbitals, d.stream());
+    }
     AccountDevice(std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
     d.FockFromG(0, d.g_buffer(0), false);
     d.FockFromG(1, d.g_buffer(1), false);
@@ -1151,6 +1164,14 @@ hfg_status run_scf(const char *basis_path, int32_t natoms, const int32_t *Z, con
     algo->incrementalFock = opts->incremental != 0;
     algo->traceIterations = opts->trace != 0;
     algo->concurrentClasses = opts->concurrent_classes >= 1;
+    if (opts->shard_count > 1) {
+      if (!opts->allreduce) throw std::invalid_argument("shard_count > 1 needs an allreduce callback");
+      algo->shardRank = opts->shard_rank;
+      algo->shardCount = opts->shard_count;
+      const hfd_allreduce_fn fn = opts->allreduce;
+      void *user = opts->allreduce_user;
+      algo->allReduce = [fn, user](double *g, size_t count, void *stream) { fn(g, (int64_t)count, stream, user); };
+    }
     algo->cudaGraphs = opts->concurrent_classes >= 2;
     // the hook sees the terminate flag for the algorithm's whole life
     struct Publish {

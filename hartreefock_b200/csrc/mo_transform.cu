@@ -43,14 +43,14 @@ __global__ void unpack_eri(const double *__restrict__ packed, double *__restrict
   }
 }
 
-// K[(l s),(j b)] = C[l][i0+j] C[s][a0+b], C row-major n x n (AO rows, MO columns)
-__global__ void pair_coefficients(const double *__restrict__ C, int n, int i0, int ni, int a0, int na,
-                                  double *__restrict__ K) {
-  const long long ov = (long long)ni * na, total = (long long)n * n * ov;
+// K[(l s),(j b)] = Cj[l][j0+j] Cb[s][b0+b], Cj and Cb row-major n x n
+__global__ void pair_coefficients(const double *__restrict__ Cj, int j0, int nj, const double *__restrict__ Cb, int b0,
+                                  int nb, int n, double *__restrict__ K) {
+  const long long ov = (long long)nj * nb, total = (long long)n * n * ov;
   for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total; x += (long long)gridDim.x * blockDim.x) {
     const long long r = x / ov, c = x - r * ov;
-    const int l = (int)(r / n), s = (int)(r - (long long)l * n), j = (int)(c / na), b = (int)(c - (long long)j * na);
-    K[x] = C[(long long)l * n + i0 + j] * C[(long long)s * n + a0 + b];
+    const int l = (int)(r / n), s = (int)(r - (long long)l * n), j = (int)(c / nb), b = (int)(c - (long long)j * nb);
+    K[x] = Cj[(long long)l * n + j0 + j] * Cb[(long long)s * n + b0 + b];
   }
 }
 
@@ -162,16 +162,21 @@ hfg_status prepare(hfg_ctx *ctx, long long ov_max, cudaStream_t s, Buffers &buf,
   return HFG_OK;
 }
 
-// X[(i a),(j b)] = (i a | j b) with the bra pair's orbitals from C1 (i in
-// [i0, i0+ni), a in [a0, a0+na)) and the ket pair's from C2 (j in [j0, j0+nj),
-// b in [b0, b0+nb)); C1, C2 row-major n x n (AO rows, MO columns).
-hfg_status block(MoTables &t, const double *C1, int i0, int ni, int a0, int na, const double *C2, int j0, int nj,
-                 int b0, int nb, double *dX, cudaStream_t s, const char *who) {
+// One orbital index range of a transformed block: columns [first, first+count)
+// of the coefficient matrix C (row-major n x n, AO rows, MO columns).
+struct Range {
+  const double *C;
+  int first, count;
+};
+
+// X[(i a),(j b)] = (i a | j b), each of the four indices over its own range
+// and coefficient matrix.
+hfg_status block(MoTables &t, Range i, Range a, Range j, Range b, double *dX, cudaStream_t s, const char *who) {
   const int n = t.n;
-  const long long nn = (long long)n * n, ov1 = (long long)ni * na, ov2 = (long long)nj * nb;
+  const long long nn = (long long)n * n, ov1 = (long long)i.count * a.count, ov2 = (long long)j.count * b.count;
   if (ov1 > t.cap || ov2 > t.cap) return hfg::fail_external(HFG_INVALID_ARG, std::string(who) + ": block size");
-  pair_coefficients<<<grid_for(nn * ov1), 256, 0, s>>>(C1, n, i0, ni, a0, na, t.K1);
-  pair_coefficients<<<grid_for(nn * ov2), 256, 0, s>>>(C2, n, j0, nj, b0, nb, t.K2);
+  pair_coefficients<<<grid_for(nn * ov1), 256, 0, s>>>(i.C, i.first, i.count, a.C, a.first, a.count, n, t.K1);
+  pair_coefficients<<<grid_for(nn * ov2), 256, 0, s>>>(j.C, j.first, j.count, b.C, b.first, b.count, n, t.K2);
   const double one = 1.0, zero = 0.0;
   // row-major Y = M K2  <=>  column-major Y^T = K2^T M^T
   if (cublasDgemm(t.blas.h, CUBLAS_OP_N, CUBLAS_OP_N, (int)ov2, (int)nn, (int)nn, &one, t.K2, (int)ov2, t.M, (int)nn,
@@ -200,7 +205,7 @@ hfg_status transform(hfg_ctx *ctx, const double *dC, int i0, int ni, int a0, int
   MoTables t;
   hfg_status st = prepare(ctx, (long long)ni * na, s, buf, t, "hfg_mo_eri_ovov");
   if (st != HFG_OK) return st;
-  st = block(t, dC, i0, ni, a0, na, dC, i0, ni, a0, na, dX, s, "hfg_mo_eri_ovov");
+  st = block(t, {dC, i0, ni}, {dC, a0, na}, {dC, i0, ni}, {dC, a0, na}, dX, s, "hfg_mo_eri_ovov");
   if (st != HFG_OK) return st;
   return finish(s, "hfg_mo_eri_ovov");
 }
@@ -246,23 +251,38 @@ extern "C" hfg_status hfg_mp2_rhf(hfg_ctx *ctx, const double *C, const double *e
 // through one MolecularOrbitalsIntegralsRepository whose four caches are
 // keyed by orbital indices only (IntegralsRepository.h:190-291), so the
 // second sum reuses values the first one cached with the other spin's
-// coefficients.  With n+ >= n- occupied (occupied- within occupied+), the
-// quartet (i a | j b) of the second sum is therefore
-//   all C+                 when a and b are virtual in both spins,
-//   (i- a- | j+ b+)        when a is occupied+ only and b virtual+,
-//   all C-                 when b is occupied+ only,
-// with the second spin's orbital energies throughout; this reproduces it.
+// coefficients.  The first sum leaves, with n+ occupied+ orbitals,
+//   level 1 (m n | l b~)     for b virtual+            (b transformed)
+//   level 2 (m n | j~ b~)    for j occupied+, b virtual+
+//   level 3 (m a~ | j~ b~)   for a virtual+ too
+//   level 4 (i~ a~ | j~ b~)  for i occupied+ too
+// (~ = with C+).  In the second sum each quartet takes the deepest cached
+// level, so index b is transformed with C+ when b is virtual+, j with C+
+// when also j is occupied+, a when also a is virtual+, i when also i is
+// occupied+, and every other index with C-; the orbital energies are the
+// second spin's throughout.  The blocks below partition the second sum's
+// (i, a, j, b) ranges by that rule, for n+ >= n- (the reference's default
+// occupation of Molecule::Init gives n+ = n- or n- = n+ + 1 -- the beta
+// spin holds the odd electron) and for n+ < n- alike.
+namespace {
+
+struct Mp2Block {
+  Range i, a, j, b;
+};
+
+}  // namespace
+
 extern "C" hfg_status hfg_mp2_uhf(hfg_ctx *ctx, const double *Cp, const double *ep, int32_t np, const double *Cm,
                                   const double *em, int32_t nm, double *e_mp2) {
   const char *who = "hfg_mp2_uhf";
   if (!ctx || !Cp || !ep || !Cm || !em || !e_mp2) return hfg::fail_external(HFG_INVALID_ARG, "hfg_mp2_uhf: arguments");
   const int n = hfg_ctx_nbf(ctx);
-  if (n <= 0 || np < 1 || nm < 1 || np >= n || nm > np)
-    return hfg::fail_external(HFG_INVALID_ARG, "hfg_mp2_uhf: occupied counts (need 1 <= n- <= n+ < nbf)");
-  const int vp = n - np, vm = n - nm, ns = np - nm;
+  if (n <= 0 || np < 0 || nm < 0 || np > n || nm > n)
+    return hfg::fail_external(HFG_INVALID_ARG, "hfg_mp2_uhf: occupied counts (need 0 <= n+, n- <= nbf)");
+  const int vp = n - np, vm = n - nm, lo = std::min(np, nm), hi = std::max(np, nm);
   Buffers buf;
   double *dCp = nullptr, *dCm = nullptr, *dEp = nullptr, *dEm = nullptr, *dX = nullptr, *dOut = nullptr;
-  const long long ovmax = std::max<long long>((long long)np * vp, (long long)nm * vm);
+  const long long ovmax = std::max<long long>(1, std::max<long long>((long long)np * vp, (long long)nm * vm));
   cudaError_t e = buf.get(&dCp, (size_t)n * n);
   if (e == cudaSuccess) e = buf.get(&dCm, (size_t)n * n);
   if (e == cudaSuccess) e = buf.get(&dEp, (size_t)n);
@@ -280,22 +300,29 @@ extern "C" hfg_status hfg_mp2_uhf(hfg_ctx *ctx, const double *Cp, const double *
   MoTables t;
   hfg_status st = prepare(ctx, ovmax, s, buf, t, who);
   if (st != HFG_OK) return st;
-  // S+: (ia|jb) with C+, i, j < n+, a, b >= n+
-  if ((st = block(t, dCp, 0, np, np, vp, dCp, 0, np, np, vp, dX, s, who)) != HFG_OK) return st;
-  const long long ovp = (long long)np * vp;
-  mp2_sum_sq<<<grid_for(ovp * ovp), 256, 0, s>>>(dX, ovp, np, vp, np, vp, dEp, dEp + np, dEp, dEp + np, dOut);
-  // S-, a and b virtual in both spins: the C+ block above, i, j < n-, with e-
-  mp2_sum_sq<<<grid_for((long long)nm * vp * nm * vp), 256, 0, s>>>(dX, ovp, nm, vp, nm, vp, dEm, dEm + np, dEm,
-                                                                   dEm + np, dOut);
-  if (ns > 0) {
-    // S-, a occupied+ only, b virtual+: (i- a- | j+ b+)
-    if ((st = block(t, dCm, 0, nm, nm, ns, dCp, 0, nm, np, vp, dX, s, who)) != HFG_OK) return st;
-    mp2_sum_sq<<<grid_for((long long)nm * ns * nm * vp), 256, 0, s>>>(dX, (long long)nm * vp, nm, ns, nm, vp, dEm,
-                                                                     dEm + nm, dEm, dEm + np, dOut);
-    // S-, b occupied+ only, any virtual- a: all C-
-    if ((st = block(t, dCm, 0, nm, nm, vm, dCm, 0, nm, nm, ns, dX, s, who)) != HFG_OK) return st;
-    mp2_sum_sq<<<grid_for((long long)nm * vm * nm * ns), 256, 0, s>>>(dX, (long long)nm * ns, nm, vm, nm, ns, dEm,
-                                                                     dEm + nm, dEm, dEm + nm, dOut);
+  // first sum: all C+, i, j < n+, a, b >= n+
+  std::vector<std::pair<Mp2Block, const double *>> blocks;
+  blocks.push_back({{{dCp, 0, np}, {dCp, np, vp}, {dCp, 0, np}, {dCp, np, vp}}, dEp});
+  // second sum, i, j < n-, a, b >= n-, partitioned by the cache rule above
+  const Range iAll{dCm, 0, nm}, aAll{dCm, nm, vm};
+  // b virtual+ (b >= max): j occupied+ (j < min) ...
+  //   ... a virtual+: i occupied+ from C+, i in [n+, n-) from C-
+  blocks.push_back({{{dCp, 0, lo}, {dCp, hi, n - hi}, {dCp, 0, lo}, {dCp, hi, n - hi}}, dEm});
+  if (nm > np) blocks.push_back({{{dCm, np, nm - np}, {dCp, hi, n - hi}, {dCp, 0, lo}, {dCp, hi, n - hi}}, dEm});
+  //   ... a in [n-, n+) occupied+ only: a and i from C-
+  if (np > nm) blocks.push_back({{iAll, {dCm, nm, np - nm}, {dCp, 0, lo}, {dCp, hi, n - hi}}, dEm});
+  // b virtual+, j in [n+, n-): j, a and i from C-
+  if (nm > np) blocks.push_back({{iAll, aAll, {dCm, np, nm - np}, {dCp, hi, n - hi}}, dEm});
+  // b in [n-, n+) occupied+ only: all C-
+  if (np > nm) blocks.push_back({{iAll, aAll, {dCm, 0, nm}, {dCm, nm, np - nm}}, dEm});
+  for (const auto &[q, eps] : blocks) {
+    if (q.i.count <= 0 || q.a.count <= 0 || q.j.count <= 0 || q.b.count <= 0) continue;
+    if ((st = block(t, q.i, q.a, q.j, q.b, dX, s, who)) != HFG_OK) return st;
+    const long long rows = (long long)q.i.count * q.a.count, cols = (long long)q.j.count * q.b.count;
+    // orbital energies of the sum's spin at the block's absolute orbital indices
+    mp2_sum_sq<<<grid_for(rows * cols), 256, 0, s>>>(dX, cols, q.i.count, q.a.count, q.j.count, q.b.count,
+                                                      eps + q.i.first, eps + q.a.first, eps + q.j.first,
+                                                      eps + q.b.first, dOut);
   }
   if ((st = finish(s, who)) != HFG_OK) return st;
   double sum = 0;
@@ -336,7 +363,7 @@ extern "C" hfg_status hfg_mo_eri_full(hfg_ctx *ctx, const double *dC, double *dX
   MoTables t;
   hfg_status st = prepare(ctx, (long long)n * n, s, buf, t, who);
   if (st != HFG_OK) return st;
-  if ((st = block(t, dC, 0, n, 0, n, dC, 0, n, 0, n, dX, s, who)) != HFG_OK) return st;
+  if ((st = block(t, {dC, 0, n}, {dC, 0, n}, {dC, 0, n}, {dC, 0, n}, dX, s, who)) != HFG_OK) return st;
   return finish(s, who);
 }
 

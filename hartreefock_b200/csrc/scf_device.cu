@@ -406,4 +406,87 @@ extern "C" hfg_status hfg_eigh_batched(const double *dA, double *dV, double *dW,
   }
 }
 
+// ---------------------------------------------------------------------------
+// hfg_pulay_solve_device (include/hfgpu.h): the DIIS system B c = (0 .. 0 1)
+// of every molecule of a batch, on the device, by the same column-pivoted
+// Householder QR with rank cut-off as the host SCF's solve
+// (hfgpu::detail::pulay_solve, the role of Eigen's colPivHouseholderQr at
+// DIIS.h:72).  One thread per system; systems up to kPulayMax unknowns.
+namespace {
+constexpr int kPulayMax = 8;
+__global__ void pulay_kernel(const double *__restrict__ B, int n, int batch, double *__restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= batch) return;
+  double A[kPulayMax * kPulayMax], b[kPulayMax], v[kPulayMax], z[kPulayMax];
+  int perm[kPulayMax];
+  for (int i = 0; i < n * n; ++i) A[i] = B[(size_t)t * n * n + i];
+  for (int i = 0; i < n; ++i) {
+    b[i] = i == n - 1 ? 1.0 : 0.0;
+    perm[i] = i;
+  }
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    double best = -1;
+    for (int j = k; j < n; ++j) {
+      double s = 0;
+      for (int i = k; i < n; ++i) s += A[i * n + j] * A[i * n + j];
+      if (s > best) {
+        best = s;
+        p = j;
+      }
+    }
+    if (p != k) {
+      for (int i = 0; i < n; ++i) {
+        const double x = A[i * n + k];
+        A[i * n + k] = A[i * n + p];
+        A[i * n + p] = x;
+      }
+      const int q = perm[k];
+      perm[k] = perm[p];
+      perm[p] = q;
+    }
+    double al = 0;
+    for (int i = k; i < n; ++i) al += A[i * n + k] * A[i * n + k];
+    al = sqrt(al);
+    if (al == 0) continue;
+    if (A[k * n + k] > 0) al = -al;
+    v[0] = A[k * n + k] - al;
+    for (int i = k + 1; i < n; ++i) v[i - k] = A[i * n + k];
+    double vn = 0;
+    for (int i = 0; i < n - k; ++i) vn += v[i] * v[i];
+    const double beta = vn > 0 ? 2.0 / vn : 0.0;
+    for (int j = k; j < n; ++j) {
+      double s = 0;
+      for (int i = k; i < n; ++i) s += v[i - k] * A[i * n + j];
+      s *= beta;
+      for (int i = k; i < n; ++i) A[i * n + j] -= s * v[i - k];
+    }
+    double s = 0;
+    for (int i = k; i < n; ++i) s += v[i - k] * b[i];
+    s *= beta;
+    for (int i = k; i < n; ++i) b[i] -= s * v[i - k];
+  }
+  const double tol = fabs(A[0]) * 1e-15 * n;
+  int rank = 0;
+  while (rank < n && fabs(A[rank * n + rank]) > tol) ++rank;
+  for (int i = 0; i < n; ++i) z[i] = 0.0;
+  for (int i = rank - 1; i >= 0; --i) {
+    double s = b[i];
+    for (int j = i + 1; j < rank; ++j) s -= A[i * n + j] * z[j];
+    z[i] = s / A[i * n + i];
+  }
+  for (int j = 0; j < n; ++j) out[(size_t)t * n + perm[j]] = z[j];
+}
+}  // namespace
+
+extern "C" hfg_status hfg_pulay_solve_device(const double *dB, int32_t m1, int32_t batch, double *dC, void *stream) {
+  if (!dB || !dC || m1 < 2 || m1 > kPulayMax || batch < 0)
+    return hfg::fail_external(HFG_INVALID_ARG, "hfg_pulay_solve_device: arguments (2 <= m1 <= 8)");
+  if (batch == 0) return HFG_OK;
+  pulay_kernel<<<(batch + 127) / 128, 128, 0, static_cast<cudaStream_t>(stream)>>>(dB, m1, batch, dC);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return hfg::fail_external(HFG_DEVICE_ERROR, cudaGetErrorString(e));
+  return HFG_OK;
+}
+
 extern "C" void hfg_release_thread(void) { g_eigh.release(); }

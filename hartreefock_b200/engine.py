@@ -26,9 +26,11 @@ EXPORTED = ["hfg_default_opts", "hfg_last_error", "hfg_device_count", "hfg_ctx_c
             "hfg_fock_rhf", "hfg_fock_uhf", "hfg_fock_rhf_device", "hfg_fock_uhf_device", "hfg_schwarz",
             "hfg_ctx_stats", "hfg_set_profiling", "hfg_class_profile", "hfg_measure_fp64_peak", "hfg_measure_fp32_peak",
             "hfg_fock_rhf_noalloc", "hfg_fock_reset", "hfg_set_mixed_cutoff", "hfg_set_incremental",
-            "hfg_set_shard", "hfg_batch_create", "hfg_batch_size", "hfg_batch_layout", "hfg_fock_rhf_batch_device",
-            "hfg_fock_uhf_batch_device", "hfg_eigh_batched", "hfg_one_electron",
-            "hfg_mo_eri_ovov", "hfg_mp2_rhf", "hfg_mp2_uhf", "hfg_mo_eri_full", "hfg_spin_orbital_eri", "hfg_autotune", "hfg_set_graphs", "hfg_set_streams",
+            "hfg_set_shard", "hfg_copy_device", "hfg_batch_create", "hfg_batch_size", "hfg_batch_layout", "hfg_fock_rhf_batch_device",
+            "hfg_fock_uhf_batch_device", "hfg_fock_rhf_batch_async", "hfg_fock_uhf_batch_async", "hfg_eigh_batched", "hfg_one_electron",
+            "hfg_pulay_solve_device", "hfg_mo_eri_ovov", "hfg_mp2_rhf", "hfg_mp2_uhf", "hfg_mo_eri_full", "hfg_spin_orbital_eri", "hfg_autotune", "hfg_autotune_tasks", "hfg_set_prim_target", "hfg_set_graphs",
+            "hfg_set_class_path", "hfg_autotune_paths", "hfg_shard_range",
+            "hfg_set_streams",
             "hfg_release_thread"]
 
 
@@ -107,7 +109,10 @@ def library(path: str = LIB_PATH):
     L.hfg_batch_layout.argtypes = [vp, vp, vp, ctypes.POINTER(i64)]
     L.hfg_fock_rhf_batch_device.argtypes = [vp, dp, dp, vp, vp]
     L.hfg_fock_uhf_batch_device.argtypes = [vp, dp, dp, dp, dp, vp, vp]
-    for name in ("hfg_batch_create", "hfg_batch_layout", "hfg_fock_rhf_batch_device", "hfg_fock_uhf_batch_device"):
+    L.hfg_fock_rhf_batch_async.argtypes = [vp, dp, dp, vp, vp]
+    L.hfg_fock_uhf_batch_async.argtypes = [vp, dp, dp, dp, dp, vp, vp]
+    for name in ("hfg_batch_create", "hfg_batch_layout", "hfg_fock_rhf_batch_device", "hfg_fock_uhf_batch_device",
+                 "hfg_fock_rhf_batch_async", "hfg_fock_uhf_batch_async"):
         getattr(L, name).restype = ctypes.c_int
     L.hfg_fock_rhf_noalloc.restype = ctypes.c_int
     L.hfg_set_profiling.argtypes = [vp, i32]
@@ -118,8 +123,13 @@ def library(path: str = LIB_PATH):
     L.hfg_set_mixed_cutoff.argtypes = [vp, ctypes.c_double]
     L.hfg_set_incremental.argtypes = [vp, i32]
     L.hfg_set_shard.argtypes = [vp, i32, i32]
+    L.hfg_shard_range.argtypes = [dp, ctypes.c_int64, i32, i32, ctypes.POINTER(ctypes.c_int64),
+                                  ctypes.POINTER(ctypes.c_int64)]
+    L.hfg_shard_range.restype = ctypes.c_int
     L.hfg_eigh_batched.argtypes = [dp, dp, dp, i32, i32, i32, vp]
     L.hfg_eigh_batched.restype = ctypes.c_int
+    L.hfg_pulay_solve_device.argtypes = [dp, i32, i32, dp, vp]
+    L.hfg_pulay_solve_device.restype = ctypes.c_int
     L.hfg_one_electron.argtypes = [ctypes.POINTER(hfg_shells), dp, dp, i32, i32, dp, dp, dp]
     L.hfg_one_electron.restype = ctypes.c_int
     L.hfg_mo_eri_ovov.argtypes = [vp, dp, i32, i32, i32, i32, dp, vp]
@@ -132,6 +142,14 @@ def library(path: str = LIB_PATH):
     L.hfg_spin_orbital_eri.restype = ctypes.c_int
     L.hfg_autotune.argtypes = [vp, dp, vp, i32, ctypes.POINTER(i32), vp]
     L.hfg_autotune.restype = ctypes.c_int
+    L.hfg_autotune_tasks.argtypes = [vp, dp, vp, i32, ctypes.POINTER(i32), vp]
+    L.hfg_autotune_tasks.restype = ctypes.c_int
+    L.hfg_set_prim_target.argtypes = [vp, i32]
+    L.hfg_set_prim_target.restype = ctypes.c_int
+    L.hfg_set_class_path.argtypes = [vp, i32, i32, i32, i32, i32]
+    L.hfg_set_class_path.restype = ctypes.c_int
+    L.hfg_autotune_paths.argtypes = [vp, dp, vp, i32, ctypes.POINTER(i32), vp]
+    L.hfg_autotune_paths.restype = ctypes.c_int
     L.hfg_set_graphs.argtypes = [vp, i32]
     L.hfg_set_graphs.restype = ctypes.c_int
     L.hfg_set_streams.argtypes = [vp, i32]
@@ -159,6 +177,17 @@ def _check(st):
 
 def _ptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def shard_range(cost_prefix, rank: int, count: int) -> tuple:
+    """Task range (first, n) of shard `rank` of `count` for tasks with
+    running cost `cost_prefix` (len = tasks + 1, starting at 0): the
+    partition the sharded builds use (hfg_shard_range; host only)."""
+    pre = np.ascontiguousarray(cost_prefix, dtype=np.float64)
+    first, n = ctypes.c_int64(), ctypes.c_int64()
+    _check(library().hfg_shard_range(_ptr(pre), len(pre) - 1, int(rank), int(count), ctypes.byref(first),
+                                     ctypes.byref(n)))
+    return first.value, n.value
 
 
 def measure_fp64_peak(device: int = 0) -> float:
@@ -214,6 +243,17 @@ def eigh_batched(A, method: int = 0):
                                       ctypes.c_void_p(w.data_ptr()), n, b, method,
                                       ctypes.c_void_p(_torch_stream())))
     return w, X.transpose(1, 2)
+
+
+def pulay_solve_device(B, out=None):
+    """DIIS solutions of a [batch, m1, m1] float64 CUDA tensor on torch's
+    current stream (hfg_pulay_solve_device); returns [batch, m1]."""
+    import torch
+    B = B.contiguous()
+    if out is None:
+        out = torch.empty(B.shape[0], B.shape[1], dtype=torch.float64, device=B.device)
+    _check(library().hfg_pulay_solve_device(B.data_ptr(), B.shape[1], B.shape[0], out.data_ptr(), _torch_stream()))
+    return out
 
 
 def default_opts() -> hfg_opts:
@@ -330,6 +370,40 @@ class Engine:
         """Pick each fused class's grid (blocks per SM) by timing it on the
         density P (numpy or torch CUDA tensor); returns {class: blocks/SM}."""
         return _autotune(self._h, P)
+
+    def autotune_tasks(self, P) -> dict:
+        """Pick each thread-per-quartet class's lane-group target (primitive
+        quartets per lane; 0 = one lane per quartet) by timing it on the
+        density P; returns {class: target}."""
+        import torch
+        dP = torch.as_tensor(np.asarray(P) if not isinstance(P, torch.Tensor) else P, dtype=torch.float64)
+        dP = dP.cuda().contiguous()
+        rec = np.zeros(5 * 32, dtype=np.int32)
+        n = ctypes.c_int32()
+        _check(library().hfg_autotune_tasks(self._h, ctypes.c_void_p(dP.data_ptr()), _ptr(rec), len(rec),
+                                            ctypes.byref(n), ctypes.c_void_p(_torch_stream())))
+        return {f"({r[0]}{r[1]}|{r[2]}{r[3]})": int(r[4]) for r in rec[:5 * n.value].reshape(-1, 5)}
+
+    def set_prim_target(self, target: int):
+        _check(library().hfg_set_prim_target(self._h, int(target)))
+
+    def set_class_path(self, cls: str, warp: bool):
+        """Kernel of a large class with two, e.g. cls="(22|22)": the
+        warp-cooperative kernel (warp=True) or the split path."""
+        la, lb, lc, ld = (int(ch) for ch in cls.strip("()").replace("|", ""))
+        _check(library().hfg_set_class_path(self._h, la, lb, lc, ld, int(bool(warp))))
+
+    def autotune_paths(self, P) -> dict:
+        """Time both kernels of every large class with two on the density P
+        and keep the faster; returns {class: "warp" | "split"}."""
+        import torch
+        dP = torch.as_tensor(np.asarray(P) if not isinstance(P, torch.Tensor) else P, dtype=torch.float64)
+        dP = dP.cuda().contiguous()
+        rec = np.zeros(5 * 32, dtype=np.int32)
+        n = ctypes.c_int32()
+        _check(library().hfg_autotune_paths(self._h, ctypes.c_void_p(dP.data_ptr()), _ptr(rec), len(rec),
+                                            ctypes.byref(n), ctypes.c_void_p(_torch_stream())))
+        return {f"({r[0]}{r[1]}|{r[2]}{r[3]})": ("warp" if r[4] else "split") for r in rec[:5 * n.value].reshape(-1, 5)}
 
     def mp2_rhf(self, C: np.ndarray, eps: np.ndarray, nocc: int) -> float:
         """RHF MP2 correlation energy (hfg_mp2_rhf) from MO coefficients C
@@ -460,6 +534,22 @@ class BatchEngine:
                                                    ctypes.c_void_p(G.data_ptr()), ap,
                                                    ctypes.c_void_p(_torch_stream())))
         return G
+
+    def fock_rhf_async(self, P, G, active_dev):
+        """fock_rhf with the active mask a uint8 CUDA tensor (nmol): no host
+        synchronisation, capturable in a CUDA graph after a first call."""
+        _check(library().hfg_fock_rhf_batch_async(self._h, ctypes.c_void_p(P.data_ptr()),
+                                                  ctypes.c_void_p(G.data_ptr()),
+                                                  ctypes.c_void_p(active_dev.data_ptr()),
+                                                  ctypes.c_void_p(_torch_stream())))
+        return G
+
+    def fock_uhf_async(self, Pa, Pb, Ga, Gb, active_dev):
+        _check(library().hfg_fock_uhf_batch_async(self._h, ctypes.c_void_p(Pa.data_ptr()),
+                                                  ctypes.c_void_p(Pb.data_ptr()), ctypes.c_void_p(Ga.data_ptr()),
+                                                  ctypes.c_void_p(Gb.data_ptr()),
+                                                  ctypes.c_void_p(active_dev.data_ptr()),
+                                                  ctypes.c_void_p(_torch_stream())))
 
     def fock_uhf(self, Pa, Pb, Ga, Gb, active=None):
         import torch

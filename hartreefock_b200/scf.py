@@ -25,7 +25,12 @@ class hfd_scf_opts(ctypes.Structure):
                 ("incremental", ctypes.c_int32), ("trace", ctypes.c_int32),
                 ("stop_at_precision_test", ctypes.c_int32), ("max_iterations", ctypes.c_int32),
                 ("mp2", ctypes.c_int32), ("concurrent_classes", ctypes.c_int32),
-                ("electric_field", ctypes.c_double * 3)]
+                ("electric_field", ctypes.c_double * 3), ("shard_rank", ctypes.c_int32),
+                ("shard_count", ctypes.c_int32), ("allreduce", ctypes.c_void_p), ("allreduce_user", ctypes.c_void_p)]
+
+
+# hfd_allreduce_fn: (device G, count, stream, user)
+ALLREDUCE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p)
 
 
 class hfd_scf_result(ctypes.Structure):
@@ -59,6 +64,8 @@ def _lib():
         L.hfd_load_xyz.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]
         L.hfd_load_xyz.restype = ctypes.c_int
+        L.hfg_copy_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
+        L.hfg_copy_device.restype = ctypes.c_int
         L.hfd_pulay_solve.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p]
         L.hfd_pulay_solve.restype = ctypes.c_int
         L.hfd_release_thread.argtypes = []
@@ -105,15 +112,46 @@ def result_dict(r: hfd_scf_result) -> dict:
             "dipole": [r.dipole[0], r.dipole[1], r.dipole[2]]}
 
 
-def run_scf(Z, xyz, basis: str, unrestricted=False, want_density=True, **kw):
+def torch_allreduce(group=None):
+    """An hfd_allreduce_fn that sums G over a torch.distributed group: the
+    device buffer is copied into a torch tensor (through host memory for the
+    gloo backend), all-reduced and copied back."""
+    import torch
+    import torch.distributed as dist
+
+    def fn(dG, count, stream, user):
+        t = torch.empty(int(count), dtype=torch.float64, device="cuda")
+        E._check(_lib().hfg_copy_device(ctypes.c_void_p(t.data_ptr()), ctypes.c_void_p(dG), int(count) * 8,
+                                        ctypes.c_void_p(stream)))
+        if dist.get_backend(group) == "gloo":
+            h = t.cpu()
+            dist.all_reduce(h, group=group)
+            t.copy_(h)
+        else:
+            dist.all_reduce(t, group=group)
+        torch.cuda.synchronize()
+        E._check(_lib().hfg_copy_device(ctypes.c_void_p(dG), ctypes.c_void_p(t.data_ptr()), int(count) * 8,
+                                        ctypes.c_void_p(stream)))
+    return fn
+
+
+def run_scf(Z, xyz, basis: str, unrestricted=False, want_density=True, shard=None, allreduce=None, **kw):
     """RestrictedHartreeFock / UnrestrictedHartreeFock Init + Calculate
     (scf_opts keywords).
 
     mixed_cutoff > 0 selects the precision form of the Fock builds (FP32
     below the cutoff, incremental from the density difference, all-FP64
-    final iterations); incremental=True alone gives FP64 incremental builds."""
+    final iterations); incremental=True alone gives FP64 incremental builds.
+    shard=(rank, count) with allreduce(dG_ptr, count, stream, user) (e.g.
+    torch_allreduce()) runs the sharded SCF: every build evaluates this
+    rank's shard and the callback sums G over the ranks."""
     L = _lib()
     o = scf_opts(unrestricted=unrestricted, **kw)
+    cb = None
+    if shard is not None and shard[1] > 1:
+        cb = ALLREDUCE_FN(allreduce)
+        o.shard_rank, o.shard_count = int(shard[0]), int(shard[1])
+        o.allreduce = ctypes.cast(cb, ctypes.c_void_p)
     z = np.ascontiguousarray(Z, dtype=np.int32)
     x = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
     nbf_guess = 40 * len(z) + 64

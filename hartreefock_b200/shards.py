@@ -3,8 +3,8 @@
 One process per GPU (torch.distributed, NCCL).  Every rank holds the whole
 molecule's context (shell pairs, Schwarz bounds, class task lists: a few
 hundred MB at most) and the full density; `hfg_set_shard(rank, world)` makes
-its builds evaluate every world-th task of each quartet class, so each rank
-produces a partial G.  G is linear in the J/K sums, so one all-reduce (sum)
+its builds evaluate the rank-th of `world` contiguous task ranges of equal
+estimated cost in each quartet class, so each rank produces a partial G.  G is linear in the J/K sums, so one all-reduce (sum)
 of the n x n partials gives every rank the full G (a few MB: latency-bound
 over NVLink).  Nothing else crosses between ranks: the density every rank
 feeds in is the same because every rank runs the same replicated SCF algebra.

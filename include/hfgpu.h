@@ -167,13 +167,26 @@ hfg_status hfg_set_incremental(hfg_ctx *ctx, int32_t on);
 
 /* Sharded direct builds (one molecule over several GPUs; no reference
  * counterpart): with shard (rank, count) set, hfg_fock_rhf/uhf[_device]
- * evaluate only every count-th task of each quartet class starting at rank,
+ * evaluate only the rank-th of `count` contiguous task ranges of each
+ * quartet class, ranges of equal estimated cost (primitive quartets times the
+ * class's per-primitive flops, plus its per-quartet horizontal recursions),
  * and return that shard's partial G.  The partial G of the `count` shards
  * sum to the full G (G is linear in the J/K sums); the caller reduces them,
  * e.g. with one NCCL all-reduce (hartreefock_b200/shards.py).  Incremental
  * builds keep a per-shard history.  Stored builds (hfg_eri_packed) and
  * hfg_fock_rhf_noalloc are not sharded.  Default (0, 1). */
 hfg_status hfg_set_shard(hfg_ctx *ctx, int32_t rank, int32_t count);
+/* The shard partition itself (host arithmetic, no device): given the
+ * running cost of a class's `ntasks` tasks (cost_prefix[0] = 0,
+ * cost_prefix[t + 1] = cost of tasks 0..t, ntasks + 1 entries), the
+ * contiguous task range [*first, *first + *ntasks_out) of shard `rank` of
+ * `count`: shard r starts at the first task whose prefix reaches
+ * r / count of the total.  The ranges of ranks 0..count-1 tile the tasks. */
+hfg_status hfg_shard_range(const double *cost_prefix, int64_t ntasks, int32_t rank, int32_t count, int64_t *first,
+                           int64_t *ntasks_out);
+/* Device-to-device copy of `bytes` on `stream`, finished when the call
+ * returns (for callers that move a sharded G into their own buffers). */
+hfg_status hfg_copy_device(void *dst, const void *src, int64_t bytes, void *stream);
 
 /* Batched contexts (many independent molecules; no reference counterpart:
  * the reference runs one molecule per algorithm object).  hfg_batch_create
@@ -192,6 +205,17 @@ hfg_status hfg_batch_layout(const hfg_ctx *ctx, int32_t *nbf, int64_t *offset, i
 hfg_status hfg_fock_rhf_batch_device(hfg_ctx *ctx, const double *dP, double *dG, const uint8_t *active, void *stream);
 hfg_status hfg_fock_uhf_batch_device(hfg_ctx *ctx, const double *dPa, const double *dPb, double *dGa, double *dGb,
                                      const uint8_t *active, void *stream);
+/* The same builds with the active mask in device memory (d_active[nmol],
+ * 0 = skip the molecule) and no host synchronisation: the active molecules'
+ * tasks are compacted on the device and the class kernels take them from a
+ * device work queue (one atomic task counter per class, a fixed grid), so a
+ * caller can capture a whole batched SCF iteration in a CUDA graph.  The
+ * first call allocates the context's work buffers; capture after it.  No
+ * reference counterpart (one molecule per algorithm object there). */
+hfg_status hfg_fock_rhf_batch_async(hfg_ctx *ctx, const double *dP, double *dG, const uint8_t *d_active,
+                                    void *stream);
+hfg_status hfg_fock_uhf_batch_async(hfg_ctx *ctx, const double *dPa, const double *dPb, double *dGa, double *dGb,
+                                    const uint8_t *d_active, void *stream);
 
 /* One-electron matrices on `device`: overlap S, kinetic energy T and
  * nuclear attraction V (h = T + V), each row-major nbf x nbf in host memory,
@@ -240,12 +264,14 @@ hfg_status hfg_mp2_rhf(hfg_ctx *ctx, const double *C, const double *eps, int32_t
  * (UnrestrictedHartreeFock.cpp:295-375): 0.25 (S+ + S-), S = sum over the
  * spin's occupied i, j and virtual a, b of (ia|jb)^2 / (e_i + e_j - e_a - e_b),
  * from host C+ / C- (row-major nbf x nbf), orbital energies e+ / e- and the
- * occupied counts n+ >= n- (lowest orbitals).  The reference evaluates both
- * sums through one MolecularOrbitalsIntegralsRepository whose caches are
- * keyed by orbital indices only (IntegralsRepository.h:190-291), so its S-
- * reuses values cached with C+; this reproduces that: in S-, quartets with a
- * and b virtual in both spins take C+, those with a occupied in + only take
- * (i- a- | j+ b+), those with b occupied in + only take C-. */
+ * occupied counts 0 <= n+, n- <= nbf (lowest orbitals; either may be the
+ * larger -- Molecule::Init, Molecule.cpp:132-139, gives the odd electron to
+ * the minus spin).  The reference evaluates both sums through one
+ * MolecularOrbitalsIntegralsRepository whose caches are keyed by orbital
+ * indices only (IntegralsRepository.h:190-291), so its S- reuses values
+ * cached with C+; this reproduces that: in S- index b takes C+ when virtual+,
+ * j when also occupied+, a when also virtual+, i when also occupied+, and
+ * every other index C-. */
 hfg_status hfg_mp2_uhf(hfg_ctx *ctx, const double *Cplus, const double *eplus, int32_t nplus, const double *Cminus,
                        const double *eminus, int32_t nminus, double *e_mp2);
 
@@ -265,6 +291,14 @@ void hfg_release_thread(void);
  * (RestrictedHartreeFock.cpp:121-124).  Workspace is kept per host thread. */
 hfg_status hfg_eigh_batched(const double *dA, double *dV, double *dW, int32_t n, int32_t batch, int32_t method,
                             void *stream);
+
+/* The DIIS systems of a batch of molecules on the device: for each of
+ * `batch` row-major m1 x m1 matrices in dB (the Pulay matrix bordered by
+ * ones, DIIS.h:34-96), dC receives the m1 solution entries of
+ * B c = (0, ..., 0, 1) by column-pivoted Householder QR with a rank cut-off
+ * (the role of colPivHouseholderQr, DIIS.h:72), the same algorithm as the
+ * host SCF's solve.  2 <= m1 <= 8.  Asynchronous on `stream`. */
+hfg_status hfg_pulay_solve_device(const double *dB, int32_t m1, int32_t batch, double *dC, void *stream);
 
 /* Allocation-free variant of hfg_fock_rhf_device, for callers that must not
  * allocate device memory while they run: a serving loop under a fixed HBM
@@ -308,6 +342,31 @@ hfg_status hfg_set_graphs(hfg_ctx *ctx, int32_t on);
  * events; J/K accumulate by atomics, each split class stream has its own
  * scratch region), so small molecules' class kernels overlap. */
 hfg_status hfg_set_streams(hfg_ctx *ctx, int32_t on);
+/* Task shape of the thread-per-quartet classes (no reference counterpart):
+ * a quartet whose primitive quartets exceed `target` per lane is spread over
+ * a group of 2..32 lanes that split its primitive loop and sum the
+ * contraction with warp shuffles, and tasks carry correspondingly fewer kets
+ * (0: one lane per quartet; default 96).  Rebuilds the task lists. */
+hfg_status hfg_set_prim_target(hfg_ctx *ctx, int32_t target);
+/* Picks that target per class (0, 48, 96, 192, 384) by timing each class's
+ * J/K kernel on the caller's device density dP; `chosen` receives
+ * (La, Lb, Lc, Ld, target) per tuned class.  Single-molecule contexts. */
+hfg_status hfg_autotune_tasks(hfg_ctx *ctx, const double *dP, int32_t *chosen, int32_t cap, int32_t *count,
+                              void *stream);
+
+/* Kernel of the large classes that have two (no reference counterpart):
+ * `path` 1 runs quartet class (La Lb | Lc Ld) on the warp-cooperative kernel
+ * (one warp per shell quartet, recursions from a level-ordered program in
+ * shared memory, no scratch), 0 on the split path (primitive kernel, then the
+ * HRR / digestion kernel over scratch).  Default: warp for (dd|dd), split for
+ * the rest.  HFG_INVALID_ARG for a class without both kernels.  Batched
+ * asynchronous builds and hfg_fock_rhf_noalloc always use the warp kernel. */
+hfg_status hfg_set_class_path(hfg_ctx *ctx, int32_t la, int32_t lb, int32_t lc, int32_t ld, int32_t path);
+/* Picks that kernel per class by timing both on the caller's device density
+ * dP (one warm-up, two timed launches each, CUDA events); `chosen` receives
+ * (La, Lb, Lc, Ld, path) per tuned class.  Single-molecule contexts. */
+hfg_status hfg_autotune_paths(hfg_ctx *ctx, const double *dP, int32_t *chosen, int32_t cap, int32_t *count,
+                              void *stream);
 
 /* Grid autotuner (no reference counterpart): times every fused quartet
  * class's J/K kernel at 1, 2, 4, 8 and 16 blocks per SM on the density dP

@@ -14,6 +14,10 @@
 extern "C" {
 #endif
 
+/* Sums a partial two-electron matrix over the shards of a sharded SCF, in
+ * place: dG holds `count` doubles on the device, produced on `stream`. */
+typedef void (*hfd_allreduce_fn)(double *dG, int64_t count, void *stream, void *user);
+
 typedef struct {
   int32_t unrestricted;      /* 0 RHF, 1 UHF */
   double alpha;              /* density mixing (HartreeFockAlgorithm::alpha) */
@@ -43,6 +47,12 @@ typedef struct {
                                 replay of plain builds (cudaGraphs), for one host thread
                                 driving the device; 0: neither */
   double electric_field[3];  /* Molecule::ElectricField: h += E . dipole moments (HartreeFockAlgorithm.cpp:38) */
+  /* sharded builds (HartreeFockAlgorithm::shardRank / shardCount / allReduce):
+   * shard_count > 1 makes every build evaluate this rank's shard and
+   * `allreduce(dG, count, stream, allreduce_user)` sum G over the ranks */
+  int32_t shard_rank, shard_count;
+  hfd_allreduce_fn allreduce;
+  void *allreduce_user;
 } hfd_scf_opts;
 
 typedef struct {

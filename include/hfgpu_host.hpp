@@ -23,6 +23,7 @@
 #pragma once
 
 #include <atomic>
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -305,6 +306,14 @@ class HartreeFockAlgorithm {
   // build's classes on concurrent streams.
   bool cudaGraphs = false;
   bool concurrentClasses = false;
+  // Sharded Fock builds over several processes / GPUs (no reference
+  // counterpart): this algorithm's engine evaluates shard (shardRank,
+  // shardCount) of every two-electron build (hfg_set_shard) and allReduce
+  // sums the partial G over the shards -- device buffer of `count` doubles,
+  // on `stream` -- before F is formed.  Every shard then runs the same SCF
+  // algebra on the same G.  shardCount 1: no sharding.
+  int shardRank = 0, shardCount = 1;
+  std::function<void(double *dG, size_t count, void *stream)> allReduce;
   double mp2Energy = 0;
 
  protected:

@@ -317,6 +317,74 @@ def g_uhf(n, packed, Pa, Pb):
     return Ga, Gb
 
 
+def unpack_eri(packed, n):
+    """full[m, n, l, s] = (mn|ls) from the 8-fold packed table
+    (IntegralsRepository.h:151-162)."""
+    idx = np.arange(n)
+    ij = np.maximum(idx[:, None], idx[None, :])
+    ij = ij * (ij + 1) // 2 + np.minimum(idx[:, None], idx[None, :])
+    p, q = ij[:, :, None, None], ij[None, None, :, :]
+    return np.asarray(packed)[np.maximum(p, q) * (np.maximum(p, q) + 1) // 2 + np.minimum(p, q)]
+
+
+class MoCache:
+    """MolecularOrbitalsIntegralsRepository (IntegralsRepository.h:190-291)
+    restated literally: four quarter-transform levels, each cached in a dict
+    keyed by the four orbital indices only -- not by the coefficient matrix
+    the value was computed with.  ``eri`` is the full AO table, C column
+    ``p`` the MO p (C[AO, MO])."""
+
+    def __init__(self, eri):
+        self.eri = eri
+        self.levels = ({}, {}, {}, {})
+
+    def _l1(self, o1, o2, o3, o4, C):  # IntegralsRepository.h:237-251
+        key = (o1, o2, o3, o4)
+        if key not in self.levels[0]:
+            self.levels[0][key] = float(C[:, o4] @ self.eri[o1, o2, o3, :])
+        return self.levels[0][key]
+
+    def _l2(self, o1, o2, o3, o4, C):  # :253-268
+        key = (o1, o2, o3, o4)
+        if key not in self.levels[1]:
+            self.levels[1][key] = sum(C[l, o3] * self._l1(o1, o2, l, o4, C) for l in range(C.shape[1]))
+        return self.levels[1][key]
+
+    def _l3(self, o1, o2, o3, o4, C):  # :270-284
+        key = (o1, o2, o3, o4)
+        if key not in self.levels[2]:
+            self.levels[2][key] = sum(C[nu, o2] * self._l2(o1, nu, o3, o4, C) for nu in range(C.shape[1]))
+        return self.levels[2][key]
+
+    def get(self, o1, o2, o3, o4, C):  # :198-234
+        key = (o1, o2, o3, o4)
+        if key not in self.levels[3]:
+            self.levels[3][key] = sum(C[mu, o1] * self._l3(mu, o2, o3, o4, C) for mu in range(C.shape[1]))
+        return self.levels[3][key]
+
+
+def mp2_uhf(eri, Cp, ep, nplus, Cm, em, nminus):
+    """UnrestrictedHartreeFock::CalculateMp2Energy (UnrestrictedHartreeFock.cpp:295-375):
+    0.25 (S+ + S-) through ONE MoCache, S+ first, so S- reuses what S+
+    cached with C+.  Pure-Python loops: small cases only."""
+    n = Cp.shape[0]
+    repo = MoCache(eri)
+
+    def spin_sum(C, e, nocc):  # CalculateMp2EnergyPlus :309-338 / Minus :340-369
+        s = 0.0
+        for i in range(nocc):
+            for j in range(nocc):
+                for a in range(nocc, n):
+                    for b in range(nocc, n):
+                        v = repo.get(i, a, j, b, C)
+                        s += v * v / (e[i] + e[j] - e[a] - e[b])
+        return s
+
+    total = spin_sum(Cp, ep, nplus)
+    total += spin_sum(Cm, em, nminus)
+    return 0.25 * total
+
+
 def one_electron(mol: Molecule):
     n = mol.nbf
     S, T, V = np.zeros((n, n)), np.zeros((n, n)), np.zeros((n, n))
@@ -538,14 +606,16 @@ def read_records(path: str) -> dict:
 
 
 def run_reference(mol: Molecule, mode: str, out_path: str, alpha=0.75, init_guess=0.75, use_diis=True,
-                  post_diis=500, extra: str = "", timeout=3600) -> dict:
+                  post_diis=500, extra: str = "", timeout=3600, driver: str = "") -> dict:
+    """Runs the reference's classes compiled headless (oracle/_ref/ref_driver,
+    or `driver`: the drop-in builds ref_driver_gpu / ref_driver_gpu_direct)."""
     lines = [f"basis {mol.basis_path}"]
     for z, p in zip(mol.Z, mol.xyz):
         lines.append(f"atom {int(z)} {float(p[0]):.17g} {float(p[1]):.17g} {float(p[2]):.17g}")
     lines += [f"alpha {float(alpha):.17g}", f"initguess {float(init_guess):.17g}", f"diis {int(use_diis)}",
               f"postdiis {int(post_diis)}",
               f"mode {mode}", f"out {out_path}", extra]
-    r = subprocess.run([DRIVER_PATH], input="\n".join(lines) + "\n", capture_output=True, text=True,
+    r = subprocess.run([driver or DRIVER_PATH], input="\n".join(lines) + "\n", capture_output=True, text=True,
                        timeout=timeout)
     if r.returncode != 0:
         raise RuntimeError(f"ref_driver failed: {r.stderr}")

@@ -97,3 +97,56 @@ def test_fock_uhf_matches_oracle(name):
     scale = max(1.0, np.abs(wa).max())
     assert np.abs(ga - wa).max() < 1e-10 * scale
     assert np.abs(gb - wb).max() < 1e-10 * scale
+
+
+def test_lane_group_task_shapes_give_the_same_fock_build():
+    """One lane per quartet and lane groups of every size (the task builder's
+    primitive-quartets-per-lane target) give the same G; the screened
+    quartet count does not change."""
+    from hartreefock_b200 import molecules
+    Z, xyz = molecules.water_cluster(4, seed=2)
+    eng = E.Engine(Z, xyz, "6-31g*", schwarz_threshold=1e-12)
+    rng = np.random.default_rng(5)
+    A = rng.normal(size=(eng.nbf, eng.nbf)) * 0.1
+    P = A + A.T
+    eng.set_prim_target(0)
+    want = eng.fock_rhf(P)
+    count = eng.stats()["function_quartets"]
+    for target in (8, 48, 384):
+        eng.set_prim_target(target)
+        got = eng.fock_rhf(P)
+        assert np.abs(got - want).max() < 1e-11 * np.abs(want).max(), target
+        assert eng.stats()["function_quartets"] == count
+    tuned = eng.autotune_tasks(P)
+    assert tuned and all(t in (0, 48, 96, 192, 384) for t in tuned.values())
+    assert np.abs(eng.fock_rhf(P) - want).max() < 1e-11 * np.abs(want).max()
+    eng.close()
+
+
+LARGE = ["(21|11)", "(21|20)", "(21|21)", "(22|10)", "(22|11)", "(22|20)", "(22|21)", "(22|22)"]
+
+
+def test_both_kernels_of_the_large_classes_agree():
+    """The warp-cooperative kernel and the split path give the same packed
+    ERIs (to the 1e-12 parity bar) and the same G for every large class;
+    the path autotuner keeps one of the two and the build stays the same."""
+    from hartreefock_b200 import molecules
+    Z, xyz = molecules.water_cluster(3, seed=4)
+    eng = E.Engine(Z, xyz, "6-31g*", schwarz_threshold=1e-12)
+    rng = np.random.default_rng(6)
+    A = rng.normal(size=(eng.nbf, eng.nbf)) * 0.1
+    P = A + A.T
+    out = {}
+    for warp in (False, True):
+        for cls in LARGE:
+            eng.set_class_path(cls, warp)
+        out[warp] = (eng.fock_rhf(P), eng.eri_packed())
+    scale = np.abs(out[False][0]).max()
+    assert np.abs(out[True][0] - out[False][0]).max() < 1e-12 * scale
+    assert np.abs(out[True][1] - out[False][1]).max() < 1e-12
+    tuned = eng.autotune_paths(P)
+    assert set(tuned) <= set(LARGE) and all(v in ("warp", "split") for v in tuned.values())
+    assert np.abs(eng.fock_rhf(P) - out[False][0]).max() < 1e-12 * scale
+    with pytest.raises(E.HfgError):
+        eng.set_class_path("(10|00)", True)  # one kernel only
+    eng.close()

@@ -69,6 +69,28 @@ def test_scf_mp2_matches_canonical_orbitals_of_the_converged_density():
     assert abs(r["mp2_energy"] - want) < 1e-8, (r["mp2_energy"], want)
 
 
+@pytest.mark.parametrize("nplus,nminus", [(5, 5), (5, 4), (4, 5), (5, 2), (2, 5), (7, 0)])
+def test_uhf_mp2_cache_rule_on_random_orbitals(nplus, nminus):
+    """hfg_mp2_uhf against the oracle's literal restatement of the reference's
+    index-keyed MO cache (IntegralsRepository.h:190-291), unrelated C+ and C-
+    so every mixed-spin block of the second sum shows, for both orders of the
+    occupied counts."""
+    g = load_golden("h2o_sto3g")
+    Z, xyz = list(g["Z"]), g["xyz"]
+    eng = E.Engine(Z, xyz, "sto-3g", schwarz_threshold=0.0)
+    mol = O.Molecule(Z, xyz, basis_path("sto-3g"))
+    n = mol.nbf
+    rng = np.random.default_rng(10 * nplus + nminus)
+    Cp, _ = np.linalg.qr(rng.normal(size=(n, n)))
+    Cm, _ = np.linalg.qr(rng.normal(size=(n, n)))
+    ep = np.concatenate([np.sort(rng.uniform(-20, -0.3, nplus)), np.sort(rng.uniform(0.2, 5, n - nplus))])
+    em = np.concatenate([np.sort(rng.uniform(-20, -0.3, nminus)), np.sort(rng.uniform(0.2, 5, n - nminus))])
+    want = O.mp2_uhf(full_eri(O.eri_packed(mol), n), Cp, ep, nplus, Cm, em, nminus)
+    got = eng.mp2_uhf(Cp, ep, nplus, Cm, em, nminus)
+    eng.close()
+    assert abs(got - want) <= 1e-11 * max(1.0, abs(want)), (got, want)
+
+
 MP2_TOL = 1e-8  # Eh: MP2 energies of SCF runs that match the reference's energies within 1e-9
 
 

@@ -51,6 +51,29 @@ def test_oracle_scf_energy_matches_reference(name, kind):
     assert abs(r["energy"] - float(g[f"{kind}_energy"][0])) < 1e-9
 
 
+@pytest.mark.parametrize("name", ["h2o_sto3g", "oh_631g"])
+def test_oracle_uhf_mp2_matches_reference(name):
+    """The literal restatement of the index-keyed MO cache
+    (IntegralsRepository.h:190-291) on the canonical orbitals of the
+    reference's converged UHF densities gives the MP2 energy the reference
+    printed (UnrestrictedHartreeFock.cpp:295-375).  OH: Molecule::Init puts
+    the odd electron in the minus spin (n+ = 4, n- = 5), so S- reads C+
+    values cached by S+ for i, j < 4 and mixes spins for i or j = 4."""
+    g = load_golden(name)
+    mol = mol_of(g)
+    n, packed = mol.nbf, g["eri_packed"]
+    S, T, V = O.one_electron(mol)
+    Pa, Pb = g["uhf_density_alpha"], g["uhf_density_beta"]
+    Ga, Gb = O.g_uhf(n, packed, Pa, Pb)
+    s, U = np.linalg.eigh(S)
+    X = U @ np.diag(s ** -0.5) @ U.T
+    ea, Ca = np.linalg.eigh(X @ (T + V + Ga) @ X)
+    eb, Cb = np.linalg.eigh(X @ (T + V + Gb) @ X)
+    na, nb = int(round(np.trace(Pa @ S))), int(round(np.trace(Pb @ S)))
+    got = O.mp2_uhf(O.unpack_eri(packed, n), X @ Ca, ea, na, X @ Cb, eb, nb)
+    assert abs(got - float(g["uhf_mp2"][0])) < 1e-10, (got, float(g["uhf_mp2"][0]))
+
+
 @pytest.mark.parametrize("m,T", [(0, 0.0), (0, 1e-12), (3, 0.7), (8, 5.0), (8, 12.3), (4, 35.9), (8, 36.5),
                                  (2, 80.0), (9, 170.0)])
 def test_boys_against_series(m, T):
