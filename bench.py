@@ -288,7 +288,8 @@ def batch_molecules(count: int, seed: int = 0):
             Z, xyz = molecules.alkane(k)
         else:
             Z, xyz = molecules.hydroxyl() if kind == "oh" else molecules.methyl_planar()
-        (uhf if kind in ("oh", "ch3") else rhf).append(dict(Z=list(Z), xyz=xyz, basis=basis))
+        name = {"w": f"(H2O)_{k}", "a": f"C{k}H{2 * k + 2}", "oh": "OH", "ch3": "CH3"}[kind] + " " + basis
+        (uhf if kind in ("oh", "ch3") else rhf).append(dict(Z=list(Z), xyz=xyz, basis=basis, name=name))
     return rhf, uhf
 
 
@@ -302,7 +303,7 @@ def batching(count: int, check: int = 8):
     out = {"workload": f"{count} molecules: (H2O)_1-6, alkanes C1-C10, UHF OH / CH3; STO-3G / 6-31G", "runs": {}}
     total_wall = 0.0
     for name, mols, un, kw in (("rhf", rhf, False, dict(alpha=0.75, init_guess=0.75)),
-                               ("uhf", uhf, True, dict(alpha=0.5, init_guess=0.0))):
+                               ("uhf", uhf, True, dict(alpha=0.5, init_guess=0.75))):
         if not mols:
             continue
         t0 = time.perf_counter()
@@ -322,7 +323,8 @@ def batching(count: int, check: int = 8):
                              "seconds": {k: round(v, 4) for k, v in bs.seconds.items()}, "fock_launch_rounds": bs.builds,
                              "max_iterations": int(bs.iterations.max()), "converged": int(bs.converged.sum()),
                              "nbf_max": bs.nmax, "max_abs_dE_vs_single_fp64": max(errs) if errs else None,
-                             "cuda_graph_captures": bs.graph_captures}
+                             "cuda_graph_captures": bs.graph_captures, "graph_captured_loop": bool(bs.graphs_used),
+                             "not_converged": sorted({m["name"] for m, ok in zip(mols, bs.converged) if not ok})}
     out["molecules_per_s"] = count / total_wall if total_wall else None
     return out
 

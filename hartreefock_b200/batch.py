@@ -137,7 +137,11 @@ class BatchSCF:
         return w, U
 
     def run(self):
-        if self.graphs and self.dev.type == "cuda":
+        # the per-matrix dsyevd of open shells (eigh method 1) synchronises
+        # with the host inside cuSOLVER and cannot be captured: UHF batches
+        # run the host-driven loop
+        self.graphs_used = self.graphs and self.dev.type == "cuda" and self.eigh_method == 0
+        if self.graphs_used:
             return self._run_graphs()
         return self._run_eager()
 

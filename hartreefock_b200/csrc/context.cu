@@ -1054,17 +1054,14 @@ static hfg_status batch_build(hfg_ctx *c, bool uhf, const double *dPa, const dou
 // a CUDA graph): the active mask is read from device memory, every class's
 // active tasks are compacted on the device and the class kernels take them
 // from a device work queue (count and counter in device memory, one fixed
-// grid per class), then G per active molecule.  Large classes must run the
-// warp-cooperative kernels (no scratch, no host-sized chunks).  Buffers are
-// allocated by the first call.
+// grid per class), then G per active molecule.  The large classes run the
+// warp-cooperative kernels whatever the context's per-class choice (no
+// scratch, no host-sized chunks).  Buffers are allocated by the first call.
 static hfg_status batch_build_async(hfg_ctx *c, bool uhf, const double *dPa, const double *dPb, double *dGa,
                                     double *dGb, const unsigned char *d_active, cudaStream_t s) {
   const size_t tot = (size_t)c->batch_elems;
   const size_t nq = c->qclasses.size();
   hfg_status st;
-  for (size_t i = 0; i < nq; ++i)
-    if (uses_split(c, c->qclasses[i].cls))
-      return fail(HFG_INVALID_ARG, "asynchronous batched builds need the warp-cooperative large-class kernels");
   if ((st = ensure(&c->d_J, tot)) != HFG_OK || (st = ensure(&c->d_Ka, tot)) != HFG_OK) return st;
   if (uhf && ((st = ensure(&c->d_Kb, tot)) != HFG_OK || (st = ensure(&c->d_Pt, tot)) != HFG_OK)) return st;
   if (!c->d_task_active) {

@@ -56,9 +56,10 @@ __device__ __noinline__ void boys_edges_fp64(double *F, double T, double scale) 
 #pragma unroll
     for (int m = 0; m <= M; ++m) F[m] = fm[m] * scale;
   } else {
-    double f = 0.88622692545275801365 * rsqrt(T);
+    const double r = rsqrt(T);
+    double f = 0.88622692545275801365 * r;
     F[0] = f * scale;
-    const double e = exp(-T), h = 0.5 / T;
+    const double e = exp_neg_far(T), h = 0.5 * r * r;
 #pragma unroll
     for (int m = 0; m < M; ++m) {
       f = ((2 * m + 1) * f - e) * h;
@@ -77,10 +78,11 @@ constexpr float kBoysF32Band = 4.0f;
 template <int M>
 __device__ __forceinline__ void boys_eval_f32(float *F, float T, float scale, const double *__restrict__ tab) {
   if (T >= (float)kBoysTmax + kBoysF32Band) {
-    float f = 0.88622692545275801365f * rsqrtf(T);  // sqrt(pi)/2 / sqrt(T)
+    const float r = rsqrtf(T);
+    float f = 0.88622692545275801365f * r;  // sqrt(pi)/2 / sqrt(T)
     F[0] = f * scale;
     if (M > 0) {
-      const float e = __expf(-T), h = 0.5f / T;
+      const float e = __expf(-T), h = 0.5f * r * r;
 #pragma unroll
       for (int m = 0; m < M; ++m) {
         f = ((2 * m + 1) * f - e) * h;

@@ -62,10 +62,11 @@ __device__ __forceinline__ void boys_global(double *F, double T, double scale, c
 #pragma unroll
     for (int m = 0; m <= M; ++m) F[m] = fm[m] * scale;
   } else {
-    double f = 0.88622692545275801365 * rsqrt(T);
+    const double r = rsqrt(T);
+    double f = 0.88622692545275801365 * r;
     F[0] = f * scale;
     if (M > 0) {
-      const double e = exp(-T), h = 0.5 / T;
+      const double e = exp_neg_far(T), h = 0.5 * r * r;
 #pragma unroll
       for (int m = 0; m < M; ++m) {
         f = ((2 * m + 1) * f - e) * h;

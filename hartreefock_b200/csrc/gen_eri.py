@@ -600,7 +600,7 @@ def emit_split(out_dir):
     modes = ("kStorePacked", "kJkRhf", "kJkUhf")
 
     def launch(lines, ind, k, ref, grid):
-        tail = f"(v, cl, ch, {grid}, s);" if k.startswith("launch_prim_split") else f"<<<{grid}, kThreads, 0, s>>>(v, cl, ch);"
+        tail = f"(v, cl, ch, {grid}, s);" if k.startswith("launch_") else f"<<<{grid}, kThreads, 0, s>>>(v, cl, ch);"
         if ref:
             lines.append(f"{ind}if (ref) {k.format(r='true')}{tail}")
             lines.append(f"{ind}else {k.format(r='false')}{tail}")
@@ -626,7 +626,10 @@ def emit_split(out_dir):
         lines.append("  switch (mode) {")
         for mode in modes:
             lines.append(f"    case {mode}:")
-            launch(lines, "      ", f"eri_hrr_digest_kernel<{a}, {b}, {c}, {d}, {mode}, {{r}}>", ref, "gridB")
+            if mode == "kStorePacked":
+                launch(lines, "      ", f"eri_hrr_store_kernel<{a}, {b}, {c}, {d}, {{r}}>", ref, "gridB")
+            else:
+                launch(lines, "      ", f"launch_hrr_jk<{a}, {b}, {c}, {d}, {mode}, {{r}}>", ref, "gridB")
             lines.append("      break;")
         lines += ["    default:", "      break;", "  }"]
         if not ref:
@@ -646,7 +649,7 @@ def emit_split(out_dir):
         lines.append("  switch (mode) {")
         for mode in ("kJkRhf", "kJkUhf"):
             lines.append(f"    case {mode}:")
-            launch(lines, "      ", f"eri_hrr_digest_kernel<{a}, {b}, {c}, {d}, {mode}, {{r}}, true>", ref, "gridB")
+            launch(lines, "      ", f"launch_hrr_jk<{a}, {b}, {c}, {d}, {mode}, {{r}}, true>", ref, "gridB")
             lines.append("      break;")
         lines += ["    default:", "      break;", "  }"]
         if not ref:

@@ -201,6 +201,19 @@ __device__ __forceinline__ long long tri(long long a, long long b) {
   return a < b ? b * (b + 1) / 2 + a : a * (a + 1) / 2 + b;
 }
 
+// e^-T for T >= kBoysTmax (36), to ~1.2e-7 relative: there e^-T enters F_m
+// only through the upward recursion below, where it is under 1e-6 of
+// (2m+1) F_m for m <= 8, so single precision in this factor moves F_m by less
+// than 1e-13 relative.  2^y with y = -T log2(e) in FP64: the integer part
+// goes into the exponent field, the fraction through exp2f (underflows to
+// ~2^-1022 and below, far under anything that survives the recursion).
+__device__ __forceinline__ double exp_neg_far(double T) {
+  const double y = -T * 1.4426950408889634074;  // log2(e)
+  const double n = floor(y);
+  const int ni = max((int)n, -1022);
+  return (double)exp2f((float)(y - n)) * __hiloint2double((ni + 1023) << 20, 0);
+}
+
 // Boys function F_0..F_M at T.  Below kBoysTmax: 7-term Taylor expansion of
 // F_M about the nearest grid point, F_M(T) = sum_k F_{M+k}(T_i) (-dT)^k / k!,
 // from the shared-memory slice tab[i][k] = F_{M+k}(T_i)/k! (k < 7), then the
@@ -208,8 +221,8 @@ __device__ __forceinline__ long long tri(long long a, long long b) {
 // with e^-T = e^-T_i * e^(T_i - T), tab[i][7] = e^-T_i and the second factor
 // from its 8-term Taylor series (|T_i - T| <= 0.025: truncation < 4e-18).
 // Above: F_0 = sqrt(pi/T)/2 (erfc(sqrt T) < 3e-17 there) and the upward
-// recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T).  The scale folds the
-// quartet prefactor into every order.
+// recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T), 1/T as rsqrt(T)^2 and e^-T
+// from exp_neg_far.  The scale folds the quartet prefactor into every order.
 template <int M, class R>
 __device__ __forceinline__ void boys_eval(R *F, double T, double scale, const double *__restrict__ tab) {
   if (T < kBoysTmax) {
@@ -239,11 +252,12 @@ __device__ __forceinline__ void boys_eval(R *F, double T, double scale, const do
 #pragma unroll
     for (int m = 0; m <= M; ++m) F[m] = (R)(fm[m] * scale);
   } else {
-    double f = 0.88622692545275801365 * rsqrt(T);  // sqrt(pi)/2 / sqrt(T)
+    const double r = rsqrt(T);
+    double f = 0.88622692545275801365 * r;  // sqrt(pi)/2 / sqrt(T)
     F[0] = (R)(f * scale);
     if (M > 0) {
-      const double e = exp(-T);
-      const double h = 0.5 / T;
+      const double e = exp_neg_far(T);
+      const double h = 0.5 * r * r;
 #pragma unroll
       for (int m = 0; m < M; ++m) {
         f = ((2 * m + 1) * f - e) * h;

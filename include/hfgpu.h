@@ -210,7 +210,9 @@ hfg_status hfg_fock_uhf_batch_device(hfg_ctx *ctx, const double *dPa, const doub
  * tasks are compacted on the device and the class kernels take them from a
  * device work queue (one atomic task counter per class, a fixed grid), so a
  * caller can capture a whole batched SCF iteration in a CUDA graph.  The
- * first call allocates the context's work buffers; capture after it.  No
+ * large classes always run on the warp-cooperative kernels here (no scratch
+ * sized on the host).  The first call allocates the context's work buffers;
+ * capture after it.  No
  * reference counterpart (one molecule per algorithm object there). */
 hfg_status hfg_fock_rhf_batch_async(hfg_ctx *ctx, const double *dP, double *dG, const uint8_t *d_active,
                                     void *stream);

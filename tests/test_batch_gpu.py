@@ -139,4 +139,6 @@ def test_device_pulay_solve_matches_host():
     B[0, :, 5] = B[0, :, 4]
     got = E.pulay_solve_device(torch.from_numpy(B).cuda()).cpu().numpy()
     want = scf.pulay_solve(B)
-    assert np.abs(got - want).max() < 1e-10
+    # the same QR in a different order of operations: agreement relative to
+    # the solution's size (the rank-deficient system's entries reach 1e3)
+    assert np.abs(got - want).max() < 1e-11 * max(1.0, np.abs(want).max())
