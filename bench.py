@@ -64,6 +64,10 @@ def workload():
     return Z, xyz
 
 
+# DRAM bytes (read + write) per launch of a class kernel on this workload,
+# from one ncu capture of the bench's own build (profiles/)
+TRAFFIC = {}
+
 # the large classes with a split path (primitive kernel, then HRR/digest)
 SPLIT_CLASSES = {(2, 1, 1, 1), (2, 1, 2, 0), (2, 1, 2, 1), (2, 2, 1, 0), (2, 2, 1, 1), (2, 2, 2, 0), (2, 2, 2, 1),
                  (2, 2, 2, 2)}
@@ -581,9 +585,20 @@ def main():
     top = max(prof, key=lambda c: c["ms"])
     peak = E.measure_fp64_peak(local)
     peak32 = E.measure_fp32_peak(local)
-    # class flops are whole-class figures; a shard runs 1/world of them
-    achieved = top["flops"] / world / (top["ms"] / 1e3) / 1e12
-    build_flops = stats_full["flops"]
+    # algorithmic flops: the reference's recursion loops walked per class
+    # (hartreefock_b200/flops.py) x the class's primitive and shell quartets;
+    # the engine's own count of its generated code beside it.  Class figures
+    # are whole-class; a shard runs 1/world of them.
+    from hartreefock_b200 import flops as FL
+
+    def walk(c):
+        fp, fs = FL.class_flops(c["la"], c["lb"], c["lc"], c["ld"])
+        return c["primitive_quartets"] * fp + c["shell_quartets"] * fs
+
+    achieved = walk(top) / world / (top["ms"] / 1e3) / 1e12
+    achieved_gen = top["flops"] / world / (top["ms"] / 1e3) / 1e12
+    build_flops = sum(walk(c) for c in prof)
+    build_flops_gen = stats_full["flops"]
 
     line = {
         "metric": METRIC, "value": value, "unit": "quartets/s", "n_gpus": world, "steps": args.steps,
@@ -604,9 +619,14 @@ def main():
         "roofline": {"bound": "fp64", "kernel": f"({top['la']}{top['lb']}|{top['lc']}{top['ld']}) J/K class kernel",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "peak_source": "measured in-run: FP64 FMA microbenchmark (hfg_measure_fp64_peak)",
-                     "traffic": None, "traffic_unit": "bytes per launch",
+                     "flop_count": "reference recursion loops walked per class (hartreefock_b200/flops.py)",
+                     "achieved_generated_code_count": achieved_gen,
+                     "traffic": TRAFFIC.get((top["la"], top["lb"], top["lc"], top["ld"])),
+                     "traffic_unit": "DRAM bytes per launch (ncu capture of this workload, profiles/)",
                      "build": {"achieved": build_flops / world / (total_ms / args.steps / 1e3) / 1e12,
-                               "frac": build_flops / world / (total_ms / args.steps / 1e3) / 1e12 / peak},
+                               "frac": build_flops / world / (total_ms / args.steps / 1e3) / 1e12 / peak,
+                               "achieved_generated_code_count":
+                                   build_flops_gen / world / (total_ms / args.steps / 1e3) / 1e12},
                      "fp32_peak": peak32},
         "classes": [{"class": f"({c['la']}{c['lb']}|{c['lc']}{c['ld']})", "ms": round(c["ms"], 4),
                      "tflops": round(c["flops"] / max(c["ms"], 1e-9) / 1e9, 3), "tasks": c["tasks"],

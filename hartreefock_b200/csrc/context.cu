@@ -1256,6 +1256,8 @@ static hfg_status create_context(const hfg_shells *sh, const int *shell_mol, int
     ctx->warp_class[k] = kWarp[k] && e.la + e.lb + e.lc + e.ld >= 8 ? 1 : 0;
   }
   if (const char *e = std::getenv("HFG_WORK_QUEUE")) ctx->use_queue = std::atoi(e) != 0;
+  // tuning: HFG_SCRATCH_MB bounds the split path's scratch (all regions together)
+  if (const char *e = std::getenv("HFG_SCRATCH_MB")) ctx->scratch_budget_bytes = size_t(std::max(16, std::atoi(e))) << 20;
   if (const char *e = std::getenv("HFG_SPLIT_PATH"); e && std::atoi(e) != 0)
     std::fill(std::begin(ctx->warp_class), std::end(ctx->warp_class), int8_t(0));
   if (const char *e = std::getenv("HFG_WARP_PATH"); e && std::atoi(e) != 0)

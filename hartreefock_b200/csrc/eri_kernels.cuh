@@ -177,12 +177,16 @@ __device__ __forceinline__ void accumulate_primitives_grouped(const EngineView &
     for (int x = 0; x < Cls::kAcc; ++x) acc[x] += __shfl_xor_sync(0xffffffffu, acc[x], o);
 }
 
-template <int LA, int LB, int LC, int LD, bool REF, class R>
+// `acc`: the block's accumulators, a register array (R*), or an accessor
+// into memory (the split path's scratch, which takes only lg == 0).
+template <int LA, int LB, int LC, int LD, bool REF, class R, class A>
 __device__ __forceinline__ void accumulate_primitives(const EngineView &v, const double *tab, int bp, int kp, int npk,
-                                                      R *acc, int lg = 0) {
-  if (lg > 0) {
-    accumulate_primitives_grouped<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, npk, acc, lg);
-    return;
+                                                      A acc, int lg = 0) {
+  if constexpr (std::is_pointer<A>::value) {
+    if (lg > 0) {
+      accumulate_primitives_grouped<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, npk, acc, lg);
+      return;
+    }
   }
   constexpr int LTOT = LA + LB + LC + LD;
   using Cls = EriClass<LA, LB, LC, LD, REF>;

@@ -152,18 +152,19 @@ class ClassGen:
         return name
 
     def prim_body(self):
-        """Accumulate every [e0|f0], e in [La, La+Lb], f in [Lc, Lc+Ld]."""
+        """Accumulate every [e0|f0], e in [La, La+Lb], f in [Lc, Lc+Ld].  Each
+        element is added to its accumulator right after the statements that
+        compute it, so a target value need not stay live to the end."""
         E = comps_range(self.la, self.la + self.lb)
         Fc = comps_range(self.lc, self.lc + self.ld)
-        acc = []
         for ie, e in enumerate(E):
             for jf, f in enumerate(Fc):
                 v = self.et(e, f)
                 idx = ie * len(Fc) + jf
                 if v is not None:
-                    acc.append(f"acc[{idx}] += {v};")
+                    self.lines.append(f"acc[{idx}] += {v};")
                     self.flops += 1
-        return self.lines + acc, len(E), len(Fc)
+        return self.lines, len(E), len(Fc)
 
 
 def hrr_code(la, lb, lc, ld):
@@ -254,7 +255,7 @@ def main(out_path):
             body, ne, nf = g.prim_body()
             tag = f"{la}{lb}{lc}{ld}" + ("r" if ref else "")
             hdr.append(f"// ({la}{lb}|{lc}{ld}) {variant}: [e0|f0] block {ne}x{nf}, ~{g.flops} flops per primitive quartet")
-            hdr.append(f"template <class R> __device__ __forceinline__ void eri_prim_{tag}(R* __restrict__ acc, const R* __restrict__ F,")
+            hdr.append(f"template <class R, class A> __device__ __forceinline__ void eri_prim_{tag}(A acc, const R* __restrict__ F,")
             hdr.append("    R PA0, R PA1, R PA2, R WP0, R WP1, R WP2, R oo2z, R roz,")
             hdr.append("    R delta0, R delta1, R delta2, R zoe, R oo2e) {")
             hdr += ["  " + l for l in body]
@@ -276,9 +277,11 @@ def main(out_path):
         for ref in (False, True):
             ptag = base + "r" if (ref and (base + "r") in tags) else base
             hdr.append(f"template <> struct EriClass<{la}, {lb}, {lc}, {ld}, {'true' if ref else 'false'}> {{")
-            hdr.append("  template <class R> static __device__ __forceinline__ void prim(R* acc, const R* F, R PA0, R PA1, R PA2,")
-            hdr.append("      R WP0, R WP1, R WP2, R oo2z, R roz, R delta0, R delta1, R delta2, R zoe, R oo2e) {")
-            hdr.append(f"    eri_prim_{ptag}<R>(acc, F, PA0, PA1, PA2, WP0, WP1, WP2, oo2z, roz, delta0, delta1, delta2, zoe, oo2e);")
+            hdr.append("  // acc: the accumulator block, a register array (R*) or any type with")
+            hdr.append("  // operator[] returning an assignable element")
+            hdr.append("  template <class R, class A> static __device__ __forceinline__ void prim(A acc, const R* F, R PA0, R PA1,")
+            hdr.append("      R PA2, R WP0, R WP1, R WP2, R oo2z, R roz, R delta0, R delta1, R delta2, R zoe, R oo2e) {")
+            hdr.append(f"    eri_prim_{ptag}<R, A>(acc, F, PA0, PA1, PA2, WP0, WP1, WP2, oo2z, roz, delta0, delta1, delta2, zoe, oo2e);")
             hdr.append("  }")
             hdr.append("  template <class R> static __device__ __forceinline__ void hrr(R* out, const R* acc, R AB0, R AB1, R AB2,")
             hdr.append("      R CD0, R CD1, R CD2) {")

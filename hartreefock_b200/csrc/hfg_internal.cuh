@@ -32,15 +32,12 @@ __host__ __device__ constexpr int ncart(int L) { return (L + 1) * (L + 2) / 2; }
 __host__ __device__ constexpr int fused_warps(int la, int lb, int lc, int ld) {
   return ncart(la) * ncart(lb) * ncart(lc) * ncart(ld) <= 9 ? 8 : 4;
 }
-// Resident blocks per SM the compiler must allow for the light classes (the
-// register cap that follows: 65536 / (32 * warps * blocks)); 1 leaves the
-// register allocation free.
-#ifndef HFG_FUSED_MIN_BLOCKS
-#define HFG_FUSED_MIN_BLOCKS 1
-#endif
-__host__ __device__ constexpr int fused_min_blocks(int la, int lb, int lc, int ld) {
-  return ncart(la) * ncart(lb) * ncart(lc) * ncart(ld) <= 9 ? HFG_FUSED_MIN_BLOCKS : 1;
-}
+// Resident blocks per SM the compiler must allow (1: the register
+// allocation is free).  A 64-register cap (four 8-warp blocks per SM) fits
+// (ss|ss) and (ps|ss) without spills but made (ps|ss) 20% slower alone
+// (1.20 -> 1.43 ms per (H2O)16 launch) for a change within noise in the
+// concurrent build; the other light classes spill under it.
+__host__ __device__ constexpr int fused_min_blocks(int, int, int, int) { return 1; }
 // unroll factor of the inner (bra) primitive loop
 #ifndef HFG_PRIM_UNROLL
 #define HFG_PRIM_UNROLL 1
