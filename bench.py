@@ -263,7 +263,7 @@ def scf_comparison(waters: int):
     }
 
 
-def serving(count: int, slots: int = 8, seed: int = 5):
+def serving(count: int, slots: int = 8, seed: int = 5, batch_nbf: int = 60):
     """The request loop (hartreefock_b200.serve) on a seeded Poisson stream of
     `count` RHF/UHF jobs, precision form and plain FP64 builds: saturation
     (every job submitted at once), then offered rates below it (0.25, 0.5 and
@@ -274,18 +274,20 @@ def serving(count: int, slots: int = 8, seed: int = 5):
     out = {"workload": f"{count} jobs, seed {seed}: 80% RHF water clusters / C1-C10 alkanes, sizes log-uniform "
                        "over 5-600 functions; 20% UHF OH / planar CH3; bases 6-31G, 6-31G*, 6-31+G** (Cartesian)",
            "nbf": sorted(shell_table(Z, x, b).nbf for Z, x, b, u in jobs), "slots": slots,
-           "hbm_budget_gib": 40, "eri_convention": "exact"}
+           "hbm_budget_gib": 40, "eri_convention": "exact",
+           "batch_lane": f"jobs of <= {batch_nbf} functions share batched SCFs (plain FP64 builds)" if batch_nbf
+           else "off"}
     energies, converged = {}, {}
     for name, mixed in (("mixed", True), ("fp64", False)):
         runs = {}
-        with serve.Server(slots=slots, hbm_budget=40 << 30, mixed=mixed) as s:
+        with serve.Server(slots=slots, hbm_budget=40 << 30, mixed=mixed, batch_nbf=batch_nbf) as s:
             hs, sat = serve.poisson_stream(s, jobs, rate=0.0, seed=1)
         energies[name] = [h.result["energy"] if h.error is None else None for h in hs]
         converged[name] = [h.error is None and h.result["converged"] for h in hs]
         sat["not_converged"] = sum(1 for h in hs if h.error is not None or not h.result["converged"])
         runs["saturation"] = sat
         for frac in ((0.25, 0.5, 0.75) if mixed else (0.5,)):
-            with serve.Server(slots=slots, hbm_budget=40 << 30, mixed=mixed) as s:
+            with serve.Server(slots=slots, hbm_budget=40 << 30, mixed=mixed, batch_nbf=batch_nbf) as s:
                 hs, part = serve.poisson_stream(s, jobs, rate=frac * sat["jobs_per_s"], seed=1)
             runs["half_load" if frac == 0.5 else f"load_{frac:.2f}"] = part
         out[name] = runs

@@ -35,7 +35,7 @@ class BatchSCF:
 
     def __init__(self, molecules, unrestricted=False, alpha=0.75, init_guess=0.75, max_iter=300,
                  use_diis=True, schwarz_threshold=1e-12, device="cuda", concurrent_classes=False, graphs=False,
-                 replay=8):
+                 replay=8, eri_convention=E.ERI_REFERENCE):
         self.mols = list(molecules)
         self.uhf = unrestricted
         self.alpha, self.init_guess, self.max_iter, self.use_diis = alpha, init_guess, max_iter, use_diis
@@ -49,7 +49,7 @@ class BatchSCF:
         self.graph_captures = 0
         self.dev = torch.device(device)
         self.eng = E.BatchEngine([(m["Z"], m["xyz"], m["basis"]) for m in self.mols],
-                                 schwarz_threshold=schwarz_threshold)
+                                 schwarz_threshold=schwarz_threshold, eri_convention=eri_convention)
         self.eng.set_streams(concurrent_classes)
         M = len(self.mols)
         self.M = M
@@ -170,7 +170,9 @@ class BatchSCF:
         active = torch.ones(M, dtype=torch.bool, device=dev)
         flatG = [torch.zeros(self.eng.total, dtype=torch.float64, device=dev) for _ in range(nspin)]
         builds = 0
-        sync = torch.cuda.synchronize if self.dev.type == "cuda" else (lambda: None)
+        # this thread's stream only: in a serving process other threads' jobs
+        # keep the device busy and must not be waited for
+        sync = torch.cuda.current_stream(self.dev).synchronize if self.dev.type == "cuda" else (lambda: None)
 
         def tick():
             sync()

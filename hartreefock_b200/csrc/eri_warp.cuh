@@ -36,8 +36,9 @@ namespace hfg {
 template <int M>
 __device__ __forceinline__ void boys_global(double *F, double T, double scale, const double *__restrict__ g) {
   if (T < kBoysTmax) {
-    const int i = __double2int_rn(T * (1.0 / kBoysStep));
-    const double dt = i * kBoysStep - T;
+    const BoysGridPoint gp = boys_grid_point(T);
+    const int i = gp.i;
+    const double dt = gp.dt;
     const double *t = g + i * kBoysOrders + M;
     // sum_k F_{M+k}(T_i) dt^k / k!, k < 7, nested as F_M + dt (F_{M+1} + dt/2 (F_{M+2} + ...))
     double f = __ldg(t + 6);

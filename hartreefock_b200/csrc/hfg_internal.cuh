@@ -198,6 +198,20 @@ __device__ __forceinline__ long long tri(long long a, long long b) {
   return a < b ? b * (b + 1) / 2 + a : a * (a + 1) / 2 + b;
 }
 
+// Nearest Boys grid point of 0 <= T < kBoysTmax: index i = round(T / step)
+// and dT = i * step - T.  The integer comes out of the low mantissa bits of
+// T / step + 1.5 * 2^52 (the sum rounds to an integer there), so no
+// float-integer conversion is issued either way.
+struct BoysGridPoint {
+  int i;
+  double dt;
+};
+__device__ __forceinline__ BoysGridPoint boys_grid_point(double T) {
+  constexpr double kShift = 6755399441055744.0;  // 1.5 * 2^52
+  const double y = fma(T, 1.0 / kBoysStep, kShift);
+  return {__double2loint(y), (y - kShift) * kBoysStep - T};
+}
+
 // e^-T for T >= kBoysTmax (36), to ~1.2e-7 relative: there e^-T enters F_m
 // only through the upward recursion below, where it is under 1e-6 of
 // (2m+1) F_m for m <= 8, so single precision in this factor moves F_m by less
@@ -223,8 +237,9 @@ __device__ __forceinline__ double exp_neg_far(double T) {
 template <int M, class R>
 __device__ __forceinline__ void boys_eval(R *F, double T, double scale, const double *__restrict__ tab) {
   if (T < kBoysTmax) {
-    const int i = __double2int_rn(T * (1.0 / kBoysStep));
-    const double dt = i * kBoysStep - T;  // -(T - T_i)
+    const BoysGridPoint gp = boys_grid_point(T);
+    const int i = gp.i;
+    const double dt = gp.dt;  // -(T - T_i)
     const double *t = tab + i * kBoysRow;
     const int sw = (i >> 1) & 7;
     double f = t[6 ^ sw];

@@ -72,6 +72,7 @@ class Job:
         self.id, self.Z, self.xyz, self.basis = jid, list(Z), np.asarray(xyz, dtype=np.float64), basis
         self.unrestricted, self.kwargs = unrestricted, dict(kwargs)
         self.bytes = footprint_bytes(self.Z, self.xyz, basis, unrestricted)
+        self.nbf = shell_table(self.Z, self.xyz, basis).nbf
         self.t_submit = self.t_start = self.t_end = None
         self.result, self.error = None, None
         self._done = threading.Event()
@@ -112,10 +113,20 @@ class Server:
     (host-side tests)."""
 
     def __init__(self, slots: int = 8, hbm_budget: int = 32 << 30, mixed: bool = True, mixed_cutoff: float = 1e-4,
-                 scf_kwargs=None, runner=None, concurrent_classes: bool = True):
+                 scf_kwargs=None, runner=None, concurrent_classes: bool = True, batch_nbf: int = 0,
+                 batch_max: int = 64, batch_window_s: float = 0.005):
         if slots < 1 or hbm_budget <= 0:
             raise ValueError("slots >= 1 and a positive budget are required")
         self.slots, self.budget = slots, int(hbm_budget)
+        # small jobs (at most batch_nbf functions) go to one batch lane: the
+        # jobs queued there with the same SCF settings (up to batch_max, after
+        # waiting batch_window_s for more to arrive) run as one batched SCF
+        # (hartreefock_b200.batch.BatchSCF: one Fock launch per quartet class
+        # over all of them per iteration, plain FP64 builds, the reference's
+        # convergence test per molecule)
+        self.batch_nbf, self.batch_max, self.batch_window_s = int(batch_nbf), int(batch_max), float(batch_window_s)
+        self._small = collections.deque()
+        self.batches = []  # sizes of the batches run
         # the switch rule's DIIS error at 1e-7 (the SCF default is 1e-6): jobs of
         # the stream with diffuse functions otherwise end up to ~1.3e-6 Eh apart
         # between the two forms
@@ -137,6 +148,8 @@ class Server:
         self.peak_running = 0
         self.finished = []
         self._workers = [threading.Thread(target=self._work, name=f"hfg-slot-{i}", daemon=True) for i in range(slots)]
+        if self.batch_nbf > 0:
+            self._workers.append(threading.Thread(target=self._batch_work, name="hfg-batch", daemon=True))
         for w in self._workers:
             w.start()
 
@@ -155,9 +168,85 @@ class Server:
                 job.t_start = job.t_end = job.t_submit
                 job._done.set()
                 return job
-            self._queue.append(job)
+            if self.batch_nbf > 0 and self.runner is _driver_runner and job.nbf <= self.batch_nbf:
+                self._small.append(job)
+            else:
+                self._queue.append(job)
             self._cv.notify_all()
         return job
+
+    @staticmethod
+    def _batch_key(job):
+        k = job.kwargs
+        return (job.unrestricted, k.get("alpha", 0.75), k.get("init_guess", 0.75), k.get("max_iterations", 0),
+                k.get("eri_convention", E.ERI_REFERENCE), k.get("schwarz_threshold", 1e-12))
+
+    def _take_batch(self):
+        """Queued small jobs with the head's settings, up to batch_max, if they
+        fit the budget together (caller holds the lock)."""
+        key = self._batch_key(self._small[0])
+        picked, rest, used = [], collections.deque(), 0
+        while self._small:
+            j = self._small.popleft()
+            if (len(picked) < self.batch_max and self._batch_key(j) == key
+                    and self._in_use + used + j.bytes <= self.budget):
+                picked.append(j)
+                used += j.bytes
+            else:
+                rest.append(j)
+        self._small = rest
+        if picked:
+            self._in_use += used
+            self._running += len(picked)
+            self.peak_bytes = max(self.peak_bytes, self._in_use)
+            self.peak_running = max(self.peak_running, self._running)
+        return picked
+
+    def _batch_work(self):
+        from . import batch as _batch
+        while True:
+            with self._cv:
+                while not self._small:
+                    if self._closing:
+                        from . import scf
+                        scf.release_thread()
+                        return
+                    self._cv.wait()
+            time.sleep(self.batch_window_s)  # let jobs arriving together share the batch
+            with self._cv:
+                jobs = self._take_batch()
+                if not jobs:
+                    self._cv.wait(0.01)  # the budget is held by running jobs
+                    continue
+            t0 = time.perf_counter()
+            for j in jobs:
+                j.t_start = t0
+            try:
+                k = jobs[0].kwargs
+                bs = _batch.BatchSCF([dict(Z=j.Z, xyz=j.xyz, basis=j.basis) for j in jobs],
+                                     unrestricted=jobs[0].unrestricted, alpha=k.get("alpha", 0.75),
+                                     init_guess=k.get("init_guess", 0.75), max_iter=k.get("max_iterations", 0) or 3000,
+                                     schwarz_threshold=k.get("schwarz_threshold", 1e-12),
+                                     eri_convention=k.get("eri_convention", E.ERI_REFERENCE), graphs=False)
+                energies = bs.run()
+                for i, j in enumerate(jobs):
+                    j.result = {"energy": float(energies[i]), "converged": bool(bs.converged[i]),
+                                "iterations": int(bs.iterations[i]), "batched": len(jobs)}
+                bs.eng.close()
+            except Exception as e:  # reported through Job.wait
+                for j in jobs:
+                    j.error = e
+            t1 = time.perf_counter()
+            with self._cv:
+                for j in jobs:
+                    j.t_end = t1
+                    self._in_use -= j.bytes
+                    self._running -= 1
+                    self.finished.append(j)
+                self.batches.append(len(jobs))
+                self._cv.notify_all()
+            for j in jobs:
+                j._done.set()
 
     def _admit(self):
         """Head of the queue if it fits (caller holds the lock)."""
@@ -199,7 +288,7 @@ class Server:
         """Wait until every submitted job has finished."""
         deadline = None if timeout is None else time.monotonic() + timeout
         with self._cv:
-            while self._queue or self._running:
+            while self._queue or self._small or self._running:
                 left = None if deadline is None else deadline - time.monotonic()
                 if left is not None and left <= 0:
                     raise TimeoutError("jobs still queued or running")
@@ -443,4 +532,7 @@ def poisson_stream(server: Server, jobs, rate: float, seed: int = 0, timeout=Non
                "jobs_per_s": len(handles) / (t_end - t0), "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
                "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
                "peak_running": server.peak_running, "peak_bytes": server.peak_bytes}
+    if getattr(server, "batch_nbf", 0) > 0:
+        summary["batched_jobs"] = int(sum(server.batches))
+        summary["batches"] = len(server.batches)
     return handles, summary
