@@ -65,8 +65,9 @@ def workload():
 
 
 # DRAM bytes (read + write) per launch of a class kernel on this workload,
-# from one ncu capture of the bench's own build (profiles/)
-TRAFFIC = {}
+# from one ncu capture of the bench's own build, caches flushed before the
+# launch (profiles/eri_class_kernel_ps_ss_h2o32_traffic.md)
+TRAFFIC = {(1, 0, 0, 0): 26716928, (0, 0, 0, 0): 21508864}
 
 # the large classes with a split path (primitive kernel, then HRR/digest)
 SPLIT_CLASSES = {(2, 1, 1, 1), (2, 1, 2, 0), (2, 1, 2, 1), (2, 2, 1, 0), (2, 2, 1, 1), (2, 2, 2, 0), (2, 2, 2, 1),

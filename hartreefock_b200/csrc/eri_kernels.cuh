@@ -177,8 +177,8 @@ __device__ __forceinline__ void accumulate_primitives_grouped(const EngineView &
     for (int x = 0; x < Cls::kAcc; ++x) acc[x] += __shfl_xor_sync(0xffffffffu, acc[x], o);
 }
 
-// `acc`: the block's accumulators, a register array (R*), or an accessor
-// into memory (the split path's scratch, which takes only lg == 0).
+// `acc`: the block's accumulators, a register array (R*) or any indexable
+// accumulator type (lane groups need the register array).
 template <int LA, int LB, int LC, int LD, bool REF, class R, class A>
 __device__ __forceinline__ void accumulate_primitives(const EngineView &v, const double *tab, int bp, int kp, int npk,
                                                       A acc, int lg = 0) {

@@ -21,25 +21,21 @@
 
 namespace hfg {
 
-// Accumulator block living in the chunk's scratch: element x of the
-// quartet in slot `slot` at p[x * stride] (column-major across the chunk's
-// quartets, so a warp's accesses to one element coalesce).  The block of a
-// large class (96 to 496 doubles) plus the recursion's live values overflow
-// the register file; accumulating in place keeps only the latter there.
-struct ScratchAcc {
-  double *p;
-  long long stride;
-  __device__ __forceinline__ double &operator[](int x) const { return p[x * stride]; }
-};
-
-// contracted [e0|f0] of one shell quartet, accumulated in scr[x * stride]
+// contracted [e0|f0] of one shell quartet, written to scr[x * stride]
+// (accumulating in place in scratch instead of registers removes the
+// spills of the large blocks but made the classes 1.3-2x slower: global
+// read-modify-writes per primitive quartet cost more than local-memory
+// spills, which stay in L1)
 template <int LA, int LB, int LC, int LD, bool REF, class R>
 __device__ __forceinline__ void prim_block_to_scratch(const EngineView &v, const double *tab, int bp, int kp, int npk,
                                                       double *scr, long long stride) {
   using Cls = EriClass<LA, LB, LC, LD, REF>;
-#pragma unroll 8
-  for (int x = 0; x < Cls::kAcc; ++x) scr[x * stride] = 0.0;
-  accumulate_primitives<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, npk, ScratchAcc{scr, stride});
+  R acc[Cls::kAcc];
+#pragma unroll
+  for (int x = 0; x < Cls::kAcc; ++x) acc[x] = R(0);
+  accumulate_primitives<LA, LB, LC, LD, REF, R>(v, tab, bp, kp, npk, acc);
+#pragma unroll
+  for (int x = 0; x < Cls::kAcc; ++x) scr[x * stride] = (double)acc[x];
 }
 
 // One quartet's contracted [e0|f0] block(s) in precision R, to its slot.

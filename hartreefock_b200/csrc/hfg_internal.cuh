@@ -230,7 +230,8 @@ __device__ __forceinline__ double exp_neg_far(double T) {
 // from the shared-memory slice tab[i][k] = F_{M+k}(T_i)/k! (k < 7), then the
 // downward recursion F_m = (2T F_{m+1} + e^-T) / (2m+1) (BoysFunctions.cpp:17-20)
 // with e^-T = e^-T_i * e^(T_i - T), tab[i][7] = e^-T_i and the second factor
-// from its 8-term Taylor series (|T_i - T| <= 0.025: truncation < 4e-18).
+// from its 8-term Taylor series (|T_i - T| <= 0.025: truncation < 4e-18);
+// both polynomials evaluated in Estrin's scheme.
 // Above: F_0 = sqrt(pi/T)/2 (erfc(sqrt T) < 3e-17 there) and the upward
 // recursion F_{m+1} = ((2m+1) F_m - e^-T) / (2T), 1/T as rsqrt(T)^2 and e^-T
 // from exp_neg_far.  The scale folds the quartet prefactor into every order.
@@ -242,20 +243,17 @@ __device__ __forceinline__ void boys_eval(R *F, double T, double scale, const do
     const double dt = gp.dt;  // -(T - T_i)
     const double *t = tab + i * kBoysRow;
     const int sw = (i >> 1) & 7;
-    double f = t[6 ^ sw];
-#pragma unroll
-    for (int k = 5; k >= 0; --k) f = fma(f, dt, t[k ^ sw]);
+    // both polynomials in Estrin's scheme (pairs, then powers dt^2 and dt^4):
+    // three dependent multiply-adds instead of six and seven in Horner's
+    const double d2 = dt * dt, d4 = d2 * d2;
+    const double p01 = fma(t[1 ^ sw], dt, t[0 ^ sw]), p23 = fma(t[3 ^ sw], dt, t[2 ^ sw]);
+    const double p45 = fma(t[5 ^ sw], dt, t[4 ^ sw]);
     double fm[M + 1];
-    fm[M] = f;
+    fm[M] = fma(fma(t[6 ^ sw], d2, p45), d4, fma(p23, d2, p01));
     if (M > 0) {
-      double x = 1.0 / 5040.0;
-      x = fma(x, dt, 1.0 / 720.0);
-      x = fma(x, dt, 1.0 / 120.0);
-      x = fma(x, dt, 1.0 / 24.0);
-      x = fma(x, dt, 1.0 / 6.0);
-      x = fma(x, dt, 0.5);
-      x = fma(x, dt, 1.0);
-      x = fma(x, dt, 1.0);
+      const double a01 = 1.0 + dt, a23 = fma(dt, 1.0 / 6.0, 0.5);
+      const double a45 = fma(dt, 1.0 / 120.0, 1.0 / 24.0), a67 = fma(dt, 1.0 / 5040.0, 1.0 / 720.0);
+      const double x = fma(fma(a67, d2, a45), d4, fma(a23, d2, a01));
       const double e = t[7 ^ sw] * x;
       const double t2 = 2.0 * T;
 #pragma unroll

@@ -114,18 +114,21 @@ class Server:
 
     def __init__(self, slots: int = 8, hbm_budget: int = 32 << 30, mixed: bool = True, mixed_cutoff: float = 1e-4,
                  scf_kwargs=None, runner=None, concurrent_classes: bool = True, batch_nbf: int = 0,
-                 batch_max: int = 64, batch_window_s: float = 0.005):
+                 batch_min: int = 4, batch_max: int = 64, batch_window_s: float = 0.005):
         if slots < 1 or hbm_budget <= 0:
             raise ValueError("slots >= 1 and a positive budget are required")
         self.slots, self.budget = slots, int(hbm_budget)
-        # small jobs (at most batch_nbf functions) go to one batch lane: the
-        # jobs queued there with the same SCF settings (up to batch_max, after
-        # waiting batch_window_s for more to arrive) run as one batched SCF
+        # batch lane for small jobs (at most batch_nbf functions): when at
+        # least batch_min of them with the same SCF settings wait in the queue,
+        # one more worker takes them (up to batch_max, after batch_window_s for
+        # others arriving together) and runs them as one batched SCF
         # (hartreefock_b200.batch.BatchSCF: one Fock launch per quartet class
         # over all of them per iteration, plain FP64 builds, the reference's
-        # convergence test per molecule)
+        # convergence test per molecule).  Below that the slots take them in
+        # arrival order like any job: a batch of one or two runs the batched
+        # loop's per-iteration host work for little gain.
         self.batch_nbf, self.batch_max, self.batch_window_s = int(batch_nbf), int(batch_max), float(batch_window_s)
-        self._small = collections.deque()
+        self.batch_min = int(batch_min)
         self.batches = []  # sizes of the batches run
         # the switch rule's DIIS error at 1e-7 (the SCF default is 1e-6): jobs of
         # the stream with diffuse functions otherwise end up to ~1.3e-6 Eh apart
@@ -168,12 +171,18 @@ class Server:
                 job.t_start = job.t_end = job.t_submit
                 job._done.set()
                 return job
-            if self.batch_nbf > 0 and self.runner is _driver_runner and job.nbf <= self.batch_nbf:
-                self._small.append(job)
-            else:
-                self._queue.append(job)
+            self._queue.append(job)
             self._cv.notify_all()
         return job
+
+    def _small_groups(self):
+        """{SCF settings: queued small jobs} (caller holds the lock)."""
+        groups = {}
+        if self.batch_nbf > 0 and self.runner is _driver_runner:
+            for j in self._queue:
+                if j.nbf <= self.batch_nbf:
+                    groups.setdefault(self._batch_key(j), []).append(j)
+        return groups
 
     @staticmethod
     def _batch_key(job):
@@ -182,41 +191,45 @@ class Server:
                 k.get("eri_convention", E.ERI_REFERENCE), k.get("schwarz_threshold", 1e-12))
 
     def _take_batch(self):
-        """Queued small jobs with the head's settings, up to batch_max, if they
-        fit the budget together (caller holds the lock)."""
-        key = self._batch_key(self._small[0])
-        picked, rest, used = [], collections.deque(), 0
-        while self._small:
-            j = self._small.popleft()
-            if (len(picked) < self.batch_max and self._batch_key(j) == key
-                    and self._in_use + used + j.bytes <= self.budget):
+        """The largest group of queued small jobs with the same settings if it
+        has batch_min of them, up to batch_max that fit the budget together,
+        out of the queue (caller holds the lock)."""
+        groups = self._small_groups()
+        if not groups:
+            return []
+        group = max(groups.values(), key=len)
+        if len(group) < self.batch_min:
+            return []
+        picked, used = [], 0
+        for j in group[:self.batch_max]:
+            if self._in_use + used + j.bytes <= self.budget:
                 picked.append(j)
                 used += j.bytes
-            else:
-                rest.append(j)
-        self._small = rest
-        if picked:
-            self._in_use += used
-            self._running += len(picked)
-            self.peak_bytes = max(self.peak_bytes, self._in_use)
-            self.peak_running = max(self.peak_running, self._running)
+        if len(picked) < self.batch_min:
+            return []
+        ids = {id(j) for j in picked}
+        self._queue = collections.deque(j for j in self._queue if id(j) not in ids)
+        self._in_use += used
+        self._running += len(picked)
+        self.peak_bytes = max(self.peak_bytes, self._in_use)
+        self.peak_running = max(self.peak_running, self._running)
         return picked
 
     def _batch_work(self):
         from . import batch as _batch
         while True:
             with self._cv:
-                while not self._small:
+                while max((len(g) for g in self._small_groups().values()), default=0) < self.batch_min:
                     if self._closing:
                         from . import scf
                         scf.release_thread()
                         return
-                    self._cv.wait()
+                    self._cv.wait(0.05)
             time.sleep(self.batch_window_s)  # let jobs arriving together share the batch
             with self._cv:
                 jobs = self._take_batch()
                 if not jobs:
-                    self._cv.wait(0.01)  # the budget is held by running jobs
+                    self._cv.wait(0.01)  # taken by the slots meanwhile, or the budget is held
                     continue
             t0 = time.perf_counter()
             for j in jobs:
@@ -288,7 +301,7 @@ class Server:
         """Wait until every submitted job has finished."""
         deadline = None if timeout is None else time.monotonic() + timeout
         with self._cv:
-            while self._queue or self._small or self._running:
+            while self._queue or self._running:
                 left = None if deadline is None else deadline - time.monotonic()
                 if left is not None and left <= 0:
                     raise TimeoutError("jobs still queued or running")
