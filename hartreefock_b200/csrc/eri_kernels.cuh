@@ -218,7 +218,7 @@ __device__ __forceinline__ void accumulate_primitives(const EngineView &v, const
     const PrimPair *bsrc = v.prim + offb;
     for (int ik = 0; ik < npk; ++ik) {
       const PrimPair pk = v.prim[offk + ik];
-#pragma unroll kPrimUnroll
+#pragma unroll prim_unroll(LA, LB, LC, LD)
       for (int ib = 0; ib < npb; ++ib) {
         const PrimPair pb = bsrc[ib];
         const double rs = rsqrt(pb.zeta + pk.zeta);

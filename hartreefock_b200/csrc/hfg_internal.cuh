@@ -38,11 +38,17 @@ __host__ __device__ constexpr int fused_warps(int la, int lb, int lc, int ld) {
 // (1.20 -> 1.43 ms per (H2O)16 launch) for a change within noise in the
 // concurrent build; the other light classes spill under it.
 __host__ __device__ constexpr int fused_min_blocks(int, int, int, int) { return 1; }
-// unroll factor of the inner (bra) primitive loop
-#ifndef HFG_PRIM_UNROLL
-#define HFG_PRIM_UNROLL 1
-#endif
-constexpr int kPrimUnroll = HFG_PRIM_UNROLL;
+// Unroll factor of the inner (bra) primitive loop of the thread-per-quartet
+// kernels (two primitive quartets in flight per lane).  Measured per class on
+// the (H2O)32 / 6-31G* build: unrolling by 2 takes (ds|ps) from 2.68 to
+// 2.14 ms and (ps|ss) from 4.44 to 4.34 ms, but slows (ss|ss) (2.59 -> 3.80)
+// and (ps|ps) (1.75 -> 2.22), so it is per class.
+__host__ __device__ constexpr int prim_unroll(int la, int lb, int lc, int ld) {
+  return (la == 2 && lb == 0 && lc == 1 && ld == 0) || (la == 1 && lb == 0 && lc == 0 && ld == 0) ||
+                 (la == 2 && lb == 0 && lc == 0 && ld == 0)
+             ? 2
+             : 1;
+}
 
 enum Mode { kStorePacked = 0, kJkRhf = 1, kJkUhf = 2, kSchwarz = 3, kBlock = 4 };
 
