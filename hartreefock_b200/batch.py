@@ -35,7 +35,7 @@ class BatchSCF:
 
     def __init__(self, molecules, unrestricted=False, alpha=0.75, init_guess=0.75, max_iter=300,
                  use_diis=True, schwarz_threshold=1e-12, device="cuda", concurrent_classes=False, graphs=False,
-                 replay=8, eri_convention=E.ERI_REFERENCE):
+                 replay=8, eri_convention=E.ERI_REFERENCE, eigh_method=None):
         self.mols = list(molecules)
         self.uhf = unrestricted
         self.alpha, self.init_guess, self.max_iter, self.use_diis = alpha, init_guess, max_iter, use_diis
@@ -88,10 +88,11 @@ class BatchSCF:
         self.V = 0.5 * (V + V.transpose(1, 2)) * mask2
         self.mask2 = mask2
         self.shift = torch.diag_embed((~valid).double() * PAD_SHIFT)
-        # open shells: which orbital of a degenerate level gets the unpaired
-        # electron depends on the solver's basis for that level, so UHF uses
-        # the single-molecule SCF's per-matrix solver (same states as alone)
-        self.eigh_method = 1 if unrestricted else 0
+        # eigensolver: 0 cuSOLVER batched Jacobi, 1 one dsyevd per matrix.
+        # Open shells default to 1: which orbital of a degenerate level gets
+        # the unpaired electron depends on the solver's basis for that level,
+        # and the per-matrix solver is the single-molecule SCF's
+        self.eigh_method = (1 if unrestricted else 0) if eigh_method is None else int(eigh_method)
         self.seconds = {"fock": 0.0, "diis": 0.0, "eigh": 0.0, "total": 0.0}
 
     # ---- the working set: molecules still iterating, padded to their largest
