@@ -142,3 +142,21 @@ def test_device_pulay_solve_matches_host():
     # the same QR in a different order of operations: agreement relative to
     # the solution's size (the rank-deficient system's entries reach 1e3)
     assert np.abs(got - want).max() < 1e-11 * max(1.0, np.abs(want).max())
+
+
+@pytest.mark.parametrize("method", [0, 1])
+def test_batched_uhf_doublets_with_both_eigensolvers(method):
+    """The bench's UHF doublets (OH, planar CH3; STO-3G, 6-31G; alpha 0.5,
+    initGuess 0.75) batched with the batched Jacobi solver (0, the default)
+    and with one dsyevd per matrix (1) reach the single-molecule energies."""
+    mols = []
+    for basis in ("sto-3g", "6-31g"):
+        for Z, xyz in (molecules.hydroxyl(), molecules.methyl_planar()):
+            mols.append(dict(Z=list(Z), xyz=xyz, basis=basis))
+    kw = dict(alpha=0.5, init_guess=0.75)
+    bs = batch.BatchSCF(mols + mols, unrestricted=True, max_iter=1000, eigh_method=method, **kw)
+    energies = bs.run()
+    assert bs.converged.all()
+    for i, m in enumerate(mols + mols):
+        ref = scf.run_scf(m["Z"], m["xyz"], m["basis"], unrestricted=True, post_diis=0, want_density=False, **kw)
+        assert abs(energies[i] - ref["energy"]) < 1e-9, (i, m["basis"], energies[i], ref["energy"])
