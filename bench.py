@@ -502,7 +502,10 @@ def main():
     # autotuner, then the classes of every build over concurrent streams
     # and the grid from the grid autotuner (both timed on this density,
     # before warm-up)
-    tasks = eng.autotune_tasks(dP) if not args.no_autotune else {}
+    # (one rank only: the lane-group targets decide how the quartets split
+    # into tasks, and the shards are task ranges, so every rank of a sharded
+    # run must build the same task lists: they keep the default target)
+    tasks = eng.autotune_tasks(dP) if not args.no_autotune and world == 1 else {}
     # the large classes' kernel (warp-cooperative or split), timed both ways
     paths = eng.autotune_paths(dP) if not args.no_autotune else {}
     eng.set_streams(not args.no_streams)
