@@ -14,7 +14,10 @@ from __future__ import annotations
 
 class ShardedFock:
     """`engine`: an object with set_shard(rank, count), fock_rhf_tensor(P, G)
-    and fock_uhf_tensor(Pa, Pb, Ga, Gb) (hartreefock_b200.engine.Engine)."""
+    and fock_uhf_tensor(Pa, Pb, Ga, Gb) (hartreefock_b200.engine.Engine).
+    Shards are ranges of each class's task list, so every rank's engine must
+    hold the same task lists: the same molecule, options and lane-group
+    targets (no per-rank Engine.autotune_tasks / set_prim_target choices)."""
 
     def __init__(self, engine, group=None):
         import torch.distributed as dist
