@@ -163,6 +163,10 @@ struct hfg_ctx {
   // tasks from a device work queue (one counter per class, one atomic per
   // warp and task) instead of a grid-stride walk
   bool use_queue = false;
+  // density-screened builds compact the live tasks before the class kernels
+  // (HFG_NO_COMPACT=1: every task goes to the class kernels, which skip the
+  // dead ones themselves)
+  bool use_compaction = true;
   cudaEvent_t ev_done = nullptr;  // end of the last build on its stream
   unsigned config_version = 0;  // bumped by every setter that changes a build
   struct GraphKey {
@@ -686,6 +690,9 @@ static hfg_status grow_scratch(hfg_ctx *c, int slot, size_t need) {
   return HFG_OK;
 }
 
+static hfg_status ensure_task_scratch(hfg_ctx *c);
+__global__ void compact_screened_tasks(const EngineView v, const ClassLaunch cl, Task *__restrict__ out, int *count);
+
 static hfg_status launch_class(hfg_ctx *c, const QuartetClass &q, const ClassLaunch &cl, int mode, bool ref,
                                int prec, cudaStream_t s, int *launches, int slot = 0) {
   const ClassEntry &e = kClasses[q.cls];
@@ -768,10 +775,18 @@ static hfg_status direct_build_body(hfg_ctx *c, bool uhf, const double *dPa, con
   }
   const bool ref = c->opts.eri_convention == HFG_ERI_REFERENCE;
   const size_t nq = c->qclasses.size();
-  if (c->use_queue && nq > 0) {
-    if (!c->d_queue) HFG_CUDA(cudaMalloc((void **)&c->d_queue, nq * sizeof(int)));
+  // density-screened builds first compact each fused / warp class's tasks to
+  // those with a quartet above the threshold (late incremental builds keep
+  // a small fraction); the class kernels then take them from the queue
+  const bool compact = precise && c->use_compaction && nq > 0;
+  if ((c->use_queue || compact) && nq > 0) {
+    if ((st = ensure_task_scratch(c)) != HFG_OK) return st;
     HFG_CUDA(cudaMemsetAsync(c->d_queue, 0, nq * sizeof(int), s));
     ++launches;
+    if (compact) {
+      HFG_CUDA(cudaMemsetAsync(c->d_task_counts, 0, nq * sizeof(int), s));
+      ++launches;
+    }
   }
   ClassStreams cs{c, s, c->use_streams && !c->profiling};
   {
@@ -787,7 +802,6 @@ static hfg_status direct_build_body(hfg_ctx *c, bool uhf, const double *dPa, con
     QuartetClass &q = c->qclasses[qi];
     ClassLaunch cl = base_launch(c, q, true);
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_a, s));
-    if (c->use_queue && !uses_split(c, q.cls)) cl.queue = c->d_queue + qi;
     cl.Da = Da;
     cl.Db = Db;
     cl.Dt = uhf ? c->d_Pt : Da;
@@ -799,7 +813,19 @@ static hfg_status direct_build_body(hfg_ctx *c, bool uhf, const double *dPa, con
     cl.counters = precise ? c->d_counters : nullptr;
     if (cl.ntasks > 0) {
       const cudaStream_t cls_stream = cs.pick(uses_split(c, q.cls));
-      st = launch_class(c, q, cl, uhf ? kJkUhf : kJkRhf, ref, prec, cls_stream, &launches, cs.slot);
+      ClassLaunch cll = cl;
+      if ((c->use_queue || compact) && !uses_split(c, q.cls)) cll.queue = c->d_queue + qi;
+      if (compact && !uses_split(c, q.cls)) {
+        const int cg = std::max(1, std::min(c->num_sms * 8, (cl.ntasks + 7) / 8));
+        compact_screened_tasks<<<cg, 256, 0, cls_stream>>>(c->view(), cl, c->d_task_active + c->task_base[qi],
+                                                            c->d_task_counts + qi);
+        ++launches;
+        cll.tasks = c->d_task_active + c->task_base[qi];
+        cll.task_offset = 0;
+        cll.task_stride = 1;
+        cll.ntasks_dev = c->d_task_counts + qi;  // cll.ntasks stays the bound the grid is sized from
+      }
+      st = launch_class(c, q, cll, uhf ? kJkUhf : kJkRhf, ref, prec, cls_stream, &launches, cs.slot);
       if (st != HFG_OK) return st;
     }
     if (c->profiling) HFG_CUDA(cudaEventRecord(q.ev_b, s));
@@ -916,6 +942,25 @@ __global__ void finalize_uhf_batch(const double *J, const double *Ka, const doub
 // Tasks of active molecules, in the class's order up to warp-sized groups:
 // each warp writes its kept tasks as one contiguous run (ballot + one
 // atomic per warp).
+// Device lists of compacted tasks (one region per quartet class, as long as
+// the class's task list), their counts and work-queue counters; allocated by
+// the first build that compacts, freed when the task lists are rebuilt.
+static hfg_status ensure_task_scratch(hfg_ctx *c) {
+  const size_t nq = c->qclasses.size();
+  if (!c->d_task_active) {
+    size_t total = 0;
+    c->task_base.assign(nq, 0);
+    for (size_t i = 0; i < nq; ++i) {
+      c->task_base[i] = (int)total;
+      total += c->qclasses[i].tasks.size();
+    }
+    HFG_CUDA(cudaMalloc((void **)&c->d_task_active, std::max<size_t>(1, total) * sizeof(Task)));
+    HFG_CUDA(cudaMalloc((void **)&c->d_task_counts, std::max<size_t>(1, nq) * sizeof(int)));
+  }
+  if (!c->d_queue) HFG_CUDA(cudaMalloc((void **)&c->d_queue, std::max<size_t>(1, nq) * sizeof(int)));
+  return HFG_OK;
+}
+
 __global__ void compact_active_tasks(const Task *__restrict__ tasks, int ntasks, const int *__restrict__ bra_list,
                                      const int *__restrict__ pair_mol, const unsigned char *__restrict__ active,
                                      Task *__restrict__ out, int *count) {
@@ -933,6 +978,25 @@ __global__ void compact_active_tasks(const Task *__restrict__ tasks, int ntasks,
     if (lane == 0 && m) at = atomicAdd(count, __popc(m));
     at = __shfl_sync(0xffffffffu, at, 0);
     if (keep) out[at + __popc(m & ((1u << lane) - 1))] = tk;
+  }
+}
+
+// Density-screened builds: the tasks of one class launch (its shard range)
+// with at least one quartet whose density-weighted bound reaches the
+// threshold -- the test the class kernels apply per lane (screen_task) -- in
+// task order within each warp's group, appended to `out`; `count` ends as
+// their number.  One warp per task.
+__global__ void compact_screened_tasks(const EngineView v, const ClassLaunch cl, Task *__restrict__ out,
+                                       int *count) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int t = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < cl.ntasks; t += warps) {
+    const Task task = launch_task(cl, t);
+    const int bp = cl.bra_list[task.bra_pos];
+    bool keep = false;
+    for (int k = task.ket_start + lane; k < task.ket_end; k += 32)
+      keep = keep || density_bound(v, bp, cl.ket_list[k]) >= cl.dens_threshold;
+    if (__any_sync(0xffffffffu, keep) && lane == 0) out[atomicAdd(count, 1)] = task;
   }
 }
 
@@ -967,16 +1031,7 @@ static hfg_status batch_build(hfg_ctx *c, bool uhf, const double *dPa, const dou
   }
   if (compact) {
     const size_t nq = c->qclasses.size();
-    if (!c->d_task_active) {
-      size_t total = 0;
-      c->task_base.assign(nq, 0);
-      for (size_t i = 0; i < nq; ++i) {
-        c->task_base[i] = (int)total;
-        total += c->qclasses[i].tasks.size();
-      }
-      HFG_CUDA(cudaMalloc((void **)&c->d_task_active, std::max<size_t>(1, total) * sizeof(Task)));
-      HFG_CUDA(cudaMalloc((void **)&c->d_task_counts, std::max<size_t>(1, nq) * sizeof(int)));
-    }
+    if ((st = ensure_task_scratch(c)) != HFG_OK) return st;
     HFG_CUDA(cudaMemsetAsync(c->d_task_counts, 0, nq * sizeof(int), s));
     for (size_t i = 0; i < nq; ++i) {
       const QuartetClass &q = c->qclasses[i];
@@ -1064,17 +1119,7 @@ static hfg_status batch_build_async(hfg_ctx *c, bool uhf, const double *dPa, con
   hfg_status st;
   if ((st = ensure(&c->d_J, tot)) != HFG_OK || (st = ensure(&c->d_Ka, tot)) != HFG_OK) return st;
   if (uhf && ((st = ensure(&c->d_Kb, tot)) != HFG_OK || (st = ensure(&c->d_Pt, tot)) != HFG_OK)) return st;
-  if (!c->d_task_active) {
-    size_t total = 0;
-    c->task_base.assign(nq, 0);
-    for (size_t i = 0; i < nq; ++i) {
-      c->task_base[i] = (int)total;
-      total += c->qclasses[i].tasks.size();
-    }
-    HFG_CUDA(cudaMalloc((void **)&c->d_task_active, std::max<size_t>(1, total) * sizeof(Task)));
-    HFG_CUDA(cudaMalloc((void **)&c->d_task_counts, std::max<size_t>(1, nq) * sizeof(int)));
-  }
-  if (!c->d_queue) HFG_CUDA(cudaMalloc((void **)&c->d_queue, std::max<size_t>(1, nq) * sizeof(int)));
+  if ((st = ensure_task_scratch(c)) != HFG_OK) return st;
   HFG_CUDA(cudaMemsetAsync(c->d_J, 0, tot * sizeof(double), s));
   HFG_CUDA(cudaMemsetAsync(c->d_Ka, 0, tot * sizeof(double), s));
   int launches = 2;
@@ -1256,6 +1301,7 @@ static hfg_status create_context(const hfg_shells *sh, const int *shell_mol, int
     ctx->warp_class[k] = kWarp[k] && e.la + e.lb + e.lc + e.ld >= 8 ? 1 : 0;
   }
   if (const char *e = std::getenv("HFG_WORK_QUEUE")) ctx->use_queue = std::atoi(e) != 0;
+  if (const char *e = std::getenv("HFG_NO_COMPACT")) ctx->use_compaction = std::atoi(e) == 0;
   // tuning: HFG_SCRATCH_MB bounds the split path's scratch (all regions together)
   if (const char *e = std::getenv("HFG_SCRATCH_MB")) ctx->scratch_budget_bytes = size_t(std::max(16, std::atoi(e))) << 20;
   if (const char *e = std::getenv("HFG_SPLIT_PATH"); e && std::atoi(e) != 0)
