@@ -63,6 +63,16 @@ static const std::vector<double> &boys_table_host() {
       }
       tab[(size_t)kBoysGrid * kBoysOrders + i] = (double)expl(-T);  // e^-T_i
     }
+    // the per-order rows (the same products the kernels form when they
+    // stage a slice into shared memory)
+    const double inv_fact[kBoysTaylor] = {1.0, 1.0, 0.5, 1.0 / 6.0, 1.0 / 24.0, 1.0 / 120.0, 1.0 / 720.0};
+    tab.resize((size_t)kBoysFoldedOff + (size_t)(kMaxLtot + 1) * kBoysFoldedSize);
+    for (int L = 0; L <= kMaxLtot; ++L)
+      for (int i = 0; i < kBoysGrid; ++i)
+        for (int k = 0; k < kBoysRow; ++k)
+          tab[(size_t)kBoysFoldedOff + (size_t)L * kBoysFoldedSize + boys_swizzle(i, k)] =
+              k < kBoysTaylor ? tab[(size_t)i * kBoysOrders + L + k] * inv_fact[k]
+                              : tab[(size_t)kBoysGrid * kBoysOrders + i];
   });
   return tab;
 }

@@ -2,7 +2,8 @@
 // warp per (bra pair, 32 consecutive ket pairs).  The bra pair is shared by
 // the warp (its primitive pairs are broadcast loads), the ket pairs come from
 // the Schwarz-sorted ket list of the class.  The Boys table slice the class
-// needs is staged into shared memory once per block.
+// needs is staged into shared memory once per block, or read from global
+// memory through L1 (boys_from_global).
 #pragma once
 
 #include <type_traits>
@@ -364,14 +365,27 @@ __global__ void __launch_bounds__(32 * fused_warps(LA, LB, LC, LD), fused_min_bl
   constexpr int NA = ncart(LA), NB = ncart(LB), NC = ncart(LC), ND = ncart(LD);
   constexpr int N = NA * NB * NC * ND;
   static_assert(SCR == kScreenNone || MODE == kJkRhf || MODE == kJkUhf, "screening applies to J/K builds");
-  __shared__ double tab[kBoysGrid * kBoysRow];
-  stage_boys<LTOT>(tab, v.boys_table);
+  // the class's Boys slice: per-order rows in global memory, or staged
+  __shared__ double tab_sh[boys_from_global(LA, LB, LC, LD) ? 1 : kBoysGrid * kBoysRow];
+  const double *__restrict__ tab = tab_sh;
+  if constexpr (boys_from_global(LA, LB, LC, LD)) {
+    tab = v.boys_table + kBoysFoldedOff + LTOT * kBoysFoldedSize;
+  } else {
+    stage_boys<LTOT>(tab_sh, v.boys_table);
+  }
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int ntasks = launch_ntasks(cl);
-  for (int t = first_task(cl, blockIdx.x * kW + warp); t < ntasks; t = next_task(cl, t, gridDim.x * kW)) {
-    const Task task = launch_task(cl, t);
+  // the warp's next task record is loaded while it works on this one (the
+  // task lists stream from DRAM once per build: a miss on every task)
+  int t = first_task(cl, blockIdx.x * kW + warp);
+  Task task_next;
+  if (t < ntasks) task_next = launch_task(cl, t);
+  for (int tn; t < ntasks; t = tn) {
+    const Task task = task_next;
+    tn = next_task(cl, t, gridDim.x * kW);
+    if (tn < ntasks) task_next = launch_task(cl, tn);
     const int bp = cl.bra_list[task.bra_pos];
     // the task's molecule (batched contexts): its matrices and size
     const MolView mv = task_molecule(v, bp);

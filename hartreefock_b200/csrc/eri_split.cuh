@@ -62,8 +62,13 @@ template <int LA, int LB, int LC, int LD, bool REF, int SCR = kScreenNone>
 __global__ void __launch_bounds__(kThreads) eri_prim_split_kernel(const EngineView v, const ClassLaunch cl,
                                                                   const SplitChunk ch) {
   constexpr int LTOT = LA + LB + LC + LD;
-  __shared__ double tab[kBoysGrid * kBoysRow];
-  stage_boys<LTOT>(tab, v.boys_table);
+  __shared__ double tab_sh[boys_from_global_split(LA, LB, LC, LD) ? 1 : kBoysGrid * kBoysRow];
+  const double *__restrict__ tab = tab_sh;
+  if constexpr (boys_from_global_split(LA, LB, LC, LD)) {
+    tab = v.boys_table + kBoysFoldedOff + LTOT * kBoysFoldedSize;
+  } else {
+    stage_boys<LTOT>(tab_sh, v.boys_table);
+  }
   const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= (long long)ch.ntasks * 32) return;  // whole warps
   const Task task = launch_task(cl, ch.task0 + (int)(slot >> 5));

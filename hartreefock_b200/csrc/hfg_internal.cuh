@@ -19,6 +19,11 @@ constexpr int kBoysOrders = kMaxLtot + kBoysTaylor;  // orders 0 .. 14 tabulated
 // 32 banks (plain rows put a whole warp's column on one bank pair).
 constexpr int kBoysRow = kBoysTaylor + 1;
 __host__ __device__ constexpr int boys_swizzle(int i, int k) { return i * kBoysRow + (k ^ ((i >> 1) & 7)); }
+// Per-order rows ready for evaluation, after the e^-T tail of the table:
+// table L (L = 0 .. kMaxLtot) holds in each grid row F_{L+k}(T_i) / k!
+// (k < kBoysTaylor) and e^-T_i, swizzled as boys_swizzle places them.
+constexpr int kBoysFoldedOff = kBoysGrid * kBoysOrders + kBoysGrid;
+constexpr int kBoysFoldedSize = kBoysGrid * kBoysRow;
 
 constexpr int kWarpsPerBlock = 4;
 constexpr int kThreads = 32 * kWarpsPerBlock;
@@ -48,6 +53,26 @@ __host__ __device__ constexpr int prim_unroll(int la, int lb, int lc, int ld) {
                  (la == 2 && lb == 0 && lc == 0 && ld == 0)
              ? 2
              : 1;
+}
+// Where a class kernel reads its Boys slice: staged into shared memory
+// (46 KB per block, which also caps an SM at four such blocks over all the
+// classes running at once) or straight from the per-order rows in global
+// memory through L1 (kBoysFoldedOff; no shared memory).  Measured per class
+// on the (H2O)32 / 6-31G* build, classes one after another: from global
+// memory (ss|ss) 3.13 -> 2.66 ms, (pp|pp) 0.25 -> 0.21, (dd|ss) 0.33 -> 0.30,
+// (ds|ds) 0.68 -> 0.66, (ds|pp) 0.61 -> 0.59, but (ps|ss) 4.35 -> 4.58 and
+// (ds|ps), (ds|ss) 1-2% slower.
+__host__ __device__ constexpr bool boys_from_global(int la, int lb, int lc, int ld) {
+  return (la == 0 && lb == 0 && lc == 0 && ld == 0) || (la == 1 && lb == 1 && lc == 1 && ld == 1) ||
+         (la == 2 && lb == 2 && lc == 0 && ld == 0) || (la == 2 && lb == 0 && lc == 2 && ld == 0) ||
+         (la == 2 && lb == 0 && lc == 1 && ld == 1);
+}
+// The same choice for the split path's primitive kernel: from global memory
+// (dp|ds) 1.78 -> 1.33 ms, (dp|pp) 0.95 -> 0.74, (dd|ps) 1.15 -> 0.90, (dp|dp)
+// 0.87 -> 0.77, (dd|ds) 0.81 -> 0.71, (dd|pp) 0.55 -> 0.50; (dd|dp) 0.91 ->
+// 2.13 ms, so it keeps the staged slice, as does (dd|dd).
+__host__ __device__ constexpr bool boys_from_global_split(int la, int lb, int lc, int ld) {
+  return !(la == 2 && lb == 2 && lc == 2 && (ld == 1 || ld == 2));
 }
 
 enum Mode { kStorePacked = 0, kJkRhf = 1, kJkUhf = 2, kSchwarz = 3, kBlock = 4 };
