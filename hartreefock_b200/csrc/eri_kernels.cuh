@@ -377,15 +377,23 @@ __global__ void __launch_bounds__(32 * fused_warps(LA, LB, LC, LD), fused_min_bl
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int ntasks = launch_ntasks(cl);
-  // the warp's next task record is loaded while it works on this one (the
-  // task lists stream from DRAM once per build: a miss on every task)
+  // task_prefetch: the warp's next task record is loaded while it works on
+  // this one (the task lists stream from DRAM once per build: a miss on
+  // every task)
+  constexpr bool kPrefetch = task_prefetch(LA, LB, LC, LD);
   int t = first_task(cl, blockIdx.x * kW + warp);
   Task task_next;
-  if (t < ntasks) task_next = launch_task(cl, t);
+  if (kPrefetch && t < ntasks) task_next = launch_task(cl, t);
   for (int tn; t < ntasks; t = tn) {
-    const Task task = task_next;
-    tn = next_task(cl, t, gridDim.x * kW);
-    if (tn < ntasks) task_next = launch_task(cl, tn);
+    Task task;
+    if constexpr (kPrefetch) {
+      task = task_next;
+      tn = next_task(cl, t, gridDim.x * kW);
+      if (tn < ntasks) task_next = launch_task(cl, tn);
+    } else {
+      task = launch_task(cl, t);
+      tn = next_task(cl, t, gridDim.x * kW);
+    }
     const int bp = cl.bra_list[task.bra_pos];
     // the task's molecule (batched contexts): its matrices and size
     const MolView mv = task_molecule(v, bp);

@@ -67,6 +67,14 @@ __host__ __device__ constexpr bool boys_from_global(int la, int lb, int lc, int 
          (la == 2 && lb == 2 && lc == 0 && ld == 0) || (la == 2 && lb == 0 && lc == 2 && ld == 0) ||
          (la == 2 && lb == 0 && lc == 1 && ld == 1);
 }
+// Fused class kernels whose warps load their next task record while they
+// work on the current one (every class but (ss|ss): with its Boys slice in
+// global memory the prefetch made it slower, 2.66 -> 3.15 ms per (H2O)32
+// build; without the prefetch the class is 4% slower with the staged slice
+// and 15% faster with the global one).
+__host__ __device__ constexpr bool task_prefetch(int la, int lb, int lc, int ld) {
+  return la + lb + lc + ld > 0;
+}
 // The same choice for the split path's primitive kernel: from global memory
 // (dp|ds) 1.78 -> 1.33 ms, (dp|pp) 0.95 -> 0.74, (dd|ps) 1.15 -> 0.90, (dp|dp)
 // 0.87 -> 0.77, (dd|ds) 0.81 -> 0.71, (dd|pp) 0.55 -> 0.50; (dd|dp) 0.91 ->
@@ -114,7 +122,7 @@ struct EngineView {
   const double *pair_Q;       // Schwarz bound
   const float *shell_dmax;    // [nshells][nshells] max |D| over each shell block (density screening)
   int nshells;
-  const double *boys_table;   // [kBoysGrid][kBoysOrders] F_m(T_i)
+  const double *boys_table;   // [kBoysGrid][kBoysOrders] F_m(T_i), e^-T_i, then the per-order rows
   int nbf;
   int reference_convention;   // 1: reproduce the reference's (dd|dd) ET rows
   // batched contexts (many molecules, one launch per class); null otherwise
