@@ -1848,7 +1848,8 @@ hfg_status hfg_autotune(hfg_ctx *c, const double *dP, int32_t *chosen, int32_t c
   const int cand[] = {1, 2, 4, 8, 16};
   int written = 0;
   if (c->use_streams && !c->batch && !c->precision_form()) {
-    // classes share the SMs: one cap for all, timed on whole builds
+    // classes share the SMs: one cap for all, timed on whole builds, then
+    // a higher one for the classes without shared memory
     const size_t nn = (size_t)c->nbf * c->nbf;
     if ((st = ensure(&c->d_G, nn)) != HFG_OK) return st;
     float best = 1e30f;
@@ -1868,10 +1869,41 @@ hfg_status hfg_autotune(hfg_ctx *c, const double *dP, int32_t *chosen, int32_t c
       }
     }
     for (int k = 0; k < kNumClasses; ++k) c->tuned_bps[k] = best_bps;
+    // the fused classes that read their Boys rows from global memory hold no
+    // shared memory: a higher cap for them alone, timed the same way
+    auto no_smem = [](int k) {
+      const ClassEntry &e = kClasses[k];
+      return !kSplit[k] && !kWarp[k] && boys_from_global(e.la, e.lb, e.lc, e.ld);
+    };
+    int best_free = best_bps;
+    for (int b : {2 * best_bps, 4 * best_bps}) {
+      for (int k = 0; k < kNumClasses; ++k)
+        if (no_smem(k)) c->tuned_bps[k] = b;
+      ++c->config_version;
+      float ms_sum = 0;
+      for (int r = 0; r < 3; ++r) {
+        if ((st = direct_build(c, false, dP, nullptr, c->d_G, nullptr, s)) != HFG_OK) return st;
+        if ((st = finish_timing(c)) != HFG_OK) return st;
+        if (r > 0) ms_sum += c->stats.last_build_ms;
+      }
+      if (ms_sum < best) {
+        best = ms_sum;
+        best_free = b;
+      }
+    }
+    for (int k = 0; k < kNumClasses; ++k)
+      if (no_smem(k)) c->tuned_bps[k] = best_free;
     if (chosen && cap >= 5) {
       const int rec[5] = {-1, -1, -1, -1, best_bps};  // all classes
       std::copy(rec, rec + 5, chosen);
       written = 5;
+    }
+    for (int k = 0; k < kNumClasses && best_free != best_bps; ++k) {
+      if (!chosen || !no_smem(k) || written + 5 > cap) continue;
+      const ClassEntry &e = kClasses[k];
+      const int rec[5] = {e.la, e.lb, e.lc, e.ld, best_free};
+      std::copy(rec, rec + 5, chosen + written);
+      written += 5;
     }
     if (count) *count = written / 5;
     ++c->config_version;

@@ -379,7 +379,10 @@ hfg_status hfg_autotune_paths(hfg_ctx *ctx, const double *dP, int32_t *chosen, i
  * class streams (hfg_set_streams) on a single-molecule plain-form context,
  * the classes share the SMs, so one cap for all classes (1, 2 or 4 blocks
  * per SM) is chosen from whole builds instead; its record is
- * (-1, -1, -1, -1, blocks per SM). */
+ * (-1, -1, -1, -1, blocks per SM).  The classes whose kernels hold no
+ * shared memory (their Boys rows read from global memory) then try twice
+ * and four times that cap, again on whole builds; a higher cap that wins
+ * adds one record per such class. */
 hfg_status hfg_autotune(hfg_ctx *ctx, const double *dP, int32_t *chosen, int32_t cap, int32_t *count, void *stream);
 
 /* Per-class timing of the builds (no reference counterpart: instrumentation
