@@ -462,6 +462,7 @@ def main():
     ap.add_argument("--no-precision", action="store_true", help="skip the precision-form builds")
     ap.add_argument("--no-autotune", action="store_true", help="fixed grid (4 blocks per SM) for every class")
     ap.add_argument("--no-streams", action="store_true", help="every class kernel on the build stream")
+    ap.add_argument("--no-graphs", action="store_true", help="launch every build's kernels (no CUDA graph replay)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     WATERS = args.waters
@@ -485,6 +486,9 @@ def main():
     eng = E.Engine(Z, xyz, BASIS, schwarz_threshold=THRESHOLD, device=local)
     n = eng.nbf
     P_host = synthetic_density(n)
+    # a created stream: the builds on it can be captured as a CUDA graph (the
+    # legacy default stream cannot)
+    torch.cuda.set_stream(torch.cuda.Stream())
     stream = torch.cuda.current_stream()
     sptr = E._torch_stream()  # the builds run on torch's stream, between the timing events
     dP = torch.from_numpy(P_host).cuda()
@@ -510,6 +514,10 @@ def main():
     paths = eng.autotune_paths(dP) if not args.no_autotune else {}
     eng.set_streams(not args.no_streams)
     grids = eng.autotune(dP) if not args.no_autotune else {}
+    # the plain-form build replays one CUDA graph per buffers and stream
+    # (captured during the warm-up steps; the host-buffer entry point gets
+    # its own on the context's stream)
+    eng.set_graphs(not args.no_graphs)
     # N > 1: every rank builds its shard of each class's tasks, one NCCL
     # all-reduce of G per build (hartreefock_b200/shards.py)
     sf = None
@@ -568,7 +576,8 @@ def main():
         else:
             eng.fock_rhf(P_pin.numpy(), out=G_pin.numpy())
 
-    e2e_step()
+    for _ in range(2):  # the second call captures the host-buffer build's graph
+        e2e_step()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -619,6 +628,7 @@ def main():
                    "large_class_kernels": paths or "default: warp for (22|22), split for the rest",
                    "prim_quartets_per_lane_target": tasks or "fixed 96",
                    "class_streams": 1 if args.no_streams else 13,
+                   "cuda_graph": not args.no_graphs,
                    "parallelism": f"task shards x{world}, one NCCL all-reduce of G per build" if world > 1
                    else "single GPU"},
         "e2e": {"value": e2e, "unit": "quartets/s", "h2d_bytes_per_step": n * n * 8, "d2h_bytes_per_step": n * n * 8},
@@ -644,6 +654,8 @@ def main():
         "clocks": clocks.summary(),
     }
     eng.close()
+    torch.cuda.synchronize()
+    torch.cuda.set_stream(torch.cuda.default_stream())  # the remaining parts as before
     if rank == 0 and world == 1 and not args.no_precision:
         line["precision_form"] = precision_form(Z, xyz, P_host, local, peak, peak32)
         line["roofline"]["fp32"] = line["precision_form"]["first_full_build"]["roofline"]

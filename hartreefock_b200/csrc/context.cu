@@ -1833,6 +1833,21 @@ hfg_status hfg_set_mixed_cutoff(hfg_ctx *c, double cutoff) {
 // keep the fastest for the context's later builds.  Split classes keep
 // their fixed chunked launch.  The J/K scratch it writes is cleared by the
 // next build.
+// Median of five timed direct builds after an untimed one, for the
+// whole-build autotuner (single concurrent builds vary by a few per cent).
+static hfg_status median_build_ms(hfg_ctx *c, const double *dP, cudaStream_t s, float *out) {
+  float t[5];
+  hfg_status st;
+  for (int r = 0; r < 6; ++r) {
+    if ((st = direct_build(c, false, dP, nullptr, c->d_G, nullptr, s)) != HFG_OK) return st;
+    if ((st = finish_timing(c)) != HFG_OK) return st;
+    if (r > 0) t[r - 1] = c->stats.last_build_ms;
+  }
+  std::sort(t, t + 5);
+  *out = t[2];
+  return HFG_OK;
+}
+
 hfg_status hfg_autotune(hfg_ctx *c, const double *dP, int32_t *chosen, int32_t cap, int32_t *count, void *stream) {
   if (!c || !dP) return hfg::fail(HFG_INVALID_ARG, "null context or density");
   using namespace hfg;
@@ -1858,11 +1873,7 @@ hfg_status hfg_autotune(hfg_ctx *c, const double *dP, int32_t *chosen, int32_t c
       for (int k = 0; k < kNumClasses; ++k) c->tuned_bps[k] = b;
       ++c->config_version;
       float ms_sum = 0;
-      for (int r = 0; r < 3; ++r) {
-        if ((st = direct_build(c, false, dP, nullptr, c->d_G, nullptr, s)) != HFG_OK) return st;
-        if ((st = finish_timing(c)) != HFG_OK) return st;
-        if (r > 0) ms_sum += c->stats.last_build_ms;  // the first is a warm-up
-      }
+      if ((st = median_build_ms(c, dP, s, &ms_sum)) != HFG_OK) return st;
       if (ms_sum < best) {
         best = ms_sum;
         best_bps = b;
@@ -1881,11 +1892,7 @@ hfg_status hfg_autotune(hfg_ctx *c, const double *dP, int32_t *chosen, int32_t c
         if (no_smem(k)) c->tuned_bps[k] = b;
       ++c->config_version;
       float ms_sum = 0;
-      for (int r = 0; r < 3; ++r) {
-        if ((st = direct_build(c, false, dP, nullptr, c->d_G, nullptr, s)) != HFG_OK) return st;
-        if ((st = finish_timing(c)) != HFG_OK) return st;
-        if (r > 0) ms_sum += c->stats.last_build_ms;
-      }
+      if ((st = median_build_ms(c, dP, s, &ms_sum)) != HFG_OK) return st;
       if (ms_sum < best) {
         best = ms_sum;
         best_free = b;
